@@ -1,0 +1,59 @@
+/*
+ * melon3d_gpu.h — extensions of the GPU world beyond Melon3D's C API.
+ *
+ * None of these has a counterpart in the reference's public header; they
+ * exist because a GPU world is used differently from a CPU one:
+ *  - batch readback of every body slot in one copy (the per-body getters of
+ *    melon3d.h stay available and exact, but cost one call per body);
+ *  - device-side timing of the last step (CUDA events on the world's stream);
+ *  - an error status word (kernels never trap: a failed launch, an exhausted
+ *    allocation or a bounded wait that ran out is reported here);
+ *  - the snapshot functions of melon3d_debug.h (m3d_dbg_*), which the test
+ *    suite uses to compare the world with the reference field by field.
+ * All functions take the world created by m3d_world_create (melon3d.h).
+ */
+#ifndef MELON3D_GPU_H
+#define MELON3D_GPU_H
+
+#include "melon3d.h"
+#include "melon3d_debug.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define M3D_GPU_OK 0
+#define M3D_GPU_ERR_CUDA (-1)    /* a CUDA call failed; see m3d_gpu_last_error_string */
+#define M3D_GPU_ERR_ALLOC (-2)   /* device memory could not be grown */
+#define M3D_GPU_ERR_HASH (-3)    /* a pair hash table overflowed (internal sizing bug) */
+
+/* Number of body slots (live or free); slot i is body index i. */
+M3D_API int32_t m3d_gpu_body_capacity(m3d_world* world);
+
+/* Copy position (xyz) and rotation (xyzw) of the first `capacity` slots,
+ * straight from device memory, into caller-owned host arrays
+ * (3*capacity and 4*capacity floats).  Either pointer may be NULL. */
+M3D_API void m3d_gpu_read_poses(m3d_world* world, float* positions, float* rotations, int32_t capacity);
+
+/* Device time of the last m3d_world_step, milliseconds (CUDA events on the
+ * world's stream around the step's work, uploads included). */
+M3D_API float m3d_gpu_last_step_device_ms(m3d_world* world);
+
+/* 0 when healthy, else the first M3D_GPU_ERR_* seen since creation. */
+M3D_API int32_t m3d_gpu_status(m3d_world* world);
+M3D_API const char* m3d_gpu_last_error_string(m3d_world* world);
+
+/* Snapshot records (melon3d_debug.h) — for tests and debugging. */
+M3D_API int32_t m3d_dbg_body_capacity(m3d_world* world);
+M3D_API void m3d_dbg_bodies(m3d_world* world, m3d_dbg_body* out, int32_t capacity);
+M3D_API int32_t m3d_dbg_contact_count(m3d_world* world);
+M3D_API void m3d_dbg_contacts(m3d_world* world, m3d_dbg_contact* out, int32_t capacity);
+M3D_API void m3d_dbg_island_labels(m3d_world* world, int32_t* out, int32_t capacity);
+M3D_API void m3d_dbg_contact_colors(m3d_world* world, int32_t* out, int32_t capacity);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MELON3D_GPU_H */

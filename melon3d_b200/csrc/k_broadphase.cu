@@ -1,0 +1,989 @@
+// Broadphase and contact bookkeeping of one step:
+//   fat-AABB refresh -> active/stable cell entries -> stable radix sort ->
+//   cell runs -> pair enumeration with the admission filters -> oversized
+//   pairs -> first-occurrence dedupe -> contact creation -> removal of pairs
+//   whose fat boxes separated.
+//
+// Contact ORDER is part of the result (the Gauss-Seidel solver and the graph
+// colouring follow it), so every stage reproduces the reference's order:
+// pairs are emitted cell run by cell run (runs in ascending cell key), inside
+// a run active x active pairs in (i, j > i) entry order and then active x
+// stable pairs stable-entry-major, then the oversized loops; a pair already
+// present (before the step or earlier in the stream) is skipped; removal is
+// the closed form of the reference's descending swap-remove.
+// (reference src/world.cpp:156-229, 1456-1735; src/grid.cpp:19-95)
+#include "m3d_collide.cuh"
+#include "m3d_dev.cuh"
+
+namespace m3g
+{
+
+__device__ __forceinline__ int64_t cellCoord(float v, float inv) { return (int64_t)floorf(v * inv); }
+
+__device__ __forceinline__ uint64_t packCell(int64_t x, int64_t y, int64_t z)
+{
+	const int64_t offset = 1 << 20;
+	uint64_t ux = (uint64_t)(x + offset) & 0x1FFFFFull;
+	uint64_t uy = (uint64_t)(y + offset) & 0x1FFFFFull;
+	uint64_t uz = (uint64_t)(z + offset) & 0x1FFFFFull;
+	return (ux << 42) | (uy << 21) | uz;
+}
+
+__device__ __forceinline__ uint64_t cellKeyOf(V3 p, float inv)
+{
+	return packCell(cellCoord(p.x, inv), cellCoord(p.y, inv), cellCoord(p.z, inv));
+}
+
+__device__ __forceinline__ uint64_t pairKey(int32_t lo, int32_t hi)
+{
+	return ((uint64_t)(uint32_t)lo << 32) | (uint64_t)(uint32_t)hi;
+}
+
+__device__ __forceinline__ Box loadFat(const BodySoA& B, int i)
+{
+	Box b;
+	b.lo = ld3(B.fatLo[i]);
+	b.hi = ld3(B.fatHi[i]);
+	return b;
+}
+
+// cells covered by a fat box; > kOversizedCellSpan means "coarse list"
+__device__ __forceinline__ int64_t cellSpan(const Box& b, float inv)
+{
+	int64_t x0 = cellCoord(b.lo.x, inv), y0 = cellCoord(b.lo.y, inv), z0 = cellCoord(b.lo.z, inv);
+	int64_t x1 = cellCoord(b.hi.x, inv), y1 = cellCoord(b.hi.y, inv), z1 = cellCoord(b.hi.z, inv);
+	return (x1 - x0 + 1) * (y1 - y0 + 1) * (z1 - z0 + 1);
+}
+
+// ---------------------------------------------------------------------------
+// fat AABB refresh (reference src/world.cpp:143-211)
+// ---------------------------------------------------------------------------
+
+__global__ void kRefresh(BodySoA B, int32_t n, float dt, int rebuildStable, float inv, uint32_t* cntA, uint32_t* overA,
+						 uint32_t* cntS, uint32_t* overS, uint8_t* inActiveCells)
+{
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+	{
+		return;
+	}
+	uint8_t st = B.state[i];
+	bool inUse = (st & kStInUse) != 0;
+	bool awake = (st & kStAwake) != 0;
+	const BodyCold& cold = B.cold[i];
+	bool stable = inUse && !awake;
+	bool active = inUse && (awake || !B.inStableTier[i]);
+	B.isActive[i] = active ? 1 : 0;
+	B.isStable[i] = stable ? 1 : 0;
+	B.moved[i] = 0;
+	B.bFlags[i] = (uint8_t)((inUse ? kBFInUse : 0) | ((inUse && cold.type == kDynamic) ? kBFDynamic : 0) |
+							((inUse && cold.type == kKinematic) ? kBFKinematic : 0) | (awake ? kBFAwake : 0));
+	V3 margin = v3(kAABBMargin, kAABBMargin, kAABBMargin);
+	if (active)
+	{
+		Box pred = shapeAABB(cold.shape, bodyXf(B, i));
+		V3 vel = ld3(B.vel[i]);
+		V3 stp = scale(dt, vel);
+		if (stp.x < 0.0f) pred.lo.x += stp.x; else pred.hi.x += stp.x;
+		if (stp.y < 0.0f) pred.lo.y += stp.y; else pred.hi.y += stp.y;
+		if (stp.z < 0.0f) pred.lo.z += stp.z; else pred.hi.z += stp.z;
+		if (!B.hasFat[i] || !contains(loadFat(B, i), pred))
+		{
+			Box fat;
+			fat.lo = sub(pred.lo, margin);
+			fat.hi = add(pred.hi, margin);
+			V3 slack = scale(2.0f * dt, vel);
+			if (slack.x < 0.0f) fat.lo.x += slack.x; else fat.hi.x += slack.x;
+			if (slack.y < 0.0f) fat.lo.y += slack.y; else fat.hi.y += slack.y;
+			if (slack.z < 0.0f) fat.lo.z += slack.z; else fat.hi.z += slack.z;
+			B.fatLo[i] = st3(fat.lo);
+			B.fatHi[i] = st3(fat.hi);
+			B.hasFat[i] = 1;
+			B.moved[i] = 1;
+		}
+	}
+	else if (stable && rebuildStable && !B.hasFat[i])
+	{
+		Box box = shapeAABB(cold.shape, bodyXf(B, i));
+		box.lo = sub(box.lo, margin);
+		box.hi = add(box.hi, margin);
+		V3 d = scale(dt, ld3(B.vel[i]));
+		if (d.x < 0.0f) box.lo.x += d.x; else box.hi.x += d.x;
+		if (d.y < 0.0f) box.lo.y += d.y; else box.hi.y += d.y;
+		if (d.z < 0.0f) box.lo.z += d.z; else box.hi.z += d.z;
+		B.fatLo[i] = st3(box.lo);
+		B.fatHi[i] = st3(box.hi);
+		B.hasFat[i] = 1;
+	}
+
+	// tier membership and cell counts (reference src/grid.cpp:39-78)
+	uint32_t ca = 0, oa = 0;
+	uint8_t inCellsA = 0;
+	if (active)
+	{
+		int64_t span = cellSpan(loadFat(B, i), inv);
+		if (span > kOversizedCellSpan)
+		{
+			oa = 1;
+		}
+		else
+		{
+			ca = (uint32_t)span;
+			inCellsA = 1;
+		}
+	}
+	cntA[i] = ca;
+	overA[i] = oa;
+	inActiveCells[i] = inCellsA;
+	if (rebuildStable)
+	{
+		uint32_t cs = 0, os = 0;
+		uint8_t inCellsS = 0;
+		if (stable)
+		{
+			int64_t span = cellSpan(loadFat(B, i), inv);
+			if (span > kOversizedCellSpan)
+			{
+				os = 1;
+			}
+			else
+			{
+				cs = (uint32_t)span;
+				inCellsS = 1;
+			}
+		}
+		cntS[i] = cs;
+		overS[i] = os;
+		B.inStableCells[i] = inCellsS;
+		B.inStableTier[i] = stable ? 1 : 0;
+	}
+}
+
+void launchRefresh(DevWorld& w, int32_t n, float dt, bool rebuildStable, float cellSize)
+{
+	float inv = 1.0f / cellSize;
+	size_t n4 = (size_t)(n + 1) * sizeof(uint32_t);
+	w.cellCountA.ensure(n4);
+	w.overFlagA.ensure(n4);
+	w.cellCountS.ensure(n4);
+	w.overFlagS.ensure(n4);
+	w.inActiveCells.ensure((size_t)n + 1);
+	if (n <= 0)
+	{
+		return;
+	}
+	kRefresh<<<blocksFor(n, 256), 256, 0, w.stream>>>(w.B, n, dt, rebuildStable ? 1 : 0, inv,
+													   w.cellCountA.as<uint32_t>(), w.overFlagA.as<uint32_t>(),
+													   w.cellCountS.as<uint32_t>(), w.overFlagS.as<uint32_t>(),
+													   w.inActiveCells.as<uint8_t>());
+}
+
+// ---------------------------------------------------------------------------
+// tier build: entries (cell key, body) in body order, then a stable sort by
+// key, which yields the unique (key, body) order (reference src/grid.cpp:39-95)
+// ---------------------------------------------------------------------------
+
+__global__ void kEmitEntries(BodySoA B, int32_t n, float inv, const uint32_t* cnt, const uint32_t* offs,
+							 uint64_t* keys, uint32_t* vals)
+{
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n || cnt[i] == 0)
+	{
+		return;
+	}
+	Box b = loadFat(B, i);
+	int64_t x0 = cellCoord(b.lo.x, inv), y0 = cellCoord(b.lo.y, inv), z0 = cellCoord(b.lo.z, inv);
+	int64_t x1 = cellCoord(b.hi.x, inv), y1 = cellCoord(b.hi.y, inv), z1 = cellCoord(b.hi.z, inv);
+	uint32_t o = offs[i];
+	for (int64_t x = x0; x <= x1; ++x)
+	{
+		for (int64_t y = y0; y <= y1; ++y)
+		{
+			for (int64_t z = z0; z <= z1; ++z)
+			{
+				keys[o] = packCell(x, y, z);
+				vals[o] = (uint32_t)i;
+				++o;
+			}
+		}
+	}
+}
+
+__global__ void kCompactIndices(const uint32_t* flags, const uint32_t* offs, int32_t n, int32_t* out)
+{
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n && flags[i])
+	{
+		out[offs[i]] = i;
+	}
+}
+
+// One tier: counts -> offsets -> entries -> sort; oversized list in body order.
+static void buildTier(DevWorld& w, int32_t n, float inv, DevBuf& cnt, DevBuf& over, DevBuf& keys, DevBuf& vals,
+					  DevBuf& overList, uint32_t* entryTotal, uint32_t* overTotal, int64_t& entriesOut,
+					  int32_t& overCountOut)
+{
+	StepCounters* dc = devCounters(w);
+	DevBuf& offs = w.runFlag; // scratch reuse: offsets of this tier
+	offs.ensure((size_t)(n + 1) * sizeof(uint32_t));
+	DevBuf& ooffs = w.runPairCount;
+	ooffs.ensure((size_t)(n + 1) * sizeof(uint32_t));
+	scanExclusive(cnt.as<uint32_t>(), offs.as<uint32_t>(), n, entryTotal, w.prim, w.stream);
+	scanExclusive(over.as<uint32_t>(), ooffs.as<uint32_t>(), n, overTotal, w.prim, w.stream);
+	(void)dc;
+	readCounters(w);
+	int64_t total = entryTotal == &dc->activeEntries ? w.hostCounters->activeEntries : w.hostCounters->stableEntries;
+	int32_t ototal =
+		(int32_t)(overTotal == &dc->activeOversized ? w.hostCounters->activeOversized : w.hostCounters->stableOversized);
+	keys.ensure((size_t)(total + 1) * sizeof(uint64_t));
+	vals.ensure((size_t)(total + 1) * sizeof(uint32_t));
+	overList.ensure((size_t)(ototal + 1) * sizeof(int32_t));
+	if (n > 0)
+	{
+		kEmitEntries<<<blocksFor(n, 128), 128, 0, w.stream>>>(w.B, n, inv, cnt.as<uint32_t>(), offs.as<uint32_t>(),
+															   keys.as<uint64_t>(), vals.as<uint32_t>());
+		kCompactIndices<<<blocksFor(n, 256), 256, 0, w.stream>>>(over.as<uint32_t>(), ooffs.as<uint32_t>(), n,
+																  overList.as<int32_t>());
+	}
+	if (total > 1)
+	{
+		reduceKeyRange(keys.as<uint64_t>(), total, w.prim, w.stream);
+		cudaStreamSynchronize(w.stream);
+		uint64_t vary = w.prim.hostReduce[0] ^ w.prim.hostReduce[1];
+		radixSortPairs(keys.as<uint64_t>(), vals.as<uint32_t>(), total, vary, w.prim, w.stream);
+	}
+	entriesOut = total;
+	overCountOut = ototal;
+}
+
+void launchBuildActiveGrid(DevWorld& w, int32_t n, float cellSize)
+{
+	StepCounters* dc = devCounters(w);
+	buildTier(w, n, 1.0f / cellSize, w.cellCountA, w.overFlagA, w.activeKeys, w.activeVals, w.activeOver,
+			  &dc->activeEntries, &dc->activeOversized, w.activeEntries, w.activeOverCount);
+}
+
+void launchBuildStableGrid(DevWorld& w, int32_t n, float cellSize)
+{
+	StepCounters* dc = devCounters(w);
+	buildTier(w, n, 1.0f / cellSize, w.cellCountS, w.overFlagS, w.stableKeys, w.stableVals, w.stableOver,
+			  &dc->stableEntries, &dc->stableOversized, w.stableEntries, w.stableOverCount);
+}
+
+// ---------------------------------------------------------------------------
+// cell runs over the sorted active entries (reference src/world.cpp:1576-1587)
+// ---------------------------------------------------------------------------
+
+__global__ void kRunFlags(const uint64_t* keys, int64_t n, uint32_t* flag)
+{
+	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n)
+	{
+		flag[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+	}
+}
+
+__global__ void kRunStarts(const uint32_t* flag, const uint32_t* offs, int64_t n, int32_t* starts, const uint32_t* total)
+{
+	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n && flag[i])
+	{
+		starts[offs[i]] = (int32_t)i;
+	}
+	if (i == 0)
+	{
+		starts[*total] = (int32_t)n;
+	}
+}
+
+void launchFindRuns(DevWorld& w)
+{
+	StepCounters* dc = devCounters(w);
+	int64_t n = w.activeEntries;
+	w.runFlag.ensure((size_t)(n + 1) * sizeof(uint32_t));
+	w.runPairCount.ensure((size_t)(n + 1) * sizeof(uint32_t));
+	w.runStarts.ensure((size_t)(n + 2) * sizeof(int32_t));
+	if (n <= 0)
+	{
+		w.runCount = 0;
+		return;
+	}
+	kRunFlags<<<blocksFor(n, 256), 256, 0, w.stream>>>(w.activeKeys.as<uint64_t>(), n, w.runFlag.as<uint32_t>());
+	uint32_t* offs = w.runPairCount.as<uint32_t>();
+	scanExclusive(w.runFlag.as<uint32_t>(), offs, n, &dc->runs, w.prim, w.stream);
+	kRunStarts<<<blocksFor(n, 256), 256, 0, w.stream>>>(w.runFlag.as<uint32_t>(), offs, n, w.runStarts.as<int32_t>(),
+														 &dc->runs);
+	readCounters(w);
+	w.runCount = (int32_t)w.hostCounters->runs;
+}
+
+// ---------------------------------------------------------------------------
+// pair enumeration (reference src/world.cpp:1486-1641, 1663-1702)
+// ---------------------------------------------------------------------------
+
+struct PairCtx
+{
+	BodySoA B;
+	const uint64_t* existing;
+	uint32_t existingMask;
+	const uint64_t* jointed;
+	int32_t jointedCount;
+	float inv;
+};
+
+__device__ __forceinline__ bool jointedContains(const uint64_t* keys, int32_t n, uint64_t k)
+{
+	int32_t lo = 0, hi = n;
+	while (lo < hi)
+	{
+		int32_t mid = (lo + hi) >> 1;
+		if (keys[mid] < k)
+		{
+			lo = mid + 1;
+		}
+		else
+		{
+			hi = mid;
+		}
+	}
+	return lo < n && keys[lo] == k;
+}
+
+// every read-only admission filter of the reference (src/world.cpp:1486-1538)
+__device__ bool admissible(const PairCtx& P, int32_t a, int32_t b, uint64_t* keyOut)
+{
+	if (a == b)
+	{
+		return false;
+	}
+	if (!P.B.moved[a] && !P.B.moved[b])
+	{
+		return false;
+	}
+	int32_t lo = a < b ? a : b;
+	int32_t hi = a < b ? b : a;
+	uint8_t sl = P.B.state[lo], sh = P.B.state[hi];
+	if (!(sl & kStInUse) || !(sh & kStInUse))
+	{
+		return false;
+	}
+	const BodyCold& cl = P.B.cold[lo];
+	const BodyCold& ch = P.B.cold[hi];
+	if (cl.type != kDynamic && ch.type != kDynamic)
+	{
+		return false;
+	}
+	if (!(sl & kStAwake) && !(sh & kStAwake))
+	{
+		return false;
+	}
+	if (!overlap(loadFat(P.B, lo), loadFat(P.B, hi)))
+	{
+		return false;
+	}
+	if (cl.groupIndex != 0 && cl.groupIndex == ch.groupIndex)
+	{
+		if (cl.groupIndex < 0)
+		{
+			return false;
+		}
+	}
+	else if ((cl.categoryBits & ch.maskBits) == 0 || (ch.categoryBits & cl.maskBits) == 0)
+	{
+		return false;
+	}
+	uint64_t key = pairKey(lo, hi);
+	if (hashContains(P.existing, P.existingMask, key))
+	{
+		return false;
+	}
+	if (P.jointedCount > 0 && jointedContains(P.jointed, P.jointedCount, key))
+	{
+		return false;
+	}
+	*keyOut = key;
+	return true;
+}
+
+__device__ __forceinline__ int64_t lowerBoundKey(const uint64_t* keys, int64_t n, uint64_t k)
+{
+	int64_t lo = 0, hi = n;
+	while (lo < hi)
+	{
+		int64_t mid = (lo + hi) >> 1;
+		if (keys[mid] < k)
+		{
+			lo = mid + 1;
+		}
+		else
+		{
+			hi = mid;
+		}
+	}
+	return lo;
+}
+
+// One thread per cell run: count (EMIT=false) or write (EMIT=true) the
+// admitted pair keys of the run in the reference's enumeration order.
+template <bool EMIT>
+__global__ void kRunPairs(PairCtx P, const uint64_t* actKeys, const uint32_t* actVals, const int32_t* runStarts,
+						  int32_t runs, const uint64_t* stabKeys, const uint32_t* stabVals, int64_t stabCount,
+						  uint32_t* counts, const uint32_t* offsets, uint64_t* out)
+{
+	int r = blockIdx.x * blockDim.x + threadIdx.x;
+	if (r >= runs)
+	{
+		return;
+	}
+	int32_t s = runStarts[r], e = runStarts[r + 1];
+	uint64_t key = actKeys[s];
+	uint32_t k = EMIT ? offsets[r] : 0u;
+	for (int32_t i = s; i < e; ++i)
+	{
+		int32_t a = (int32_t)actVals[i];
+		V3 la = ld3(P.B.fatLo[a]);
+		for (int32_t j = i + 1; j < e; ++j)
+		{
+			int32_t b = (int32_t)actVals[j];
+			V3 lo2 = vmax(la, ld3(P.B.fatLo[b]));
+			uint64_t pk;
+			if (cellKeyOf(lo2, P.inv) == key && admissible(P, a, b, &pk))
+			{
+				if (EMIT)
+				{
+					out[k] = pk;
+				}
+				++k;
+			}
+		}
+	}
+	for (int64_t t = lowerBoundKey(stabKeys, stabCount, key); t < stabCount && stabKeys[t] == key; ++t)
+	{
+		int32_t b = (int32_t)stabVals[t];
+		V3 lb = ld3(P.B.fatLo[b]);
+		for (int32_t i = s; i < e; ++i)
+		{
+			int32_t a = (int32_t)actVals[i];
+			if (a == b)
+			{
+				continue; // stale stable entry of a body that woke
+			}
+			V3 lo2 = vmax(ld3(P.B.fatLo[a]), lb);
+			uint64_t pk;
+			if (cellKeyOf(lo2, P.inv) == key && admissible(P, a, b, &pk))
+			{
+				if (EMIT)
+				{
+					out[k] = pk;
+				}
+				++k;
+			}
+		}
+	}
+	if (!EMIT)
+	{
+		counts[r] = k;
+	}
+}
+
+// Oversized pairs, flattened in the reference's loop order:
+//   for each active oversized a (list order): every in-grid body b != a, then
+//   the later active oversized bodies, then every stable oversized b != a;
+//   then for each stable oversized a: every body in active cells.
+struct OverCtx
+{
+	const int32_t* actOver;
+	int32_t nAO;
+	const int32_t* stabOver;
+	int32_t nSO;
+	int32_t n;
+	const uint8_t* inActiveCells;
+};
+
+__device__ bool overCandidate(const OverCtx& O, int64_t idx, int32_t* aOut, int32_t* bOut)
+{
+	for (int32_t oi = 0; oi < O.nAO; ++oi)
+	{
+		int32_t a = O.actOver[oi];
+		int64_t blk = (int64_t)O.n + (O.nAO - oi - 1) + O.nSO;
+		if (idx < blk)
+		{
+			int32_t b;
+			if (idx < O.n)
+			{
+				b = (int32_t)idx;
+				if (b == a)
+				{
+					return false;
+				}
+				*aOut = a;
+				*bOut = b;
+				return true; // in-grid test done by the caller
+			}
+			idx -= O.n;
+			if (idx < O.nAO - oi - 1)
+			{
+				*aOut = a;
+				*bOut = O.actOver[oi + 1 + idx];
+				return true;
+			}
+			idx -= O.nAO - oi - 1;
+			b = O.stabOver[idx];
+			if (b == a)
+			{
+				return false;
+			}
+			*aOut = a;
+			*bOut = b;
+			return true;
+		}
+		idx -= blk;
+	}
+	int64_t si = idx / O.n;
+	int32_t b = (int32_t)(idx - si * O.n);
+	if (!O.inActiveCells[b])
+	{
+		return false;
+	}
+	*aOut = O.stabOver[si];
+	*bOut = b;
+	return true;
+}
+
+__global__ void kOverPairs(PairCtx P, OverCtx O, int64_t total, uint32_t* flags, uint64_t* keys)
+{
+	int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= total)
+	{
+		return;
+	}
+	int32_t a, b;
+	uint32_t ok = 0;
+	uint64_t pk = 0;
+	if (overCandidate(O, idx, &a, &b))
+	{
+		// first segment of an active oversized body: only bodies in either grid
+		bool gridOnly = false;
+		{
+			int64_t j = idx;
+			for (int32_t oi = 0; oi < O.nAO; ++oi)
+			{
+				int64_t blk = (int64_t)O.n + (O.nAO - oi - 1) + O.nSO;
+				if (j < blk)
+				{
+					gridOnly = j < O.n;
+					break;
+				}
+				j -= blk;
+			}
+		}
+		bool inGrid = !gridOnly || O.inActiveCells[b] || P.B.inStableCells[b];
+		if (inGrid && admissible(P, a, b, &pk))
+		{
+			ok = 1;
+		}
+	}
+	flags[idx] = ok;
+	keys[idx] = pk;
+}
+
+__global__ void kScatterKeys(const uint32_t* flags, const uint32_t* offs, const uint64_t* keys, int64_t n, uint64_t* out)
+{
+	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n && flags[i])
+	{
+		out[offs[i]] = keys[i];
+	}
+}
+
+__global__ void kInsertExisting(const int2* bodies, int32_t count, uint64_t* table, uint32_t mask, uint32_t* fail)
+{
+	int c = blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= count)
+	{
+		return;
+	}
+	int2 ab = bodies[c];
+	if (hashInsert(table, mask, pairKey(ab.x, ab.y)) == 0xFFFFFFFFu)
+	{
+		atomicAdd(fail, 1u);
+	}
+}
+
+// first occurrence of each key in the admitted stream wins
+__global__ void kDedupeMark(const uint64_t* keys, int64_t n, uint64_t* table, uint32_t* pos, uint32_t mask,
+							uint32_t* fail)
+{
+	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+	{
+		return;
+	}
+	uint32_t slot = hashInsert(table, mask, keys[i]);
+	if (slot == 0xFFFFFFFFu)
+	{
+		atomicAdd(fail, 1u);
+		return;
+	}
+	atomicMin(&pos[slot], (uint32_t)i);
+}
+
+__device__ __forceinline__ uint32_t hashFind(const uint64_t* table, uint32_t capMask, uint64_t key)
+{
+	uint32_t slot = hashKey(key) & capMask;
+	for (uint32_t probe = 0; probe <= capMask; ++probe)
+	{
+		uint64_t k = table[slot];
+		if (k == key)
+		{
+			return slot;
+		}
+		if (k == kEmptyKey)
+		{
+			return 0xFFFFFFFFu;
+		}
+		slot = (slot + 1) & capMask;
+	}
+	return 0xFFFFFFFFu;
+}
+
+__global__ void kDedupeKeep(const uint64_t* keys, int64_t n, const uint64_t* table, const uint32_t* pos, uint32_t mask,
+							uint32_t* keep)
+{
+	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+	{
+		return;
+	}
+	uint32_t slot = hashFind(table, mask, keys[i]);
+	keep[i] = (slot != 0xFFFFFFFFu && pos[slot] == (uint32_t)i) ? 1u : 0u;
+}
+
+static uint32_t tableCapacity(int64_t keys)
+{
+	uint64_t cap = 1024;
+	while (cap < (uint64_t)keys * 2 + 16)
+	{
+		cap <<= 1;
+	}
+	return (uint32_t)cap;
+}
+
+void launchPairs(DevWorld& w, int32_t n, float cellSize)
+{
+	StepCounters* dc = devCounters(w);
+	cudaStream_t s = w.stream;
+
+	// existing contact keys
+	uint32_t ecap = tableCapacity(w.contactCount);
+	w.existingSet.ensure((size_t)ecap * sizeof(uint64_t));
+	w.existingMask = ecap - 1;
+	cudaMemsetAsync(w.existingSet.ptr, 0xFF, (size_t)ecap * sizeof(uint64_t), s);
+	if (w.contactCount > 0)
+	{
+		kInsertExisting<<<blocksFor(w.contactCount, 256), 256, 0, s>>>(w.C.bodies, w.contactCount,
+																		 w.existingSet.as<uint64_t>(), w.existingMask,
+																		 &dc->hashFail);
+	}
+
+	PairCtx P;
+	P.B = w.B;
+	P.existing = w.existingSet.as<uint64_t>();
+	P.existingMask = w.existingMask;
+	P.jointed = w.jointedPairs.as<uint64_t>();
+	P.jointedCount = w.jointedCount;
+	P.inv = 1.0f / cellSize;
+
+	// grid runs: count, scan, emit
+	int32_t runs = w.runCount;
+	w.runPairCount.ensure((size_t)(runs + 1) * sizeof(uint32_t));
+	w.keepFlag.ensure((size_t)(runs + 1) * sizeof(uint32_t));
+	uint32_t* counts = w.runPairCount.as<uint32_t>();
+	uint32_t* offs = w.keepFlag.as<uint32_t>();
+	if (runs > 0)
+	{
+		kRunPairs<false><<<blocksFor(runs, 128), 128, 0, s>>>(
+			P, w.activeKeys.as<uint64_t>(), w.activeVals.as<uint32_t>(), w.runStarts.as<int32_t>(), runs,
+			w.stableKeys.as<uint64_t>(), w.stableVals.as<uint32_t>(), w.stableEntries, counts, nullptr, nullptr);
+	}
+	scanExclusive(counts, offs, runs, &dc->gridPairs, w.prim, s);
+
+	// oversized candidates
+	OverCtx O;
+	O.actOver = w.activeOver.as<int32_t>();
+	O.nAO = w.activeOverCount;
+	O.stabOver = w.stableOver.as<int32_t>();
+	O.nSO = w.stableOverCount;
+	O.n = n;
+	O.inActiveCells = w.inActiveCells.as<uint8_t>();
+	int64_t overTotal = (int64_t)O.nAO * ((int64_t)n + O.nSO) + (int64_t)O.nAO * (O.nAO - 1) / 2 + (int64_t)O.nSO * n;
+	w.overFlag.ensure((size_t)(overTotal + 1) * sizeof(uint32_t));
+	w.overScan.ensure((size_t)(overTotal + 1) * sizeof(uint32_t));
+	w.newContactKeys.ensure((size_t)(overTotal + 1) * sizeof(uint64_t));
+	if (overTotal > 0)
+	{
+		kOverPairs<<<blocksFor(overTotal, 256), 256, 0, s>>>(P, O, overTotal, w.overFlag.as<uint32_t>(),
+															  w.newContactKeys.as<uint64_t>());
+	}
+	scanExclusive(w.overFlag.as<uint32_t>(), w.overScan.as<uint32_t>(), overTotal, &dc->overPairs, w.prim, s);
+	readCounters(w);
+	int64_t gridPairs = w.hostCounters->gridPairs;
+	int64_t overPairs = w.hostCounters->overPairs;
+	int64_t total = gridPairs + overPairs;
+	w.pairKeys.ensure((size_t)(total + 1) * sizeof(uint64_t));
+	uint64_t* pk = w.pairKeys.as<uint64_t>();
+	if (runs > 0 && gridPairs > 0)
+	{
+		kRunPairs<true><<<blocksFor(runs, 128), 128, 0, s>>>(
+			P, w.activeKeys.as<uint64_t>(), w.activeVals.as<uint32_t>(), w.runStarts.as<int32_t>(), runs,
+			w.stableKeys.as<uint64_t>(), w.stableVals.as<uint32_t>(), w.stableEntries, nullptr, offs, pk);
+	}
+	if (overPairs > 0)
+	{
+		kScatterKeys<<<blocksFor(overTotal, 256), 256, 0, s>>>(w.overFlag.as<uint32_t>(), w.overScan.as<uint32_t>(),
+																w.newContactKeys.as<uint64_t>(), overTotal,
+																pk + gridPairs);
+	}
+
+	// first-occurrence dedupe of the admitted stream
+	uint32_t ncap = tableCapacity(total);
+	w.newSet.ensure((size_t)ncap * sizeof(uint64_t));
+	w.newSetPos.ensure((size_t)ncap * sizeof(uint32_t));
+	w.newMask = ncap - 1;
+	w.keepFlag.ensure((size_t)(total + 1) * sizeof(uint32_t));
+	w.overScan.ensure((size_t)(total + 1) * sizeof(uint32_t));
+	w.newContactKeys.ensure((size_t)(total + 1) * sizeof(uint64_t));
+	if (total > 0)
+	{
+		cudaMemsetAsync(w.newSet.ptr, 0xFF, (size_t)ncap * sizeof(uint64_t), s);
+		cudaMemsetAsync(w.newSetPos.ptr, 0xFF, (size_t)ncap * sizeof(uint32_t), s);
+		kDedupeMark<<<blocksFor(total, 256), 256, 0, s>>>(pk, total, w.newSet.as<uint64_t>(),
+														   w.newSetPos.as<uint32_t>(), w.newMask, &dc->hashFail);
+		kDedupeKeep<<<blocksFor(total, 256), 256, 0, s>>>(pk, total, w.newSet.as<uint64_t>(),
+														   w.newSetPos.as<uint32_t>(), w.newMask,
+														   w.keepFlag.as<uint32_t>());
+	}
+	scanExclusive(w.keepFlag.as<uint32_t>(), w.overScan.as<uint32_t>(), total, &dc->newContacts, w.prim, s);
+	if (total > 0)
+	{
+		kScatterKeys<<<blocksFor(total, 256), 256, 0, s>>>(w.keepFlag.as<uint32_t>(), w.overScan.as<uint32_t>(), pk,
+															total, w.newContactKeys.as<uint64_t>());
+	}
+	readCounters(w);
+}
+
+// ---------------------------------------------------------------------------
+// contact creation (reference src/world.cpp:1540-1568)
+// ---------------------------------------------------------------------------
+
+__global__ void kCreateContacts(BodySoA B, ContactSoA C, const uint64_t* keys, int32_t count, int32_t base)
+{
+	int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k >= count)
+	{
+		return;
+	}
+	int c = base + k;
+	uint64_t key = keys[k];
+	int32_t lo = (int32_t)(key >> 32), hi = (int32_t)(uint32_t)key;
+	const BodyCold& a = B.cold[lo];
+	const BodyCold& b = B.cold[hi];
+	C.bodies[c] = make_int2(lo, hi);
+	C.pointCount[c] = 0;
+	bool sensor = ((B.state[lo] | B.state[hi]) & kStSensor) != 0;
+	bool curved = a.shape.type != kBox || b.shape.type != kBox;
+	C.flags[c] = (uint8_t)((sensor ? kCFSensor : 0) | (curved ? kCFCurved : 0));
+	C.normal[c] = make_float4(0.0f, 1.0f, 0.0f, sqrtf(a.friction * b.friction));
+	C.mat[c] = make_float2(a.restitution > b.restitution ? a.restitution : b.restitution,
+						   sqrtf(a.rollingResistance * b.rollingResistance));
+	float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	C.cachePosA[c] = z;
+	C.cacheRotA[c] = z;
+	C.cachePosB[c] = z;
+	C.cacheRotB[c] = z;
+	for (int s = 0; s < 4; ++s)
+	{
+		size_t p = pidx(C, c, s);
+		C.pAnchorA[p] = z;
+		C.pAnchorB[p] = z;
+		C.pFricA[p] = z;
+		C.pFricB[p] = z;
+		C.pSlip[p] = z;
+		C.pRA[p] = z;
+		C.pRB[p] = z;
+		C.pJA[p] = z;
+		C.pJB[p] = z;
+	}
+}
+
+void launchCreateContacts(DevWorld& w, int32_t newCount)
+{
+	if (newCount <= 0)
+	{
+		return;
+	}
+	kCreateContacts<<<blocksFor(newCount, 128), 128, 0, w.stream>>>(w.B, w.C, w.newContactKeys.as<uint64_t>(),
+																	  newCount, w.contactCount);
+	w.contactCount += newCount;
+}
+
+// ---------------------------------------------------------------------------
+// removal of separated pairs: closed form of the descending swap-remove
+// (reference src/world.cpp:100-119, 1705-1735).  With S = count - removed,
+// the k-th largest removed index below S receives the k-th largest surviving
+// index at or above S; end events go out in descending index order.
+// ---------------------------------------------------------------------------
+
+__global__ void kRemovalFlags(BodySoA B, ContactSoA C, int32_t count, uint32_t* removeFlag, uint32_t* evFlag)
+{
+	int c = blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= count)
+	{
+		return;
+	}
+	int2 ab = C.bodies[c];
+	uint32_t rm = 0;
+	if ((B.bFlags[ab.x] & kBFAwake) || (B.bFlags[ab.y] & kBFAwake))
+	{
+		if (!overlap(loadFat(B, ab.x), loadFat(B, ab.y)))
+		{
+			rm = 1;
+		}
+	}
+	removeFlag[c] = rm;
+	evFlag[c] = (rm && (C.flags[c] & kCFTouching)) ? 1u : 0u;
+}
+
+__global__ void kRemovalEvents(const ContactSoA C, int32_t count, const uint32_t* evFlag, const uint32_t* evScan,
+							   const uint32_t* evTotal, int4* events)
+{
+	int c = blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= count || !evFlag[c])
+	{
+		return;
+	}
+	uint32_t t = *evTotal;
+	int2 ab = C.bodies[c];
+	events[t - 1 - evScan[c]] = make_int4(ab.x, ab.y, (C.flags[c] & kCFSensor) ? 1 : 0, 0);
+}
+
+__global__ void kRemovalSources(int32_t count, int32_t S, const uint32_t* removeFlag, const uint32_t* removeScan,
+								int32_t* moveSrc)
+{
+	int t = S + blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= count || removeFlag[t])
+	{
+		return;
+	}
+	int32_t H = (int32_t)removeScan[S];
+	int32_t survivorsBelow = (t - S) - ((int32_t)removeScan[t] - H);
+	moveSrc[H - 1 - survivorsBelow] = t;
+}
+
+__device__ void copyContact(const ContactSoA& C, int dst, int src)
+{
+	C.bodies[dst] = C.bodies[src];
+	C.pointCount[dst] = C.pointCount[src];
+	C.flags[dst] = C.flags[src];
+	C.normal[dst] = C.normal[src];
+	C.mat[dst] = C.mat[src];
+	C.cachePosA[dst] = C.cachePosA[src];
+	C.cacheRotA[dst] = C.cacheRotA[src];
+	C.cachePosB[dst] = C.cachePosB[src];
+	C.cacheRotB[dst] = C.cacheRotB[src];
+	for (int s = 0; s < 4; ++s)
+	{
+		size_t d = pidx(C, dst, s), o = pidx(C, src, s);
+		C.pAnchorA[d] = C.pAnchorA[o];
+		C.pAnchorB[d] = C.pAnchorB[o];
+		C.pFricA[d] = C.pFricA[o];
+		C.pFricB[d] = C.pFricB[o];
+		C.pSlip[d] = C.pSlip[o];
+		C.pRA[d] = C.pRA[o];
+		C.pRB[d] = C.pRB[o];
+		C.pJA[d] = C.pJA[o];
+		C.pJB[d] = C.pJB[o];
+	}
+}
+
+__global__ void kRemovalMoves(ContactSoA C, int32_t S, const uint32_t* removeFlag, const uint32_t* removeScan,
+							  const int32_t* moveSrc)
+{
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= S || !removeFlag[i])
+	{
+		return;
+	}
+	int32_t H = (int32_t)removeScan[S];
+	int32_t rankTop = H - 1 - (int32_t)removeScan[i];
+	copyContact(C, i, moveSrc[rankTop]);
+}
+
+__global__ void kContactMoves(ContactSoA C, const int2* moves, int32_t count)
+{
+	int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k < count)
+	{
+		copyContact(C, moves[k].x, moves[k].y);
+	}
+}
+
+// Sources of destroy-time moves all lie at or above the new contact count and
+// destinations below it, so the moves are independent.
+void launchContactMoves(DevWorld& w, const int2* hostMoves, int32_t count)
+{
+	if (count <= 0)
+	{
+		return;
+	}
+	w.moveSrc.ensure(sizeof(int2) * (size_t)count);
+	cudaMemcpyAsync(w.moveSrc.ptr, hostMoves, sizeof(int2) * (size_t)count, cudaMemcpyHostToDevice, w.stream);
+	kContactMoves<<<blocksFor(count, 128), 128, 0, w.stream>>>(w.C, (const int2*)w.moveSrc.ptr, count);
+	cudaStreamSynchronize(w.stream); // the host vector backing hostMoves is freed on return
+}
+
+void launchRemoval(DevWorld& w)
+{
+	StepCounters* dc = devCounters(w);
+	cudaStream_t s = w.stream;
+	int32_t count = w.contactCount;
+	size_t c4 = (size_t)(count + 1) * sizeof(uint32_t);
+	w.removeFlag.ensure(c4);
+	w.removeScan.ensure(c4);
+	w.evEndFlag.ensure(c4);
+	w.evBeginFlag.ensure(c4);
+	w.evRemoval.ensure((size_t)(count + 1) * sizeof(int4));
+	w.moveSrc.ensure(c4);
+	if (count <= 0)
+	{
+		cudaMemsetAsync(&dc->removed, 0, sizeof(uint32_t), s);
+		cudaMemsetAsync(&dc->endRemoval, 0, sizeof(uint32_t), s);
+		readCounters(w);
+		return;
+	}
+	kRemovalFlags<<<blocksFor(count, 256), 256, 0, s>>>(w.B, w.C, count, w.removeFlag.as<uint32_t>(),
+														  w.evEndFlag.as<uint32_t>());
+	// the scan covers count + 1 entries so removeScan[count] exists
+	cudaMemsetAsync(w.removeFlag.as<uint32_t>() + count, 0, sizeof(uint32_t), s);
+	scanExclusive(w.removeFlag.as<uint32_t>(), w.removeScan.as<uint32_t>(), count + 1, &dc->removed, w.prim, s);
+	scanExclusive(w.evEndFlag.as<uint32_t>(), w.evBeginFlag.as<uint32_t>(), count, &dc->endRemoval, w.prim, s);
+	kRemovalEvents<<<blocksFor(count, 256), 256, 0, s>>>(w.C, count, w.evEndFlag.as<uint32_t>(),
+														   w.evBeginFlag.as<uint32_t>(), &dc->endRemoval,
+														   w.evRemoval.as<int4>());
+	readCounters(w);
+	int32_t removed = (int32_t)w.hostCounters->removed;
+	if (removed > 0)
+	{
+		int32_t S = count - removed;
+		kRemovalSources<<<blocksFor(removed, 256), 256, 0, s>>>(count, S, w.removeFlag.as<uint32_t>(),
+																 w.removeScan.as<uint32_t>(), w.moveSrc.as<int32_t>());
+		if (S > 0)
+		{
+			kRemovalMoves<<<blocksFor(S, 256), 256, 0, s>>>(w.C, S, w.removeFlag.as<uint32_t>(),
+															 w.removeScan.as<uint32_t>(), w.moveSrc.as<int32_t>());
+		}
+		w.contactCount = S;
+	}
+}
+
+} // namespace m3g

@@ -1,0 +1,422 @@
+// Island solve of one step: all substeps of every awake island.
+//
+//  - free islands (one body, no contacts, no joints): integrate and
+//    reconstruct per substep, one thread per body;
+//  - small islands (< 300 contacts): the reference's serial Gauss-Seidel in
+//    ascending contact order (src/xpbd.cpp:898-974), one thread per island;
+//  - big islands (>= 300 contacts): the reference's graph-coloured solve
+//    (src/xpbd.cpp:1167-1369), one CTA per island: greedy first-fit colouring
+//    in contact order, colour buckets solved in parallel (bodies in a bucket
+//    are disjoint), the overflow bucket and the joints serially, with
+//    __syncthreads() where the reference joins its fork-join stages.
+// Islands are disjoint in their dynamic bodies, so all islands run at once.
+#include "m3d_dev.cuh"
+#include "m3d_solve.cuh"
+
+namespace m3g
+{
+
+struct SolveParams
+{
+	float h, invH, maxCorrection, gravityLen;
+	V3 gravity;
+	int substeps;
+	int iterations;
+};
+
+__global__ void kSolveFree(BodySoA B, const IslandRec* islands, int32_t ni, const uint32_t* bodyVals, SolveParams P)
+{
+	int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k >= ni)
+	{
+		return;
+	}
+	const IslandRec r = islands[k];
+	if (r.kind != 0)
+	{
+		return;
+	}
+	for (int b = 0; b < r.bodyCount; ++b)
+	{
+		int i = (int)bodyVals[r.bodyStart + b];
+		for (int sub = 0; sub < P.substeps; ++sub)
+		{
+			integrateBody(B, i, P.h, P.gravity);
+			reconstructBody(B, i, P.invH);
+		}
+	}
+}
+
+__device__ __forceinline__ void jointPosition(const BodySoA& B, JointRec* J, int ji, float h)
+{
+	JointRec jr = J[ji];
+	solveJointPosition(B, jr, h);
+	J[ji] = jr;
+}
+__device__ __forceinline__ void jointVelocity(const BodySoA& B, JointRec* J, int ji, float h)
+{
+	JointRec jr = J[ji];
+	solveJointVelocity(B, jr, h);
+	J[ji] = jr;
+}
+__device__ __forceinline__ void jointPrepare(const BodySoA& B, JointRec* J, int ji)
+{
+	JointRec jr = J[ji];
+	prepareJoint(B, jr);
+	J[ji] = jr;
+}
+__device__ __forceinline__ void jointReset(JointRec* J, int ji)
+{
+	J[ji].lambda = 0.0f;
+	J[ji].motorLambda = 0.0f;
+}
+
+__global__ void kSolveSerial(BodySoA B, ContactSoA C, JointRec* J, const IslandRec* islands, int32_t ni,
+							 const uint32_t* bodyVals, const uint32_t* contactVals, const uint32_t* jointVals,
+							 SolveParams P)
+{
+	int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k >= ni)
+	{
+		return;
+	}
+	const IslandRec r = islands[k];
+	if (r.kind != 1)
+	{
+		return;
+	}
+	const uint32_t* bodies = bodyVals + r.bodyStart;
+	const uint32_t* contacts = contactVals + r.contactStart;
+	const uint32_t* joints = jointVals + r.jointStart;
+	if (r.jointCount > 0)
+	{
+		for (int b = 0; b < r.bodyCount; ++b)
+		{
+			refreshInvInertia(B, (int)bodies[b]);
+		}
+		for (int j = 0; j < r.jointCount; ++j)
+		{
+			jointPrepare(B, J, (int)joints[j]);
+		}
+	}
+	for (int sub = 0; sub < P.substeps; ++sub)
+	{
+		for (int b = 0; b < r.bodyCount; ++b)
+		{
+			integrateBody(B, (int)bodies[b], P.h, P.gravity);
+		}
+		for (int c = 0; c < r.contactCount; ++c)
+		{
+			prepareContact(B, C, (int)contacts[c], P.h);
+		}
+		for (int j = 0; j < r.jointCount; ++j)
+		{
+			jointReset(J, (int)joints[j]);
+		}
+		for (int it = 0; it < P.iterations; ++it)
+		{
+			for (int j = 0; j < r.jointCount; ++j)
+			{
+				jointPosition(B, J, (int)joints[j], P.h);
+			}
+			for (int c = 0; c < r.contactCount; ++c)
+			{
+				solveContactNormals(B, C, (int)contacts[c], P.maxCorrection);
+			}
+		}
+		for (int c = 0; c < r.contactCount; ++c)
+		{
+			applyContactFriction(B, C, (int)contacts[c]);
+		}
+		for (int b = 0; b < r.bodyCount; ++b)
+		{
+			reconstructBody(B, (int)bodies[b], P.invH);
+		}
+		for (int c = 0; c < r.contactCount; ++c)
+		{
+			solveContactVelocity(B, C, (int)contacts[c], P.h, P.gravityLen);
+		}
+		for (int j = 0; j < r.jointCount; ++j)
+		{
+			jointVelocity(B, J, (int)joints[j], P.h);
+		}
+	}
+}
+
+constexpr int kColorThreads = 256;
+
+__global__ void __launch_bounds__(kColorThreads)
+	kSolveColored(BodySoA B, ContactSoA C, JointRec* J, const IslandRec* islands, int32_t ni, const uint32_t* bodyVals,
+				  const uint32_t* contactVals, const uint32_t* jointVals, uint32_t* colorMask, int32_t* colorOrder,
+				  int32_t* packetMax, int32_t* contactColor, SolveParams P)
+{
+	__shared__ int32_t bucketStart[kMaxGraphColors + 2];
+	__shared__ int32_t colorCount;
+	int k = blockIdx.x;
+	if (k >= ni)
+	{
+		return;
+	}
+	const IslandRec r = islands[k];
+	if (r.kind != 2)
+	{
+		return;
+	}
+	const int tid = threadIdx.x, nt = blockDim.x;
+	const uint32_t* bodies = bodyVals + r.bodyStart;
+	const uint32_t* contacts = contactVals + r.contactStart;
+	const uint32_t* joints = jointVals + r.jointStart;
+	int32_t* order = colorOrder + r.contactStart;
+	int32_t* pmax = packetMax + r.contactStart;
+
+	// ---- greedy first-fit colouring in contact order (src/xpbd.cpp:1179-1235)
+	for (int b = tid; b < r.bodyCount; b += nt)
+	{
+		colorMask[bodies[b]] = 0;
+	}
+	__syncthreads();
+	if (tid == 0)
+	{
+		int32_t counts[kMaxGraphColors + 1];
+		for (int c = 0; c <= kMaxGraphColors; ++c)
+		{
+			counts[c] = 0;
+		}
+		int32_t cc = 0;
+		// pass 1: colours (stored temporarily in `order`)
+		for (int p = 0; p < r.contactCount; ++p)
+		{
+			int ci = (int)contacts[p];
+			int2 ab = C.bodies[ci];
+			bool dynA = B.massInv[ab.x].x > 0.0f;
+			bool dynB = B.massInv[ab.y].x > 0.0f;
+			uint32_t used = 0;
+			if (dynA)
+			{
+				used |= colorMask[ab.x];
+			}
+			if (dynB)
+			{
+				used |= colorMask[ab.y];
+			}
+			uint32_t freeBits = ~used;
+			int color = freeBits != 0 ? __ffs((int)freeBits) - 1 : kMaxGraphColors;
+			if (color >= kMaxGraphColors)
+			{
+				color = kMaxGraphColors;
+			}
+			else
+			{
+				uint32_t bit = 1u << color;
+				if (dynA)
+				{
+					colorMask[ab.x] |= bit;
+				}
+				if (dynB)
+				{
+					colorMask[ab.y] |= bit;
+				}
+				cc = color + 1 > cc ? color + 1 : cc;
+			}
+			order[p] = color;
+			contactColor[ci] = color;
+			++counts[color];
+		}
+		int32_t run = 0;
+		for (int c = 0; c <= kMaxGraphColors; ++c)
+		{
+			bucketStart[c] = run;
+			run += counts[c];
+		}
+		bucketStart[kMaxGraphColors + 1] = run;
+		colorCount = cc;
+		// pass 2: regroup by colour, keeping contact order inside each bucket
+		int32_t cursor[kMaxGraphColors + 1];
+		for (int c = 0; c <= kMaxGraphColors; ++c)
+		{
+			cursor[c] = bucketStart[c];
+		}
+		for (int p = 0; p < r.contactCount; ++p)
+		{
+			int color = contactColor[contacts[p]];
+			pmax[cursor[color]++] = (int32_t)contacts[p];
+		}
+		for (int p = 0; p < r.contactCount; ++p)
+		{
+			order[p] = pmax[p];
+		}
+	}
+	__syncthreads();
+	const int ncol = colorCount;
+
+	if (r.jointCount > 0)
+	{
+		for (int b = tid; b < r.bodyCount; b += nt)
+		{
+			refreshInvInertia(B, (int)bodies[b]);
+		}
+		__syncthreads();
+		if (tid == 0)
+		{
+			for (int j = 0; j < r.jointCount; ++j)
+			{
+				jointPrepare(B, J, (int)joints[j]);
+			}
+		}
+		__syncthreads();
+	}
+
+	const int colored = bucketStart[kMaxGraphColors];
+	const int overflowStart = colored, overflowEnd = bucketStart[kMaxGraphColors + 1];
+	for (int sub = 0; sub < P.substeps; ++sub)
+	{
+		for (int b = tid; b < r.bodyCount; b += nt)
+		{
+			integrateBody(B, (int)bodies[b], P.h, P.gravity);
+		}
+		__syncthreads();
+		for (int c = tid; c < r.contactCount; c += nt)
+		{
+			prepareContact(B, C, (int)contacts[c], P.h);
+		}
+		if (tid == 0)
+		{
+			for (int j = 0; j < r.jointCount; ++j)
+			{
+				jointReset(J, (int)joints[j]);
+			}
+		}
+		__syncthreads();
+		// packets of 8 consecutive bucket entries share the largest point count
+		for (int q = tid; q < colored; q += nt)
+		{
+			int color = 0;
+			while (q >= bucketStart[color + 1])
+			{
+				++color;
+			}
+			int bs = bucketStart[color], be = bucketStart[color + 1];
+			int p0 = bs + ((q - bs) & ~7);
+			int p1 = p0 + 8 < be ? p0 + 8 : be;
+			int m = 0;
+			for (int p = p0; p < p1; ++p)
+			{
+				int pc = C.pointCount[order[p]];
+				m = pc > m ? pc : m;
+			}
+			pmax[q] = m;
+		}
+		__syncthreads();
+		for (int it = 0; it < P.iterations; ++it)
+		{
+			if (tid == 0)
+			{
+				for (int j = 0; j < r.jointCount; ++j)
+				{
+					jointPosition(B, J, (int)joints[j], P.h);
+				}
+			}
+			__syncthreads();
+			for (int color = 0; color < ncol; ++color)
+			{
+				for (int q = bucketStart[color] + tid; q < bucketStart[color + 1]; q += nt)
+				{
+					solvePacketLane(B, C, order[q], pmax[q], P.maxCorrection);
+				}
+				__syncthreads();
+			}
+			if (tid == 0)
+			{
+				for (int q = overflowStart; q < overflowEnd; ++q)
+				{
+					solveContactNormals(B, C, order[q], P.maxCorrection);
+				}
+			}
+			__syncthreads();
+		}
+		for (int color = 0; color < ncol; ++color)
+		{
+			for (int q = bucketStart[color] + tid; q < bucketStart[color + 1]; q += nt)
+			{
+				applyContactFriction(B, C, order[q]);
+			}
+			__syncthreads();
+		}
+		if (tid == 0)
+		{
+			for (int q = overflowStart; q < overflowEnd; ++q)
+			{
+				applyContactFriction(B, C, order[q]);
+			}
+		}
+		__syncthreads();
+		for (int b = tid; b < r.bodyCount; b += nt)
+		{
+			reconstructBody(B, (int)bodies[b], P.invH);
+		}
+		__syncthreads();
+		for (int color = 0; color < ncol; ++color)
+		{
+			for (int q = bucketStart[color] + tid; q < bucketStart[color + 1]; q += nt)
+			{
+				solveContactVelocity(B, C, order[q], P.h, P.gravityLen);
+			}
+			__syncthreads();
+		}
+		if (tid == 0)
+		{
+			for (int q = overflowStart; q < overflowEnd; ++q)
+			{
+				solveContactVelocity(B, C, order[q], P.h, P.gravityLen);
+			}
+			for (int j = 0; j < r.jointCount; ++j)
+			{
+				jointVelocity(B, J, (int)joints[j], P.h);
+			}
+		}
+		__syncthreads();
+	}
+}
+
+void launchSolve(DevWorld& w, float dt, int substeps, V3 gravity, int positionIterations)
+{
+	int32_t ni = w.islandCount;
+	if (ni <= 0)
+	{
+		return;
+	}
+	SolveParams P;
+	P.h = dt / (float)substeps;
+	P.invH = P.h > 0.0f ? 1.0f / P.h : 0.0f;
+	P.maxCorrection = kMaxDepenetrationSpeed * P.h;
+	P.gravity = gravity;
+	P.gravityLen = len(gravity);
+	P.substeps = substeps;
+	P.iterations = positionIterations > 0 ? positionIterations : 2;
+	cudaStream_t s = w.stream;
+	const IslandRec* isl = w.islands.as<IslandRec>();
+	const StepCounters* hc = w.hostCounters;
+	if (hc->freeIslands > 0)
+	{
+		kSolveFree<<<blocksFor(ni, 128), 128, 0, s>>>(w.B, isl, ni, w.bodyVals.as<uint32_t>(), P);
+	}
+	if (hc->serialIslands > 0)
+	{
+		kSolveSerial<<<blocksFor(ni, 64), 64, 0, s>>>(w.B, w.C, w.joints.as<JointRec>(), isl, ni,
+													   w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(),
+													   w.jointVals.as<uint32_t>(), P);
+	}
+	if (hc->coloredIslands > 0)
+	{
+		size_t nc = (size_t)hc->islandContacts + 1;
+		w.colorMask.ensure((size_t)(w.bodyCap + 1) * sizeof(uint32_t));
+		w.colorOrder.ensure(nc * sizeof(int32_t));
+		w.packetMax.ensure(nc * sizeof(int32_t));
+		kSolveColored<<<ni, kColorThreads, 0, s>>>(w.B, w.C, w.joints.as<JointRec>(), isl, ni, w.bodyVals.as<uint32_t>(),
+													w.contactVals.as<uint32_t>(), w.jointVals.as<uint32_t>(),
+													w.colorMask.as<uint32_t>(), w.colorOrder.as<int32_t>(),
+													w.packetMax.as<int32_t>(), w.contactColor.as<int32_t>(), P);
+	}
+}
+
+} // namespace m3g

@@ -1,0 +1,207 @@
+// The device half of a world: SoA arenas in HBM, per-step scratch, and the
+// launchers of every stage of the step.  Host code (world.cu) owns one
+// DevWorld per m3d_world and drives the stages in the reference's order.
+#pragma once
+
+#include "m3d_types.cuh"
+#include "prims.cuh"
+
+namespace m3g
+{
+
+// Counters written by the kernels and read back by the host at the few
+// points where the step needs a size (pinned host copy, one D2H each).
+struct StepCounters
+{
+	uint32_t activeEntries;
+	uint32_t stableEntries;
+	uint32_t activeOversized;
+	uint32_t stableOversized;
+	uint32_t runs;
+	uint32_t gridPairs;
+	uint32_t overPairs;
+	uint32_t newContacts;
+	uint32_t removed;
+	uint32_t endRemoval;
+	uint32_t beginNP;
+	uint32_t endNP;
+	uint32_t anyAwakeDynamic;
+	uint32_t islandCount;
+	uint32_t touchingCount;
+	uint32_t awakeIslands;
+	uint32_t islandContacts;
+	uint32_t islandJoints;
+	uint32_t islandBodies;
+	uint32_t stableDirty;
+	uint32_t bodyCount;
+	uint32_t awakeBodyCount;
+	uint32_t hashFail;
+	uint32_t coloredIslands;
+	uint32_t serialIslands;
+	uint32_t freeIslands;
+	uint32_t solveErrors;
+	uint32_t pad[5];
+};
+
+// Host -> device body update record (one per body touched by the API
+// between two steps).
+enum UploadMask : uint32_t
+{
+	kUpAll = 1u << 0,       // freshly created body: every field
+	kUpPose = 1u << 1,      // position + rotation
+	kUpVel = 1u << 2,       // linear + angular velocity
+	kUpIW = 1u << 3,        // world inverse inertia
+	kUpForce = 1u << 4,     // force + torque
+	kUpState = 1u << 5,     // inUse / awake / enableSleep / sensor + sleep timers
+	kUpCold = 1u << 6,      // materials (also refreshes live contacts)
+	kUpFatReset = 1u << 7,  // fat AABB invalid (teleport / recycled slot)
+};
+
+struct BodyUpload
+{
+	int32_t index;
+	uint32_t mask;
+	float4 pos, rot, vel, angVel;
+	float4 massInv;
+	float4 iw0, iw1, iw2;
+	float4 force, torque;
+	float2 sleep;
+	uint32_t state;
+	BodyCold cold;
+};
+
+// Island table entry.  Ranges index the label-sorted body / contact / joint
+// lists of the step.
+struct IslandRec
+{
+	int32_t bodyStart, bodyCount;
+	int32_t contactStart, contactCount;
+	int32_t jointStart, jointCount;
+	int32_t label;
+	int32_t kind; // 0 free bodies, 1 serial Gauss-Seidel, 2 graph coloured
+};
+
+struct DevWorld
+{
+	cudaStream_t stream = nullptr;
+	PrimScratch prim;
+
+	BodySoA B = {};
+	ContactSoA C = {};
+	int32_t bodyCap = 0;
+	int32_t contactCap = 0;
+	int32_t contactCount = 0;
+
+	// joints (mirror of the host table) and the sorted jointed-pair keys
+	DevBuf joints;
+	int32_t jointCount = 0;
+	DevBuf jointedPairs;
+	int32_t jointedCount = 0;
+
+	// per-body step scratch
+	DevBuf inActiveCells, inStableCells; // u8
+	DevBuf cellCountA, cellCountS;       // u32
+	DevBuf overFlagA, overFlagS;         // u32
+	DevBuf label;                        // i32 union-find parent / island label
+	DevBuf islandFlag;                   // u32 per label: awake
+	DevBuf colorMask;                    // u32
+	DevBuf matDirty;                     // u8
+	DevBuf sleepFirstNo, sleepMin;       // per label
+	DevBuf bodyKeys, bodyVals;           // label-sorted island bodies
+
+	// grid (active tier rebuilt every step, stable tier on demand)
+	DevBuf activeKeys, activeVals, stableKeys, stableVals;
+	DevBuf activeOver, stableOver;
+	int64_t activeEntries = 0, stableEntries = 0;
+	int32_t activeOverCount = 0, stableOverCount = 0;
+	DevBuf runStarts, runFlag;
+	int32_t runCount = 0;
+
+	// pair build
+	DevBuf runPairCount;          // u32 per run
+	DevBuf pairKeys;              // u64 admitted candidates in emission order
+	DevBuf overFlag, overScan;    // oversized candidate flags
+	DevBuf existingSet;           // hash set of existing contact keys
+	uint32_t existingMask = 0;
+	DevBuf newSet, newSetPos;     // first-occurrence dedupe
+	uint32_t newMask = 0;
+	DevBuf keepFlag;              // u32 per admitted candidate
+	DevBuf newContactKeys;
+
+	// removal / narrowphase / events
+	DevBuf removeFlag, removeScan; // u32 per contact
+	DevBuf moveSrc;                // i32 per hole rank
+	DevBuf transition;             // i8 per contact
+	DevBuf evBeginFlag, evEndFlag; // u32 per contact
+	DevBuf evBegin, evEnd;         // int4 (bodyA, bodyB, sensor, 0)
+	DevBuf evRemoval;              // int4, descending contact index
+
+	// islands
+	DevBuf contactKeys, contactVals; // label-sorted island contacts
+	DevBuf jointKeys, jointVals;
+	DevBuf islandStartFlag, islands; // IslandRec
+	DevBuf islandKinds;
+	int32_t islandCount = 0;
+	int32_t islandsBuiltFor = 0; // body count of the last island build (0: never)
+	DevBuf colorOf;      // per island-contact position: colour 0..8
+	DevBuf colorOrder;   // island contacts regrouped by colour
+	DevBuf colorStart;   // per island: 10 offsets into colorOrder
+	DevBuf packetMax;    // per colorOrder position: max points of its packet
+	DevBuf contactColor; // per contact: colour for introspection
+
+	DevBuf uploads;      // BodyUpload staging (device)
+	DevBuf counters;     // StepCounters
+	StepCounters* hostCounters = nullptr; // pinned
+
+	DevBuf queryOut;     // query results
+};
+
+// ---- launchers (defined in k_*.cu) -----------------------------------------
+
+bool growBodies(DevWorld& w, int32_t capacity);
+bool growContacts(DevWorld& w, int32_t capacity);
+void readCounters(DevWorld& w); // stream sync + D2H of StepCounters
+StepCounters* devCounters(DevWorld& w);
+
+void launchApplyUploads(DevWorld& w, const BodyUpload* hostRecs, int32_t count);
+void launchMaterialRefresh(DevWorld& w);
+
+// broadphase (k_broadphase.cu)
+void launchRefresh(DevWorld& w, int32_t n, float dt, bool rebuildStable, float cellSize);
+void launchBuildActiveGrid(DevWorld& w, int32_t n, float cellSize);
+void launchBuildStableGrid(DevWorld& w, int32_t n, float cellSize);
+void launchFindRuns(DevWorld& w);
+void launchPairs(DevWorld& w, int32_t n, float cellSize);
+void launchCreateContacts(DevWorld& w, int32_t newCount);
+void launchRemoval(DevWorld& w);
+// destroy-time swap-removes computed on the host: move (dst, src) pairs
+void launchContactMoves(DevWorld& w, const int2* hostMoves, int32_t count);
+
+// narrowphase (k_narrow.cu)
+void launchNarrowphase(DevWorld& w, float dt);
+
+// islands, sleep, kinematics (k_islands.cu)
+void launchAnyAwakeDynamic(DevWorld& w, int32_t n);
+void launchIslands(DevWorld& w, int32_t n);
+void launchSleep(DevWorld& w, float dt);
+void launchFinish(DevWorld& w, int32_t n, float dt, bool clearForces);
+
+// solver (k_solve.cu)
+void launchSolve(DevWorld& w, float dt, int substeps, V3 gravity, int positionIterations);
+
+// queries (k_query.cu)
+struct RayQueryOut
+{
+	int32_t body;
+	float fraction;
+	float point[3];
+	float normal[3];
+	int32_t hit;
+};
+void launchRayCast(DevWorld& w, int32_t n, V3 origin, V3 translation, uint32_t maskBits, float cellSize,
+				   RayQueryOut* hostOut);
+void launchSphereCast(DevWorld& w, int32_t n, V3 origin, float radius, V3 translation, uint32_t maskBits,
+					  RayQueryOut* hostOut);
+void launchOverlap(DevWorld& w, int32_t n, Box box, uint8_t* hostFlags);
+
+} // namespace m3g

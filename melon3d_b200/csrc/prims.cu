@@ -1,0 +1,411 @@
+// Exclusive scan, stable LSD radix sort and key-range reduction.
+#include "prims.cuh"
+
+#include <stdio.h>
+
+namespace m3g
+{
+
+bool DevBuf::ensure(size_t need)
+{
+	if (need <= bytes && ptr != nullptr)
+	{
+		return true;
+	}
+	size_t nb = bytes * 2 > need ? bytes * 2 : need;
+	if (nb < 256)
+	{
+		nb = 256;
+	}
+	void* p = nullptr;
+	if (cudaMalloc(&p, nb) != cudaSuccess)
+	{
+		return false;
+	}
+	if (ptr != nullptr)
+	{
+		cudaFree(ptr);
+	}
+	ptr = p;
+	bytes = nb;
+	return true;
+}
+
+bool DevBuf::ensureZeroed(size_t need, cudaStream_t stream)
+{
+	void* before = ptr;
+	if (!ensure(need))
+	{
+		return false;
+	}
+	if (ptr != before)
+	{
+		cudaMemsetAsync(ptr, 0, bytes, stream);
+	}
+	return true;
+}
+
+void DevBuf::release()
+{
+	if (ptr != nullptr)
+	{
+		cudaFree(ptr);
+	}
+	ptr = nullptr;
+	bytes = 0;
+}
+
+void PrimScratch::release()
+{
+	scanA.release();
+	scanB.release();
+	scanC.release();
+	sortKeys.release();
+	sortVals.release();
+	sortCounts.release();
+	reduce.release();
+	if (hostReduce != nullptr)
+	{
+		cudaFreeHost(hostReduce);
+		hostReduce = nullptr;
+	}
+}
+
+// ---------------------------------------------------------------------------
+// scan: 256 threads x 8 items per block; block totals are scanned recursively
+// ---------------------------------------------------------------------------
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ uint32_t warpInclusive(uint32_t v)
+{
+	int lane = threadIdx.x & 31;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1)
+	{
+		uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+		if (lane >= o)
+		{
+			v += t;
+		}
+	}
+	return v;
+}
+
+// exclusive scan of one tile in place; returns the tile total to thread 0..N
+__device__ uint32_t blockExclusive(uint32_t v, uint32_t* warpSums)
+{
+	int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	uint32_t inc = warpInclusive(v);
+	if (lane == 31)
+	{
+		warpSums[warp] = inc;
+	}
+	__syncthreads();
+	if (warp == 0)
+	{
+		uint32_t ws = lane < (kScanThreads / 32) ? warpSums[lane] : 0u;
+		uint32_t wi = warpInclusive(ws);
+		if (lane < (kScanThreads / 32))
+		{
+			warpSums[lane] = wi - ws;
+		}
+		if (lane == (kScanThreads / 32) - 1)
+		{
+			warpSums[kScanThreads / 32] = wi;
+		}
+	}
+	__syncthreads();
+	uint32_t r = inc - v + warpSums[warp];
+	return r;
+}
+
+__global__ void kScanTiles(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* tileSums)
+{
+	__shared__ uint32_t warpSums[kScanThreads / 32 + 1];
+	int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+	uint32_t vals[kScanItems];
+	uint32_t sum = 0;
+#pragma unroll
+	for (int k = 0; k < kScanItems; ++k)
+	{
+		int64_t i = base + k;
+		vals[k] = i < n ? in[i] : 0u;
+		sum += vals[k];
+	}
+	uint32_t pre = blockExclusive(sum, warpSums);
+#pragma unroll
+	for (int k = 0; k < kScanItems; ++k)
+	{
+		int64_t i = base + k;
+		if (i < n)
+		{
+			out[i] = pre;
+		}
+		pre += vals[k];
+	}
+	if (threadIdx.x == 0 && tileSums != nullptr)
+	{
+		tileSums[blockIdx.x] = warpSums[kScanThreads / 32];
+	}
+}
+
+__global__ void kScanAdd(uint32_t* out, int64_t n, const uint32_t* tileOffsets)
+{
+	int64_t base = (int64_t)blockIdx.x * kScanTile;
+	uint32_t add = tileOffsets[blockIdx.x];
+	for (int k = threadIdx.x; k < kScanTile; k += kScanThreads)
+	{
+		int64_t i = base + k;
+		if (i < n)
+		{
+			out[i] += add;
+		}
+	}
+}
+
+__global__ void kScanTotal(const uint32_t* in, const uint32_t* out, int64_t n, uint32_t* total)
+{
+	*total = n > 0 ? out[n - 1] + in[n - 1] : 0u;
+}
+
+// total of a single-tile scan is produced by kScanTiles into tileSums
+static void scanLevel(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total, DevBuf* levels, int level,
+					  cudaStream_t stream)
+{
+	int64_t tiles = (n + kScanTile - 1) / kScanTile;
+	if (tiles <= 1)
+	{
+		kScanTiles<<<1, kScanThreads, 0, stream>>>(in, out, n, total);
+		return;
+	}
+	levels[level].ensure((size_t)tiles * sizeof(uint32_t));
+	uint32_t* sums = levels[level].as<uint32_t>();
+	kScanTiles<<<(unsigned)tiles, kScanThreads, 0, stream>>>(in, out, n, sums);
+	scanLevel(sums, sums, tiles, total, levels, level + 1, stream);
+	kScanAdd<<<(unsigned)tiles, kScanThreads, 0, stream>>>(out, n, sums);
+}
+
+void scanExclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total, PrimScratch& s,
+				   cudaStream_t stream)
+{
+	if (n <= 0)
+	{
+		if (total != nullptr)
+		{
+			cudaMemsetAsync(total, 0, sizeof(uint32_t), stream);
+		}
+		return;
+	}
+	DevBuf levels[3] = {};
+	levels[0] = s.scanA;
+	levels[1] = s.scanB;
+	levels[2] = s.scanC;
+	// the in-place aliasing is fine: each tile reads all its inputs before
+	// writing, and tiles are disjoint
+	if (total == nullptr)
+	{
+		// scan the tile sums without a total: reuse a scratch word
+		levels[2].ensure(sizeof(uint32_t) * 4);
+	}
+	uint32_t* tot = total != nullptr ? total : levels[2].as<uint32_t>();
+	scanLevel(in, out, n, tot, levels, 0, stream);
+	s.scanA = levels[0];
+	s.scanB = levels[1];
+	s.scanC = levels[2];
+}
+
+// ---------------------------------------------------------------------------
+// radix sort: 8-bit digits, 256 threads x 8 items per tile, warp-contiguous
+// item ownership so the tile order equals the input order (stability)
+// ---------------------------------------------------------------------------
+
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 8;
+constexpr int kSortTile = kSortThreads * kSortItems;
+constexpr int kRadix = 256;
+
+__global__ void kSortHistogram(const uint64_t* keys, int64_t n, int shift, uint32_t* counts, int tiles)
+{
+	__shared__ uint32_t hist[kRadix];
+	for (int d = threadIdx.x; d < kRadix; d += kSortThreads)
+	{
+		hist[d] = 0;
+	}
+	__syncthreads();
+	int64_t base = (int64_t)blockIdx.x * kSortTile;
+	for (int k = threadIdx.x; k < kSortTile; k += kSortThreads)
+	{
+		int64_t i = base + k;
+		if (i < n)
+		{
+			atomicAdd(&hist[(uint32_t)(keys[i] >> shift) & 0xFFu], 1u);
+		}
+	}
+	__syncthreads();
+	for (int d = threadIdx.x; d < kRadix; d += kSortThreads)
+	{
+		counts[(int64_t)d * tiles + blockIdx.x] = hist[d];
+	}
+}
+
+__global__ void kSortScatter(const uint64_t* keysIn, const uint32_t* valsIn, uint64_t* keysOut, uint32_t* valsOut,
+							 int64_t n, int shift, const uint32_t* offsets, int tiles)
+{
+	__shared__ uint32_t warpHist[kSortWarps][kRadix];
+	int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	for (int d = threadIdx.x; d < kSortWarps * kRadix; d += kSortThreads)
+	{
+		(&warpHist[0][0])[d] = 0;
+	}
+	__syncthreads();
+	int64_t base = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * (32 * kSortItems);
+	uint32_t lt = (1u << lane) - 1u;
+
+	// pass 1: per-warp digit counts
+	for (int r = 0; r < kSortItems; ++r)
+	{
+		int64_t i = base + r * 32 + lane;
+		bool valid = i < n;
+		uint32_t d = valid ? ((uint32_t)(keysIn[i] >> shift) & 0xFFu) : 0x100u;
+		uint32_t peers = __match_any_sync(0xffffffffu, d);
+		if (valid && (peers & lt) == 0)
+		{
+			warpHist[warp][d] += __popc(peers);
+		}
+		__syncwarp();
+	}
+	__syncthreads();
+	// exclusive prefix over warps, plus the tile's global digit base
+	for (int d = threadIdx.x; d < kRadix; d += kSortThreads)
+	{
+		uint32_t run = offsets[(int64_t)d * tiles + blockIdx.x];
+		for (int w = 0; w < kSortWarps; ++w)
+		{
+			uint32_t c = warpHist[w][d];
+			warpHist[w][d] = run;
+			run += c;
+		}
+	}
+	__syncthreads();
+	// pass 2: stable ranks and scatter
+	for (int r = 0; r < kSortItems; ++r)
+	{
+		int64_t i = base + r * 32 + lane;
+		bool valid = i < n;
+		uint64_t key = valid ? keysIn[i] : 0ull;
+		uint32_t d = valid ? ((uint32_t)(key >> shift) & 0xFFu) : 0x100u;
+		uint32_t peers = __match_any_sync(0xffffffffu, d);
+		if (valid)
+		{
+			uint32_t pos = warpHist[warp][d] + __popc(peers & lt);
+			keysOut[pos] = key;
+			valsOut[pos] = valsIn[i];
+		}
+		__syncwarp();
+		if (valid && (peers & lt) == 0)
+		{
+			warpHist[warp][d] += __popc(peers);
+		}
+		__syncwarp();
+	}
+}
+
+__global__ void kCopyPairs(const uint64_t* ks, const uint32_t* vs, uint64_t* kd, uint32_t* vd, int64_t n)
+{
+	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n)
+	{
+		kd[i] = ks[i];
+		vd[i] = vs[i];
+	}
+}
+
+void radixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, uint64_t varyMask, PrimScratch& s,
+					cudaStream_t stream)
+{
+	if (n <= 1)
+	{
+		return;
+	}
+	int tiles = (int)((n + kSortTile - 1) / kSortTile);
+	s.sortKeys.ensure((size_t)n * sizeof(uint64_t));
+	s.sortVals.ensure((size_t)n * sizeof(uint32_t));
+	s.sortCounts.ensure((size_t)kRadix * tiles * sizeof(uint32_t));
+	uint64_t* k0 = keys;
+	uint32_t* v0 = vals;
+	uint64_t* k1 = s.sortKeys.as<uint64_t>();
+	uint32_t* v1 = s.sortVals.as<uint32_t>();
+	uint32_t* counts = s.sortCounts.as<uint32_t>();
+	int passes = 0;
+	for (int shift = 0; shift < 64; shift += 8)
+	{
+		if (((varyMask >> shift) & 0xFFull) == 0)
+		{
+			continue;
+		}
+		kSortHistogram<<<tiles, kSortThreads, 0, stream>>>(k0, n, shift, counts, tiles);
+		scanExclusive(counts, counts, (int64_t)kRadix * tiles, nullptr, s, stream);
+		kSortScatter<<<tiles, kSortThreads, 0, stream>>>(k0, v0, k1, v1, n, shift, counts, tiles);
+		uint64_t* tk = k0;
+		k0 = k1;
+		k1 = tk;
+		uint32_t* tv = v0;
+		v0 = v1;
+		v1 = tv;
+		++passes;
+	}
+	if (passes & 1)
+	{
+		kCopyPairs<<<blocksFor(n, 256), 256, 0, stream>>>(k0, v0, keys, vals, n);
+	}
+}
+
+__global__ void kReduceInit(uint64_t* r)
+{
+	r[0] = 0ull;
+	r[1] = ~0ull;
+}
+
+__global__ void kReduceKeys(const uint64_t* keys, int64_t n, uint64_t* r)
+{
+	uint64_t o = 0ull, a = ~0ull;
+	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+	{
+		uint64_t k = keys[i];
+		o |= k;
+		a &= k;
+	}
+	for (int off = 16; off > 0; off >>= 1)
+	{
+		o |= __shfl_xor_sync(0xffffffffu, o, off);
+		a &= __shfl_xor_sync(0xffffffffu, a, off);
+	}
+	if ((threadIdx.x & 31) == 0)
+	{
+		atomicOr((unsigned long long*)&r[0], (unsigned long long)o);
+		atomicAnd((unsigned long long*)&r[1], (unsigned long long)a);
+	}
+}
+
+void reduceKeyRange(const uint64_t* keys, int64_t n, PrimScratch& s, cudaStream_t stream)
+{
+	s.reduce.ensure(2 * sizeof(uint64_t));
+	if (s.hostReduce == nullptr)
+	{
+		cudaMallocHost((void**)&s.hostReduce, 2 * sizeof(uint64_t));
+	}
+	kReduceInit<<<1, 1, 0, stream>>>(s.reduce.as<uint64_t>());
+	if (n > 0)
+	{
+		int blocks = blocksFor(n, 256);
+		blocks = blocks > 1184 ? 1184 : blocks;
+		kReduceKeys<<<blocks, 256, 0, stream>>>(keys, n, s.reduce.as<uint64_t>());
+	}
+	cudaMemcpyAsync(s.hostReduce, s.reduce.ptr, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream);
+}
+
+} // namespace m3g

@@ -1,0 +1,112 @@
+// Data-parallel building blocks used by the step: exclusive scan, stable
+// LSD radix sort of (u64 key, u32 value) pairs, key-range reduction and an
+// open-addressing set of 64-bit pair keys.  All hand-written for sm_100a;
+// no library sort or scan is used on the stepping path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace m3g
+{
+
+// Grow-only device buffer.
+struct DevBuf
+{
+	void* ptr = nullptr;
+	size_t bytes = 0;
+	bool ensure(size_t need);
+	// like ensure(), but a fresh allocation is zero-filled on `stream`
+	bool ensureZeroed(size_t need, cudaStream_t stream);
+	void release();
+	template <typename T>
+	T* as() const
+	{
+		return (T*)ptr;
+	}
+};
+
+// Scratch owned by the caller of the primitives.
+struct PrimScratch
+{
+	DevBuf scanA, scanB, scanC;   // block sums for up to three scan levels
+	DevBuf sortKeys, sortVals;   // ping-pong partner of a radix sort
+	DevBuf sortCounts;           // per-tile digit histograms
+	DevBuf reduce;               // 2 x u64: OR and AND of the keys
+	DevBuf hostPinned;           // not device memory: see hostReduce
+	uint64_t* hostReduce = nullptr; // pinned host copy of the reduce words
+	void release();
+};
+
+// out[i] = sum(in[0..i)) for i < n; *total = sum(in[0..n)) when total != null.
+// in and out may alias.
+void scanExclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total, PrimScratch& s,
+				   cudaStream_t stream);
+
+// Stable sort of n (key, val) pairs by key.  Only the key bits in `varyMask`
+// are examined: 8-bit digits whose bits are all outside the mask are skipped
+// (the caller passes keyOr ^ keyAnd from reduceKeyRange, or ~0ull).
+// Result lands back in keys/vals.
+void radixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, uint64_t varyMask, PrimScratch& s,
+					cudaStream_t stream);
+
+// Device-side OR / AND of n keys into s.reduce (two u64 words), then copied
+// to the pinned host words s.hostReduce[0..1] (stream-ordered, no sync).
+void reduceKeyRange(const uint64_t* keys, int64_t n, PrimScratch& s, cudaStream_t stream);
+
+// Keys of an open-addressing hash set: 0xFFFF...F marks an empty slot.
+constexpr uint64_t kEmptyKey = ~0ull;
+
+__device__ __forceinline__ uint32_t hashKey(uint64_t k)
+{
+	k ^= k >> 33;
+	k *= 0xff51afd7ed558ccdull;
+	k ^= k >> 33;
+	k *= 0xc4ceb9fe1a85ec53ull;
+	k ^= k >> 33;
+	return (uint32_t)k;
+}
+
+// insert; returns the slot index holding the key (capacity is a power of two)
+__device__ __forceinline__ uint32_t hashInsert(uint64_t* table, uint32_t capMask, uint64_t key)
+{
+	uint32_t slot = hashKey(key) & capMask;
+	for (uint32_t probe = 0; probe <= capMask; ++probe)
+	{
+		unsigned long long prev = atomicCAS((unsigned long long*)&table[slot], (unsigned long long)kEmptyKey,
+											(unsigned long long)key);
+		if (prev == kEmptyKey || prev == key)
+		{
+			return slot;
+		}
+		slot = (slot + 1) & capMask;
+	}
+	return 0xFFFFFFFFu; // full (the caller sizes the table to at least 2x the keys)
+}
+
+__device__ __forceinline__ bool hashContains(const uint64_t* table, uint32_t capMask, uint64_t key)
+{
+	uint32_t slot = hashKey(key) & capMask;
+	for (uint32_t probe = 0; probe <= capMask; ++probe)
+	{
+		uint64_t k = table[slot];
+		if (k == key)
+		{
+			return true;
+		}
+		if (k == kEmptyKey)
+		{
+			return false;
+		}
+		slot = (slot + 1) & capMask;
+	}
+	return false;
+}
+
+inline int blocksFor(int64_t n, int threads)
+{
+	int64_t b = (n + threads - 1) / threads;
+	return (int)(b < 1 ? 1 : b);
+}
+
+} // namespace m3g

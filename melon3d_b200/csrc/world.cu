@@ -1,0 +1,1660 @@
+// Host side of the GPU world: the C API of include/melon3d.h.
+//
+// The world's state lives in HBM (DevWorld).  The host keeps
+//  - the slot allocator (free lists + generations), joint table and the
+//    per-body records the API reads and writes (a mirror of the device
+//    state, refreshed lazily by one bulk copy after a step);
+//  - the list of bodies changed through the API since the last step, which
+//    is uploaded at the start of the next step;
+//  - the contacts' (bodyA, bodyB, flags) sidecar, downloaded only when a body
+//    is destroyed, so destroy-time contact removal and end events follow the
+//    reference exactly.
+// m3d_world_step drives the device stages in the reference's order
+// (src/world.cpp:1437-2167) and returns once the step's events and counters
+// are on the host.
+#include "m3d_collide.cuh"
+#include "m3d_dev.cuh"
+#include "melon3d.h"
+#include "melon3d_debug.h"
+#include "melon3d_gpu.h"
+
+#include <chrono>
+#include <stdio.h>
+#include <string.h>
+#include <algorithm>
+#include <vector>
+
+using namespace m3g;
+
+namespace
+{
+
+using Clock = std::chrono::steady_clock;
+
+float toMs(Clock::time_point a, Clock::time_point b) { return std::chrono::duration<float, std::milli>(b - a).count(); }
+
+struct HostBody
+{
+	m3d_vec3 position;
+	m3d_quat rotation;
+	m3d_vec3 linearVelocity;
+	m3d_vec3 angularVelocity;
+	float invMass;
+	m3d_vec3 invInertiaLocal;
+	m3d_mat3 invInertiaWorld;
+	float mass;
+	m3d_vec3 force;
+	m3d_vec3 torque;
+	float sleepTime;
+	float smoothedEnergy;
+	bool enableSleep;
+	bool isAwake;
+	bool inUse;
+	bool isSensor;
+	uint32_t generation;
+	uint64_t userData;
+	BodyCold cold;
+};
+
+} // namespace
+
+struct m3d_world
+{
+	m3d_world_def def;
+	DevWorld dev;
+
+	std::vector<HostBody> bodies;
+	std::vector<int32_t> freeBodies;
+	std::vector<JointRec> joints;
+	std::vector<int32_t> freeJoints;
+	bool jointsDirty = true;
+	std::vector<uint64_t> jointedPairs;
+	bool jointedPairsDirty = true;
+
+	std::vector<uint32_t> dirtyMask;
+	std::vector<int32_t> dirtyList;
+	bool anyMaterialChange = false;
+
+	bool gridDirty = true;
+	bool stableDirty = true;
+	bool stableForce = false;
+	int32_t stepsSinceStableBuild = 1000;
+	bool anyForcesApplied = false;
+	bool mirrorStale = false;
+
+	// contact sidecar (valid between a step and the next flush)
+	bool contactMirrorValid = false;
+	std::vector<int2> cBodies;
+	std::vector<uint8_t> cFlags;
+	std::vector<int32_t> cPerm; // original device index of each host-side slot
+	bool contactsEdited = false;
+
+	std::vector<m3d_contact_event> beginEvents;
+	std::vector<m3d_contact_event> endEvents;
+	m3d_profile profile;
+
+	cudaEvent_t evStart = nullptr, evStop = nullptr;
+	float lastDeviceMs = 0.0f;
+	int32_t status = M3D_GPU_OK;
+	char errorText[256] = { 0 };
+
+	// pinned staging
+	std::vector<BodyUpload> uploadRecs;
+	float4* pinPos = nullptr;
+	float4* pinRot = nullptr;
+	float4* pinVel = nullptr;
+	float4* pinAng = nullptr;
+	uint8_t* pinState = nullptr;
+	float2* pinSleep = nullptr;
+	int32_t pinCap = 0;
+};
+
+namespace
+{
+
+void setError(m3d_world* w, int32_t code, const char* what)
+{
+	if (w->status == M3D_GPU_OK)
+	{
+		w->status = code;
+		snprintf(w->errorText, sizeof(w->errorText), "%s", what);
+		fprintf(stderr, "melon3d_gpu: %s\n", what);
+	}
+}
+
+void checkCuda(m3d_world* w, const char* where)
+{
+	cudaError_t e = cudaGetLastError();
+	if (e != cudaSuccess)
+	{
+		char buf[256];
+		snprintf(buf, sizeof(buf), "%s: %s", where, cudaGetErrorString(e));
+		setError(w, M3D_GPU_ERR_CUDA, buf);
+	}
+}
+
+HostBody* getBody(m3d_world* w, m3d_body_id id)
+{
+	if (id.index < 0 || id.index >= (int32_t)w->bodies.size())
+	{
+		return nullptr;
+	}
+	HostBody& b = w->bodies[id.index];
+	if (!b.inUse || b.generation != id.generation)
+	{
+		return nullptr;
+	}
+	return &b;
+}
+
+m3d_body_id makeId(m3d_world* w, int32_t index) { return { index, w->bodies[index].generation }; }
+
+void markDirty(m3d_world* w, int32_t index, uint32_t mask)
+{
+	if ((int32_t)w->dirtyMask.size() < (int32_t)w->bodies.size())
+	{
+		w->dirtyMask.resize(w->bodies.size(), 0);
+	}
+	if (w->dirtyMask[index] == 0)
+	{
+		w->dirtyList.push_back(index);
+	}
+	w->dirtyMask[index] |= mask;
+}
+
+uint32_t stateBits(const HostBody& b)
+{
+	return (b.inUse ? kStInUse : 0) | (b.isAwake ? kStAwake : 0) | (b.enableSleep ? kStEnableSleep : 0) |
+		   (b.isSensor ? kStSensor : 0);
+}
+
+void ensurePinned(m3d_world* w, int32_t n)
+{
+	if (n <= w->pinCap)
+	{
+		return;
+	}
+	int32_t cap = w->pinCap * 2 > n ? w->pinCap * 2 : n;
+	cap = cap < 1024 ? 1024 : cap;
+	cudaFreeHost(w->pinPos);
+	cudaFreeHost(w->pinRot);
+	cudaFreeHost(w->pinVel);
+	cudaFreeHost(w->pinAng);
+	cudaFreeHost(w->pinState);
+	cudaFreeHost(w->pinSleep);
+	cudaMallocHost((void**)&w->pinPos, sizeof(float4) * cap);
+	cudaMallocHost((void**)&w->pinRot, sizeof(float4) * cap);
+	cudaMallocHost((void**)&w->pinVel, sizeof(float4) * cap);
+	cudaMallocHost((void**)&w->pinAng, sizeof(float4) * cap);
+	cudaMallocHost((void**)&w->pinState, sizeof(uint8_t) * cap);
+	cudaMallocHost((void**)&w->pinSleep, sizeof(float2) * cap);
+	w->pinCap = cap;
+}
+
+// Refresh the host mirror from the device after a step (one bulk copy).
+void syncMirror(m3d_world* w)
+{
+	if (!w->mirrorStale)
+	{
+		return;
+	}
+	int32_t n = (int32_t)w->bodies.size();
+	if (n > 0)
+	{
+		ensurePinned(w, n);
+		DevWorld& d = w->dev;
+		cudaStream_t s = d.stream;
+		cudaMemcpyAsync(w->pinPos, d.B.pos, sizeof(float4) * n, cudaMemcpyDeviceToHost, s);
+		cudaMemcpyAsync(w->pinRot, d.B.rot, sizeof(float4) * n, cudaMemcpyDeviceToHost, s);
+		cudaMemcpyAsync(w->pinVel, d.B.vel, sizeof(float4) * n, cudaMemcpyDeviceToHost, s);
+		cudaMemcpyAsync(w->pinAng, d.B.angVel, sizeof(float4) * n, cudaMemcpyDeviceToHost, s);
+		cudaMemcpyAsync(w->pinState, d.B.state, sizeof(uint8_t) * n, cudaMemcpyDeviceToHost, s);
+		cudaMemcpyAsync(w->pinSleep, d.B.sleep, sizeof(float2) * n, cudaMemcpyDeviceToHost, s);
+		cudaStreamSynchronize(s);
+		checkCuda(w, "mirror download");
+		bool anyDirty = !w->dirtyList.empty();
+		for (int32_t i = 0; i < n; ++i)
+		{
+			HostBody& b = w->bodies[i];
+			// a body created since the step has no device state yet
+			if (!b.inUse || (anyDirty && i < (int32_t)w->dirtyMask.size() && (w->dirtyMask[i] & kUpAll)))
+			{
+				continue;
+			}
+			b.position = m3d_v3(w->pinPos[i].x, w->pinPos[i].y, w->pinPos[i].z);
+			b.rotation = { w->pinRot[i].x, w->pinRot[i].y, w->pinRot[i].z, w->pinRot[i].w };
+			b.linearVelocity = m3d_v3(w->pinVel[i].x, w->pinVel[i].y, w->pinVel[i].z);
+			b.angularVelocity = m3d_v3(w->pinAng[i].x, w->pinAng[i].y, w->pinAng[i].z);
+			b.isAwake = (w->pinState[i] & kStAwake) != 0;
+			b.sleepTime = w->pinSleep[i].x;
+			b.smoothedEnergy = w->pinSleep[i].y;
+		}
+	}
+	w->mirrorStale = false;
+}
+
+void ensureContactMirror(m3d_world* w)
+{
+	if (w->contactMirrorValid)
+	{
+		return;
+	}
+	DevWorld& d = w->dev;
+	int32_t c = d.contactCount;
+	w->cBodies.resize(c);
+	w->cFlags.resize(c);
+	w->cPerm.resize(c);
+	if (c > 0)
+	{
+		cudaMemcpyAsync(w->cBodies.data(), d.C.bodies, sizeof(int2) * c, cudaMemcpyDeviceToHost, d.stream);
+		cudaMemcpyAsync(w->cFlags.data(), d.C.flags, sizeof(uint8_t) * c, cudaMemcpyDeviceToHost, d.stream);
+		cudaStreamSynchronize(d.stream);
+		checkCuda(w, "contact sidecar download");
+	}
+	for (int32_t i = 0; i < c; ++i)
+	{
+		w->cPerm[i] = i;
+	}
+	w->contactMirrorValid = true;
+	w->contactsEdited = false;
+}
+
+// RemoveContactAt on the host sidecar (reference src/world.cpp:100-119)
+void removeContactAt(m3d_world* w, int32_t i)
+{
+	int32_t last = (int32_t)w->cBodies.size() - 1;
+	if (i != last)
+	{
+		w->cBodies[i] = w->cBodies[last];
+		w->cFlags[i] = w->cFlags[last];
+		w->cPerm[i] = w->cPerm[last];
+	}
+	w->cBodies.pop_back();
+	w->cFlags.pop_back();
+	w->cPerm.pop_back();
+	w->contactsEdited = true;
+}
+
+void wakeBodyHost(m3d_world* w, int32_t index)
+{
+	HostBody& b = w->bodies[index];
+	if (b.cold.type == kStatic)
+	{
+		return;
+	}
+	if (!b.isAwake)
+	{
+		w->stableDirty = true;
+	}
+	b.isAwake = true;
+	b.sleepTime = 0.0f;
+	b.smoothedEnergy = 4.0f * kSleepEnergyThresh;
+	markDirty(w, index, kUpState);
+}
+
+m3d_mat3 toMat(const M3& m)
+{
+	m3d_mat3 r;
+	r.cx = m3d_v3(m.cx.x, m.cx.y, m.cx.z);
+	r.cy = m3d_v3(m.cy.x, m.cy.y, m.cy.z);
+	r.cz = m3d_v3(m.cz.x, m.cz.y, m.cz.z);
+	return r;
+}
+
+void updateInvInertiaWorld(HostBody& b)
+{
+	M3 m = invInertiaWorld(q4(b.rotation.x, b.rotation.y, b.rotation.z, b.rotation.w),
+						   v3(b.invInertiaLocal.x, b.invInertiaLocal.y, b.invInertiaLocal.z));
+	b.invInertiaWorld = toMat(m);
+}
+
+// mass, inverse mass and local inverse inertia (reference src/world.cpp:46-98)
+void computeMassProperties(HostBody& body, const m3d_shape_def* def)
+{
+	float density = def->density > 0.0f ? def->density : 1000.0f;
+	float mass = 0.0f;
+	m3d_vec3 inertia = m3d_v3_zero();
+	switch (def->type)
+	{
+		case M3D_SHAPE_SPHERE:
+		{
+			float r = def->radius;
+			mass = density * (4.0f / 3.0f) * M3D_PI * r * r * r;
+			float i = 0.4f * mass * r * r;
+			inertia = m3d_v3(i, i, i);
+			break;
+		}
+		case M3D_SHAPE_BOX:
+		{
+			m3d_vec3 e = def->halfExtents;
+			mass = density * 8.0f * e.x * e.y * e.z;
+			inertia = m3d_v3(mass / 3.0f * (e.y * e.y + e.z * e.z), mass / 3.0f * (e.x * e.x + e.z * e.z),
+							 mass / 3.0f * (e.x * e.x + e.y * e.y));
+			break;
+		}
+		case M3D_SHAPE_CAPSULE:
+		{
+			float r = def->radius;
+			float h = def->halfHeight;
+			float mc = density * M3D_PI * r * r * (2.0f * h);
+			float ms = density * (4.0f / 3.0f) * M3D_PI * r * r * r;
+			mass = mc + ms;
+			float iy = 0.5f * mc * r * r + 0.4f * ms * r * r;
+			float d = h + 0.375f * r;
+			float ixz = mc * (0.25f * r * r + h * h / 3.0f) + (83.0f / 320.0f) * ms * r * r + ms * d * d;
+			inertia = m3d_v3(ixz, iy, ixz);
+			break;
+		}
+	}
+	body.mass = mass;
+	if (body.cold.type == kDynamic && mass > 0.0f)
+	{
+		body.invMass = 1.0f / mass;
+		body.invInertiaLocal = m3d_v3(inertia.x > 0.0f ? 1.0f / inertia.x : 0.0f, inertia.y > 0.0f ? 1.0f / inertia.y : 0.0f,
+									  inertia.z > 0.0f ? 1.0f / inertia.z : 0.0f);
+	}
+	else
+	{
+		body.invMass = 0.0f;
+		body.invInertiaLocal = m3d_v3_zero();
+	}
+}
+
+float4 f4(m3d_vec3 v) { return make_float4(v.x, v.y, v.z, 0.0f); }
+float4 f4q(m3d_quat q) { return make_float4(q.x, q.y, q.z, q.w); }
+
+// Upload every body touched through the API, apply destroy-time contact
+// removals, refresh materials, joints and the jointed-pair list.
+void flushHostChanges(m3d_world* w)
+{
+	DevWorld& d = w->dev;
+	int32_t n = (int32_t)w->bodies.size();
+	if (!growBodies(d, n + 1))
+	{
+		setError(w, M3D_GPU_ERR_ALLOC, "body arena growth failed");
+	}
+	if (!w->dirtyList.empty())
+	{
+		w->uploadRecs.resize(w->dirtyList.size());
+		for (size_t k = 0; k < w->dirtyList.size(); ++k)
+		{
+			int32_t i = w->dirtyList[k];
+			const HostBody& b = w->bodies[i];
+			BodyUpload& u = w->uploadRecs[k];
+			memset(&u, 0, sizeof(u));
+			u.index = i;
+			u.mask = w->dirtyMask[i];
+			u.pos = f4(b.position);
+			u.rot = f4q(b.rotation);
+			u.vel = f4(b.linearVelocity);
+			u.angVel = f4(b.angularVelocity);
+			u.massInv = make_float4(b.invMass, b.invInertiaLocal.x, b.invInertiaLocal.y, b.invInertiaLocal.z);
+			u.iw0 = f4(b.invInertiaWorld.cx);
+			u.iw1 = f4(b.invInertiaWorld.cy);
+			u.iw2 = f4(b.invInertiaWorld.cz);
+			u.force = f4(b.force);
+			u.torque = f4(b.torque);
+			u.sleep = make_float2(b.sleepTime, b.smoothedEnergy);
+			u.state = stateBits(b);
+			u.cold = b.cold;
+			w->dirtyMask[i] = 0;
+		}
+		launchApplyUploads(d, w->uploadRecs.data(), (int32_t)w->uploadRecs.size());
+		w->dirtyList.clear();
+	}
+	if (w->contactMirrorValid && w->contactsEdited)
+	{
+		// destroy-time swap-removes: move the survivors the host moved
+		std::vector<int2> moves;
+		for (int32_t k = 0; k < (int32_t)w->cPerm.size(); ++k)
+		{
+			if (w->cPerm[k] != k)
+			{
+				moves.push_back(make_int2(k, w->cPerm[k]));
+			}
+		}
+		launchContactMoves(d, moves.data(), (int32_t)moves.size());
+		d.contactCount = (int32_t)w->cPerm.size();
+		w->contactsEdited = false;
+	}
+	w->contactMirrorValid = false;
+	if (w->anyMaterialChange)
+	{
+		launchMaterialRefresh(d);
+		w->anyMaterialChange = false;
+	}
+	if (w->jointsDirty)
+	{
+		d.jointCount = (int32_t)w->joints.size();
+		if (d.jointCount > 0)
+		{
+			d.joints.ensure(sizeof(JointRec) * w->joints.size());
+			cudaMemcpyAsync(d.joints.ptr, w->joints.data(), sizeof(JointRec) * w->joints.size(), cudaMemcpyHostToDevice,
+							d.stream);
+		}
+		w->jointsDirty = false;
+	}
+	if (w->jointedPairsDirty)
+	{
+		w->jointedPairs.clear();
+		for (const JointRec& j : w->joints)
+		{
+			if (j.inUse)
+			{
+				int32_t lo = j.bodyA < j.bodyB ? j.bodyA : j.bodyB;
+				int32_t hi = j.bodyA < j.bodyB ? j.bodyB : j.bodyA;
+				w->jointedPairs.push_back(((uint64_t)(uint32_t)lo << 32) | (uint32_t)hi);
+			}
+		}
+		std::sort(w->jointedPairs.begin(), w->jointedPairs.end());
+		d.jointedCount = (int32_t)w->jointedPairs.size();
+		if (d.jointedCount > 0)
+		{
+			d.jointedPairs.ensure(sizeof(uint64_t) * w->jointedPairs.size());
+			cudaMemcpyAsync(d.jointedPairs.ptr, w->jointedPairs.data(), sizeof(uint64_t) * w->jointedPairs.size(),
+							cudaMemcpyHostToDevice, d.stream);
+		}
+		w->jointedPairsDirty = false;
+	}
+	checkCuda(w, "flush");
+}
+
+// RefreshBroadphase (reference src/world.cpp:156-229): fat boxes, active tier
+// every call, stable tier when forced or dirty for >= 4 steps.
+void refreshBroadphase(m3d_world* w, float dt)
+{
+	DevWorld& d = w->dev;
+	int32_t n = (int32_t)w->bodies.size();
+	bool rebuildStable = w->stableForce || (w->stableDirty && w->stepsSinceStableBuild >= 4);
+	launchRefresh(d, n, dt, rebuildStable, w->def.gridCellSize);
+	launchBuildActiveGrid(d, n, w->def.gridCellSize);
+	if (rebuildStable)
+	{
+		launchBuildStableGrid(d, n, w->def.gridCellSize);
+		w->stableDirty = false;
+		w->stableForce = false;
+		w->stepsSinceStableBuild = 0;
+	}
+	else
+	{
+		++w->stepsSinceStableBuild;
+	}
+	w->gridDirty = false;
+}
+
+void appendEvents(m3d_world* w, std::vector<m3d_contact_event>& out, const int4* dev, int32_t count)
+{
+	if (count <= 0)
+	{
+		return;
+	}
+	std::vector<int4> tmp((size_t)count);
+	cudaMemcpyAsync(tmp.data(), dev, sizeof(int4) * count, cudaMemcpyDeviceToHost, w->dev.stream);
+	cudaStreamSynchronize(w->dev.stream);
+	for (int32_t k = 0; k < count; ++k)
+	{
+		m3d_contact_event e;
+		e.bodyA = makeId(w, tmp[k].x);
+		e.bodyB = makeId(w, tmp[k].y);
+		e.isSensor = tmp[k].z != 0;
+		out.push_back(e);
+	}
+}
+
+} // namespace
+
+extern "C"
+{
+
+m3d_world_def m3d_world_def_default(void)
+{
+	m3d_world_def def;
+	def.gravity = m3d_v3(0.0f, -9.81f, 0.0f);
+	def.workerCount = 1;
+	def.positionIterations = 2;
+	def.gridCellSize = 1.5f;
+	def.enableSleep = true;
+	return def;
+}
+
+m3d_body_def m3d_body_def_default(void)
+{
+	m3d_body_def def;
+	memset(&def, 0, sizeof(def));
+	def.type = M3D_BODY_STATIC;
+	def.position = m3d_v3_zero();
+	def.orientation = m3d_quat_identity();
+	def.linearVelocity = m3d_v3_zero();
+	def.angularVelocity = m3d_v3_zero();
+	def.linearDamping = 0.0f;
+	def.angularDamping = 0.05f;
+	def.gravityScale = 1.0f;
+	def.enableSleep = true;
+	def.isAwake = true;
+	def.userData = 0;
+	return def;
+}
+
+m3d_shape_def m3d_shape_def_default(void)
+{
+	m3d_shape_def def;
+	memset(&def, 0, sizeof(def));
+	def.type = M3D_SHAPE_SPHERE;
+	def.radius = 0.5f;
+	def.halfHeight = 0.5f;
+	def.halfExtents = m3d_v3(0.5f, 0.5f, 0.5f);
+	def.density = 1000.0f;
+	def.friction = 0.6f;
+	def.restitution = 0.0f;
+	def.rollingResistance = 0.02f;
+	def.filter = m3d_filter_default();
+	def.isSensor = false;
+	return def;
+}
+
+m3d_hinge_joint_def m3d_hinge_joint_def_default(void)
+{
+	m3d_hinge_joint_def def;
+	memset(&def, 0, sizeof(def));
+	def.bodyA = m3d_body_id_null();
+	def.bodyB = m3d_body_id_null();
+	def.localAxisA = m3d_v3(0.0f, 1.0f, 0.0f);
+	return def;
+}
+
+m3d_weld_joint_def m3d_weld_joint_def_default(void)
+{
+	m3d_weld_joint_def def;
+	memset(&def, 0, sizeof(def));
+	def.bodyA = m3d_body_id_null();
+	def.bodyB = m3d_body_id_null();
+	return def;
+}
+
+m3d_world* m3d_world_create(const m3d_world_def* def)
+{
+	int devCount = 0;
+	if (cudaGetDeviceCount(&devCount) != cudaSuccess || devCount <= 0)
+	{
+		fprintf(stderr, "melon3d_gpu: no CUDA device available; the GPU world cannot be created\n");
+		cudaGetLastError();
+		return nullptr;
+	}
+	m3d_world* w = new (std::nothrow) m3d_world();
+	if (w == nullptr)
+	{
+		return nullptr;
+	}
+	w->def = def != nullptr ? *def : m3d_world_def_default();
+	if (w->def.workerCount < 1)
+	{
+		w->def.workerCount = 1;
+	}
+	if (w->def.gridCellSize <= 0.1f)
+	{
+		w->def.gridCellSize = 2.5f;
+	}
+	if (cudaStreamCreateWithFlags(&w->dev.stream, cudaStreamNonBlocking) != cudaSuccess ||
+		cudaEventCreate(&w->evStart) != cudaSuccess || cudaEventCreate(&w->evStop) != cudaSuccess)
+	{
+		fprintf(stderr, "melon3d_gpu: CUDA stream creation failed\n");
+		cudaGetLastError();
+		delete w;
+		return nullptr;
+	}
+	memset(&w->profile, 0, sizeof(w->profile));
+	devCounters(w->dev);
+	if (!growBodies(w->dev, 1024) || !growContacts(w->dev, 4096))
+	{
+		fprintf(stderr, "melon3d_gpu: initial device allocation failed\n");
+		delete w;
+		return nullptr;
+	}
+	return w;
+}
+
+void m3d_world_destroy(m3d_world* world)
+{
+	if (world == nullptr)
+	{
+		return;
+	}
+	DevWorld& d = world->dev;
+	cudaStreamSynchronize(d.stream);
+	BodySoA& B = d.B;
+	void* bp[] = { B.pos, B.rot, B.vel, B.angVel, B.prevPos, B.prevRot, B.prevVel, B.prevAngVel, B.massInv,
+				   B.iw0, B.iw1, B.iw2, B.force, B.torque, B.sleep, B.state, B.cold, B.fatLo, B.fatHi,
+				   B.hasFat, B.moved, B.isActive, B.isStable, B.inStableTier, B.inStableCells, B.bFlags };
+	for (void* p : bp)
+	{
+		cudaFree(p);
+	}
+	ContactSoA& C = d.C;
+	void* cp[] = { C.bodies, C.pointCount, C.flags, C.normal, C.mat, C.cachePosA, C.cacheRotA, C.cachePosB,
+				   C.cacheRotB, C.pAnchorA, C.pAnchorB, C.pFricA, C.pFricB, C.pSlip, C.pRA, C.pRB, C.pJA, C.pJB };
+	for (void* p : cp)
+	{
+		cudaFree(p);
+	}
+	DevBuf* bufs[] = { &d.joints, &d.jointedPairs, &d.inActiveCells, &d.inStableCells, &d.cellCountA, &d.cellCountS,
+					   &d.overFlagA, &d.overFlagS, &d.label, &d.islandFlag, &d.colorMask, &d.matDirty, &d.sleepFirstNo,
+					   &d.sleepMin, &d.bodyKeys, &d.bodyVals, &d.activeKeys, &d.activeVals, &d.stableKeys,
+					   &d.stableVals, &d.activeOver, &d.stableOver, &d.runStarts, &d.runFlag, &d.runPairCount,
+					   &d.pairKeys, &d.overFlag, &d.overScan, &d.existingSet, &d.newSet, &d.newSetPos, &d.keepFlag,
+					   &d.newContactKeys, &d.removeFlag, &d.removeScan, &d.moveSrc, &d.transition, &d.evBeginFlag,
+					   &d.evEndFlag, &d.evBegin, &d.evEnd, &d.evRemoval, &d.contactKeys, &d.contactVals,
+					   &d.jointKeys, &d.jointVals, &d.islandStartFlag, &d.islands, &d.islandKinds, &d.colorOf,
+					   &d.colorOrder, &d.colorStart, &d.packetMax, &d.contactColor, &d.uploads, &d.counters,
+					   &d.queryOut };
+	for (DevBuf* b : bufs)
+	{
+		b->release();
+	}
+	d.prim.release();
+	if (d.hostCounters != nullptr)
+	{
+		cudaFreeHost(d.hostCounters);
+	}
+	cudaFreeHost(world->pinPos);
+	cudaFreeHost(world->pinRot);
+	cudaFreeHost(world->pinVel);
+	cudaFreeHost(world->pinAng);
+	cudaFreeHost(world->pinState);
+	cudaFreeHost(world->pinSleep);
+	cudaEventDestroy(world->evStart);
+	cudaEventDestroy(world->evStop);
+	cudaStreamDestroy(d.stream);
+	delete world;
+}
+
+// ---- bodies ------------------------------------------------------------------
+
+m3d_body_id m3d_body_create(m3d_world* world, const m3d_body_def* bodyDef, const m3d_shape_def* shapeDef)
+{
+	int32_t index;
+	if (!world->freeBodies.empty())
+	{
+		index = world->freeBodies.back();
+		world->freeBodies.pop_back();
+	}
+	else
+	{
+		index = (int32_t)world->bodies.size();
+		world->bodies.emplace_back();
+		memset(&world->bodies[index], 0, sizeof(HostBody));
+		world->bodies[index].generation = 1;
+	}
+	HostBody& b = world->bodies[index];
+	uint32_t gen = b.generation;
+	memset(&b, 0, sizeof(HostBody));
+	b.generation = gen;
+	b.inUse = true;
+	b.cold.type = (int32_t)bodyDef->type;
+	b.position = bodyDef->position;
+	b.rotation = m3d_quat_normalize(bodyDef->orientation);
+	b.linearVelocity = bodyDef->linearVelocity;
+	b.angularVelocity = bodyDef->angularVelocity;
+	b.cold.linearDamping = bodyDef->linearDamping;
+	b.cold.angularDamping = bodyDef->angularDamping;
+	b.cold.gravityScale = bodyDef->gravityScale;
+	b.enableSleep = bodyDef->enableSleep && world->def.enableSleep;
+	b.isAwake = bodyDef->type == M3D_BODY_STATIC ? false : bodyDef->isAwake;
+	b.sleepTime = 0.0f;
+	b.smoothedEnergy = 4.0f * kSleepEnergyThresh;
+	b.userData = bodyDef->userData;
+	b.cold.shape.type = (int32_t)shapeDef->type;
+	b.cold.shape.radius = shapeDef->radius;
+	b.cold.shape.halfHeight = shapeDef->halfHeight;
+	b.cold.shape.he = v3(shapeDef->halfExtents.x, shapeDef->halfExtents.y, shapeDef->halfExtents.z);
+	b.cold.friction = shapeDef->friction;
+	b.cold.restitution = shapeDef->restitution;
+	b.cold.rollingResistance = shapeDef->rollingResistance;
+	b.cold.categoryBits = shapeDef->filter.categoryBits;
+	b.cold.maskBits = shapeDef->filter.maskBits;
+	b.cold.groupIndex = shapeDef->filter.groupIndex;
+	b.isSensor = shapeDef->isSensor;
+	computeMassProperties(b, shapeDef);
+	updateInvInertiaWorld(b);
+	markDirty(world, index, kUpAll);
+	world->gridDirty = true;
+	world->stableDirty = true;
+	return makeId(world, index);
+}
+
+void m3d_body_destroy(m3d_world* world, m3d_body_id id)
+{
+	syncMirror(world);
+	HostBody* b = getBody(world, id);
+	if (b == nullptr)
+	{
+		return;
+	}
+	int32_t index = id.index;
+	ensureContactMirror(world);
+	for (int32_t i = (int32_t)world->cBodies.size() - 1; i >= 0; --i)
+	{
+		int2 ab = world->cBodies[i];
+		if (ab.x == index || ab.y == index)
+		{
+			int32_t other = ab.x == index ? ab.y : ab.x;
+			uint8_t fl = world->cFlags[i];
+			if (fl & kCFTouching)
+			{
+				if (!(fl & kCFSensor))
+				{
+					wakeBodyHost(world, other);
+				}
+				m3d_contact_event e;
+				e.bodyA = makeId(world, ab.x);
+				e.bodyB = makeId(world, ab.y);
+				e.isSensor = (fl & kCFSensor) != 0;
+				world->endEvents.push_back(e);
+			}
+			removeContactAt(world, i);
+		}
+	}
+	for (int32_t i = 0; i < (int32_t)world->joints.size(); ++i)
+	{
+		JointRec& j = world->joints[i];
+		if (j.inUse && (j.bodyA == index || j.bodyB == index))
+		{
+			wakeBodyHost(world, j.bodyA == index ? j.bodyB : j.bodyA);
+			j.inUse = 0;
+			j.generation++;
+			world->freeJoints.push_back(i);
+			world->jointedPairsDirty = true;
+			world->jointsDirty = true;
+		}
+	}
+	b->inUse = false;
+	b->generation++;
+	world->freeBodies.push_back(index);
+	markDirty(world, index, kUpState);
+	world->gridDirty = true;
+	world->stableDirty = true;
+	world->stableForce = true;
+}
+
+bool m3d_body_is_valid(m3d_world* world, m3d_body_id id) { return getBody(world, id) != nullptr; }
+
+m3d_vec3 m3d_body_position(m3d_world* world, m3d_body_id id)
+{
+	syncMirror(world);
+	HostBody* b = getBody(world, id);
+	return b != nullptr ? b->position : m3d_v3_zero();
+}
+
+m3d_quat m3d_body_rotation(m3d_world* world, m3d_body_id id)
+{
+	syncMirror(world);
+	HostBody* b = getBody(world, id);
+	return b != nullptr ? b->rotation : m3d_quat_identity();
+}
+
+m3d_transform m3d_body_transform(m3d_world* world, m3d_body_id id)
+{
+	syncMirror(world);
+	HostBody* b = getBody(world, id);
+	if (b == nullptr)
+	{
+		return { m3d_v3_zero(), m3d_quat_identity() };
+	}
+	return { b->position, b->rotation };
+}
+
+void m3d_body_set_transform(m3d_world* world, m3d_body_id id, m3d_vec3 position, m3d_quat rotation)
+{
+	syncMirror(world);
+	HostBody* b = getBody(world, id);
+	if (b == nullptr)
+	{
+		return;
+	}
+	b->position = position;
+	b->rotation = m3d_quat_normalize(rotation);
+	updateInvInertiaWorld(*b);
+	markDirty(world, id.index, kUpPose | kUpIW | kUpFatReset);
+	world->gridDirty = true;
+	world->stableDirty = true;
+	wakeBodyHost(world, id.index);
+}
+
+m3d_vec3 m3d_body_linear_velocity(m3d_world* world, m3d_body_id id)
+{
+	syncMirror(world);
+	HostBody* b = getBody(world, id);
+	return b != nullptr ? b->linearVelocity : m3d_v3_zero();
+}
+
+m3d_vec3 m3d_body_angular_velocity(m3d_world* world, m3d_body_id id)
+{
+	syncMirror(world);
+	HostBody* b = getBody(world, id);
+	return b != nullptr ? b->angularVelocity : m3d_v3_zero();
+}
+
+void m3d_body_set_linear_velocity(m3d_world* world, m3d_body_id id, m3d_vec3 v)
+{
+	syncMirror(world);
+	HostBody* b = getBody(world, id);
+	if (b == nullptr || b->cold.type == kStatic)
+	{
+		return;
+	}
+	b->linearVelocity = v;
+	markDirty(world, id.index, kUpVel);
+	wakeBodyHost(world, id.index);
+}
+
+void m3d_body_set_angular_velocity(m3d_world* world, m3d_body_id id, m3d_vec3 w)
+{
+	syncMirror(world);
+	HostBody* b = getBody(world, id);
+	if (b == nullptr || b->cold.type == kStatic)
+	{
+		return;
+	}
+	b->angularVelocity = w;
+	markDirty(world, id.index, kUpVel);
+	wakeBodyHost(world, id.index);
+}
+
+void m3d_body_apply_impulse(m3d_world* world, m3d_body_id id, m3d_vec3 impulse, m3d_vec3 worldPoint)
+{
+	syncMirror(world);
+	HostBody* b = getBody(world, id);
+	if (b == nullptr || b->cold.type != kDynamic)
+	{
+		return;
+	}
+	updateInvInertiaWorld(*b);
+	b->linearVelocity = m3d_mul_add(b->linearVelocity, b->invMass, impulse);
+	m3d_vec3 r = m3d_sub(worldPoint, b->position);
+	b->angularVelocity = m3d_add(b->angularVelocity, m3d_mat3_mulv(&b->invInertiaWorld, m3d_cross(r, impulse)));
+	markDirty(world, id.index, kUpVel | kUpIW);
+	wakeBodyHost(world, id.index);
+}
+
+float m3d_body_mass(m3d_world* world, m3d_body_id id)
+{
+	HostBody* b = getBody(world, id);
+	return b != nullptr ? b->mass : 0.0f;
+}
+
+bool m3d_body_is_awake(m3d_world* world, m3d_body_id id)
+{
+	syncMirror(world);
+	HostBody* b = getBody(world, id);
+	return b != nullptr && b->isAwake;
+}
+
+void m3d_body_wake(m3d_world* world, m3d_body_id id)
+{
+	syncMirror(world);
+	if (getBody(world, id) != nullptr)
+	{
+		wakeBodyHost(world, id.index);
+	}
+}
+
+uint64_t m3d_body_user_data(m3d_world* world, m3d_body_id id)
+{
+	HostBody* b = getBody(world, id);
+	return b != nullptr ? b->userData : 0;
+}
+
+void m3d_body_set_user_data(m3d_world* world, m3d_body_id id, uint64_t userData)
+{
+	HostBody* b = getBody(world, id);
+	if (b != nullptr)
+	{
+		b->userData = userData;
+	}
+}
+
+m3d_body_type m3d_body_get_type(m3d_world* world, m3d_body_id id)
+{
+	HostBody* b = getBody(world, id);
+	return b != nullptr ? (m3d_body_type)b->cold.type : M3D_BODY_STATIC;
+}
+
+void m3d_body_apply_force(m3d_world* world, m3d_body_id id, m3d_vec3 force)
+{
+	syncMirror(world);
+	HostBody* b = getBody(world, id);
+	if (b == nullptr || b->cold.type != kDynamic)
+	{
+		return;
+	}
+	b->force = m3d_add(b->force, force);
+	world->anyForcesApplied = true;
+	markDirty(world, id.index, kUpForce);
+	wakeBodyHost(world, id.index);
+}
+
+void m3d_body_apply_force_at_point(m3d_world* world, m3d_body_id id, m3d_vec3 force, m3d_vec3 worldPoint)
+{
+	syncMirror(world);
+	HostBody* b = getBody(world, id);
+	if (b == nullptr || b->cold.type != kDynamic)
+	{
+		return;
+	}
+	b->force = m3d_add(b->force, force);
+	m3d_vec3 r = m3d_sub(worldPoint, b->position);
+	b->torque = m3d_add(b->torque, m3d_cross(r, force));
+	world->anyForcesApplied = true;
+	markDirty(world, id.index, kUpForce);
+	wakeBodyHost(world, id.index);
+}
+
+void m3d_body_apply_torque(m3d_world* world, m3d_body_id id, m3d_vec3 torque)
+{
+	syncMirror(world);
+	HostBody* b = getBody(world, id);
+	if (b == nullptr || b->cold.type != kDynamic)
+	{
+		return;
+	}
+	b->torque = m3d_add(b->torque, torque);
+	world->anyForcesApplied = true;
+	markDirty(world, id.index, kUpForce);
+	wakeBodyHost(world, id.index);
+}
+
+void m3d_body_apply_angular_impulse(m3d_world* world, m3d_body_id id, m3d_vec3 impulse)
+{
+	syncMirror(world);
+	HostBody* b = getBody(world, id);
+	if (b == nullptr || b->cold.type != kDynamic)
+	{
+		return;
+	}
+	updateInvInertiaWorld(*b);
+	b->angularVelocity = m3d_add(b->angularVelocity, m3d_mat3_mulv(&b->invInertiaWorld, impulse));
+	markDirty(world, id.index, kUpVel | kUpIW);
+	wakeBodyHost(world, id.index);
+}
+
+float m3d_body_friction(m3d_world* world, m3d_body_id id)
+{
+	HostBody* b = getBody(world, id);
+	return b != nullptr ? b->cold.friction : 0.0f;
+}
+
+void m3d_body_set_friction(m3d_world* world, m3d_body_id id, float friction)
+{
+	HostBody* b = getBody(world, id);
+	if (b == nullptr)
+	{
+		return;
+	}
+	b->cold.friction = friction < 0.0f ? 0.0f : friction;
+	markDirty(world, id.index, kUpCold);
+	world->anyMaterialChange = true;
+}
+
+float m3d_body_restitution(m3d_world* world, m3d_body_id id)
+{
+	HostBody* b = getBody(world, id);
+	return b != nullptr ? b->cold.restitution : 0.0f;
+}
+
+void m3d_body_set_restitution(m3d_world* world, m3d_body_id id, float restitution)
+{
+	HostBody* b = getBody(world, id);
+	if (b == nullptr)
+	{
+		return;
+	}
+	b->cold.restitution = restitution < 0.0f ? 0.0f : restitution;
+	markDirty(world, id.index, kUpCold);
+	world->anyMaterialChange = true;
+}
+
+m3d_vec3 m3d_world_gravity(m3d_world* world) { return world->def.gravity; }
+void m3d_world_set_gravity(m3d_world* world, m3d_vec3 gravity) { world->def.gravity = gravity; }
+
+// ---- joints (reference src/world.cpp:868-1075) ------------------------------
+
+static m3d_joint_id allocateJoint(m3d_world* world, JointRec** out)
+{
+	int32_t index;
+	if (!world->freeJoints.empty())
+	{
+		index = world->freeJoints.back();
+		world->freeJoints.pop_back();
+	}
+	else
+	{
+		index = (int32_t)world->joints.size();
+		world->joints.emplace_back();
+		memset(&world->joints[index], 0, sizeof(JointRec));
+		world->joints[index].generation = 1;
+	}
+	JointRec& j = world->joints[index];
+	uint32_t gen = j.generation;
+	memset(&j, 0, sizeof(JointRec));
+	j.generation = gen;
+	j.inUse = 1;
+	world->jointedPairsDirty = true;
+	world->jointsDirty = true;
+	*out = &j;
+	return { index, gen };
+}
+
+static V3 hv(m3d_vec3 v) { return v3(v.x, v.y, v.z); }
+static m3d_vec3 mv(V3 v) { return m3d_v3(v.x, v.y, v.z); }
+
+m3d_joint_id m3d_joint_create_distance(m3d_world* world, const m3d_distance_joint_def* def)
+{
+	syncMirror(world);
+	HostBody* a = getBody(world, def->bodyA);
+	HostBody* b = getBody(world, def->bodyB);
+	if (a == nullptr || b == nullptr || def->bodyA.index == def->bodyB.index)
+	{
+		return { -1, 0 };
+	}
+	JointRec* j;
+	m3d_joint_id id = allocateJoint(world, &j);
+	j->type = kJointDistance;
+	j->bodyA = def->bodyA.index;
+	j->bodyB = def->bodyB.index;
+	j->localAnchorA = hv(def->localAnchorA);
+	j->localAnchorB = hv(def->localAnchorB);
+	j->hertz = def->hertz;
+	j->dampingRatio = def->dampingRatio;
+	j->lambda = 0.0f;
+	if (def->length > 0.0f)
+	{
+		j->length = def->length;
+	}
+	else
+	{
+		m3d_vec3 pA = m3d_transform_point({ a->position, a->rotation }, def->localAnchorA);
+		m3d_vec3 pB = m3d_transform_point({ b->position, b->rotation }, def->localAnchorB);
+		j->length = m3d_length(m3d_sub(pB, pA));
+	}
+	int32_t ja = j->bodyA, jb = j->bodyB;
+	wakeBodyHost(world, ja);
+	wakeBodyHost(world, jb);
+	return id;
+}
+
+m3d_joint_id m3d_joint_create_ball(m3d_world* world, const m3d_ball_joint_def* def)
+{
+	syncMirror(world);
+	HostBody* a = getBody(world, def->bodyA);
+	HostBody* b = getBody(world, def->bodyB);
+	if (a == nullptr || b == nullptr || def->bodyA.index == def->bodyB.index)
+	{
+		return { -1, 0 };
+	}
+	JointRec* j;
+	m3d_joint_id id = allocateJoint(world, &j);
+	j->type = kJointBall;
+	j->bodyA = def->bodyA.index;
+	j->bodyB = def->bodyB.index;
+	j->localAnchorA = hv(def->localAnchorA);
+	j->localAnchorB = hv(def->localAnchorB);
+	j->lambda = 0.0f;
+	int32_t ja = j->bodyA, jb = j->bodyB;
+	wakeBodyHost(world, ja);
+	wakeBodyHost(world, jb);
+	return id;
+}
+
+m3d_joint_id m3d_joint_create_hinge(m3d_world* world, const m3d_hinge_joint_def* def)
+{
+	syncMirror(world);
+	HostBody* a = getBody(world, def->bodyA);
+	HostBody* b = getBody(world, def->bodyB);
+	if (a == nullptr || b == nullptr || def->bodyA.index == def->bodyB.index)
+	{
+		return { -1, 0 };
+	}
+	JointRec* j;
+	m3d_joint_id id = allocateJoint(world, &j);
+	j->type = kJointHinge;
+	j->bodyA = def->bodyA.index;
+	j->bodyB = def->bodyB.index;
+	j->localAnchorA = hv(def->localAnchorA);
+	j->localAnchorB = hv(def->localAnchorB);
+	m3d_vec3 axisA = m3d_normalize(def->localAxisA);
+	if (m3d_length_sq(axisA) < 0.5f)
+	{
+		axisA = m3d_v3(0.0f, 1.0f, 0.0f);
+	}
+	j->localAxisA = hv(axisA);
+	if (m3d_length_sq(def->localAxisB) > 0.5f)
+	{
+		j->localAxisB = hv(m3d_normalize(def->localAxisB));
+	}
+	else
+	{
+		m3d_vec3 axisWorld = m3d_rotate(a->rotation, axisA);
+		j->localAxisB = hv(m3d_inv_rotate(b->rotation, axisWorld));
+	}
+	{
+		m3d_vec3 axisWorld = m3d_rotate(a->rotation, axisA);
+		m3d_vec3 pick = fabsf(axisWorld.x) < 0.9f ? m3d_v3(1.0f, 0.0f, 0.0f) : m3d_v3(0.0f, 1.0f, 0.0f);
+		m3d_vec3 refWorld = m3d_normalize(m3d_cross(axisWorld, pick));
+		j->localRefA = hv(m3d_inv_rotate(a->rotation, refWorld));
+		j->localRefB = hv(m3d_inv_rotate(b->rotation, refWorld));
+	}
+	j->enableLimit = def->enableLimit ? 1 : 0;
+	j->lowerAngle = def->lowerAngle;
+	j->upperAngle = def->upperAngle;
+	j->enableMotor = def->enableMotor ? 1 : 0;
+	j->motorSpeed = def->motorSpeed;
+	j->maxMotorTorque = def->maxMotorTorque;
+	j->lambda = 0.0f;
+	j->motorLambda = 0.0f;
+	int32_t ja = j->bodyA, jb = j->bodyB;
+	wakeBodyHost(world, ja);
+	wakeBodyHost(world, jb);
+	return id;
+}
+
+m3d_joint_id m3d_joint_create_weld(m3d_world* world, const m3d_weld_joint_def* def)
+{
+	syncMirror(world);
+	HostBody* a = getBody(world, def->bodyA);
+	HostBody* b = getBody(world, def->bodyB);
+	if (a == nullptr || b == nullptr || def->bodyA.index == def->bodyB.index)
+	{
+		return { -1, 0 };
+	}
+	JointRec* j;
+	m3d_joint_id id = allocateJoint(world, &j);
+	j->type = kJointWeld;
+	j->bodyA = def->bodyA.index;
+	j->bodyB = def->bodyB.index;
+	j->localAnchorA = hv(def->localAnchorA);
+	j->localAnchorB = hv(def->localAnchorB);
+	m3d_quat rel = m3d_quat_normalize(m3d_quat_mul(m3d_quat_conj(a->rotation), b->rotation));
+	j->relRot0 = q4(rel.x, rel.y, rel.z, rel.w);
+	j->lambda = 0.0f;
+	int32_t ja = j->bodyA, jb = j->bodyB;
+	wakeBodyHost(world, ja);
+	wakeBodyHost(world, jb);
+	return id;
+}
+
+static JointRec* getJoint(m3d_world* world, m3d_joint_id id)
+{
+	if (id.index < 0 || id.index >= (int32_t)world->joints.size())
+	{
+		return nullptr;
+	}
+	JointRec& j = world->joints[id.index];
+	if (!j.inUse || j.generation != id.generation)
+	{
+		return nullptr;
+	}
+	return &j;
+}
+
+float m3d_joint_hinge_angle(m3d_world* world, m3d_joint_id id)
+{
+	syncMirror(world);
+	JointRec* j = getJoint(world, id);
+	if (j == nullptr || j->type != kJointHinge)
+	{
+		return 0.0f;
+	}
+	const HostBody& a = world->bodies[j->bodyA];
+	const HostBody& b = world->bodies[j->bodyB];
+	// HingeAngle (reference src/m3d_internal.h:354-362) on the host copy of the poses
+	m3d_vec3 axis = m3d_rotate(a.rotation, mv(j->localAxisA));
+	m3d_vec3 refA = m3d_rotate(a.rotation, mv(j->localRefA));
+	m3d_vec3 refB = m3d_rotate(b.rotation, mv(j->localRefB));
+	float s = m3d_dot(axis, m3d_cross(refA, refB));
+	float c = m3d_dot(refA, refB);
+	return atan2f(s, c);
+}
+
+void m3d_joint_hinge_set_motor(m3d_world* world, m3d_joint_id id, bool enable, float motorSpeed, float maxMotorTorque)
+{
+	syncMirror(world);
+	JointRec* j = getJoint(world, id);
+	if (j == nullptr || j->type != kJointHinge)
+	{
+		return;
+	}
+	j->enableMotor = enable ? 1 : 0;
+	j->motorSpeed = motorSpeed;
+	j->maxMotorTorque = maxMotorTorque < 0.0f ? 0.0f : maxMotorTorque;
+	world->jointsDirty = true;
+	int32_t ja = j->bodyA, jb = j->bodyB;
+	wakeBodyHost(world, ja);
+	wakeBodyHost(world, jb);
+}
+
+void m3d_joint_destroy(m3d_world* world, m3d_joint_id id)
+{
+	syncMirror(world);
+	JointRec* j = getJoint(world, id);
+	if (j == nullptr)
+	{
+		return;
+	}
+	int32_t ja = j->bodyA, jb = j->bodyB;
+	wakeBodyHost(world, ja);
+	wakeBodyHost(world, jb);
+	j->inUse = 0;
+	j->generation++;
+	world->freeJoints.push_back(id.index);
+	world->jointedPairsDirty = true;
+	world->jointsDirty = true;
+}
+
+// ---- queries -----------------------------------------------------------------
+
+static m3d_ray_result toRayResult(m3d_world* world, const RayQueryOut& q)
+{
+	m3d_ray_result r;
+	r.body = q.hit ? makeId(world, q.body) : m3d_body_id_null();
+	r.point = m3d_v3(q.point[0], q.point[1], q.point[2]);
+	r.normal = m3d_v3(q.normal[0], q.normal[1], q.normal[2]);
+	r.fraction = q.fraction;
+	r.hit = q.hit != 0;
+	return r;
+}
+
+static m3d_ray_result rayCastInternal(m3d_world* world, m3d_vec3 origin, m3d_vec3 translation, uint32_t maskBits)
+{
+	syncMirror(world);
+	flushHostChanges(world);
+	if (world->gridDirty || world->stableDirty)
+	{
+		refreshBroadphase(world, 0.0f);
+	}
+	RayQueryOut q;
+	launchRayCast(world->dev, (int32_t)world->bodies.size(), hv(origin), hv(translation), maskBits,
+				  world->def.gridCellSize, &q);
+	checkCuda(world, "ray cast");
+	return toRayResult(world, q);
+}
+
+m3d_ray_result m3d_world_ray_cast(m3d_world* world, m3d_vec3 origin, m3d_vec3 translation)
+{
+	return rayCastInternal(world, origin, translation, 0xFFFFFFFFu);
+}
+
+m3d_ray_result m3d_world_ray_cast_filtered(m3d_world* world, m3d_vec3 origin, m3d_vec3 translation, uint32_t maskBits)
+{
+	return rayCastInternal(world, origin, translation, maskBits);
+}
+
+m3d_ray_result m3d_world_sphere_cast(m3d_world* world, m3d_vec3 origin, float radius, m3d_vec3 translation,
+									 uint32_t maskBits)
+{
+	syncMirror(world);
+	flushHostChanges(world);
+	RayQueryOut q;
+	launchSphereCast(world->dev, (int32_t)world->bodies.size(), hv(origin), radius, hv(translation), maskBits, &q);
+	checkCuda(world, "sphere cast");
+	return toRayResult(world, q);
+}
+
+void m3d_world_overlap_aabb(m3d_world* world, m3d_aabb aabb, m3d_overlap_fn fn, void* context)
+{
+	if (fn == NULL)
+	{
+		return;
+	}
+	syncMirror(world);
+	flushHostChanges(world);
+	int32_t n = (int32_t)world->bodies.size();
+	std::vector<uint8_t> flags((size_t)n + 1, 0);
+	Box box;
+	box.lo = hv(aabb.lowerBound);
+	box.hi = hv(aabb.upperBound);
+	launchOverlap(world->dev, n, box, flags.data());
+	checkCuda(world, "overlap");
+	for (int32_t i = 0; i < n; ++i)
+	{
+		if (flags[i] && !fn(makeId(world, i), context))
+		{
+			return;
+		}
+	}
+}
+
+m3d_contact_events m3d_world_contact_events(m3d_world* world)
+{
+	m3d_contact_events ev;
+	ev.beginEvents = world->beginEvents.data();
+	ev.beginCount = (int32_t)world->beginEvents.size();
+	ev.endEvents = world->endEvents.data();
+	ev.endCount = (int32_t)world->endEvents.size();
+	return ev;
+}
+
+m3d_profile m3d_world_profile(m3d_world* world) { return world->profile; }
+
+// ---- step ----------------------------------------------------------------------
+
+void m3d_world_step(m3d_world* world, float dt, int substepCount)
+{
+	if (dt <= 0.0f)
+	{
+		return;
+	}
+	if (substepCount < 1)
+	{
+		substepCount = 1;
+	}
+	DevWorld& d = world->dev;
+	auto tStart = Clock::now();
+	cudaEventRecord(world->evStart, d.stream);
+	world->beginEvents.clear();
+	world->endEvents.clear();
+	const int32_t n = (int32_t)world->bodies.size();
+
+	flushHostChanges(world);
+	StepCounters* dc = devCounters(d);
+	cudaMemsetAsync(dc, 0, sizeof(StepCounters), d.stream);
+
+	// broadphase and pair bookkeeping
+	refreshBroadphase(world, dt);
+	launchFindRuns(d);
+	launchPairs(d, n, world->def.gridCellSize);
+	int32_t newContacts = (int32_t)d.hostCounters->newContacts;
+	if (d.hostCounters->hashFail != 0)
+	{
+		setError(world, M3D_GPU_ERR_HASH, "pair hash table overflow");
+	}
+	if (!growContacts(d, d.contactCount + newContacts + 1))
+	{
+		setError(world, M3D_GPU_ERR_ALLOC, "contact arena growth failed");
+		return;
+	}
+	launchCreateContacts(d, newContacts);
+	int32_t preRemoval = d.contactCount;
+	launchRemoval(d);
+	(void)preRemoval;
+	appendEvents(world, world->endEvents, d.evRemoval.as<int4>(), (int32_t)d.hostCounters->endRemoval);
+	checkCuda(world, "broadphase");
+	auto tBroad = Clock::now();
+
+	// narrowphase
+	launchNarrowphase(d, dt);
+	launchAnyAwakeDynamic(d, n);
+	readCounters(d);
+	appendEvents(world, world->beginEvents, d.evBegin.as<int4>(), (int32_t)d.hostCounters->beginNP);
+	appendEvents(world, world->endEvents, d.evEnd.as<int4>(), (int32_t)d.hostCounters->endNP);
+	checkCuda(world, "narrowphase");
+	auto tNarrow = Clock::now();
+
+	int32_t islandCount = 0, touchingCount = 0;
+	if (d.hostCounters->anyAwakeDynamic)
+	{
+		d.contactColor.ensure((size_t)(d.contactCap + 1) * sizeof(int32_t));
+		cudaMemsetAsync(d.contactColor.ptr, 0xFF, (size_t)(d.contactCount + 1) * sizeof(int32_t), d.stream);
+		launchIslands(d, n);
+		islandCount = (int32_t)d.hostCounters->islandCount;
+		touchingCount = (int32_t)d.hostCounters->touchingCount;
+		launchSolve(d, dt, substepCount, hv(world->def.gravity), world->def.positionIterations);
+		launchSleep(d, dt);
+	}
+	launchFinish(d, n, dt, world->anyForcesApplied);
+	cudaEventRecord(world->evStop, d.stream);
+	readCounters(d);
+	checkCuda(world, "solve");
+	if (d.hostCounters->stableDirty)
+	{
+		world->stableDirty = true;
+	}
+	if (world->anyForcesApplied)
+	{
+		for (HostBody& b : world->bodies)
+		{
+			if (b.inUse && b.cold.type == kDynamic)
+			{
+				b.force = m3d_v3_zero();
+				b.torque = m3d_v3_zero();
+			}
+		}
+		world->anyForcesApplied = false;
+	}
+	cudaEventElapsedTime(&world->lastDeviceMs, world->evStart, world->evStop);
+	world->mirrorStale = true;
+	world->contactMirrorValid = false;
+
+	auto tEnd = Clock::now();
+	world->profile.broadphaseMs = toMs(tStart, tBroad);
+	world->profile.narrowphaseMs = toMs(tBroad, tNarrow);
+	world->profile.solverMs = toMs(tNarrow, tEnd);
+	world->profile.stepMs = toMs(tStart, tEnd);
+	world->profile.bodyCount = (int32_t)d.hostCounters->bodyCount;
+	world->profile.awakeBodyCount = (int32_t)d.hostCounters->awakeBodyCount;
+	world->profile.contactCount = d.contactCount;
+	world->profile.touchingContactCount = touchingCount;
+	world->profile.islandCount = islandCount;
+}
+
+// ---- GPU extensions ------------------------------------------------------------
+
+int32_t m3d_gpu_body_capacity(m3d_world* world) { return (int32_t)world->bodies.size(); }
+
+void m3d_gpu_read_poses(m3d_world* world, float* positions, float* rotations, int32_t capacity)
+{
+	flushHostChanges(world);
+	int32_t n = (int32_t)world->bodies.size();
+	n = n < capacity ? n : capacity;
+	if (n <= 0)
+	{
+		return;
+	}
+	ensurePinned(world, n);
+	DevWorld& d = world->dev;
+	cudaMemcpyAsync(world->pinPos, d.B.pos, sizeof(float4) * n, cudaMemcpyDeviceToHost, d.stream);
+	cudaMemcpyAsync(world->pinRot, d.B.rot, sizeof(float4) * n, cudaMemcpyDeviceToHost, d.stream);
+	cudaStreamSynchronize(d.stream);
+	for (int32_t i = 0; i < n; ++i)
+	{
+		if (positions != nullptr)
+		{
+			positions[3 * i + 0] = world->pinPos[i].x;
+			positions[3 * i + 1] = world->pinPos[i].y;
+			positions[3 * i + 2] = world->pinPos[i].z;
+		}
+		if (rotations != nullptr)
+		{
+			rotations[4 * i + 0] = world->pinRot[i].x;
+			rotations[4 * i + 1] = world->pinRot[i].y;
+			rotations[4 * i + 2] = world->pinRot[i].z;
+			rotations[4 * i + 3] = world->pinRot[i].w;
+		}
+	}
+}
+
+float m3d_gpu_last_step_device_ms(m3d_world* world) { return world->lastDeviceMs; }
+int32_t m3d_gpu_status(m3d_world* world) { return world->status; }
+const char* m3d_gpu_last_error_string(m3d_world* world) { return world->errorText; }
+
+// ---- snapshots (include/melon3d_debug.h) ----------------------------------------
+
+int32_t m3d_dbg_body_capacity(m3d_world* world) { return (int32_t)world->bodies.size(); }
+
+void m3d_dbg_bodies(m3d_world* world, m3d_dbg_body* out, int32_t capacity)
+{
+	flushHostChanges(world);
+	int32_t n = (int32_t)world->bodies.size();
+	n = n < capacity ? n : capacity;
+	if (n <= 0)
+	{
+		return;
+	}
+	DevWorld& d = world->dev;
+	std::vector<float4> pos(n), rot(n), vel(n), ang(n), ppos(n), prot(n), i0(n), i1(n), i2(n), flo(n), fhi(n);
+	std::vector<float2> sl(n);
+	std::vector<uint8_t> st(n), hf(n);
+	cudaStream_t s = d.stream;
+	cudaMemcpyAsync(pos.data(), d.B.pos, sizeof(float4) * n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(rot.data(), d.B.rot, sizeof(float4) * n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(vel.data(), d.B.vel, sizeof(float4) * n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(ang.data(), d.B.angVel, sizeof(float4) * n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(ppos.data(), d.B.prevPos, sizeof(float4) * n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(prot.data(), d.B.prevRot, sizeof(float4) * n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(i0.data(), d.B.iw0, sizeof(float4) * n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(i1.data(), d.B.iw1, sizeof(float4) * n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(i2.data(), d.B.iw2, sizeof(float4) * n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(flo.data(), d.B.fatLo, sizeof(float4) * n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(fhi.data(), d.B.fatHi, sizeof(float4) * n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(sl.data(), d.B.sleep, sizeof(float2) * n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(st.data(), d.B.state, n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(hf.data(), d.B.hasFat, n, cudaMemcpyDeviceToHost, s);
+	cudaStreamSynchronize(s);
+	for (int32_t i = 0; i < n; ++i)
+	{
+		m3d_dbg_body& o = out[i];
+		memset(&o, 0, sizeof(o));
+		float4 v4[] = { pos[i], vel[i], ang[i], ppos[i], i0[i], i1[i], i2[i], flo[i], fhi[i] };
+		float* dst3[] = { o.position, o.linearVelocity, o.angularVelocity, o.prevPosition, o.invInertiaWorld,
+						  o.invInertiaWorld + 3, o.invInertiaWorld + 6, o.fatLower, o.fatUpper };
+		for (int k = 0; k < 9; ++k)
+		{
+			dst3[k][0] = v4[k].x;
+			dst3[k][1] = v4[k].y;
+			dst3[k][2] = v4[k].z;
+		}
+		o.rotation[0] = rot[i].x;
+		o.rotation[1] = rot[i].y;
+		o.rotation[2] = rot[i].z;
+		o.rotation[3] = rot[i].w;
+		o.prevRotation[0] = prot[i].x;
+		o.prevRotation[1] = prot[i].y;
+		o.prevRotation[2] = prot[i].z;
+		o.prevRotation[3] = prot[i].w;
+		o.sleepTime = sl[i].x;
+		o.smoothedEnergy = sl[i].y;
+		o.hasFatAABB = hf[i];
+		o.isAwake = (st[i] & kStAwake) ? 1 : 0;
+		o.inUse = (st[i] & kStInUse) ? 1 : 0;
+	}
+}
+
+int32_t m3d_dbg_contact_count(m3d_world* world)
+{
+	flushHostChanges(world);
+	return world->dev.contactCount;
+}
+
+void m3d_dbg_contacts(m3d_world* world, m3d_dbg_contact* out, int32_t capacity)
+{
+	flushHostChanges(world);
+	DevWorld& d = world->dev;
+	int32_t n = d.contactCount < capacity ? d.contactCount : capacity;
+	if (n <= 0)
+	{
+		return;
+	}
+	int32_t cap = d.contactCap;
+	std::vector<int2> bodies(n);
+	std::vector<int32_t> pc(n);
+	std::vector<uint8_t> fl(n);
+	std::vector<float4> nrm(n);
+	std::vector<float2> mat(n);
+	std::vector<float4> pa(4 * (size_t)cap), pb(4 * (size_t)cap), fa(4 * (size_t)cap), fb(4 * (size_t)cap),
+		ps(4 * (size_t)cap);
+	cudaStream_t s = d.stream;
+	cudaMemcpyAsync(bodies.data(), d.C.bodies, sizeof(int2) * n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(pc.data(), d.C.pointCount, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(fl.data(), d.C.flags, n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(nrm.data(), d.C.normal, sizeof(float4) * n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(mat.data(), d.C.mat, sizeof(float2) * n, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(pa.data(), d.C.pAnchorA, sizeof(float4) * 4 * cap, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(pb.data(), d.C.pAnchorB, sizeof(float4) * 4 * cap, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(fa.data(), d.C.pFricA, sizeof(float4) * 4 * cap, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(fb.data(), d.C.pFricB, sizeof(float4) * 4 * cap, cudaMemcpyDeviceToHost, s);
+	cudaMemcpyAsync(ps.data(), d.C.pSlip, sizeof(float4) * 4 * cap, cudaMemcpyDeviceToHost, s);
+	cudaStreamSynchronize(s);
+	for (int32_t c = 0; c < n; ++c)
+	{
+		m3d_dbg_contact& o = out[c];
+		memset(&o, 0, sizeof(o));
+		o.bodyA = bodies[c].x;
+		o.bodyB = bodies[c].y;
+		o.pointCount = pc[c];
+		o.touching = (fl[c] & kCFTouching) ? 1 : 0;
+		o.isSensor = (fl[c] & kCFSensor) ? 1 : 0;
+		o.tunnelGuard = (fl[c] & kCFTunnelGuard) ? 1 : 0;
+		o.hasCache = (fl[c] & kCFHasCache) ? 1 : 0;
+		o.normal[0] = nrm[c].x;
+		o.normal[1] = nrm[c].y;
+		o.normal[2] = nrm[c].z;
+		o.friction = nrm[c].w;
+		o.restitution = mat[c].x;
+		o.rollingResistance = mat[c].y;
+		for (int32_t p = 0; p < pc[c] && p < 4; ++p)
+		{
+			size_t k = (size_t)p * cap + c;
+			m3d_dbg_point& q = o.points[p];
+			q.localAnchorA[0] = pa[k].x;
+			q.localAnchorA[1] = pa[k].y;
+			q.localAnchorA[2] = pa[k].z;
+			q.separation = pa[k].w;
+			q.localAnchorB[0] = pb[k].x;
+			q.localAnchorB[1] = pb[k].y;
+			q.localAnchorB[2] = pb[k].z;
+			memcpy(&q.id, &pb[k].w, sizeof(uint32_t));
+			q.frictionAnchorA[0] = fa[k].x;
+			q.frictionAnchorA[1] = fa[k].y;
+			q.frictionAnchorA[2] = fa[k].z;
+			q.lambdaN = fa[k].w;
+			q.frictionAnchorB[0] = fb[k].x;
+			q.frictionAnchorB[1] = fb[k].y;
+			q.frictionAnchorB[2] = fb[k].z;
+			q.lambdaT = fb[k].w;
+			q.slipDir[0] = ps[k].x;
+			q.slipDir[1] = ps[k].y;
+			q.slipDir[2] = ps[k].z;
+			q.separationOffset = ps[k].w;
+		}
+	}
+}
+
+void m3d_dbg_island_labels(m3d_world* world, int32_t* out, int32_t capacity)
+{
+	DevWorld& d = world->dev;
+	for (int32_t i = 0; i < capacity; ++i)
+	{
+		out[i] = -1;
+	}
+	if (d.label.ptr == nullptr || d.islandsBuiltFor <= 0)
+	{
+		return;
+	}
+	// every dynamic body's label (sleeping islands included) from the last
+	// step that built islands, like the reference's persistent island lists
+	int32_t n = d.islandsBuiltFor;
+	n = n < capacity ? n : capacity;
+	std::vector<int32_t> lab(n);
+	cudaMemcpyAsync(lab.data(), d.label.ptr, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, d.stream);
+	cudaStreamSynchronize(d.stream);
+	for (int32_t i = 0; i < n; ++i)
+	{
+		out[i] = lab[i];
+	}
+}
+
+void m3d_dbg_contact_colors(m3d_world* world, int32_t* out, int32_t capacity)
+{
+	DevWorld& d = world->dev;
+	for (int32_t i = 0; i < capacity; ++i)
+	{
+		out[i] = -1;
+	}
+	int32_t n = d.contactCount < capacity ? d.contactCount : capacity;
+	if (d.contactColor.ptr == nullptr || n <= 0)
+	{
+		return;
+	}
+	cudaMemcpyAsync(out, d.contactColor.ptr, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, d.stream);
+	cudaStreamSynchronize(d.stream);
+}
+
+} // extern "C"

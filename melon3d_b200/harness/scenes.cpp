@@ -1,0 +1,363 @@
+// Seeded synthetic scenes of the benchmark configurations, driven through a
+// table of Melon3D C-API function pointers.  The same compiled code builds
+// and steps a world of ANY library that exports the C API: the GPU library,
+// or the reference built from its sources (used by the test suite and by the
+// CPU-baseline leg of bench.py).  No public dataset is involved; every scene
+// is generated from a fixed seed.
+//
+//   0  pyramid: 20-box base shrinking by one per row (210 unit boxes) on a
+//      static 100x1x100 m ground, mu 0.6, e 0
+//   1  streaming mixed rain: N bodies in thirds (spheres r~U[0.2,0.5],
+//      capsules r~U[0.15,0.35] hh~U[0.2,0.6], boxes he~U[0.2,0.5]^3) over a
+//      100x60x100 m volume, uniform random orientations, v~N(0,2) per axis,
+//      mu~U[0.3,0.8], e~U[0,0.3]; every step the `churn` lowest dynamic
+//      bodies (ties by index) are destroyed and as many new ones spawned
+//   2  settled pile: nx x ny x nz lattice of boxes he 0.5 spaced 1.02 m with
+//      +-0.01 m positional and +-1 deg rotational jitter, mu 0.6
+//   3  raft: 15x15 touching boxes plus 5 droppers (one island > 300 contacts)
+#include "melon3d.h"
+
+#include <algorithm>
+#include <chrono>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+#include <vector>
+
+extern "C"
+{
+
+struct M3dApi
+{
+	m3d_world_def (*world_def_default)(void);
+	m3d_body_def (*body_def_default)(void);
+	m3d_shape_def (*shape_def_default)(void);
+	m3d_world* (*world_create)(const m3d_world_def*);
+	void (*world_destroy)(m3d_world*);
+	void (*world_step)(m3d_world*, float, int);
+	m3d_body_id (*body_create)(m3d_world*, const m3d_body_def*, const m3d_shape_def*);
+	void (*body_destroy)(m3d_world*, m3d_body_id);
+	m3d_vec3 (*body_position)(m3d_world*, m3d_body_id);
+	m3d_profile (*world_profile)(m3d_world*);
+	// optional: batch pose readback of the GPU library (NULL elsewhere)
+	void (*read_poses)(m3d_world*, float*, float*, int32_t);
+};
+
+} // extern "C"
+
+namespace
+{
+
+struct Rng
+{
+	uint64_t s;
+	uint64_t next()
+	{
+		uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+		z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+		z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+		return z ^ (z >> 31);
+	}
+	double uniform() { return (double)(next() >> 11) * (1.0 / 9007199254740992.0); }
+	float range(double a, double b) { return (float)(a + (b - a) * uniform()); }
+	double normal()
+	{
+		double u1 = uniform(), u2 = uniform();
+		if (u1 < 1e-300)
+		{
+			u1 = 1e-300;
+		}
+		return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+	}
+	// uniform random rotation (Shoemake)
+	m3d_quat quat()
+	{
+		double u1 = uniform(), u2 = uniform(), u3 = uniform();
+		double a = sqrt(1.0 - u1), b = sqrt(u1);
+		m3d_quat q = { (float)(a * sin(6.283185307179586 * u2)), (float)(a * cos(6.283185307179586 * u2)),
+					   (float)(b * sin(6.283185307179586 * u3)), (float)(b * cos(6.283185307179586 * u3)) };
+		return q;
+	}
+};
+
+struct Scene
+{
+	M3dApi api;
+	m3d_world* world = nullptr;
+	int kind = 0;
+	int churn = 0;
+	Rng rng{ 0 };
+	std::vector<m3d_body_id> dynamic; // live dynamic bodies, creation order
+	std::vector<float> pos, rot;
+	double lastHostMs = 0.0;
+};
+
+void addGround(Scene& s, m3d_vec3 center, m3d_vec3 he)
+{
+	m3d_body_def bd = s.api.body_def_default();
+	bd.type = M3D_BODY_STATIC;
+	bd.position = center;
+	m3d_shape_def sd = s.api.shape_def_default();
+	sd.type = M3D_SHAPE_BOX;
+	sd.halfExtents = he;
+	s.api.body_create(s.world, &bd, &sd);
+}
+
+m3d_body_id addBox(Scene& s, m3d_vec3 p, m3d_quat q, m3d_vec3 he, float mu)
+{
+	m3d_body_def bd = s.api.body_def_default();
+	bd.type = M3D_BODY_DYNAMIC;
+	bd.position = p;
+	bd.orientation = q;
+	m3d_shape_def sd = s.api.shape_def_default();
+	sd.type = M3D_SHAPE_BOX;
+	sd.halfExtents = he;
+	sd.friction = mu;
+	m3d_body_id id = s.api.body_create(s.world, &bd, &sd);
+	s.dynamic.push_back(id);
+	return id;
+}
+
+m3d_body_id spawnRain(Scene& s, int kind)
+{
+	Rng& r = s.rng;
+	m3d_body_def bd = s.api.body_def_default();
+	bd.type = M3D_BODY_DYNAMIC;
+	bd.position = m3d_v3(r.range(-50.0, 50.0), r.range(1.0, 61.0), r.range(-50.0, 50.0));
+	bd.orientation = r.quat();
+	bd.linearVelocity = m3d_v3((float)(2.0 * r.normal()), (float)(2.0 * r.normal()), (float)(2.0 * r.normal()));
+	m3d_shape_def sd = s.api.shape_def_default();
+	if (kind == 0)
+	{
+		sd.type = M3D_SHAPE_SPHERE;
+		sd.radius = r.range(0.2, 0.5);
+	}
+	else if (kind == 1)
+	{
+		sd.type = M3D_SHAPE_CAPSULE;
+		sd.radius = r.range(0.15, 0.35);
+		sd.halfHeight = r.range(0.2, 0.6);
+	}
+	else
+	{
+		sd.type = M3D_SHAPE_BOX;
+		sd.halfExtents = m3d_v3(r.range(0.2, 0.5), r.range(0.2, 0.5), r.range(0.2, 0.5));
+	}
+	sd.friction = r.range(0.3, 0.8);
+	sd.restitution = r.range(0.0, 0.3);
+	m3d_body_id id = s.api.body_create(s.world, &bd, &sd);
+	s.dynamic.push_back(id);
+	return id;
+}
+
+// destroy the `churn` lowest dynamic bodies (ties by index), spawn as many
+void churnStep(Scene& s)
+{
+	size_t n = s.dynamic.size();
+	if (s.churn <= 0 || n == 0)
+	{
+		return;
+	}
+	std::vector<float> ys(n);
+	if (s.api.read_poses != nullptr)
+	{
+		int32_t cap = 0;
+		for (const m3d_body_id& id : s.dynamic)
+		{
+			cap = id.index + 1 > cap ? id.index + 1 : cap;
+		}
+		s.pos.resize((size_t)cap * 3);
+		s.api.read_poses(s.world, s.pos.data(), nullptr, cap);
+		for (size_t k = 0; k < n; ++k)
+		{
+			ys[k] = s.pos[(size_t)s.dynamic[k].index * 3 + 1];
+		}
+	}
+	else
+	{
+		for (size_t k = 0; k < n; ++k)
+		{
+			ys[k] = s.api.body_position(s.world, s.dynamic[k]).y;
+		}
+	}
+	std::vector<uint32_t> order(n);
+	for (size_t k = 0; k < n; ++k)
+	{
+		order[k] = (uint32_t)k;
+	}
+	size_t m = (size_t)s.churn < n ? (size_t)s.churn : n;
+	std::partial_sort(order.begin(), order.begin() + m, order.end(), [&](uint32_t a, uint32_t b) {
+		if (ys[a] != ys[b])
+		{
+			return ys[a] < ys[b];
+		}
+		return s.dynamic[a].index < s.dynamic[b].index;
+	});
+	std::vector<uint32_t> victims(order.begin(), order.begin() + m);
+	std::sort(victims.begin(), victims.end(),
+			  [&](uint32_t a, uint32_t b) { return s.dynamic[a].index < s.dynamic[b].index; });
+	std::vector<char> dead(n, 0);
+	for (uint32_t k : victims)
+	{
+		s.api.body_destroy(s.world, s.dynamic[k]);
+		dead[k] = 1;
+	}
+	std::vector<m3d_body_id> keep;
+	keep.reserve(n);
+	for (size_t k = 0; k < n; ++k)
+	{
+		if (!dead[k])
+		{
+			keep.push_back(s.dynamic[k]);
+		}
+	}
+	s.dynamic.swap(keep);
+	for (size_t k = 0; k < m; ++k)
+	{
+		spawnRain(s, (int)(s.rng.next() % 3));
+	}
+}
+
+} // namespace
+
+extern "C"
+{
+
+// kind / params: see the file header.  a,b,c = pyramid base | rain count,
+// churn | pile nx,ny,nz.
+void* scn_create(const M3dApi* api, int kind, uint64_t seed, int a, int b, int c)
+{
+	Scene* s = new Scene();
+	s->api = *api;
+	s->kind = kind;
+	s->rng.s = seed;
+	m3d_world_def wd = s->api.world_def_default();
+	s->world = s->api.world_create(&wd);
+	if (s->world == nullptr)
+	{
+		delete s;
+		return nullptr;
+	}
+	if (kind == 0)
+	{
+		addGround(*s, m3d_v3(0.0f, -0.5f, 0.0f), m3d_v3(50.0f, 0.5f, 50.0f));
+		int base = a > 0 ? a : 20;
+		const float he = 0.5f;
+		for (int row = 0; row < base; ++row)
+		{
+			int count = base - row;
+			float y = he + 2.0f * he * (float)row;
+			float x0 = -he * (float)(count - 1);
+			for (int i = 0; i < count; ++i)
+			{
+				addBox(*s, m3d_v3(x0 + 2.0f * he * (float)i, y, 0.0f), m3d_quat_identity(), m3d_v3(he, he, he), 0.6f);
+			}
+		}
+	}
+	else if (kind == 1)
+	{
+		addGround(*s, m3d_v3(0.0f, -0.5f, 0.0f), m3d_v3(50.0f, 0.5f, 50.0f));
+		int count = a > 0 ? a : 20000;
+		s->churn = b;
+		for (int i = 0; i < count; ++i)
+		{
+			spawnRain(*s, i % 3);
+		}
+	}
+	else if (kind == 2)
+	{
+		addGround(*s, m3d_v3(0.0f, -0.5f, 0.0f), m3d_v3(50.0f, 0.5f, 50.0f));
+		int nx = a > 0 ? a : 50, ny = b > 0 ? b : 100, nz = c > 0 ? c : 50;
+		const float sp = 1.02f;
+		for (int j = 0; j < ny; ++j)
+		{
+			for (int i = 0; i < nx; ++i)
+			{
+				for (int k = 0; k < nz; ++k)
+				{
+					Rng& r = s->rng;
+					m3d_vec3 p = m3d_v3(((float)i - 0.5f * (float)(nx - 1)) * sp + r.range(-0.01, 0.01),
+										0.52f + (float)j * sp + r.range(-0.01, 0.01),
+										((float)k - 0.5f * (float)(nz - 1)) * sp + r.range(-0.01, 0.01));
+					m3d_vec3 axis = m3d_normalize(m3d_v3((float)r.normal(), (float)r.normal(), (float)r.normal()));
+					float ang = r.range(-1.0, 1.0) * (M3D_PI / 180.0f);
+					float hs = (float)sin(0.5 * (double)ang), hc = (float)cos(0.5 * (double)ang);
+					m3d_quat q = { hs * axis.x, hs * axis.y, hs * axis.z, hc };
+					addBox(*s, p, q, m3d_v3(0.5f, 0.5f, 0.5f), 0.6f);
+				}
+			}
+		}
+	}
+	else if (kind == 3)
+	{
+		addGround(*s, m3d_v3(0.0f, -1.0f, 0.0f), m3d_v3(50.0f, 1.0f, 50.0f));
+		for (int gx = 0; gx < 15; ++gx)
+		{
+			for (int gz = 0; gz < 15; ++gz)
+			{
+				addBox(*s, m3d_v3(1.0f * (float)gx - 7.0f, 0.5f, 1.0f * (float)gz - 7.0f), m3d_quat_identity(),
+					   m3d_v3(0.501f, 0.5f, 0.501f), 0.6f);
+			}
+		}
+		for (int i = 0; i < 5; ++i)
+		{
+			addBox(*s, m3d_v3(2.0f * (float)i - 4.0f, 3.0f + 0.7f * (float)i, 0.5f * (float)i - 1.0f),
+				   m3d_quat_identity(), m3d_v3(0.45f, 0.45f, 0.45f), 0.6f);
+		}
+	}
+	return s;
+}
+
+m3d_world* scn_world(void* scene) { return ((Scene*)scene)->world; }
+
+int32_t scn_dynamic_count(void* scene) { return (int32_t)((Scene*)scene)->dynamic.size(); }
+
+// Run `steps` steps at 60 Hz (churn included for the streaming scene).
+// Returns the body-substeps advanced (dynamic bodies x substeps per step,
+// summed) and writes the host wall time of the whole loop to *wallMs.
+int64_t scn_run(void* scene, int steps, int substeps, double* wallMs, float* stepMsOut)
+{
+	Scene& s = *(Scene*)scene;
+	int64_t bodySubsteps = 0;
+	auto t0 = std::chrono::steady_clock::now();
+	for (int i = 0; i < steps; ++i)
+	{
+		auto a = std::chrono::steady_clock::now();
+		churnStep(s);
+		s.api.world_step(s.world, 1.0f / 60.0f, substeps);
+		bodySubsteps += (int64_t)s.dynamic.size() * substeps;
+		if (stepMsOut != nullptr)
+		{
+			stepMsOut[i] = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - a).count();
+		}
+	}
+	if (wallMs != nullptr)
+	{
+		*wallMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+	}
+	return bodySubsteps;
+}
+
+// ids of the live dynamic bodies (creation order)
+int32_t scn_dynamic_ids(void* scene, m3d_body_id* out, int32_t cap)
+{
+	Scene& s = *(Scene*)scene;
+	int32_t n = (int32_t)s.dynamic.size() < cap ? (int32_t)s.dynamic.size() : cap;
+	for (int32_t i = 0; i < n; ++i)
+	{
+		out[i] = s.dynamic[i];
+	}
+	return n;
+}
+
+void scn_destroy(void* scene)
+{
+	Scene* s = (Scene*)scene;
+	if (s->world != nullptr)
+	{
+		s->api.world_destroy(s->world);
+	}
+	delete s;
+}
+
+} // extern "C"

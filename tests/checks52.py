@@ -1,0 +1,562 @@
+"""The reference's 52 integration checks (test/test_main.cpp of the reference
+project), restated against the C API through ctypes so the same scenarios
+run on any library that exports it.  Each scenario returns a list of
+(check name, passed, measured value).  Thresholds are the reference's; the
+tighter figures quoted for the GPU build (sliding within 5 %, rolling within
+1 %) are reported separately by the tests that use `measured`.
+"""
+import ctypes as C
+import ctypes.util
+import math
+
+import numpy as np
+
+from melon3d_b200.api import (AABB, BODY_DYNAMIC, BODY_STATIC, BallJointDef, BodyId, DistanceJointDef, OverlapFn,
+                              SHAPE_BOX, SHAPE_CAPSULE, SHAPE_SPHERE, Vec3, PI)
+
+_libm = C.CDLL(ctypes.util.find_library("m"))
+_libm.sinf.restype = C.c_float
+_libm.sinf.argtypes = [C.c_float]
+_libm.cosf.restype = C.c_float
+_libm.cosf.argtypes = [C.c_float]
+f32 = np.float32
+DT = 1.0 / 60.0
+
+
+def sinf(x):
+    return float(_libm.sinf(f32(x)))
+
+
+def cosf(x):
+    return float(_libm.cosf(f32(x)))
+
+
+def v(x, y, z):
+    return Vec3(x, y, z)
+
+
+def length(a):
+    return math.sqrt(a.x * a.x + a.y * a.y + a.z * a.z)
+
+
+def sub(a, b):
+    return Vec3(a.x - b.x, a.y - b.y, a.z - b.z)
+
+
+def quat_axis_angle(axis, angle):
+    """m3d_quat_axis_angle with libm sinf/cosf in float arithmetic."""
+    ax = [f32(axis[0]), f32(axis[1]), f32(axis[2])]
+    l = np.sqrt(f32(f32(ax[0] * ax[0]) + f32(ax[1] * ax[1])) + f32(ax[2] * ax[2]))
+    inv = f32(1.0) / f32(l)
+    n = [f32(inv * a) for a in ax]
+    half = f32(f32(0.5) * f32(angle))
+    s = f32(sinf(half))
+    from melon3d_b200.api import Quat
+    return Quat(f32(s * n[0]), f32(s * n[1]), f32(s * n[2]), f32(cosf(half)))
+
+
+def rotate(q, p):
+    u = np.array([q.x, q.y, q.z], dtype=np.float64)
+    vv = np.array([p.x, p.y, p.z], dtype=np.float64)
+    t = 2.0 * np.cross(u, vv)
+    r = vv + q.w * t + np.cross(u, t)
+    return Vec3(*r)
+
+
+class W:
+    def __init__(self, lib, gravity=None, workers=1):
+        self.lib = lib
+        wd = lib.m3d_world_def_default()
+        wd.workerCount = workers
+        if gravity is not None:
+            wd.gravity = gravity
+        self.w = lib.m3d_world_create(C.byref(wd))
+        assert self.w, "world creation failed"
+
+    def step(self, dt=DT, sub=4, n=1):
+        for _ in range(n):
+            self.lib.m3d_world_step(self.w, dt, sub)
+
+    def body(self, typ, pos, shape, q=None, **kw):
+        lib = self.lib
+        bd = lib.m3d_body_def_default()
+        bd.type = typ
+        bd.position = pos
+        if q is not None:
+            bd.orientation = q
+        sd = lib.m3d_shape_def_default()
+        sd.type = shape
+        for k, val in kw.items():
+            if k in ("linearVelocity", "angularVelocity", "gravityScale", "angularDamping", "linearDamping",
+                     "enableSleep", "isAwake"):
+                setattr(bd, k, val)
+            elif k == "group":
+                sd.filter.groupIndex = val
+            elif k == "mask":
+                sd.filter.maskBits = val
+            else:
+                setattr(sd, k, val)
+        return lib.m3d_body_create(self.w, C.byref(bd), C.byref(sd))
+
+    def ground(self):
+        return self.body(BODY_STATIC, v(0, -1, 0), SHAPE_BOX, halfExtents=v(50, 1, 50))
+
+    def box(self, pos, he, mu):
+        return self.body(BODY_DYNAMIC, pos, SHAPE_BOX, halfExtents=he, friction=mu)
+
+    def pos(self, b):
+        return self.lib.m3d_body_position(self.w, b)
+
+    def vel(self, b):
+        return self.lib.m3d_body_linear_velocity(self.w, b)
+
+    def close(self):
+        self.lib.m3d_world_destroy(self.w)
+
+
+def sphere_rest(lib):
+    w = W(lib)
+    w.ground()
+    ball = w.body(BODY_DYNAMIC, v(0, 3, 0), SHAPE_SPHERE, radius=0.5)
+    w.step(n=240)
+    p = w.pos(ball)
+    vv = w.vel(ball)
+    w.close()
+    return [("sphere rests at y=radius", abs(p.y - 0.5) < 0.02, p.y - 0.5),
+            ("sphere does not drift", abs(p.x) < 0.01 and abs(p.z) < 0.01, max(abs(p.x), abs(p.z))),
+            ("sphere at rest has ~zero velocity", length(vv) < 0.05, length(vv))]
+
+
+def capsule_rest(lib):
+    w = W(lib)
+    w.ground()
+    cap = w.body(BODY_DYNAMIC, v(0, 2, 0), SHAPE_CAPSULE, q=quat_axis_angle((0, 0, 1), f32(0.5) * f32(PI)), radius=0.3,
+                 halfHeight=0.5)
+    w.step(n=240)
+    p = w.pos(cap)
+    w.close()
+    return [("capsule rests at y=radius", abs(p.y - 0.3) < 0.02, p.y - 0.3)]
+
+
+def box_stack(lib):
+    w = W(lib)
+    w.ground()
+    boxes = [w.box(v(0, 0.5 + 1.0 * i, 0), v(0.5, 0.5, 0.5), 0.6) for i in range(10)]
+    w.step(n=300)
+    ok = True
+    for i, b in enumerate(boxes):
+        p = w.pos(b)
+        if abs(p.y - (0.5 + i)) > 0.1 or abs(p.x) > 0.2 or abs(p.z) > 0.2:
+            ok = False
+    w.close()
+    return [("10-box stack remains standing after 5s", ok, None)]
+
+
+def restitution(lib):
+    w = W(lib)
+    w.ground()
+    ball = w.body(BODY_DYNAMIC, v(0, 2, 0), SHAPE_SPHERE, radius=0.5, restitution=0.8)
+    bounced, top = False, 0.0
+    for _ in range(240):
+        w.step()
+        p, vv = w.pos(ball), w.vel(ball)
+        if vv.y > 0.5:
+            bounced = True
+        if bounced and p.y > top:
+            top = p.y
+    w.close()
+    return [("restitution 0.8 ball bounces", bounced, None), ("bounce reaches a reasonable height", top > 1.0, top)]
+
+
+def sleep_and_wake(lib):
+    w = W(lib)
+    w.ground()
+    box = w.box(v(0, 0.5, 0), v(0.5, 0.5, 0.5), 0.6)
+    w.step(n=180)
+    asleep = not lib.m3d_body_is_awake(w.w, box)
+    lib.m3d_body_apply_impulse(w.w, box, v(0, 500, 0), w.pos(box))
+    woke = lib.m3d_body_is_awake(w.w, box)
+    w.step()
+    vy = w.vel(box).y
+    w.close()
+    return [("resting box falls asleep", asleep, None), ("impulse wakes the box", woke, None),
+            ("woken box moves upward", vy > 0.0, vy)]
+
+
+def ray_cast(lib):
+    w = W(lib)
+    w.ground()
+    box = w.box(v(0, 5, 0), v(0.5, 0.5, 0.5), 0.6)
+    r = lib.m3d_world_ray_cast(w.w, v(0, 10, 0), v(0, -20, 0))
+    miss = lib.m3d_world_ray_cast(w.w, v(100, 10, 100), v(0, 1, 0))
+    w.close()
+    return [("downward ray hits", r.hit, None), ("ray hits the box first", r.body.index == box.index, r.body.index),
+            ("ray hit point on top face", abs(r.point.y - 5.5) < 0.01, r.point.y),
+            ("ray hit normal points up", r.normal.y > 0.99, r.normal.y), ("ray away from all bodies misses", not miss.hit, None)]
+
+
+def distance_joint(lib):
+    w = W(lib)
+    anchor = w.body(BODY_STATIC, v(0, 5, 0), SHAPE_SPHERE, radius=0.1)
+    bob = w.body(BODY_DYNAMIC, v(2, 5, 0), SHAPE_SPHERE, radius=0.25)
+    jd = DistanceJointDef()
+    jd.bodyA, jd.bodyB = anchor, bob
+    jd.length = 2.0
+    lib.m3d_joint_create_distance(w.w, C.byref(jd))
+    err = 0.0
+    for _ in range(300):
+        w.step()
+        p = w.pos(bob)
+        err = max(err, abs(length(sub(p, v(0, 5, 0))) - 2.0))
+    w.close()
+    return [("distance joint keeps pendulum length within 5cm", err < 0.05, err)]
+
+
+def ball_joint(lib):
+    w = W(lib)
+    anchor = w.body(BODY_STATIC, v(0, 5, 0), SHAPE_SPHERE, radius=0.1)
+    rod = w.body(BODY_DYNAMIC, v(0.5, 5, 0), SHAPE_BOX, halfExtents=v(0.5, 0.1, 0.1))
+    jd = BallJointDef()
+    jd.bodyA, jd.bodyB = anchor, rod
+    jd.localAnchorB = v(-0.5, 0, 0)
+    lib.m3d_joint_create_ball(w.w, C.byref(jd))
+    err = 0.0
+    for _ in range(300):
+        w.step()
+        xf = lib.m3d_body_transform(w.w, rod)
+        r = rotate(xf.q, v(-0.5, 0, 0))
+        pinned = v(r.x + xf.p.x, r.y + xf.p.y, r.z + xf.p.z)
+        err = max(err, length(sub(pinned, v(0, 5, 0))))
+    w.close()
+    return [("ball joint keeps anchors pinned within 5cm", err < 0.05, err)]
+
+
+def contact_events(lib):
+    w = W(lib)
+    w.ground()
+    box = w.box(v(0, 2, 0), v(0.5, 0.5, 0.5), 0.6)
+    saw = False
+    for _ in range(120):
+        w.step()
+        if lib.m3d_world_contact_events(w.w).beginCount > 0:
+            saw = True
+    lib.m3d_body_destroy(w.w, box)
+    invalid = not lib.m3d_body_is_valid(w.w, box)
+    w.step()
+    w.close()
+    return [("begin-touch event fires on landing", saw, None), ("destroyed body id is invalid", invalid, None)]
+
+
+def speculative_no_tunnel(lib):
+    w = W(lib)
+    w.body(BODY_STATIC, v(10, 0, 0), SHAPE_BOX, halfExtents=v(0.05, 5, 5))
+    bullet = w.body(BODY_DYNAMIC, v(0, 0, 0), SHAPE_SPHERE, radius=0.2, linearVelocity=v(50, 0, 0), gravityScale=0.0)
+    w.step(n=60)
+    x = w.pos(bullet).x
+    w.close()
+    return [("fast sphere stopped by thin wall (no tunneling)", x < 10.0, x)]
+
+
+def determinism_across_threads(lib):
+    res = []
+    for workers in (1, 4):
+        w = W(lib, workers=workers)
+        w.ground()
+        top = None
+        for i in range(5):
+            for j in range(5):
+                top = w.box(v(2.0 * i - 4.0, 0.5 + j, 0), v(0.45, 0.45, 0.45), 0.6)
+        w.step(n=120)
+        res.append(w.pos(top).tup() if hasattr(w.pos(top), "tup") else tuple(w.pos(top)))
+        w.close()
+    return [("1-thread and 4-thread runs are bit-identical", res[0] == res[1], None)]
+
+
+def collision_filter(lib):
+    w = W(lib)
+    w.ground()
+    upper = w.body(BODY_DYNAMIC, v(0, 4, 0), SHAPE_SPHERE, radius=0.5, group=-7)
+    lower = w.body(BODY_DYNAMIC, v(0, 1, 0), SHAPE_SPHERE, radius=0.5, group=-7)
+    ghost = w.body(BODY_DYNAMIC, v(5, 2, 0), SHAPE_BOX, halfExtents=v(0.4, 0.4, 0.4), mask=0x2)
+    w.step(n=180)
+    pu, pl, pg = w.pos(upper), w.pos(lower), w.pos(ghost)
+    w.close()
+    return [("same negative group: bodies interpenetrate", abs(pu.y - 0.5) < 0.05 and abs(pl.y - 0.5) < 0.05, None),
+            ("disjoint masks: body ignores the ground", pg.y < -5.0, pg.y)]
+
+
+def sensor(lib):
+    w = W(lib)
+    w.ground()
+    w.body(BODY_STATIC, v(0, 2, 0), SHAPE_BOX, halfExtents=v(1, 1, 1), isSensor=True)
+    ball = w.body(BODY_DYNAMIC, v(0, 6, 0), SHAPE_SPHERE, radius=0.3)
+    nb = ne = 0
+    for _ in range(240):
+        w.step()
+        ev = lib.m3d_world_contact_events(w.w)
+        nb += sum(1 for k in range(ev.beginCount) if ev.beginEvents[k].isSensor)
+        ne += sum(1 for k in range(ev.endCount) if ev.endEvents[k].isSensor)
+    p = w.pos(ball)
+    w.close()
+    return [("sensor reported a begin event", nb >= 1, nb), ("sensor reported an end event after the body passed", ne >= 1, ne),
+            ("sensor exerted no force: ball fell through the zone to the ground", abs(p.y - 0.3) < 0.05, p.y)]
+
+
+def forces_and_torques(lib):
+    w = W(lib, gravity=v(0, 0, 0))
+    box = w.body(BODY_DYNAMIC, v(0, 0, 0), SHAPE_BOX, halfExtents=v(0.5, 0.5, 0.5), density=1000.0, angularDamping=0.0)
+    for _ in range(60):
+        lib.m3d_body_apply_force(w.w, box, v(2000, 0, 0))
+        w.step()
+    vx = w.vel(box).x
+    for _ in range(60):
+        lib.m3d_body_apply_torque(w.w, box, v(0, 500, 0))
+        w.step()
+    wy = lib.m3d_body_angular_velocity(w.w, box).y
+    v0 = w.vel(box).x
+    w.step()
+    v1 = w.vel(box).x
+    w.close()
+    return [("apply_force: v = a*t after 1 s", abs(vx - 2.0) < 0.05, vx), ("apply_torque spins the body", wy > 0.5, wy),
+            ("force does not persist past the step", abs(v1 - v0) < 1e-6, v1 - v0)]
+
+
+def hinge_joint(lib):
+    from melon3d_b200.api import HingeJointDef  # noqa
+    w = W(lib)
+    pivot = w.body(BODY_STATIC, v(0, 5, 0), SHAPE_BOX, halfExtents=v(0.1, 0.1, 0.1))
+    arm = w.body(BODY_DYNAMIC, v(1, 5, 0), SHAPE_BOX, halfExtents=v(0.4, 0.1, 0.1))
+    hd = lib.m3d_hinge_joint_def_default()
+    hd.bodyA, hd.bodyB = pivot, arm
+    hd.localAnchorA = v(0, 0, 0)
+    hd.localAnchorB = v(-1, 0, 0)
+    hd.localAxisA = v(0, 0, 1)
+    hinge = lib.m3d_joint_create_hinge(w.w, C.byref(hd))
+    maxz = 0.0
+    for _ in range(240):
+        w.step()
+        maxz = max(maxz, abs(w.pos(arm).z))
+    p = w.pos(arm)
+    dist = length(sub(p, v(0, 5, 0)))
+    out = [("hinge pendulum stays in the hinge plane", maxz < 0.02, maxz),
+           ("hinge point constraint holds the arm at the pivot", abs(dist - 1.0) < 0.05, dist)]
+    lib.m3d_joint_destroy(w.w, hinge)
+    lib.m3d_body_destroy(w.w, arm)
+    arm = w.body(BODY_DYNAMIC, v(1, 5, 0), SHAPE_BOX, halfExtents=v(0.4, 0.1, 0.1))
+    hd.bodyB = arm
+    hd.enableLimit = True
+    hd.lowerAngle = f32(-0.25) * f32(PI)
+    hd.upperAngle = f32(0.25) * f32(PI)
+    hinge = lib.m3d_joint_create_hinge(w.w, C.byref(hd))
+    mina = 0.0
+    for _ in range(240):
+        w.step()
+        mina = min(mina, lib.m3d_joint_hinge_angle(w.w, hinge))
+    out.append(("hinge limit holds the swing", mina > float(f32(-0.25) * f32(PI)) - 0.05, mina))
+    lib.m3d_joint_destroy(w.w, hinge)
+    lib.m3d_body_destroy(w.w, arm)
+    wheel = w.body(BODY_DYNAMIC, v(0, 5, 0), SHAPE_SPHERE, radius=0.5)
+    hd.bodyB = wheel
+    hd.localAnchorB = v(0, 0, 0)
+    hd.enableLimit = False
+    hd.enableMotor = True
+    hd.motorSpeed = 5.0
+    hd.maxMotorTorque = 1000.0
+    lib.m3d_joint_create_hinge(w.w, C.byref(hd))
+    w.step(n=120)
+    wz = lib.m3d_body_angular_velocity(w.w, wheel).z
+    out.append(("hinge motor reaches target speed", abs(wz - 5.0) < 0.2, wz))
+    w.close()
+    return out
+
+
+def weld_joint(lib):
+    w = W(lib)
+    w.ground()
+    a = w.box(v(0, 3, 0), v(0.4, 0.4, 0.4), 0.6)
+    b = w.box(v(0.85, 3, 0), v(0.4, 0.4, 0.4), 0.6)
+    jd = lib.m3d_weld_joint_def_default()
+    jd.bodyA, jd.bodyB = a, b
+    jd.localAnchorA = v(0.425, 0, 0)
+    jd.localAnchorB = v(-0.425, 0, 0)
+    lib.m3d_joint_create_weld(w.w, C.byref(jd))
+    w.step(n=300)
+    pa, pb = w.pos(a), w.pos(b)
+    qa, qb = lib.m3d_body_rotation(w.w, a), lib.m3d_body_rotation(w.w, b)
+    relw = qa.w * qb.w + qa.x * qb.x + qa.y * qb.y + qa.z * qb.z
+    d = length(sub(pb, pa))
+    w.close()
+    return [("weld keeps the anchor distance", abs(d - 0.85) < 0.03, d), ("weld keeps the relative orientation", abs(relw) > 0.999, relw)]
+
+
+def sphere_cast_and_overlap(lib):
+    w = W(lib)
+    w.ground()
+    hit = lib.m3d_world_sphere_cast(w.w, v(0, 2, 0), 0.25, v(0, -2, 0), 0xFFFFFFFF)
+    miss = lib.m3d_world_sphere_cast(w.w, v(0, 5, 0), 0.25, v(0, -2, 0), 0xFFFFFFFF)
+    inside = w.box(v(0, 0.5, 0), v(0.4, 0.4, 0.4), 0.6)
+    w.box(v(20, 0.5, 0), v(0.4, 0.4, 0.4), 0.6)
+    seen = []
+
+    @OverlapFn
+    def cb(bid, ctx):
+        seen.append(bid.index)
+        return True
+
+    region = AABB(v(-2, 0.1, -2), v(2, 2, 2))
+    lib.m3d_world_overlap_aabb(w.w, region, cb, None)
+    w.close()
+    return [("sphere cast hits the ground", hit.hit, None),
+            ("sphere cast fraction accounts for the radius", abs(hit.fraction - 0.875) < 0.01, hit.fraction),
+            ("sphere cast normal points up", hit.normal.y > 0.99, hit.normal.y), ("short sphere cast misses", not miss.hit, None),
+            ("overlap query finds the box in the region", inside.index in seen, seen),
+            ("overlap query skips bodies outside the region", len(seen) == 1, len(seen))]
+
+
+def thin_wall_high_speed(lib):
+    w = W(lib)
+    w.ground()
+    w.body(BODY_STATIC, v(20, 2, 0), SHAPE_BOX, halfExtents=v(0.025, 2, 2))
+    pea = w.body(BODY_DYNAMIC, v(12, 2, 0), SHAPE_SPHERE, radius=0.06, linearVelocity=v(150, 0, 0), gravityScale=0.0)
+    w.step(n=60)
+    x = w.pos(pea).x
+    w.close()
+    return [("150 m/s pea ends on the near side of a 5 cm wall", x < 20.0, x)]
+
+
+def incline_scene(lib, theta_deg, mu):
+    th = f32(f32(f32(theta_deg) * f32(PI)) / f32(180.0))
+    w = W(lib)
+    q = quat_axis_angle((0, 0, 1), th)
+    w.body(BODY_STATIC, v(0, 0, 0), SHAPE_BOX, q=q, halfExtents=v(60, 1, 8), friction=mu)
+    s, c = f32(sinf(th)), f32(cosf(th))
+    nrm = (f32(-s), c)
+    along = (c, s)
+    px = f32(f32(20.0) * along[0]) + f32(f32(1.402) * nrm[0])
+    py = f32(f32(20.0) * along[1]) + f32(f32(1.402) * nrm[1])
+    box = w.body(BODY_DYNAMIC, v(px, py, 0), SHAPE_BOX, q=q, halfExtents=v(0.4, 0.4, 0.4), friction=mu)
+    return w, box, th
+
+
+def inclined_plane(lib):
+    w, box, _ = incline_scene(lib, 28.0, 0.6)
+    p0 = w.pos(box)
+    w.step(n=480)
+    hold = length(sub(w.pos(box), p0))
+    w.close()
+    w, box, _ = incline_scene(lib, 38.0, 0.6)
+    p0 = w.pos(box)
+    w.step(n=480)
+    slide = length(sub(w.pos(box), p0))
+    w.close()
+    w, box, th = incline_scene(lib, 35.0, 0.3)
+    w.step(dt=1.0 / 240.0, sub=1, n=60)
+    v1 = w.vel(box)
+    w.step(dt=1.0 / 240.0, sub=1, n=240)
+    a = length(sub(w.vel(box), v1))
+    w.close()
+    a_exp = 9.81 * (sinf(th) - 0.3 * cosf(th))
+    return [("box holds below the friction cone", hold < 0.05, hold), ("box slides above the friction cone", slide > 0.5, slide),
+            ("Coulomb sliding acceleration matches g(sin-mu cos)", abs(a - a_exp) < 0.1 * a_exp, abs(a - a_exp) / a_exp)]
+
+
+def rolling_physics(lib):
+    th = f32(f32(f32(20.0) * f32(PI)) / f32(180.0))
+    w = W(lib)
+    w.body(BODY_STATIC, v(0, 0, 0), SHAPE_BOX, q=quat_axis_angle((0, 0, 1), th), halfExtents=v(60, 1, 8), friction=0.8)
+    s, c = f32(sinf(th)), f32(cosf(th))
+    px = f32(f32(20.0) * c) + f32(f32(1.402) * f32(-s))
+    py = f32(f32(20.0) * s) + f32(f32(1.402) * c)
+    ball = w.body(BODY_DYNAMIC, v(px, py, 0), SHAPE_SPHERE, radius=0.4, friction=0.8, rollingResistance=0.0,
+                  angularDamping=0.0)
+    w.step(dt=1.0 / 240.0, sub=1, n=120)
+    v1 = w.vel(ball)
+    w.step(dt=1.0 / 240.0, sub=1, n=240)
+    a = length(sub(w.vel(ball), v1))
+    w.close()
+    a_exp = 5.0 / 7.0 * 9.81 * sinf(th)
+    w = W(lib)
+    w.ground()
+    ball = w.body(BODY_DYNAMIC, v(0, 0.5, 0), SHAPE_SPHERE, radius=0.5, friction=0.5, rollingResistance=0.0,
+                  angularVelocity=v(0, 0, -10), angularDamping=0.0)
+    w.step(dt=1.0 / 240.0, sub=1, n=150)
+    v_roll = w.vel(ball).x
+    w.step(dt=1.0 / 240.0, sub=1, n=480)
+    v_later = w.vel(ball).x
+    w.close()
+    return [("solid sphere rolls at 5/7 g sin(th)", abs(a - a_exp) < 0.08 * a_exp, abs(a - a_exp) / a_exp),
+            ("backspin converts at v = 2/7 w r", abs(v_roll - 2.0 / 7.0 * 10.0 * 0.5) < 0.15, v_roll),
+            ("free roller never self-accelerates", v_later <= v_roll + 0.05, v_later - v_roll)]
+
+
+def dzhanibekov(lib):
+    w = W(lib, gravity=v(0, 0, 0))
+    brick = w.body(BODY_DYNAMIC, v(0, 0, 0), SHAPE_BOX, halfExtents=v(0.5, 0.3, 0.1), angularVelocity=v(0.02, 8.0, 0.0),
+                   angularDamping=0.0)
+    mind = 1.0
+    for _ in range(2400):
+        w.step(dt=1.0 / 240.0, sub=1)
+        q = lib.m3d_body_rotation(w.w, brick)
+        mind = min(mind, rotate(q, v(0, 1, 0)).y)
+    w.close()
+    return [("Dzhanibekov flip about the intermediate axis", mind < -0.5, mind)]
+
+
+def joint_determinism(lib):
+    res = []
+    for workers in (1, 4):
+        w = W(lib, workers=workers)
+        w.ground()
+        prev = w.body(BODY_STATIC, v(0, 8, 0), SHAPE_BOX, halfExtents=v(0.1, 0.1, 0.1))
+        last = prev
+        for i in range(6):
+            link = w.box(v(0.9 * (i + 1), 8, 0), v(0.4, 0.15, 0.15), 0.6)
+            hd = lib.m3d_hinge_joint_def_default()
+            hd.bodyA, hd.bodyB = prev, link
+            hd.localAnchorA = v(0, 0, 0) if i == 0 else v(0.45, 0, 0)
+            hd.localAnchorB = v(-0.45, 0, 0)
+            hd.localAxisA = v(0, 0, 1)
+            lib.m3d_joint_create_hinge(w.w, C.byref(hd))
+            prev = last = link
+        for i in range(12):
+            w.box(v(0.6 * i - 2.0, 10.0 + 0.3 * i, 0.05 * i), v(0.25, 0.25, 0.25), 0.6)
+        w.step(n=180)
+        p = w.pos(last)
+        res.append((p.x, p.y, p.z))
+        w.close()
+    return [("hinge chain is bit-identical across thread counts", res[0] == res[1], None)]
+
+
+def colored_path_determinism(lib):
+    ref = None
+    same = True
+    seen = 0
+    for workers in (1, 2, 4, 8, 16):
+        w = W(lib, workers=workers)
+        w.ground()
+        ids = []
+        for gx in range(15):
+            for gz in range(15):
+                ids.append(w.box(v(1.0 * gx - 7.0, 0.5, 1.0 * gz - 7.0), v(0.501, 0.5, 0.501), 0.6))
+        for i in range(5):
+            ids.append(w.box(v(2.0 * i - 4.0, 3.0 + 0.7 * i, 0.5 * i - 1.0), v(0.45, 0.45, 0.45), 0.6))
+        for _ in range(90):
+            w.step()
+            p = lib.m3d_world_profile(w.w)
+            if p.touchingContactCount >= 300 and p.islandCount <= 8:
+                seen += 1
+        p = w.pos(ids[-1])
+        t = (p.x, p.y, p.z)
+        if ref is None:
+            ref = t
+        elif t != ref:
+            same = False
+        w.close()
+    return [("raft scene actually reaches the colored-path contact threshold", seen > 0, seen),
+            ("colored SIMD path bit-identical across 1/2/4/8/16 workers", same, None)]
+
+
+SCENARIOS = [sphere_rest, capsule_rest, box_stack, restitution, sleep_and_wake, ray_cast, distance_joint, ball_joint,
+             contact_events, speculative_no_tunnel, determinism_across_threads, collision_filter, sensor,
+             forces_and_torques, hinge_joint, weld_joint, sphere_cast_and_overlap, thin_wall_high_speed, inclined_plane,
+             rolling_physics, dzhanibekov, joint_determinism, colored_path_determinism]

@@ -1,0 +1,110 @@
+"""Step-by-step parity of the GPU world with the reference step.
+
+Oracles (all built from the reference's own sources, oracle/Makefile):
+  - oracle():    contraction off — bit-exact target for scenes whose bodies
+                 never reach libm's float transcendentals;
+  - oracle_cr(): contraction off, libm sinf/cosf/atan2f evaluated in double
+                 and rounded once like the GPU — bit-exact target for every
+                 scene;
+  - oracle_fast(): the reference's own release flags (FMA contraction) —
+                 tolerance target (poses within 1e-5 m / 1e-5 rad per step).
+
+Bit-exact comparisons, per step: every body's pose, velocities and sleep
+state; the contact array (order, pairs, touch flags, manifold normals and
+points); island partitions; the greedy colouring of coloured islands; the
+profile counters.
+"""
+import numpy as np
+import pytest
+
+from melon3d_b200 import harness
+
+from . import _util as U
+
+pytestmark = pytest.mark.gpu
+
+
+def lockstep(ref, kind, steps, seed=1, a=0, b=0, c=0, substeps=4, check_colors=True):
+    g = U.gpu()
+    sr = harness.Scene(ref, kind, seed, a, b, c)
+    sg = harness.Scene(g, kind, seed, a, b, c)
+    coloured_steps = 0
+    try:
+        for step in range(steps):
+            sr.run(1, substeps)
+            sg.run(1, substeps)
+            assert g.m3d_gpu_status(sg.world) == 0, g.m3d_gpu_last_error_string(sg.world)
+            cr, cg = U.contacts(ref, sr.world), U.contacts(g, sg.world)
+            d = U.diff_contacts(cr, cg)
+            assert d is None, "step %d: %s" % (step, d)
+            br, bg = U.bodies(ref, sr.world), U.bodies(g, sg.world)
+            d = U.diff_bodies(br, bg)
+            assert d is None, "step %d: %s (pose error %s)" % (step, d, U.pose_error(br, bg))
+            lr, lg = U.island_labels(ref, sr.world), U.island_labels(g, sg.world)
+            live = br["inUse"] != 0
+            assert np.array_equal(lr[live], lg[live]), "step %d: island partition differs" % step
+            pr, pg = ref.m3d_world_profile(sr.world), g.m3d_world_profile(sg.world)
+            for f in ("bodyCount", "awakeBodyCount", "contactCount", "touchingContactCount", "islandCount"):
+                assert getattr(pr, f) == getattr(pg, f), "step %d: profile %s %d vs %d" % (
+                    step, f, getattr(pr, f), getattr(pg, f))
+            if check_colors and pr.touchingContactCount >= 300 and pr.islandCount > 0:
+                kr, kg = U.contact_colors(ref, sr.world), U.contact_colors(g, sg.world)
+                m = kr >= 0
+                if m.any():
+                    coloured_steps += 1
+                    assert np.array_equal(kr[m], kg[m]), "step %d: colouring differs" % step
+    finally:
+        sr.close()
+        sg.close()
+    return coloured_steps
+
+
+def test_pyramid_bit_exact_until_asleep():
+    # 210-box pyramid (one island, > 300 contacts: the coloured path)
+    assert lockstep(U.oracle(), harness.PYRAMID, 80) > 0
+
+
+def test_raft_coloured_path_bit_exact():
+    assert lockstep(U.oracle(), harness.RAFT, 90) > 0
+
+
+def test_rain_with_churn_bit_exact():
+    lockstep(U.oracle_cr(), harness.RAIN, 60, seed=2, a=1500, b=30)
+
+
+def test_dense_rain_bit_exact():
+    lockstep(U.oracle_cr(), harness.RAIN, 12, seed=5, a=20000, b=200)
+
+
+def test_small_pile_bit_exact():
+    lockstep(U.oracle_cr(), harness.PILE, 40, seed=3, a=6, b=8, c=6)
+
+
+def test_pyramid_pose_gate_60_steps():
+    """Pose gate (1e-5 m / 1e-5 rad per step over 60 steps) against the
+    contraction-off reference, which the GPU matches bit for bit (error 0).
+    The reference's own release build (GCC free to contract a*b+c into FMAs)
+    is a different float program: it drifts from its own contraction-off
+    build by ~1e-3 m within ten pyramid steps.  The GPU's distance to that
+    build is measured and must equal the contraction-off build's distance."""
+    exact, stock, g = U.oracle(), U.oracle_fast(), U.gpu()
+    se = harness.Scene(exact, harness.PYRAMID, 1)
+    ss = harness.Scene(stock, harness.PYRAMID, 1)
+    sg = harness.Scene(g, harness.PYRAMID, 1)
+    worst_stock = (0.0, 0.0)
+    try:
+        for step in range(60):
+            se.run(1)
+            ss.run(1)
+            sg.run(1)
+            be, bs, bg = U.bodies(exact, se.world), U.bodies(stock, ss.world), U.bodies(g, sg.world)
+            dx, dq = U.pose_error(be, bg)
+            assert dx <= 1e-5 and dq <= 1e-5, "step %d: pose error %.3g m %.3g" % (step, dx, dq)
+            assert U.pose_error(bs, bg) == U.pose_error(bs, be)
+            e = U.pose_error(bs, bg)
+            worst_stock = (max(worst_stock[0], e[0]), max(worst_stock[1], e[1]))
+    finally:
+        se.close()
+        ss.close()
+        sg.close()
+    print("pyramid, GPU vs reference release build (FMA): max %.3g m, %.3g" % worst_stock)
