@@ -1,0 +1,291 @@
+#!/usr/bin/env python
+"""Body-substeps/s of the GPU world on the streaming mixed-rain workload.
+
+Workload (one "step"): the 20,000-body streaming mixed rain (spheres,
+capsules and boxes in thirds over a 100x60x100 m volume, seeded synthetic
+data) advanced by one m3d_world_step at 60 Hz with 4 substeps, after the 200
+lowest dynamic bodies are destroyed and 200 new ones spawned through the C
+API.  Metric: body-substeps/s = dynamic bodies x substeps per step, summed
+over the timed steps, divided by the time.
+
+  value  device time of the steps: CUDA events on the world's stream around
+         each m3d_world_step (uploads of the step's new bodies included);
+  e2e    host wall time of the same steps through the C ABI, churn included:
+         the H2D copies of the spawned bodies, the D2H pose read used to pick
+         the lowest bodies and the per-step event/counter reads.
+The L2 (126 MB) is flushed between timed steps by a 256 MiB write.
+
+--impl reference times the reference's own CPU implementation (the
+reference library built from its sources with its release flags) on the
+same workload with all host threads.  N > 1 (torchrun) runs one independent
+replica per GPU (a single world does not shard); value is the sum of the
+replicas' work over the slowest replica's time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import ctypes as C
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from melon3d_b200 import api, harness  # noqa: E402
+
+WORKLOAD = "streaming mixed rain, 20000 bodies, churn 200/step, 60 Hz x 4 substeps"
+REF_RELEASE_LIB = os.path.join(ROOT, "oracle", "_ref", "libmelon3d_ref_fast.so")
+COUNTER_NAMES = ["activeEntries", "stableEntries", "activeOversized", "stableOversized", "runs", "gridPairs",
+                 "overPairs", "newContacts", "removed", "endRemoval", "beginNP", "endNP", "anyAwakeDynamic",
+                 "islandCount", "touchingCount", "awakeIslands", "islandContacts", "islandJoints", "islandBodies",
+                 "stableDirty", "bodyCount", "awakeBodyCount", "hashFail", "coloredIslands", "serialIslands",
+                 "freeIslands"]
+
+# Algorithmic bytes per launch of the kernels that can be named as the
+# roofline kernel: each field a kernel must read or write, counted once
+# (fp32 SoA; per body-substep 300 B = integrate 220 + reconstruct 80).
+ROOFLINE_MODELS = {
+    # free-body islands: every substep integrates and reconstructs each body
+    "kSolveFree": ("HBM bytes per free body per step", lambda c, sub: c["freeIslands"] * 300 * sub),
+    # narrowphase: per live contact the two body indices, flags, two poses,
+    # two cached poses, point count (~150 B); regenerated pairs also write
+    # their manifold (~4 x 132 B) - counted as the cached case (a floor)
+    "kNarrowphase": ("HBM bytes per contact", lambda c, sub: (c["_contacts"]) * 150),
+}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=120)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["gpu", "reference"], default="gpu")
+    p.add_argument("--bodies", type=int, default=20000)
+    p.add_argument("--churn", type=int, default=200)
+    p.add_argument("--substeps", type=int, default=4)
+    p.add_argument("--roofline-kernel", default="kSolveFree")
+    p.add_argument("--cpu-baseline-seconds", type=float, default=15.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+class Dist:
+    def __init__(self, n):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg is not None:
+            self.pg.barrier()
+
+    def reduce(self, value, op):
+        if self.pg is None:
+            return value
+        import torch
+        t = torch.tensor([float(value)], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=getattr(self.pg.ReduceOp, op))
+        return float(t.item())
+
+    def close(self):
+        if self.pg is not None:
+            self.pg.destroy_process_group()
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu_index):
+        self.proc = None
+        self.index = gpu_index
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = max(mx, float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def flush_l2(buf):
+    buf.fill_(1.0)
+
+
+def run_reference_sample(steps, warmup, args, seconds_cap=None):
+    """The reference's CPU step on the same workload, all host threads."""
+    if not os.path.exists(REF_RELEASE_LIB):
+        return None, "oracle/_ref/libmelon3d_ref_fast.so not built"
+    lib = api.bind(C.CDLL(REF_RELEASE_LIB))
+    cores = os.cpu_count() or 1
+    sc = harness.Scene(lib, harness.RAIN, 2, args.bodies, args.churn, 0, workers=cores)
+    sc.run(warmup, args.substeps)
+    done, bs_total, wall_total = 0, 0, 0.0
+    while done < steps:
+        bs, wall, _ = sc.run(1, args.substeps)
+        bs_total += bs
+        wall_total += wall
+        done += 1
+        if seconds_cap is not None and wall_total > seconds_cap * 1000.0:
+            break
+    sc.close()
+    return {"value": bs_total / (wall_total / 1000.0), "unit": "body-substeps/s", "cores": cores,
+            "kind": "reference",
+            "sample": "%d steps (after %d warm-up) of the same workload, reference release build, "
+                      "workerCount=%d" % (done, warmup, cores), "ms_per_step": wall_total / max(done, 1)}, None
+
+
+def main():
+    args = parse()
+    d = Dist(args.gpus)
+    if args.impl == "reference":
+        if d.rank == 0:
+            res, why = run_reference_sample(args.steps, args.warmup, args)
+            if res is None:
+                print(json.dumps({"impl": "reference", "unavailable": why}))
+            else:
+                line = {"metric": "body-substeps/s", "value": res["value"], "unit": "body-substeps/s",
+                        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                        "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+                        "config": {"workload": WORKLOAD, "variant": "plain", "parallelism": "replicas"},
+                        "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                        "e2e": {"value": res["value"], "unit": "body-substeps/s", "h2d_bytes_per_step": 0,
+                                "d2h_bytes_per_step": 0}}
+                print(json.dumps(line))
+        d.barrier()
+        d.close()
+        return
+
+    import torch
+    torch.cuda.set_device(d.local)
+    lib = api.load_gpu()
+    scene = harness.Scene(lib, harness.RAIN, 2, args.bodies, args.churn, 0)
+    world = scene.world
+    scene.run(max(args.warmup, 3), args.substeps)
+    flush_buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB
+    counters = (C.c_uint32 * 64)()
+
+    clocks = Clocks(d.local)
+    d.barrier()
+    torch.cuda.synchronize()
+    lib.m3d_gpu_profiler_reset(args.roofline_kernel.encode())
+    clocks.start()
+    dev_ms = wall_ms = 0.0
+    body_substeps = 0
+    alg_bytes = 0.0
+    model = ROOFLINE_MODELS.get(args.roofline_kernel)
+    for _ in range(args.steps):
+        flush_l2(flush_buf)
+        torch.cuda.synchronize()
+        bs, wall, _ = scene.run(1, args.substeps)
+        dev_ms += lib.m3d_gpu_last_step_device_ms(world)
+        wall_ms += wall
+        body_substeps += bs
+        if model is not None:
+            n = lib.m3d_gpu_step_counters(world, counters, 64)
+            c = {name: counters[i] for i, name in enumerate(COUNTER_NAMES[:n])}
+            c["_contacts"] = lib.m3d_world_profile(world).contactCount
+            alg_bytes += model[1](c, args.substeps)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = lib.m3d_gpu_profiler_launches()
+    h2d, d2h = C.c_longlong(0), C.c_longlong(0)
+    lib.m3d_gpu_profiler_bytes(C.byref(h2d), C.byref(d2h))
+    kms, kl = C.c_float(0.0), C.c_int32(0)
+    lib.m3d_gpu_profiler_kernel(C.byref(kms), C.byref(kl))
+    status = lib.m3d_gpu_status(world)
+    d.barrier()
+    dev_ms_max = d.reduce(dev_ms, "MAX")
+    wall_ms_max = d.reduce(wall_ms, "MAX")
+    total_bs = d.reduce(body_substeps, "SUM")
+
+    cpu = None
+    if d.rank == 0 and d.world == 1 and not args.no_cpu_baseline:
+        cpu, _ = run_reference_sample(args.steps, args.warmup, args, seconds_cap=args.cpu_baseline_seconds)
+        if cpu is not None:
+            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    roof = None
+    if model is not None and kl.value > 0:
+        avg_s = kms.value / 1000.0 / kl.value
+        per_launch = alg_bytes / kl.value
+        achieved = per_launch / avg_s / 1e9
+        roof = {"bound": "hbm", "kernel": args.roofline_kernel, "achieved": achieved, "peak": hbm_peak,
+                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                "bytes_per_launch": per_launch, "avg_launch_us": avg_s * 1e6, "launches": kl.value,
+                "model": model[0], "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+    if d.rank == 0:
+        line = {"metric": "body-substeps/s", "value": total_bs / (dev_ms_max / 1000.0), "unit": "body-substeps/s",
+                "n_gpus": d.world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "variant": "plain", "bodies": args.bodies,
+                           "churn_per_step": args.churn, "substeps": args.substeps, "hz": 60,
+                           "l2": "flushed between timed steps (256 MiB write)",
+                           "parallelism": "replicas" if d.world > 1 else "single world"},
+                "e2e": {"value": total_bs / (wall_ms_max / 1000.0), "unit": "body-substeps/s",
+                        "h2d_bytes_per_step": h2d.value // max(args.steps, 1),
+                        "d2h_bytes_per_step": d2h.value // max(args.steps, 1),
+                        "ms_per_step": wall_ms_max / args.steps},
+                "roofline": roof, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk,
+                "status": status}
+        print(json.dumps(line))
+    scene.close()
+    d.barrier()
+    d.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -40,9 +40,28 @@ M3D_API void m3d_gpu_read_poses(m3d_world* world, float* positions, float* rotat
  * world's stream around the step's work, uploads included). */
 M3D_API float m3d_gpu_last_step_device_ms(m3d_world* world);
 
+/* Work counters of the last step, in this order: activeEntries,
+ * stableEntries, activeOversized, stableOversized, cellRuns, gridPairs,
+ * oversizedPairs, newContacts, removedContacts, removalEndEvents,
+ * beginEvents, endEvents, anyAwakeDynamic, islandCount, touchingContacts,
+ * awakeIslands, islandContacts, islandJoints, islandBodies, stableDirty,
+ * bodyCount, awakeBodyCount, hashFailures, colouredIslands, serialIslands,
+ * freeIslands.  Returns how many counters exist (writes at most capacity). */
+M3D_API int32_t m3d_gpu_step_counters(m3d_world* world, uint32_t* out, int32_t capacity);
+
 /* 0 when healthy, else the first M3D_GPU_ERR_* seen since creation. */
 M3D_API int32_t m3d_gpu_status(m3d_world* world);
 M3D_API const char* m3d_gpu_last_error_string(m3d_world* world);
+
+/* Launch accounting (process-wide).  Every kernel launch of the library is
+ * counted; the kernel named in m3d_gpu_profiler_reset (its source name, e.g.
+ * "kNarrowphase"; NULL for none) is also bracketed by CUDA events on its
+ * stream, so its average device duration can be read while the world runs. */
+M3D_API void m3d_gpu_profiler_reset(const char* kernelName);
+M3D_API long long m3d_gpu_profiler_launches(void);
+M3D_API void m3d_gpu_profiler_kernel(float* totalMs, int32_t* launches);
+/* Host->device and device->host bytes the library copied since the reset. */
+M3D_API void m3d_gpu_profiler_bytes(long long* h2d, long long* d2h);
 
 /* Snapshot records (melon3d_debug.h) — for tests and debugging. */
 M3D_API int32_t m3d_dbg_body_capacity(m3d_world* world);

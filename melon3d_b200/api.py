@@ -198,6 +198,11 @@ _GPU_PROTOS = {
     "m3d_gpu_last_step_device_ms": (C.c_float, [W]),
     "m3d_gpu_status": (C.c_int32, [W]),
     "m3d_gpu_last_error_string": (C.c_char_p, [W]),
+    "m3d_gpu_step_counters": (C.c_int32, [W, C.POINTER(C.c_uint32), C.c_int32]),
+    "m3d_gpu_profiler_reset": (None, [C.c_char_p]),
+    "m3d_gpu_profiler_launches": (C.c_longlong, []),
+    "m3d_gpu_profiler_kernel": (None, [C.POINTER(C.c_float), C.POINTER(C.c_int32)]),
+    "m3d_gpu_profiler_bytes": (None, [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
 }
 
 API_SYMBOLS = sorted(_PROTOS)

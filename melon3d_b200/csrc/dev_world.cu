@@ -226,7 +226,7 @@ void launchApplyUploads(DevWorld& w, const BodyUpload* hostRecs, int32_t count)
 	w.uploads.ensure(sizeof(BodyUpload) * (size_t)count);
 	w.matDirty.ensureZeroed((size_t)w.bodyCap, w.stream);
 	cudaMemcpyAsync(w.uploads.ptr, hostRecs, sizeof(BodyUpload) * (size_t)count, cudaMemcpyHostToDevice, w.stream);
-	kApplyUploads<<<blocksFor(count, 128), 128, 0, w.stream>>>(w.B, w.uploads.as<BodyUpload>(), count,
+	M3G_LAUNCH(kApplyUploads, blocksFor(count, 128), 128, w.stream, w.B, w.uploads.as<BodyUpload>(), count,
 																w.matDirty.as<uint8_t>());
 }
 
@@ -258,7 +258,7 @@ void launchMaterialRefresh(DevWorld& w)
 	w.matDirty.ensureZeroed((size_t)w.bodyCap, w.stream);
 	if (w.contactCount > 0)
 	{
-		kMaterialRefresh<<<blocksFor(w.contactCount, 256), 256, 0, w.stream>>>(w.B, w.C, w.contactCount,
+		M3G_LAUNCH(kMaterialRefresh, blocksFor(w.contactCount, 256), 256, w.stream, w.B, w.C, w.contactCount,
 																				 w.matDirty.as<uint8_t>());
 	}
 	cudaMemsetAsync(w.matDirty.ptr, 0, (size_t)w.bodyCap, w.stream);

@@ -172,7 +172,7 @@ void launchRefresh(DevWorld& w, int32_t n, float dt, bool rebuildStable, float c
 	{
 		return;
 	}
-	kRefresh<<<blocksFor(n, 256), 256, 0, w.stream>>>(w.B, n, dt, rebuildStable ? 1 : 0, inv,
+	M3G_LAUNCH(kRefresh, blocksFor(n, 256), 256, w.stream, w.B, n, dt, rebuildStable ? 1 : 0, inv,
 													   w.cellCountA.as<uint32_t>(), w.overFlagA.as<uint32_t>(),
 													   w.cellCountS.as<uint32_t>(), w.overFlagS.as<uint32_t>(),
 													   w.inActiveCells.as<uint8_t>());
@@ -240,9 +240,9 @@ static void buildTier(DevWorld& w, int32_t n, float inv, DevBuf& cnt, DevBuf& ov
 	overList.ensure((size_t)(ototal + 1) * sizeof(int32_t));
 	if (n > 0)
 	{
-		kEmitEntries<<<blocksFor(n, 128), 128, 0, w.stream>>>(w.B, n, inv, cnt.as<uint32_t>(), offs.as<uint32_t>(),
+		M3G_LAUNCH(kEmitEntries, blocksFor(n, 128), 128, w.stream, w.B, n, inv, cnt.as<uint32_t>(), offs.as<uint32_t>(),
 															   keys.as<uint64_t>(), vals.as<uint32_t>());
-		kCompactIndices<<<blocksFor(n, 256), 256, 0, w.stream>>>(over.as<uint32_t>(), ooffs.as<uint32_t>(), n,
+		M3G_LAUNCH(kCompactIndices, blocksFor(n, 256), 256, w.stream, over.as<uint32_t>(), ooffs.as<uint32_t>(), n,
 																  overList.as<int32_t>());
 	}
 	if (total > 1)
@@ -308,10 +308,10 @@ void launchFindRuns(DevWorld& w)
 		w.runCount = 0;
 		return;
 	}
-	kRunFlags<<<blocksFor(n, 256), 256, 0, w.stream>>>(w.activeKeys.as<uint64_t>(), n, w.runFlag.as<uint32_t>());
+	M3G_LAUNCH(kRunFlags, blocksFor(n, 256), 256, w.stream, w.activeKeys.as<uint64_t>(), n, w.runFlag.as<uint32_t>());
 	uint32_t* offs = w.runPairCount.as<uint32_t>();
 	scanExclusive(w.runFlag.as<uint32_t>(), offs, n, &dc->runs, w.prim, w.stream);
-	kRunStarts<<<blocksFor(n, 256), 256, 0, w.stream>>>(w.runFlag.as<uint32_t>(), offs, n, w.runStarts.as<int32_t>(),
+	M3G_LAUNCH(kRunStarts, blocksFor(n, 256), 256, w.stream, w.runFlag.as<uint32_t>(), offs, n, w.runStarts.as<int32_t>(),
 														 &dc->runs);
 	readCounters(w);
 	w.runCount = (int32_t)w.hostCounters->runs;
@@ -681,7 +681,7 @@ void launchPairs(DevWorld& w, int32_t n, float cellSize)
 	cudaMemsetAsync(w.existingSet.ptr, 0xFF, (size_t)ecap * sizeof(uint64_t), s);
 	if (w.contactCount > 0)
 	{
-		kInsertExisting<<<blocksFor(w.contactCount, 256), 256, 0, s>>>(w.C.bodies, w.contactCount,
+		M3G_LAUNCH(kInsertExisting, blocksFor(w.contactCount, 256), 256, s, w.C.bodies, w.contactCount,
 																		 w.existingSet.as<uint64_t>(), w.existingMask,
 																		 &dc->hashFail);
 	}
@@ -702,7 +702,7 @@ void launchPairs(DevWorld& w, int32_t n, float cellSize)
 	uint32_t* offs = w.keepFlag.as<uint32_t>();
 	if (runs > 0)
 	{
-		kRunPairs<false><<<blocksFor(runs, 128), 128, 0, s>>>(
+		M3G_LAUNCH(kRunPairs<false>, blocksFor(runs, 128), 128, s, 
 			P, w.activeKeys.as<uint64_t>(), w.activeVals.as<uint32_t>(), w.runStarts.as<int32_t>(), runs,
 			w.stableKeys.as<uint64_t>(), w.stableVals.as<uint32_t>(), w.stableEntries, counts, nullptr, nullptr);
 	}
@@ -722,7 +722,7 @@ void launchPairs(DevWorld& w, int32_t n, float cellSize)
 	w.newContactKeys.ensure((size_t)(overTotal + 1) * sizeof(uint64_t));
 	if (overTotal > 0)
 	{
-		kOverPairs<<<blocksFor(overTotal, 256), 256, 0, s>>>(P, O, overTotal, w.overFlag.as<uint32_t>(),
+		M3G_LAUNCH(kOverPairs, blocksFor(overTotal, 256), 256, s, P, O, overTotal, w.overFlag.as<uint32_t>(),
 															  w.newContactKeys.as<uint64_t>());
 	}
 	scanExclusive(w.overFlag.as<uint32_t>(), w.overScan.as<uint32_t>(), overTotal, &dc->overPairs, w.prim, s);
@@ -734,13 +734,13 @@ void launchPairs(DevWorld& w, int32_t n, float cellSize)
 	uint64_t* pk = w.pairKeys.as<uint64_t>();
 	if (runs > 0 && gridPairs > 0)
 	{
-		kRunPairs<true><<<blocksFor(runs, 128), 128, 0, s>>>(
+		M3G_LAUNCH(kRunPairs<true>, blocksFor(runs, 128), 128, s, 
 			P, w.activeKeys.as<uint64_t>(), w.activeVals.as<uint32_t>(), w.runStarts.as<int32_t>(), runs,
 			w.stableKeys.as<uint64_t>(), w.stableVals.as<uint32_t>(), w.stableEntries, nullptr, offs, pk);
 	}
 	if (overPairs > 0)
 	{
-		kScatterKeys<<<blocksFor(overTotal, 256), 256, 0, s>>>(w.overFlag.as<uint32_t>(), w.overScan.as<uint32_t>(),
+		M3G_LAUNCH(kScatterKeys, blocksFor(overTotal, 256), 256, s, w.overFlag.as<uint32_t>(), w.overScan.as<uint32_t>(),
 																w.newContactKeys.as<uint64_t>(), overTotal,
 																pk + gridPairs);
 	}
@@ -757,16 +757,16 @@ void launchPairs(DevWorld& w, int32_t n, float cellSize)
 	{
 		cudaMemsetAsync(w.newSet.ptr, 0xFF, (size_t)ncap * sizeof(uint64_t), s);
 		cudaMemsetAsync(w.newSetPos.ptr, 0xFF, (size_t)ncap * sizeof(uint32_t), s);
-		kDedupeMark<<<blocksFor(total, 256), 256, 0, s>>>(pk, total, w.newSet.as<uint64_t>(),
+		M3G_LAUNCH(kDedupeMark, blocksFor(total, 256), 256, s, pk, total, w.newSet.as<uint64_t>(),
 														   w.newSetPos.as<uint32_t>(), w.newMask, &dc->hashFail);
-		kDedupeKeep<<<blocksFor(total, 256), 256, 0, s>>>(pk, total, w.newSet.as<uint64_t>(),
+		M3G_LAUNCH(kDedupeKeep, blocksFor(total, 256), 256, s, pk, total, w.newSet.as<uint64_t>(),
 														   w.newSetPos.as<uint32_t>(), w.newMask,
 														   w.keepFlag.as<uint32_t>());
 	}
 	scanExclusive(w.keepFlag.as<uint32_t>(), w.overScan.as<uint32_t>(), total, &dc->newContacts, w.prim, s);
 	if (total > 0)
 	{
-		kScatterKeys<<<blocksFor(total, 256), 256, 0, s>>>(w.keepFlag.as<uint32_t>(), w.overScan.as<uint32_t>(), pk,
+		M3G_LAUNCH(kScatterKeys, blocksFor(total, 256), 256, s, w.keepFlag.as<uint32_t>(), w.overScan.as<uint32_t>(), pk,
 															total, w.newContactKeys.as<uint64_t>());
 	}
 	readCounters(w);
@@ -822,7 +822,7 @@ void launchCreateContacts(DevWorld& w, int32_t newCount)
 	{
 		return;
 	}
-	kCreateContacts<<<blocksFor(newCount, 128), 128, 0, w.stream>>>(w.B, w.C, w.newContactKeys.as<uint64_t>(),
+	M3G_LAUNCH(kCreateContacts, blocksFor(newCount, 128), 128, w.stream, w.B, w.C, w.newContactKeys.as<uint64_t>(),
 																	  newCount, w.contactCount);
 	w.contactCount += newCount;
 }
@@ -938,7 +938,7 @@ void launchContactMoves(DevWorld& w, const int2* hostMoves, int32_t count)
 	}
 	w.moveSrc.ensure(sizeof(int2) * (size_t)count);
 	cudaMemcpyAsync(w.moveSrc.ptr, hostMoves, sizeof(int2) * (size_t)count, cudaMemcpyHostToDevice, w.stream);
-	kContactMoves<<<blocksFor(count, 128), 128, 0, w.stream>>>(w.C, (const int2*)w.moveSrc.ptr, count);
+	M3G_LAUNCH(kContactMoves, blocksFor(count, 128), 128, w.stream, w.C, (const int2*)w.moveSrc.ptr, count);
 	cudaStreamSynchronize(w.stream); // the host vector backing hostMoves is freed on return
 }
 
@@ -961,13 +961,13 @@ void launchRemoval(DevWorld& w)
 		readCounters(w);
 		return;
 	}
-	kRemovalFlags<<<blocksFor(count, 256), 256, 0, s>>>(w.B, w.C, count, w.removeFlag.as<uint32_t>(),
+	M3G_LAUNCH(kRemovalFlags, blocksFor(count, 256), 256, s, w.B, w.C, count, w.removeFlag.as<uint32_t>(),
 														  w.evEndFlag.as<uint32_t>());
 	// the scan covers count + 1 entries so removeScan[count] exists
 	cudaMemsetAsync(w.removeFlag.as<uint32_t>() + count, 0, sizeof(uint32_t), s);
 	scanExclusive(w.removeFlag.as<uint32_t>(), w.removeScan.as<uint32_t>(), count + 1, &dc->removed, w.prim, s);
 	scanExclusive(w.evEndFlag.as<uint32_t>(), w.evBeginFlag.as<uint32_t>(), count, &dc->endRemoval, w.prim, s);
-	kRemovalEvents<<<blocksFor(count, 256), 256, 0, s>>>(w.C, count, w.evEndFlag.as<uint32_t>(),
+	M3G_LAUNCH(kRemovalEvents, blocksFor(count, 256), 256, s, w.C, count, w.evEndFlag.as<uint32_t>(),
 														   w.evBeginFlag.as<uint32_t>(), &dc->endRemoval,
 														   w.evRemoval.as<int4>());
 	readCounters(w);
@@ -975,11 +975,11 @@ void launchRemoval(DevWorld& w)
 	if (removed > 0)
 	{
 		int32_t S = count - removed;
-		kRemovalSources<<<blocksFor(removed, 256), 256, 0, s>>>(count, S, w.removeFlag.as<uint32_t>(),
+		M3G_LAUNCH(kRemovalSources, blocksFor(removed, 256), 256, s, count, S, w.removeFlag.as<uint32_t>(),
 																 w.removeScan.as<uint32_t>(), w.moveSrc.as<int32_t>());
 		if (S > 0)
 		{
-			kRemovalMoves<<<blocksFor(S, 256), 256, 0, s>>>(w.C, S, w.removeFlag.as<uint32_t>(),
+			M3G_LAUNCH(kRemovalMoves, blocksFor(S, 256), 256, s, w.C, S, w.removeFlag.as<uint32_t>(),
 															 w.removeScan.as<uint32_t>(), w.moveSrc.as<int32_t>());
 		}
 		w.contactCount = S;

@@ -30,7 +30,7 @@ void launchAnyAwakeDynamic(DevWorld& w, int32_t n)
 	cudaMemsetAsync(&dc->anyAwakeDynamic, 0, sizeof(uint32_t), w.stream);
 	if (n > 0)
 	{
-		kAnyAwakeDynamic<<<blocksFor(n, 256), 256, 0, w.stream>>>(w.B.bFlags, n, &dc->anyAwakeDynamic);
+		M3G_LAUNCH(kAnyAwakeDynamic, blocksFor(n, 256), 256, w.stream, w.B.bFlags, n, &dc->anyAwakeDynamic);
 	}
 }
 
@@ -330,7 +330,7 @@ static int32_t groupByLabel(DevWorld& w, int mode, int32_t count, DevBuf& flag, 
 	vals.ensure((size_t)(total + 1) * sizeof(uint32_t));
 	if (count > 0)
 	{
-		kLabelPairs<<<blocksFor(count, 256), 256, 0, w.stream>>>(
+		M3G_LAUNCH(kLabelPairs, blocksFor(count, 256), 256, w.stream, 
 			flag.as<uint32_t>(), offs.as<uint32_t>(), count, w.label.as<int32_t>(), w.C.bodies,
 			w.joints.as<JointRec>(), w.B.bFlags, w.B.cold, mode, keys.as<uint64_t>(), vals.as<uint32_t>());
 	}
@@ -353,36 +353,36 @@ void launchIslands(DevWorld& w, int32_t n)
 	w.islandFlag.ensure(n4);
 	w.cellCountA.ensure(n4); // reused: per-body solve flag
 	int32_t* parent = w.label.as<int32_t>();
-	kInitParent<<<blocksFor(n, 256), 256, 0, s>>>(parent, n);
+	M3G_LAUNCH(kInitParent, blocksFor(n, 256), 256, s, parent, n);
 	if (w.contactCount > 0)
 	{
-		kUnionContacts<<<blocksFor(w.contactCount, 256), 256, 0, s>>>(w.C, w.contactCount, w.B.bFlags, parent);
+		M3G_LAUNCH(kUnionContacts, blocksFor(w.contactCount, 256), 256, s, w.C, w.contactCount, w.B.bFlags, parent);
 	}
 	if (w.jointCount > 0)
 	{
-		kUnionJoints<<<blocksFor(w.jointCount, 128), 128, 0, s>>>(w.joints.as<JointRec>(), w.jointCount, w.B.cold,
+		M3G_LAUNCH(kUnionJoints, blocksFor(w.jointCount, 128), 128, s, w.joints.as<JointRec>(), w.jointCount, w.B.cold,
 																   parent);
 	}
 	cudaMemsetAsync(&dc->islandCount, 0, sizeof(uint32_t), s);
 	cudaMemsetAsync(&dc->touchingCount, 0, sizeof(uint32_t), s);
 	cudaMemsetAsync(&dc->coloredIslands, 0, 3 * sizeof(uint32_t), s);
-	kLabels<<<blocksFor(n, 256), 256, 0, s>>>(parent, n, w.B.bFlags, w.label.as<int32_t>(), w.islandFlag.as<uint32_t>(),
+	M3G_LAUNCH(kLabels, blocksFor(n, 256), 256, s, parent, n, w.B.bFlags, w.label.as<int32_t>(), w.islandFlag.as<uint32_t>(),
 											  &dc->islandCount);
-	kIslandAwake<<<blocksFor(n, 256), 256, 0, s>>>(w.B.bFlags, n, w.label.as<int32_t>(), w.islandFlag.as<uint32_t>());
-	kIslandWakeBodies<<<blocksFor(n, 256), 256, 0, s>>>(w.B, n, w.label.as<int32_t>(), w.islandFlag.as<uint32_t>(),
+	M3G_LAUNCH(kIslandAwake, blocksFor(n, 256), 256, s, w.B.bFlags, n, w.label.as<int32_t>(), w.islandFlag.as<uint32_t>());
+	M3G_LAUNCH(kIslandWakeBodies, blocksFor(n, 256), 256, s, w.B, n, w.label.as<int32_t>(), w.islandFlag.as<uint32_t>(),
 														 w.cellCountA.as<uint32_t>(), &dc->stableDirty);
 	int32_t cc = w.contactCount;
 	w.removeFlag.ensure((size_t)(cc + 1) * sizeof(uint32_t));
 	if (cc > 0)
 	{
-		kContactIslandFlags<<<blocksFor(cc, 256), 256, 0, s>>>(w.C, cc, w.B.bFlags, w.label.as<int32_t>(),
+		M3G_LAUNCH(kContactIslandFlags, blocksFor(cc, 256), 256, s, w.C, cc, w.B.bFlags, w.label.as<int32_t>(),
 																 w.islandFlag.as<uint32_t>(), w.removeFlag.as<uint32_t>(),
 																 &dc->touchingCount);
 	}
 	w.overFlagS.ensure((size_t)(w.jointCount + 1) * sizeof(uint32_t));
 	if (w.jointCount > 0)
 	{
-		kJointIslandFlags<<<blocksFor(w.jointCount, 128), 128, 0, s>>>(w.joints.as<JointRec>(), w.jointCount, w.B.cold,
+		M3G_LAUNCH(kJointIslandFlags, blocksFor(w.jointCount, 128), 128, s, w.joints.as<JointRec>(), w.jointCount, w.B.cold,
 																		w.label.as<int32_t>(),
 																		w.islandFlag.as<uint32_t>(),
 																		w.overFlagS.as<uint32_t>());
@@ -400,7 +400,7 @@ void launchIslands(DevWorld& w, int32_t n)
 	w.runPairCount.ensure((size_t)(nb + 1) * sizeof(uint32_t));
 	if (nb > 0)
 	{
-		kIslandStarts<<<blocksFor(nb, 256), 256, 0, s>>>(w.bodyKeys.as<uint64_t>(), nb,
+		M3G_LAUNCH(kIslandStarts, blocksFor(nb, 256), 256, s, w.bodyKeys.as<uint64_t>(), nb,
 														  w.islandStartFlag.as<uint32_t>());
 	}
 	scanExclusive(w.islandStartFlag.as<uint32_t>(), w.runPairCount.as<uint32_t>(), nb, &dc->awakeIslands, w.prim, s);
@@ -409,7 +409,7 @@ void launchIslands(DevWorld& w, int32_t n)
 	w.islands.ensure((size_t)(ni + 1) * sizeof(IslandRec));
 	if (nb > 0)
 	{
-		kIslandTable<<<blocksFor(nb, 256), 256, 0, s>>>(
+		M3G_LAUNCH(kIslandTable, blocksFor(nb, 256), 256, s, 
 			w.bodyKeys.as<uint64_t>(), nb, w.islandStartFlag.as<uint32_t>(), w.runPairCount.as<uint32_t>(),
 			w.contactKeys.as<uint64_t>(), nc, w.jointKeys.as<uint64_t>(), nj, w.islands.as<IslandRec>(), ni, dc);
 	}
@@ -518,13 +518,13 @@ void launchSleep(DevWorld& w, float dt)
 	w.sleepFirstNo.ensure(cap * sizeof(int32_t));
 	w.sleepMin.ensure(cap * sizeof(uint32_t));
 	cudaStream_t s = w.stream;
-	kSleepInit<<<blocksFor(ni, 256), 256, 0, s>>>(w.islands.as<IslandRec>(), ni, w.sleepFirstNo.as<int32_t>(),
+	M3G_LAUNCH(kSleepInit, blocksFor(ni, 256), 256, s, w.islands.as<IslandRec>(), ni, w.sleepFirstNo.as<int32_t>(),
 												   w.sleepMin.as<uint32_t>());
-	kSleepNoFlags<<<blocksFor(nb, 256), 256, 0, s>>>(w.B, w.bodyKeys.as<uint64_t>(), w.bodyVals.as<uint32_t>(), nb,
+	M3G_LAUNCH(kSleepNoFlags, blocksFor(nb, 256), 256, s, w.B, w.bodyKeys.as<uint64_t>(), w.bodyVals.as<uint32_t>(), nb,
 													  w.sleepFirstNo.as<int32_t>());
-	kSleepUpdate<<<blocksFor(nb, 256), 256, 0, s>>>(w.B, w.bodyKeys.as<uint64_t>(), w.bodyVals.as<uint32_t>(), nb,
+	M3G_LAUNCH(kSleepUpdate, blocksFor(nb, 256), 256, s, w.B, w.bodyKeys.as<uint64_t>(), w.bodyVals.as<uint32_t>(), nb,
 													 w.sleepFirstNo.as<int32_t>(), w.sleepMin.as<uint32_t>(), dt);
-	kSleepApply<<<blocksFor(nb, 256), 256, 0, s>>>(w.B, w.bodyKeys.as<uint64_t>(), w.bodyVals.as<uint32_t>(), nb,
+	M3G_LAUNCH(kSleepApply, blocksFor(nb, 256), 256, s, w.B, w.bodyKeys.as<uint64_t>(), w.bodyVals.as<uint32_t>(), nb,
 													w.sleepFirstNo.as<int32_t>(), w.sleepMin.as<uint32_t>(),
 													&dc->stableDirty);
 }
@@ -568,7 +568,7 @@ void launchFinish(DevWorld& w, int32_t n, float dt, bool clearForces)
 	cudaMemsetAsync(&dc->bodyCount, 0, 2 * sizeof(uint32_t), w.stream);
 	if (n > 0)
 	{
-		kFinish<<<blocksFor(n, 256), 256, 0, w.stream>>>(w.B, n, dt, clearForces ? 1 : 0, dc);
+		M3G_LAUNCH(kFinish, blocksFor(n, 256), 256, w.stream, w.B, n, dt, clearForces ? 1 : 0, dc);
 	}
 }
 

@@ -160,18 +160,18 @@ void launchNarrowphase(DevWorld& w, float dt)
 		return;
 	}
 	int8_t* tr = w.transition.as<int8_t>();
-	kNarrowphase<<<blocksFor(count, 128), 128, 0, s>>>(w.B, w.C, count, dt, tr);
-	kTransitionFlags<<<blocksFor(count, 256), 256, 0, s>>>(tr, count, w.evBeginFlag.as<uint32_t>(),
+	M3G_LAUNCH(kNarrowphase, blocksFor(count, 128), 128, s, w.B, w.C, count, dt, tr);
+	M3G_LAUNCH(kTransitionFlags, blocksFor(count, 256), 256, s, tr, count, w.evBeginFlag.as<uint32_t>(),
 															 w.evEndFlag.as<uint32_t>());
 	uint32_t* beginScan = w.removeScan.as<uint32_t>();
 	uint32_t* endScan = (uint32_t*)w.moveSrc.ptr;
 	scanExclusive(w.evBeginFlag.as<uint32_t>(), beginScan, count, &dc->beginNP, w.prim, s);
 	scanExclusive(w.evEndFlag.as<uint32_t>(), endScan, count, &dc->endNP, w.prim, s);
-	kTransitionEvents<<<blocksFor(count, 256), 256, 0, s>>>(w.C, count, tr, beginScan, endScan, w.evBegin.as<int4>(),
+	M3G_LAUNCH(kTransitionEvents, blocksFor(count, 256), 256, s, w.C, count, tr, beginScan, endScan, w.evBegin.as<int4>(),
 															  w.evEnd.as<int4>());
 	int32_t* target = (int32_t*)w.evBeginFlag.ptr; // flags no longer needed
-	kWakeDecide<<<blocksFor(count, 256), 256, 0, s>>>(w.B, w.C, count, tr, target);
-	kWakeApply<<<blocksFor(count, 256), 256, 0, s>>>(w.B, count, target, &dc->stableDirty);
+	M3G_LAUNCH(kWakeDecide, blocksFor(count, 256), 256, s, w.B, w.C, count, tr, target);
+	M3G_LAUNCH(kWakeApply, blocksFor(count, 256), 256, s, w.B, count, target, &dc->stableDirty);
 }
 
 } // namespace m3g

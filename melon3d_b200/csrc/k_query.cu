@@ -160,7 +160,7 @@ void launchRayCast(DevWorld& w, int32_t n, V3 origin, V3 translation, uint32_t m
 	cudaMemsetAsync(w.colorMask.ptr, 0, (size_t)(w.bodyCap + 1) * sizeof(uint32_t), w.stream);
 	stampCounter = 1;
 	(void)n;
-	kRayCast<<<1, 1, 0, w.stream>>>(w.B, w.activeKeys.as<uint64_t>(), w.activeVals.as<uint32_t>(), w.activeEntries,
+	M3G_LAUNCH(kRayCast, 1, 1, w.stream, w.B, w.activeKeys.as<uint64_t>(), w.activeVals.as<uint32_t>(), w.activeEntries,
 									 w.stableKeys.as<uint64_t>(), w.stableVals.as<uint32_t>(), w.stableEntries,
 									 w.activeOver.as<int32_t>(), w.activeOverCount, w.stableOver.as<int32_t>(),
 									 w.stableOverCount, w.colorMask.as<uint32_t>(), stampCounter, maskBits, origin,
@@ -401,9 +401,9 @@ void launchSphereCast(DevWorld& w, int32_t n, V3 origin, float radius, V3 transl
 	cudaMemsetAsync(keys, 0xFF, 2 * sizeof(unsigned long long), w.stream);
 	if (n > 0)
 	{
-		kSphereCast<<<blocksFor(n, 128), 128, 0, w.stream>>>(w.B, n, origin, radius, translation, maskBits, recs, keys);
+		M3G_LAUNCH(kSphereCast, blocksFor(n, 128), 128, w.stream, w.B, n, origin, radius, translation, maskBits, recs, keys);
 	}
-	kSphereCastPick<<<1, 1, 0, w.stream>>>(recs, keys, origin, translation, out);
+	M3G_LAUNCH(kSphereCastPick, 1, 1, w.stream, recs, keys, origin, translation, out);
 	cudaMemcpyAsync(hostOut, out, sizeof(RayQueryOut), cudaMemcpyDeviceToHost, w.stream);
 	cudaStreamSynchronize(w.stream);
 }
@@ -430,7 +430,7 @@ void launchOverlap(DevWorld& w, int32_t n, Box box, uint8_t* hostFlags)
 		return;
 	}
 	w.queryOut.ensure((size_t)n + 64);
-	kOverlap<<<blocksFor(n, 256), 256, 0, w.stream>>>(w.B, n, box, w.queryOut.as<uint8_t>());
+	M3G_LAUNCH(kOverlap, blocksFor(n, 256), 256, w.stream, w.B, n, box, w.queryOut.as<uint8_t>());
 	cudaMemcpyAsync(hostFlags, w.queryOut.ptr, (size_t)n, cudaMemcpyDeviceToHost, w.stream);
 	cudaStreamSynchronize(w.stream);
 }

@@ -398,11 +398,11 @@ void launchSolve(DevWorld& w, float dt, int substeps, V3 gravity, int positionIt
 	const StepCounters* hc = w.hostCounters;
 	if (hc->freeIslands > 0)
 	{
-		kSolveFree<<<blocksFor(ni, 128), 128, 0, s>>>(w.B, isl, ni, w.bodyVals.as<uint32_t>(), P);
+		M3G_LAUNCH(kSolveFree, blocksFor(ni, 128), 128, s, w.B, isl, ni, w.bodyVals.as<uint32_t>(), P);
 	}
 	if (hc->serialIslands > 0)
 	{
-		kSolveSerial<<<blocksFor(ni, 64), 64, 0, s>>>(w.B, w.C, w.joints.as<JointRec>(), isl, ni,
+		M3G_LAUNCH(kSolveSerial, blocksFor(ni, 64), 64, s, w.B, w.C, w.joints.as<JointRec>(), isl, ni,
 													   w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(),
 													   w.jointVals.as<uint32_t>(), P);
 	}
@@ -412,7 +412,7 @@ void launchSolve(DevWorld& w, float dt, int substeps, V3 gravity, int positionIt
 		w.colorMask.ensure((size_t)(w.bodyCap + 1) * sizeof(uint32_t));
 		w.colorOrder.ensure(nc * sizeof(int32_t));
 		w.packetMax.ensure(nc * sizeof(int32_t));
-		kSolveColored<<<ni, kColorThreads, 0, s>>>(w.B, w.C, w.joints.as<JointRec>(), isl, ni, w.bodyVals.as<uint32_t>(),
+		M3G_LAUNCH(kSolveColored, ni, kColorThreads, s, w.B, w.C, w.joints.as<JointRec>(), isl, ni, w.bodyVals.as<uint32_t>(),
 													w.contactVals.as<uint32_t>(), w.jointVals.as<uint32_t>(),
 													w.colorMask.as<uint32_t>(), w.colorOrder.as<int32_t>(),
 													w.packetMax.as<int32_t>(), w.contactColor.as<int32_t>(), P);

@@ -1,10 +1,112 @@
-// Exclusive scan, stable LSD radix sort and key-range reduction.
+// Exclusive scan, stable LSD radix sort and key-range reduction; the launch
+// accounting behind M3G_LAUNCH.
 #include "prims.cuh"
 
+#include <atomic>
+#include <mutex>
 #include <stdio.h>
+#include <string>
+#include <utility>
+#include <vector>
 
 namespace m3g
 {
+
+// ---- launch accounting --------------------------------------------------------
+
+namespace
+{
+std::atomic<long long> gLaunches{ 0 };
+std::mutex gMu;
+std::string gTarget;
+std::vector<cudaEvent_t> gPool;
+std::vector<std::pair<cudaEvent_t, cudaEvent_t>> gPairs;
+cudaEvent_t gOpen = nullptr;
+double gTimedMs = 0.0;
+long long gTimedLaunches = 0;
+
+cudaEvent_t takeEvent()
+{
+	if (!gPool.empty())
+	{
+		cudaEvent_t e = gPool.back();
+		gPool.pop_back();
+		return e;
+	}
+	cudaEvent_t e = nullptr;
+	cudaEventCreate(&e);
+	return e;
+}
+
+// fold finished event pairs into the running total (caller holds gMu)
+void drainPairs()
+{
+	for (auto& p : gPairs)
+	{
+		float ms = 0.0f;
+		cudaEventSynchronize(p.second);
+		cudaEventElapsedTime(&ms, p.first, p.second);
+		gTimedMs += ms;
+		++gTimedLaunches;
+		gPool.push_back(p.first);
+		gPool.push_back(p.second);
+	}
+	gPairs.clear();
+}
+} // namespace
+
+namespace
+{
+std::atomic<long long> gH2D{ 0 }, gD2H{ 0 };
+}
+
+cudaError_t countedMemcpyAsync(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s)
+{
+	if (kind == cudaMemcpyHostToDevice)
+	{
+		gH2D.fetch_add((long long)bytes, std::memory_order_relaxed);
+	}
+	else if (kind == cudaMemcpyDeviceToHost)
+	{
+		gD2H.fetch_add((long long)bytes, std::memory_order_relaxed);
+	}
+	return (cudaMemcpyAsync)(dst, src, bytes, kind, s);
+}
+
+void launchBegin(const char* name, cudaStream_t s)
+{
+	gLaunches.fetch_add(1, std::memory_order_relaxed);
+	if (gTarget.empty())
+	{
+		return;
+	}
+	std::lock_guard<std::mutex> lock(gMu);
+	if (gTarget == name)
+	{
+		gOpen = takeEvent();
+		cudaEventRecord(gOpen, s);
+	}
+}
+
+void launchEnd(const char* name, cudaStream_t s)
+{
+	if (gTarget.empty())
+	{
+		return;
+	}
+	std::lock_guard<std::mutex> lock(gMu);
+	if (gOpen != nullptr && gTarget == name)
+	{
+		cudaEvent_t stop = takeEvent();
+		cudaEventRecord(stop, s);
+		gPairs.emplace_back(gOpen, stop);
+		gOpen = nullptr;
+		if (gPairs.size() >= 4096)
+		{
+			drainPairs();
+		}
+	}
+}
 
 bool DevBuf::ensure(size_t need)
 {
@@ -178,14 +280,14 @@ static void scanLevel(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* to
 	int64_t tiles = (n + kScanTile - 1) / kScanTile;
 	if (tiles <= 1)
 	{
-		kScanTiles<<<1, kScanThreads, 0, stream>>>(in, out, n, total);
+		M3G_LAUNCH(kScanTiles, 1, kScanThreads, stream, in, out, n, total);
 		return;
 	}
 	levels[level].ensure((size_t)tiles * sizeof(uint32_t));
 	uint32_t* sums = levels[level].as<uint32_t>();
-	kScanTiles<<<(unsigned)tiles, kScanThreads, 0, stream>>>(in, out, n, sums);
+	M3G_LAUNCH(kScanTiles, (unsigned)tiles, kScanThreads, stream, in, out, n, sums);
 	scanLevel(sums, sums, tiles, total, levels, level + 1, stream);
-	kScanAdd<<<(unsigned)tiles, kScanThreads, 0, stream>>>(out, n, sums);
+	M3G_LAUNCH(kScanAdd, (unsigned)tiles, kScanThreads, stream, out, n, sums);
 }
 
 void scanExclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total, PrimScratch& s,
@@ -347,9 +449,9 @@ void radixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, uint64_t varyMask
 		{
 			continue;
 		}
-		kSortHistogram<<<tiles, kSortThreads, 0, stream>>>(k0, n, shift, counts, tiles);
+		M3G_LAUNCH(kSortHistogram, tiles, kSortThreads, stream, k0, n, shift, counts, tiles);
 		scanExclusive(counts, counts, (int64_t)kRadix * tiles, nullptr, s, stream);
-		kSortScatter<<<tiles, kSortThreads, 0, stream>>>(k0, v0, k1, v1, n, shift, counts, tiles);
+		M3G_LAUNCH(kSortScatter, tiles, kSortThreads, stream, k0, v0, k1, v1, n, shift, counts, tiles);
 		uint64_t* tk = k0;
 		k0 = k1;
 		k1 = tk;
@@ -360,7 +462,7 @@ void radixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, uint64_t varyMask
 	}
 	if (passes & 1)
 	{
-		kCopyPairs<<<blocksFor(n, 256), 256, 0, stream>>>(k0, v0, keys, vals, n);
+		M3G_LAUNCH(kCopyPairs, blocksFor(n, 256), 256, stream, k0, v0, keys, vals, n);
 	}
 }
 
@@ -398,14 +500,65 @@ void reduceKeyRange(const uint64_t* keys, int64_t n, PrimScratch& s, cudaStream_
 	{
 		cudaMallocHost((void**)&s.hostReduce, 2 * sizeof(uint64_t));
 	}
-	kReduceInit<<<1, 1, 0, stream>>>(s.reduce.as<uint64_t>());
+	M3G_LAUNCH(kReduceInit, 1, 1, stream, s.reduce.as<uint64_t>());
 	if (n > 0)
 	{
 		int blocks = blocksFor(n, 256);
 		blocks = blocks > 1184 ? 1184 : blocks;
-		kReduceKeys<<<blocks, 256, 0, stream>>>(keys, n, s.reduce.as<uint64_t>());
+		M3G_LAUNCH(kReduceKeys, blocks, 256, stream, keys, n, s.reduce.as<uint64_t>());
 	}
 	cudaMemcpyAsync(s.hostReduce, s.reduce.ptr, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream);
 }
 
 } // namespace m3g
+
+extern "C"
+{
+
+// Select the kernel to time ("" or NULL: none) and zero the counters.
+void m3d_gpu_profiler_reset(const char* kernelName)
+{
+	std::lock_guard<std::mutex> lock(m3g::gMu);
+	m3g::drainPairs();
+	m3g::gTarget = kernelName != nullptr ? kernelName : "";
+	m3g::gTimedMs = 0.0;
+	m3g::gTimedLaunches = 0;
+	m3g::gOpen = nullptr;
+	m3g::gLaunches.store(0);
+	m3g::gH2D.store(0);
+	m3g::gD2H.store(0);
+}
+
+// Host->device and device->host bytes copied by the library since the last reset.
+void m3d_gpu_profiler_bytes(long long* h2d, long long* d2h)
+{
+	if (h2d != nullptr)
+	{
+		*h2d = m3g::gH2D.load();
+	}
+	if (d2h != nullptr)
+	{
+		*d2h = m3g::gD2H.load();
+	}
+}
+
+// Kernel launches of the library since the last reset (all kernels).
+long long m3d_gpu_profiler_launches(void) { return m3g::gLaunches.load(); }
+
+// Total device time (ms) and launch count of the selected kernel since the
+// last reset, from CUDA events recorded around each of its launches.
+void m3d_gpu_profiler_kernel(float* totalMs, int32_t* launches)
+{
+	std::lock_guard<std::mutex> lock(m3g::gMu);
+	m3g::drainPairs();
+	if (totalMs != nullptr)
+	{
+		*totalMs = (float)m3g::gTimedMs;
+	}
+	if (launches != nullptr)
+	{
+		*launches = (int32_t)m3g::gTimedLaunches;
+	}
+}
+
+} // extern "C"

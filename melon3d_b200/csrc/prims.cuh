@@ -109,4 +109,25 @@ inline int blocksFor(int64_t n, int threads)
 	return (int)(b < 1 ? 1 : b);
 }
 
+// Launch accounting: every kernel launch of the library goes through
+// M3G_LAUNCH, which counts it and, when the kernel's name is the one selected
+// with m3d_gpu_profiler_reset, brackets it with CUDA events on its stream.
+void launchBegin(const char* name, cudaStream_t s);
+void launchEnd(const char* name, cudaStream_t s);
+
+// Every async copy of the library goes through this wrapper (see the macro
+// below), which adds host->device and device->host bytes to the counters
+// read by m3d_gpu_profiler_bytes.
+cudaError_t countedMemcpyAsync(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s);
+
 } // namespace m3g
+
+#define cudaMemcpyAsync(...) ::m3g::countedMemcpyAsync(__VA_ARGS__)
+
+#define M3G_LAUNCH(kern, grid, block, stream, ...)                                                                     \
+	do                                                                                                                 \
+	{                                                                                                                  \
+		::m3g::launchBegin(#kern, (stream));                                                                          \
+		kern<<<(grid), (block), 0, (stream)>>>(__VA_ARGS__);                                                           \
+		::m3g::launchEnd(#kern, (stream));                                                                            \
+	} while (0)

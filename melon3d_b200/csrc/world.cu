@@ -1472,6 +1472,17 @@ void m3d_gpu_read_poses(m3d_world* world, float* positions, float* rotations, in
 }
 
 float m3d_gpu_last_step_device_ms(m3d_world* world) { return world->lastDeviceMs; }
+
+int32_t m3d_gpu_step_counters(m3d_world* world, uint32_t* out, int32_t capacity)
+{
+	const int32_t n = (int32_t)(sizeof(StepCounters) / sizeof(uint32_t));
+	const uint32_t* src = (const uint32_t*)world->dev.hostCounters;
+	for (int32_t i = 0; i < n && i < capacity && src != nullptr; ++i)
+	{
+		out[i] = src[i];
+	}
+	return n;
+}
 int32_t m3d_gpu_status(m3d_world* world) { return world->status; }
 const char* m3d_gpu_last_error_string(m3d_world* world) { return world->errorText; }
 

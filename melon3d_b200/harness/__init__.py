@@ -38,7 +38,7 @@ def _load():
         build()
         _lib = C.CDLL(LIB)
         _lib.scn_create.restype = C.c_void_p
-        _lib.scn_create.argtypes = [C.POINTER(M3dApi), C.c_int, C.c_uint64, C.c_int, C.c_int, C.c_int]
+        _lib.scn_create.argtypes = [C.POINTER(M3dApi), C.c_int, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_int]
         _lib.scn_world.restype = C.c_void_p
         _lib.scn_world.argtypes = [C.c_void_p]
         _lib.scn_dynamic_count.restype = C.c_int32
@@ -70,11 +70,11 @@ def api_table(lib):
 class Scene:
     """A seeded scene in a world of `lib` (a library bound with api.bind)."""
 
-    def __init__(self, lib, kind, seed=1, a=0, b=0, c=0):
+    def __init__(self, lib, kind, seed=1, a=0, b=0, c=0, workers=0):
         self.lib = lib
         self.sl = _load()
         self.table = api_table(lib)
-        self.handle = self.sl.scn_create(C.byref(self.table), kind, seed, a, b, c)
+        self.handle = self.sl.scn_create(C.byref(self.table), kind, seed, a, b, c, workers)
         if not self.handle:
             raise RuntimeError("world creation failed")
         self.world = self.sl.scn_world(self.handle)

@@ -225,13 +225,17 @@ extern "C"
 
 // kind / params: see the file header.  a,b,c = pyramid base | rain count,
 // churn | pile nx,ny,nz.
-void* scn_create(const M3dApi* api, int kind, uint64_t seed, int a, int b, int c)
+void* scn_create(const M3dApi* api, int kind, uint64_t seed, int a, int b, int c, int workers)
 {
 	Scene* s = new Scene();
 	s->api = *api;
 	s->kind = kind;
 	s->rng.s = seed;
 	m3d_world_def wd = s->api.world_def_default();
+	if (workers > 0)
+	{
+		wd.workerCount = workers; // the reference's thread pool; the GPU world ignores it
+	}
 	s->world = s->api.world_create(&wd);
 	if (s->world == nullptr)
 	{
