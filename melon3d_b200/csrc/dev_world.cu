@@ -150,6 +150,10 @@ StepCounters* devCounters(DevWorld& w)
 	return w.counters.as<StepCounters>();
 }
 
+__global__ void kSetU32(uint32_t* p, uint32_t v) { *p = v; }
+
+void setDeviceCount(DevWorld& w, uint32_t* p, uint32_t v) { M3G_LAUNCH(kSetU32, 1, 1, w.stream, p, v); }
+
 void readCounters(DevWorld& w)
 {
 	devCounters(w);

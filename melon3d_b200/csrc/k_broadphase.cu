@@ -184,28 +184,42 @@ void launchRefresh(DevWorld& w, int32_t n, float dt, bool rebuildStable, float c
 // ---------------------------------------------------------------------------
 
 __global__ void kEmitEntries(BodySoA B, int32_t n, float inv, const uint32_t* cnt, const uint32_t* offs,
-							 uint64_t* keys, uint32_t* vals)
+							 uint64_t* keys, uint32_t* vals, unsigned long long* masks)
 {
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= n || cnt[i] == 0)
+	uint64_t kor = 0ull, kand = ~0ull;
+	if (i < n && cnt[i] != 0)
 	{
-		return;
-	}
-	Box b = loadFat(B, i);
-	int64_t x0 = cellCoord(b.lo.x, inv), y0 = cellCoord(b.lo.y, inv), z0 = cellCoord(b.lo.z, inv);
-	int64_t x1 = cellCoord(b.hi.x, inv), y1 = cellCoord(b.hi.y, inv), z1 = cellCoord(b.hi.z, inv);
-	uint32_t o = offs[i];
-	for (int64_t x = x0; x <= x1; ++x)
-	{
-		for (int64_t y = y0; y <= y1; ++y)
+		Box b = loadFat(B, i);
+		int64_t x0 = cellCoord(b.lo.x, inv), y0 = cellCoord(b.lo.y, inv), z0 = cellCoord(b.lo.z, inv);
+		int64_t x1 = cellCoord(b.hi.x, inv), y1 = cellCoord(b.hi.y, inv), z1 = cellCoord(b.hi.z, inv);
+		uint32_t o = offs[i];
+		for (int64_t x = x0; x <= x1; ++x)
 		{
-			for (int64_t z = z0; z <= z1; ++z)
+			for (int64_t y = y0; y <= y1; ++y)
 			{
-				keys[o] = packCell(x, y, z);
-				vals[o] = (uint32_t)i;
-				++o;
+				for (int64_t z = z0; z <= z1; ++z)
+				{
+					uint64_t k = packCell(x, y, z);
+					keys[o] = k;
+					vals[o] = (uint32_t)i;
+					kor |= k;
+					kand &= k;
+					++o;
+				}
 			}
 		}
+	}
+	// key bits that vary across the tier decide which radix passes run
+	for (int off = 16; off > 0; off >>= 1)
+	{
+		kor |= __shfl_xor_sync(0xffffffffu, kor, off);
+		kand &= __shfl_xor_sync(0xffffffffu, kand, off);
+	}
+	if ((threadIdx.x & 31) == 0)
+	{
+		atomicOr(&masks[0], (unsigned long long)kor);
+		atomicAnd(&masks[1], (unsigned long long)kand);
 	}
 }
 
@@ -218,56 +232,80 @@ __global__ void kCompactIndices(const uint32_t* flags, const uint32_t* offs, int
 	}
 }
 
-// One tier: counts -> offsets -> entries -> sort; oversized list in body order.
-static void buildTier(DevWorld& w, int32_t n, float inv, DevBuf& cnt, DevBuf& over, DevBuf& keys, DevBuf& vals,
-					  DevBuf& overList, uint32_t* entryTotal, uint32_t* overTotal, int64_t& entriesOut,
-					  int32_t& overCountOut)
+__global__ void kInitMasks(unsigned long long* masks)
 {
-	StepCounters* dc = devCounters(w);
-	DevBuf& offs = w.runFlag; // scratch reuse: offsets of this tier
+	masks[0] = 0ull;
+	masks[1] = ~0ull;
+	masks[2] = 0ull;
+	masks[3] = ~0ull;
+}
+
+// One tier: counts -> offsets -> (key, body) entries in body order and the
+// oversized list.  Entry buffers are sized by the bound of 64 cells per body,
+// so nothing waits for the host; the sort runs after the step's first sync.
+static void emitTier(DevWorld& w, int32_t n, float inv, DevBuf& cnt, DevBuf& over, DevBuf& offs, DevBuf& ooffs,
+					 DevBuf& keys, DevBuf& vals, DevBuf& overList, uint32_t* entryTotal, uint32_t* overTotal,
+					 unsigned long long* masks)
+{
+	size_t bound = (size_t)n * kOversizedCellSpan + 1;
 	offs.ensure((size_t)(n + 1) * sizeof(uint32_t));
-	DevBuf& ooffs = w.runPairCount;
 	ooffs.ensure((size_t)(n + 1) * sizeof(uint32_t));
+	keys.ensure(bound * sizeof(uint64_t));
+	vals.ensure(bound * sizeof(uint32_t));
+	overList.ensure((size_t)(n + 1) * sizeof(int32_t));
 	scanExclusive(cnt.as<uint32_t>(), offs.as<uint32_t>(), n, entryTotal, w.prim, w.stream);
 	scanExclusive(over.as<uint32_t>(), ooffs.as<uint32_t>(), n, overTotal, w.prim, w.stream);
-	(void)dc;
-	readCounters(w);
-	int64_t total = entryTotal == &dc->activeEntries ? w.hostCounters->activeEntries : w.hostCounters->stableEntries;
-	int32_t ototal =
-		(int32_t)(overTotal == &dc->activeOversized ? w.hostCounters->activeOversized : w.hostCounters->stableOversized);
-	keys.ensure((size_t)(total + 1) * sizeof(uint64_t));
-	vals.ensure((size_t)(total + 1) * sizeof(uint32_t));
-	overList.ensure((size_t)(ototal + 1) * sizeof(int32_t));
 	if (n > 0)
 	{
 		M3G_LAUNCH(kEmitEntries, blocksFor(n, 128), 128, w.stream, w.B, n, inv, cnt.as<uint32_t>(), offs.as<uint32_t>(),
-															   keys.as<uint64_t>(), vals.as<uint32_t>());
+				   keys.as<uint64_t>(), vals.as<uint32_t>(), masks);
 		M3G_LAUNCH(kCompactIndices, blocksFor(n, 256), 256, w.stream, over.as<uint32_t>(), ooffs.as<uint32_t>(), n,
-																  overList.as<int32_t>());
+				   overList.as<int32_t>());
 	}
-	if (total > 1)
+}
+
+void launchEmitGrid(DevWorld& w, int32_t n, float cellSize, bool rebuildStable)
+{
+	StepCounters* dc = devCounters(w);
+	w.keyMasks.ensure(4 * sizeof(unsigned long long));
+	unsigned long long* masks = w.keyMasks.as<unsigned long long>();
+	M3G_LAUNCH(kInitMasks, 1, 1, w.stream, masks);
+	float inv = 1.0f / cellSize;
+	emitTier(w, n, inv, w.cellCountA, w.overFlagA, w.entryOffsA, w.overOffsA, w.activeKeys, w.activeVals, w.activeOver,
+			 &dc->activeEntries, &dc->activeOversized, masks);
+	if (rebuildStable)
 	{
-		reduceKeyRange(keys.as<uint64_t>(), total, w.prim, w.stream);
-		cudaStreamSynchronize(w.stream);
-		uint64_t vary = w.prim.hostReduce[0] ^ w.prim.hostReduce[1];
-		radixSortPairs(keys.as<uint64_t>(), vals.as<uint32_t>(), total, vary, w.prim, w.stream);
+		emitTier(w, n, inv, w.cellCountS, w.overFlagS, w.entryOffsS, w.overOffsS, w.stableKeys, w.stableVals,
+				 w.stableOver, &dc->stableEntries, &dc->stableOversized, masks + 2);
 	}
-	entriesOut = total;
-	overCountOut = ototal;
+	if (w.hostMasks == nullptr)
+	{
+		cudaMallocHost((void**)&w.hostMasks, 4 * sizeof(unsigned long long));
+	}
+	cudaMemcpyAsync(w.hostMasks, masks, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, w.stream);
 }
 
-void launchBuildActiveGrid(DevWorld& w, int32_t n, float cellSize)
+// after the first sync of the step: sizes and key masks are on the host
+void launchSortGrid(DevWorld& w, bool rebuildStable)
 {
-	StepCounters* dc = devCounters(w);
-	buildTier(w, n, 1.0f / cellSize, w.cellCountA, w.overFlagA, w.activeKeys, w.activeVals, w.activeOver,
-			  &dc->activeEntries, &dc->activeOversized, w.activeEntries, w.activeOverCount);
-}
-
-void launchBuildStableGrid(DevWorld& w, int32_t n, float cellSize)
-{
-	StepCounters* dc = devCounters(w);
-	buildTier(w, n, 1.0f / cellSize, w.cellCountS, w.overFlagS, w.stableKeys, w.stableVals, w.stableOver,
-			  &dc->stableEntries, &dc->stableOversized, w.stableEntries, w.stableOverCount);
+	const StepCounters* hc = w.hostCounters;
+	w.activeEntries = hc->activeEntries;
+	w.activeOverCount = (int32_t)hc->activeOversized;
+	if (w.activeEntries > 1)
+	{
+		radixSortPairs(w.activeKeys.as<uint64_t>(), w.activeVals.as<uint32_t>(), w.activeEntries,
+					   w.hostMasks[0] ^ w.hostMasks[1], w.prim, w.stream);
+	}
+	if (rebuildStable)
+	{
+		w.stableEntries = hc->stableEntries;
+		w.stableOverCount = (int32_t)hc->stableOversized;
+		if (w.stableEntries > 1)
+		{
+			radixSortPairs(w.stableKeys.as<uint64_t>(), w.stableVals.as<uint32_t>(), w.stableEntries,
+						   w.hostMasks[2] ^ w.hostMasks[3], w.prim, w.stream);
+		}
+	}
 }
 
 // ---------------------------------------------------------------------------
@@ -301,20 +339,19 @@ void launchFindRuns(DevWorld& w)
 	StepCounters* dc = devCounters(w);
 	int64_t n = w.activeEntries;
 	w.runFlag.ensure((size_t)(n + 1) * sizeof(uint32_t));
-	w.runPairCount.ensure((size_t)(n + 1) * sizeof(uint32_t));
+	w.runOffs.ensure((size_t)(n + 1) * sizeof(uint32_t));
 	w.runStarts.ensure((size_t)(n + 2) * sizeof(int32_t));
+	w.runCount = (int32_t)n; // upper bound; the exact count stays on the device
 	if (n <= 0)
 	{
-		w.runCount = 0;
+		cudaMemsetAsync(&dc->runs, 0, sizeof(uint32_t), w.stream);
 		return;
 	}
 	M3G_LAUNCH(kRunFlags, blocksFor(n, 256), 256, w.stream, w.activeKeys.as<uint64_t>(), n, w.runFlag.as<uint32_t>());
-	uint32_t* offs = w.runPairCount.as<uint32_t>();
+	uint32_t* offs = w.runOffs.as<uint32_t>();
 	scanExclusive(w.runFlag.as<uint32_t>(), offs, n, &dc->runs, w.prim, w.stream);
 	M3G_LAUNCH(kRunStarts, blocksFor(n, 256), 256, w.stream, w.runFlag.as<uint32_t>(), offs, n, w.runStarts.as<int32_t>(),
-														 &dc->runs);
-	readCounters(w);
-	w.runCount = (int32_t)w.hostCounters->runs;
+			   &dc->runs);
 }
 
 // ---------------------------------------------------------------------------
@@ -427,12 +464,20 @@ __device__ __forceinline__ int64_t lowerBoundKey(const uint64_t* keys, int64_t n
 // admitted pair keys of the run in the reference's enumeration order.
 template <bool EMIT>
 __global__ void kRunPairs(PairCtx P, const uint64_t* actKeys, const uint32_t* actVals, const int32_t* runStarts,
-						  int32_t runs, const uint64_t* stabKeys, const uint32_t* stabVals, int64_t stabCount,
-						  uint32_t* counts, const uint32_t* offsets, uint64_t* out)
+						  int32_t runMax, const uint32_t* runsDev, const uint64_t* stabKeys, const uint32_t* stabVals,
+						  int64_t stabCount, uint32_t* counts, const uint32_t* offsets, uint64_t* out)
 {
 	int r = blockIdx.x * blockDim.x + threadIdx.x;
-	if (r >= runs)
+	if (r >= runMax)
 	{
+		return;
+	}
+	if (r >= (int)*runsDev)
+	{
+		if (!EMIT)
+		{
+			counts[r] = 0; // past the last run: contributes nothing to the scan
+		}
 		return;
 	}
 	int32_t s = runStarts[r], e = runStarts[r + 1];
@@ -669,7 +714,34 @@ static uint32_t tableCapacity(int64_t keys)
 	return (uint32_t)cap;
 }
 
-void launchPairs(DevWorld& w, int32_t n, float cellSize)
+static PairCtx pairCtx(DevWorld& w, float cellSize)
+{
+	PairCtx P;
+	P.B = w.B;
+	P.existing = w.existingSet.as<uint64_t>();
+	P.existingMask = w.existingMask;
+	P.jointed = w.jointedPairs.as<uint64_t>();
+	P.jointedCount = w.jointedCount;
+	P.inv = 1.0f / cellSize;
+	return P;
+}
+
+static OverCtx overCtx(DevWorld& w, int32_t n, int64_t* total)
+{
+	OverCtx O;
+	O.actOver = w.activeOver.as<int32_t>();
+	O.nAO = w.activeOverCount;
+	O.stabOver = w.stableOver.as<int32_t>();
+	O.nSO = w.stableOverCount;
+	O.n = n;
+	O.inActiveCells = w.inActiveCells.as<uint8_t>();
+	*total = (int64_t)O.nAO * ((int64_t)n + O.nSO) + (int64_t)O.nAO * (O.nAO - 1) / 2 + (int64_t)O.nSO * n;
+	return O;
+}
+
+// Count the admitted pairs of every cell run and of the oversized loops; the
+// step's second sync reads the two totals.
+void launchPairCount(DevWorld& w, int32_t n, float cellSize)
 {
 	StepCounters* dc = devCounters(w);
 	cudaStream_t s = w.stream;
@@ -682,104 +754,103 @@ void launchPairs(DevWorld& w, int32_t n, float cellSize)
 	if (w.contactCount > 0)
 	{
 		M3G_LAUNCH(kInsertExisting, blocksFor(w.contactCount, 256), 256, s, w.C.bodies, w.contactCount,
-																		 w.existingSet.as<uint64_t>(), w.existingMask,
-																		 &dc->hashFail);
+				   w.existingSet.as<uint64_t>(), w.existingMask, &dc->hashFail);
 	}
+	PairCtx P = pairCtx(w, cellSize);
 
-	PairCtx P;
-	P.B = w.B;
-	P.existing = w.existingSet.as<uint64_t>();
-	P.existingMask = w.existingMask;
-	P.jointed = w.jointedPairs.as<uint64_t>();
-	P.jointedCount = w.jointedCount;
-	P.inv = 1.0f / cellSize;
-
-	// grid runs: count, scan, emit
-	int32_t runs = w.runCount;
-	w.runPairCount.ensure((size_t)(runs + 1) * sizeof(uint32_t));
-	w.keepFlag.ensure((size_t)(runs + 1) * sizeof(uint32_t));
-	uint32_t* counts = w.runPairCount.as<uint32_t>();
-	uint32_t* offs = w.keepFlag.as<uint32_t>();
-	if (runs > 0)
+	int32_t runMax = w.runCount;
+	w.runPairCount.ensure((size_t)(runMax + 1) * sizeof(uint32_t));
+	w.runPairOffs.ensure((size_t)(runMax + 1) * sizeof(uint32_t));
+	if (runMax > 0)
 	{
-		M3G_LAUNCH(kRunPairs<false>, blocksFor(runs, 128), 128, s, 
-			P, w.activeKeys.as<uint64_t>(), w.activeVals.as<uint32_t>(), w.runStarts.as<int32_t>(), runs,
-			w.stableKeys.as<uint64_t>(), w.stableVals.as<uint32_t>(), w.stableEntries, counts, nullptr, nullptr);
+		M3G_LAUNCH(kRunPairs<false>, blocksFor(runMax, 128), 128, s, P, w.activeKeys.as<uint64_t>(),
+				   w.activeVals.as<uint32_t>(), w.runStarts.as<int32_t>(), runMax, &dc->runs,
+				   w.stableKeys.as<uint64_t>(), w.stableVals.as<uint32_t>(), w.stableEntries,
+				   w.runPairCount.as<uint32_t>(), nullptr, nullptr);
 	}
-	scanExclusive(counts, offs, runs, &dc->gridPairs, w.prim, s);
+	scanExclusive(w.runPairCount.as<uint32_t>(), w.runPairOffs.as<uint32_t>(), runMax, &dc->gridPairs, w.prim, s);
 
-	// oversized candidates
-	OverCtx O;
-	O.actOver = w.activeOver.as<int32_t>();
-	O.nAO = w.activeOverCount;
-	O.stabOver = w.stableOver.as<int32_t>();
-	O.nSO = w.stableOverCount;
-	O.n = n;
-	O.inActiveCells = w.inActiveCells.as<uint8_t>();
-	int64_t overTotal = (int64_t)O.nAO * ((int64_t)n + O.nSO) + (int64_t)O.nAO * (O.nAO - 1) / 2 + (int64_t)O.nSO * n;
+	int64_t overTotal;
+	OverCtx O = overCtx(w, n, &overTotal);
 	w.overFlag.ensure((size_t)(overTotal + 1) * sizeof(uint32_t));
 	w.overScan.ensure((size_t)(overTotal + 1) * sizeof(uint32_t));
-	w.newContactKeys.ensure((size_t)(overTotal + 1) * sizeof(uint64_t));
+	w.overKeys.ensure((size_t)(overTotal + 1) * sizeof(uint64_t));
 	if (overTotal > 0)
 	{
 		M3G_LAUNCH(kOverPairs, blocksFor(overTotal, 256), 256, s, P, O, overTotal, w.overFlag.as<uint32_t>(),
-															  w.newContactKeys.as<uint64_t>());
+				   w.overKeys.as<uint64_t>());
 	}
 	scanExclusive(w.overFlag.as<uint32_t>(), w.overScan.as<uint32_t>(), overTotal, &dc->overPairs, w.prim, s);
-	readCounters(w);
+}
+
+// After the second sync: write the admitted pairs in emission order, keep the
+// first occurrence of each, compact.  The count of new contacts stays on the
+// device; the host only knows its upper bound (all admitted pairs).
+void launchPairEmit(DevWorld& w, int32_t n, float cellSize)
+{
+	StepCounters* dc = devCounters(w);
+	cudaStream_t s = w.stream;
+	PairCtx P = pairCtx(w, cellSize);
+	int32_t runMax = w.runCount;
 	int64_t gridPairs = w.hostCounters->gridPairs;
 	int64_t overPairs = w.hostCounters->overPairs;
 	int64_t total = gridPairs + overPairs;
+	w.pairTotal = total;
 	w.pairKeys.ensure((size_t)(total + 1) * sizeof(uint64_t));
 	uint64_t* pk = w.pairKeys.as<uint64_t>();
-	if (runs > 0 && gridPairs > 0)
+	if (runMax > 0 && gridPairs > 0)
 	{
-		M3G_LAUNCH(kRunPairs<true>, blocksFor(runs, 128), 128, s, 
-			P, w.activeKeys.as<uint64_t>(), w.activeVals.as<uint32_t>(), w.runStarts.as<int32_t>(), runs,
-			w.stableKeys.as<uint64_t>(), w.stableVals.as<uint32_t>(), w.stableEntries, nullptr, offs, pk);
+		M3G_LAUNCH(kRunPairs<true>, blocksFor(runMax, 128), 128, s, P, w.activeKeys.as<uint64_t>(),
+				   w.activeVals.as<uint32_t>(), w.runStarts.as<int32_t>(), runMax, &dc->runs,
+				   w.stableKeys.as<uint64_t>(), w.stableVals.as<uint32_t>(), w.stableEntries, nullptr,
+				   w.runPairOffs.as<uint32_t>(), pk);
 	}
+	int64_t overTotal;
+	overCtx(w, n, &overTotal);
 	if (overPairs > 0)
 	{
-		M3G_LAUNCH(kScatterKeys, blocksFor(overTotal, 256), 256, s, w.overFlag.as<uint32_t>(), w.overScan.as<uint32_t>(),
-																w.newContactKeys.as<uint64_t>(), overTotal,
-																pk + gridPairs);
+		M3G_LAUNCH(kScatterKeys, blocksFor(overTotal, 256), 256, s, w.overFlag.as<uint32_t>(),
+				   w.overScan.as<uint32_t>(), w.overKeys.as<uint64_t>(), overTotal, pk + gridPairs);
 	}
 
-	// first-occurrence dedupe of the admitted stream
 	uint32_t ncap = tableCapacity(total);
 	w.newSet.ensure((size_t)ncap * sizeof(uint64_t));
 	w.newSetPos.ensure((size_t)ncap * sizeof(uint32_t));
 	w.newMask = ncap - 1;
 	w.keepFlag.ensure((size_t)(total + 1) * sizeof(uint32_t));
-	w.overScan.ensure((size_t)(total + 1) * sizeof(uint32_t));
+	w.keepScan.ensure((size_t)(total + 1) * sizeof(uint32_t));
 	w.newContactKeys.ensure((size_t)(total + 1) * sizeof(uint64_t));
 	if (total > 0)
 	{
 		cudaMemsetAsync(w.newSet.ptr, 0xFF, (size_t)ncap * sizeof(uint64_t), s);
 		cudaMemsetAsync(w.newSetPos.ptr, 0xFF, (size_t)ncap * sizeof(uint32_t), s);
 		M3G_LAUNCH(kDedupeMark, blocksFor(total, 256), 256, s, pk, total, w.newSet.as<uint64_t>(),
-														   w.newSetPos.as<uint32_t>(), w.newMask, &dc->hashFail);
+				   w.newSetPos.as<uint32_t>(), w.newMask, &dc->hashFail);
 		M3G_LAUNCH(kDedupeKeep, blocksFor(total, 256), 256, s, pk, total, w.newSet.as<uint64_t>(),
-														   w.newSetPos.as<uint32_t>(), w.newMask,
-														   w.keepFlag.as<uint32_t>());
+				   w.newSetPos.as<uint32_t>(), w.newMask, w.keepFlag.as<uint32_t>());
 	}
-	scanExclusive(w.keepFlag.as<uint32_t>(), w.overScan.as<uint32_t>(), total, &dc->newContacts, w.prim, s);
+	scanExclusive(w.keepFlag.as<uint32_t>(), w.keepScan.as<uint32_t>(), total, &dc->newContacts, w.prim, s);
 	if (total > 0)
 	{
-		M3G_LAUNCH(kScatterKeys, blocksFor(total, 256), 256, s, w.keepFlag.as<uint32_t>(), w.overScan.as<uint32_t>(), pk,
-															total, w.newContactKeys.as<uint64_t>());
+		M3G_LAUNCH(kScatterKeys, blocksFor(total, 256), 256, s, w.keepFlag.as<uint32_t>(), w.keepScan.as<uint32_t>(), pk,
+				   total, w.newContactKeys.as<uint64_t>());
 	}
-	readCounters(w);
 }
 
 // ---------------------------------------------------------------------------
 // contact creation (reference src/world.cpp:1540-1568)
 // ---------------------------------------------------------------------------
 
-__global__ void kCreateContacts(BodySoA B, ContactSoA C, const uint64_t* keys, int32_t count, int32_t base)
+__global__ void kCreateContacts(BodySoA B, ContactSoA C, const uint64_t* keys, int32_t maxCount,
+								const uint32_t* newCount, int32_t base, uint32_t* contactCountDev)
 {
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
-	if (k >= count)
+	uint32_t count = *newCount;
+	if (k == 0)
+	{
+		*contactCountDev = (uint32_t)base + count;
+	}
+	if (k >= maxCount || k >= (int)count)
 	{
 		return;
 	}
@@ -816,29 +887,46 @@ __global__ void kCreateContacts(BodySoA B, ContactSoA C, const uint64_t* keys, i
 	}
 }
 
-void launchCreateContacts(DevWorld& w, int32_t newCount)
+// Appends the new contacts after the w.contactCount existing ones; the new
+// count is written to the device counter, the host keeps the upper bound.
+void launchCreateContacts(DevWorld& w)
 {
-	if (newCount <= 0)
-	{
-		return;
-	}
-	M3G_LAUNCH(kCreateContacts, blocksFor(newCount, 128), 128, w.stream, w.B, w.C, w.newContactKeys.as<uint64_t>(),
-																	  newCount, w.contactCount);
-	w.contactCount += newCount;
+	StepCounters* dc = devCounters(w);
+	int32_t maxNew = (int32_t)w.pairTotal;
+	M3G_LAUNCH(kCreateContacts, blocksFor(maxNew > 0 ? maxNew : 1, 128), 128, w.stream, w.B, w.C,
+			   w.newContactKeys.as<uint64_t>(), maxNew, &dc->newContacts, w.contactCount, &dc->contactCount);
+	w.contactMax = w.contactCount + maxNew;
 }
 
 // ---------------------------------------------------------------------------
-// removal of separated pairs: closed form of the descending swap-remove
-// (reference src/world.cpp:100-119, 1705-1735).  With S = count - removed,
-// the k-th largest removed index below S receives the k-th largest surviving
-// index at or above S; end events go out in descending index order.
+// removal of separated pairs: closed form of the reference's descending
+// swap-remove (src/world.cpp:100-119, 1705-1735).  The reference visits the
+// removed indices from the highest down; the k-th one it visits receives the
+// element then at position count-k, which is either an original survivor or
+// an element an earlier (higher) removal already moved there.  With
+// S = count - removed and scan = number of removed indices below a position,
+// count-k equals S + scan[i] for a removed i, so a hole i < S receives
+//     p = S + scan[i];  while (removed[p]) p = S + scan[p];
+// (each step follows an earlier move; the chain ends at a survivor at or above
+// S).  Sources are distinct survivors >= S and destinations holes < S, so all
+// holes are filled in parallel.  End events go out in descending index order.
 // ---------------------------------------------------------------------------
 
-__global__ void kRemovalFlags(BodySoA B, ContactSoA C, int32_t count, uint32_t* removeFlag, uint32_t* evFlag)
+__global__ void kRemovalFlags(BodySoA B, ContactSoA C, int32_t maxCount, const uint32_t* countDev, uint32_t* removeFlag,
+							  uint32_t* evFlag)
 {
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
-	if (c >= count)
+	if (c > maxCount)
 	{
+		return;
+	}
+	if (c >= (int)*countDev)
+	{
+		removeFlag[c] = 0;
+		if (c < maxCount)
+		{
+			evFlag[c] = 0;
+		}
 		return;
 	}
 	int2 ab = C.bodies[c];
@@ -854,30 +942,17 @@ __global__ void kRemovalFlags(BodySoA B, ContactSoA C, int32_t count, uint32_t* 
 	evFlag[c] = (rm && (C.flags[c] & kCFTouching)) ? 1u : 0u;
 }
 
-__global__ void kRemovalEvents(const ContactSoA C, int32_t count, const uint32_t* evFlag, const uint32_t* evScan,
+__global__ void kRemovalEvents(const ContactSoA C, int32_t maxCount, const uint32_t* evFlag, const uint32_t* evScan,
 							   const uint32_t* evTotal, int4* events)
 {
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
-	if (c >= count || !evFlag[c])
+	if (c >= maxCount || !evFlag[c])
 	{
 		return;
 	}
 	uint32_t t = *evTotal;
 	int2 ab = C.bodies[c];
 	events[t - 1 - evScan[c]] = make_int4(ab.x, ab.y, (C.flags[c] & kCFSensor) ? 1 : 0, 0);
-}
-
-__global__ void kRemovalSources(int32_t count, int32_t S, const uint32_t* removeFlag, const uint32_t* removeScan,
-								int32_t* moveSrc)
-{
-	int t = S + blockIdx.x * blockDim.x + threadIdx.x;
-	if (t >= count || removeFlag[t])
-	{
-		return;
-	}
-	int32_t H = (int32_t)removeScan[S];
-	int32_t survivorsBelow = (t - S) - ((int32_t)removeScan[t] - H);
-	moveSrc[H - 1 - survivorsBelow] = t;
 }
 
 __device__ void copyContact(const ContactSoA& C, int dst, int src)
@@ -906,17 +981,22 @@ __device__ void copyContact(const ContactSoA& C, int dst, int src)
 	}
 }
 
-__global__ void kRemovalMoves(ContactSoA C, int32_t S, const uint32_t* removeFlag, const uint32_t* removeScan,
-							  const int32_t* moveSrc)
+__global__ void kRemovalMoves(ContactSoA C, int32_t maxCount, const uint32_t* countDev, const uint32_t* removedDev,
+							  const uint32_t* removeFlag, const uint32_t* removeScan)
 {
+	int32_t count = (int32_t)*countDev;
+	int32_t S = count - (int32_t)*removedDev;
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= S || !removeFlag[i])
+	if (i >= S || i >= maxCount || !removeFlag[i])
 	{
 		return;
 	}
-	int32_t H = (int32_t)removeScan[S];
-	int32_t rankTop = H - 1 - (int32_t)removeScan[i];
-	copyContact(C, i, moveSrc[rankTop]);
+	int32_t p = S + (int32_t)removeScan[i];
+	for (int guard = 0; guard <= count && p < count && removeFlag[p]; ++guard)
+	{
+		p = S + (int32_t)removeScan[p];
+	}
+	copyContact(C, i, p);
 }
 
 __global__ void kContactMoves(ContactSoA C, const int2* moves, int32_t count)
@@ -942,48 +1022,36 @@ void launchContactMoves(DevWorld& w, const int2* hostMoves, int32_t count)
 	cudaStreamSynchronize(w.stream); // the host vector backing hostMoves is freed on return
 }
 
+__global__ void kRemovalFinish(uint32_t* countDev, const uint32_t* removedDev)
+{
+	*countDev -= *removedDev;
+}
+
 void launchRemoval(DevWorld& w)
 {
 	StepCounters* dc = devCounters(w);
 	cudaStream_t s = w.stream;
-	int32_t count = w.contactCount;
-	size_t c4 = (size_t)(count + 1) * sizeof(uint32_t);
+	int32_t M = w.contactMax; // upper bound of the device count
+	size_t c4 = (size_t)(M + 2) * sizeof(uint32_t);
 	w.removeFlag.ensure(c4);
 	w.removeScan.ensure(c4);
 	w.evEndFlag.ensure(c4);
 	w.evBeginFlag.ensure(c4);
-	w.evRemoval.ensure((size_t)(count + 1) * sizeof(int4));
+	w.evRemoval.ensure((size_t)(M + 1) * sizeof(int4));
 	w.moveSrc.ensure(c4);
-	if (count <= 0)
+	M3G_LAUNCH(kRemovalFlags, blocksFor(M + 1, 256), 256, s, w.B, w.C, M, &dc->contactCount, w.removeFlag.as<uint32_t>(),
+			   w.evEndFlag.as<uint32_t>());
+	// M + 1 entries so that removeScan[count] exists
+	scanExclusive(w.removeFlag.as<uint32_t>(), w.removeScan.as<uint32_t>(), M + 1, &dc->removed, w.prim, s);
+	scanExclusive(w.evEndFlag.as<uint32_t>(), w.evBeginFlag.as<uint32_t>(), M, &dc->endRemoval, w.prim, s);
+	if (M > 0)
 	{
-		cudaMemsetAsync(&dc->removed, 0, sizeof(uint32_t), s);
-		cudaMemsetAsync(&dc->endRemoval, 0, sizeof(uint32_t), s);
-		readCounters(w);
-		return;
+		M3G_LAUNCH(kRemovalEvents, blocksFor(M, 256), 256, s, w.C, M, w.evEndFlag.as<uint32_t>(),
+				   w.evBeginFlag.as<uint32_t>(), &dc->endRemoval, w.evRemoval.as<int4>());
+		M3G_LAUNCH(kRemovalMoves, blocksFor(M, 256), 256, s, w.C, M, &dc->contactCount, &dc->removed,
+				   w.removeFlag.as<uint32_t>(), w.removeScan.as<uint32_t>());
 	}
-	M3G_LAUNCH(kRemovalFlags, blocksFor(count, 256), 256, s, w.B, w.C, count, w.removeFlag.as<uint32_t>(),
-														  w.evEndFlag.as<uint32_t>());
-	// the scan covers count + 1 entries so removeScan[count] exists
-	cudaMemsetAsync(w.removeFlag.as<uint32_t>() + count, 0, sizeof(uint32_t), s);
-	scanExclusive(w.removeFlag.as<uint32_t>(), w.removeScan.as<uint32_t>(), count + 1, &dc->removed, w.prim, s);
-	scanExclusive(w.evEndFlag.as<uint32_t>(), w.evBeginFlag.as<uint32_t>(), count, &dc->endRemoval, w.prim, s);
-	M3G_LAUNCH(kRemovalEvents, blocksFor(count, 256), 256, s, w.C, count, w.evEndFlag.as<uint32_t>(),
-														   w.evBeginFlag.as<uint32_t>(), &dc->endRemoval,
-														   w.evRemoval.as<int4>());
-	readCounters(w);
-	int32_t removed = (int32_t)w.hostCounters->removed;
-	if (removed > 0)
-	{
-		int32_t S = count - removed;
-		M3G_LAUNCH(kRemovalSources, blocksFor(removed, 256), 256, s, count, S, w.removeFlag.as<uint32_t>(),
-																 w.removeScan.as<uint32_t>(), w.moveSrc.as<int32_t>());
-		if (S > 0)
-		{
-			M3G_LAUNCH(kRemovalMoves, blocksFor(S, 256), 256, s, w.C, S, w.removeFlag.as<uint32_t>(),
-															 w.removeScan.as<uint32_t>(), w.moveSrc.as<int32_t>());
-		}
-		w.contactCount = S;
-	}
+	M3G_LAUNCH(kRemovalFinish, 1, 1, s, &dc->contactCount, &dc->removed);
 }
 
 } // namespace m3g

@@ -4,10 +4,17 @@
 // dynamic-dynamic joints, with the larger root always hooked under the
 // smaller one, so every component's root is its smallest body index - the
 // same canonical label the reference's serial union-find produces.  Awake
-// islands wake all their bodies; their contacts, joints and bodies are
-// grouped per island by a stable sort on the label, which keeps the
-// reference's ascending index order inside each island.
-// (reference src/world.cpp:1848-2010, 2060-2166)
+// islands wake all their bodies.  Contacts (and joints) of each island keep
+// the reference's ascending index order - the Gauss-Seidel and colouring
+// order - through a stable radix sort on the label.  Bodies are grouped by
+// counting; their order inside an island is free, because every per-body
+// stage (integration, reconstruction, colour-mask reset, sleep timers) is
+// independent of the other bodies.
+//
+// Every count stays on the device: kernels are bounded by host-side upper
+// bounds and read the exact counts from StepCounters, and the whole stage is
+// skipped on the device when no dynamic body is awake (the reference's
+// early-out).  (reference src/world.cpp:1848-2010, 2060-2166)
 #include "m3d_dev.cuh"
 
 #include <float.h>
@@ -34,12 +41,20 @@ void launchAnyAwakeDynamic(DevWorld& w, int32_t n)
 	}
 }
 
-__global__ void kInitParent(int32_t* parent, int32_t n)
+__global__ void kInitParent(int32_t* parent, int32_t n, const uint32_t* active, uint32_t* labelCount,
+							uint32_t* cursor)
 {
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n)
 	{
-		parent[i] = i;
+		// counts are cleared even when nothing is awake, so every later stage
+		// sees zero islands; the labels of the last build are kept
+		labelCount[i] = 0;
+		cursor[i] = 0;
+		if (*active)
+		{
+			parent[i] = i;
+		}
 	}
 }
 
@@ -84,10 +99,11 @@ __device__ void ufUnite(int32_t* parent, int32_t a, int32_t b)
 	}
 }
 
-__global__ void kUnionContacts(const ContactSoA C, int32_t count, const uint8_t* bFlags, int32_t* parent)
+__global__ void kUnionContacts(const ContactSoA C, int32_t maxCount, const uint32_t* countDev, const uint8_t* bFlags,
+							   int32_t* parent, const uint32_t* active)
 {
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
-	if (c >= count)
+	if (c >= maxCount || c >= (int)*countDev || !*active)
 	{
 		return;
 	}
@@ -103,10 +119,11 @@ __global__ void kUnionContacts(const ContactSoA C, int32_t count, const uint8_t*
 	}
 }
 
-__global__ void kUnionJoints(const JointRec* joints, int32_t count, const BodyCold* cold, int32_t* parent)
+__global__ void kUnionJoints(const JointRec* joints, int32_t count, const BodyCold* cold, int32_t* parent,
+							 const uint32_t* active)
 {
 	int j = blockIdx.x * blockDim.x + threadIdx.x;
-	if (j >= count)
+	if (j >= count || !*active)
 	{
 		return;
 	}
@@ -118,10 +135,10 @@ __global__ void kUnionJoints(const JointRec* joints, int32_t count, const BodyCo
 }
 
 __global__ void kLabels(int32_t* parent, int32_t n, const uint8_t* bFlags, int32_t* label, uint32_t* islandFlag,
-						uint32_t* islandCount)
+						uint32_t* islandCount, const uint32_t* active)
 {
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= n)
+	if (i >= n || !*active)
 	{
 		return;
 	}
@@ -141,56 +158,93 @@ __global__ void kLabels(int32_t* parent, int32_t n, const uint8_t* bFlags, int32
 	}
 }
 
-__global__ void kIslandAwake(const uint8_t* bFlags, int32_t n, const int32_t* label, uint32_t* islandFlag)
+__global__ void kIslandAwake(const uint8_t* bFlags, int32_t n, const int32_t* label, uint32_t* islandFlag,
+							 const uint32_t* active)
 {
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i < n && (bFlags[i] & kBFDynamic) && (bFlags[i] & kBFAwake))
+	if (i < n && *active && (bFlags[i] & kBFDynamic) && (bFlags[i] & kBFAwake))
 	{
 		islandFlag[label[i]] = 1;
 	}
 }
 
-// wake every body of an awake island; flag the bodies to solve
-__global__ void kIslandWakeBodies(BodySoA B, int32_t n, const int32_t* label, const uint32_t* islandFlag,
-								  uint32_t* bodyFlag, uint32_t* stableDirty)
+// wake every body of an awake island and count the island's bodies
+__global__ void kIslandBodies(BodySoA B, int32_t n, const int32_t* label, const uint32_t* islandFlag,
+							  uint32_t* labelCount, uint32_t* stableDirty, const uint32_t* active)
 {
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= n)
+	if (i >= n || !*active)
 	{
 		return;
 	}
-	uint32_t f = 0;
 	if ((B.bFlags[i] & kBFDynamic) && islandFlag[label[i]])
 	{
-		f = 1;
 		if (!(B.state[i] & kStAwake))
 		{
 			wakeBody(B, i, stableDirty);
 		}
+		atomicAdd(&labelCount[label[i]], 1u);
 	}
-	bodyFlag[i] = f;
 }
 
-__global__ void kContactIslandFlags(const ContactSoA C, int32_t count, const uint8_t* bFlags, const int32_t* label,
-									const uint32_t* islandFlag, uint32_t* flag, uint32_t* touchingCount)
+__global__ void kIslandListFlags(const uint32_t* labelCount, int32_t n, uint32_t* flag)
 {
-	int c = blockIdx.x * blockDim.x + threadIdx.x;
-	if (c >= count)
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n)
+	{
+		flag[i] = labelCount[i] > 0 ? 1u : 0u;
+	}
+}
+
+__global__ void kIslandListCompact(const uint32_t* flag, const uint32_t* offs, int32_t n, int32_t* islandLabels)
+{
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n && flag[i])
+	{
+		islandLabels[offs[i]] = i;
+	}
+}
+
+__global__ void kPlaceBodies(const BodySoA B, int32_t n, const int32_t* label, const uint32_t* islandFlag,
+							 const uint32_t* labelStart, uint32_t* cursor, uint32_t* bodyVals, const uint32_t* active)
+{
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n || !*active)
 	{
 		return;
 	}
-	uint8_t fl = C.flags[c];
-	uint32_t f = 0;
-	if (fl & kCFTouching)
+	if ((B.bFlags[i] & kBFDynamic) && islandFlag[label[i]])
 	{
-		atomicAdd(touchingCount, 1u);
-		if (!(fl & kCFSensor))
+		int32_t l = label[i];
+		uint32_t slot = atomicAdd(&cursor[l], 1u);
+		bodyVals[labelStart[l] + slot] = (uint32_t)i;
+	}
+}
+
+__global__ void kContactIslandFlags(const ContactSoA C, int32_t maxCount, const uint32_t* countDev,
+									const uint8_t* bFlags, const int32_t* label, const uint32_t* islandFlag,
+									uint32_t* flag, uint32_t* touchingCount, const uint32_t* active)
+{
+	int c = blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= maxCount)
+	{
+		return;
+	}
+	uint32_t f = 0;
+	if (c < (int)*countDev && *active)
+	{
+		uint8_t fl = C.flags[c];
+		if (fl & kCFTouching)
 		{
-			int2 ab = C.bodies[c];
-			int32_t dyn = (bFlags[ab.x] & kBFDynamic) ? ab.x : ab.y;
-			if ((bFlags[dyn] & kBFDynamic) && islandFlag[label[dyn]])
+			atomicAdd(touchingCount, 1u);
+			if (!(fl & kCFSensor))
 			{
-				f = 1;
+				int2 ab = C.bodies[c];
+				int32_t dyn = (bFlags[ab.x] & kBFDynamic) ? ab.x : ab.y;
+				if ((bFlags[dyn] & kBFDynamic) && islandFlag[label[dyn]])
+				{
+					f = 1;
+				}
 			}
 		}
 	}
@@ -198,16 +252,16 @@ __global__ void kContactIslandFlags(const ContactSoA C, int32_t count, const uin
 }
 
 __global__ void kJointIslandFlags(const JointRec* joints, int32_t count, const BodyCold* cold, const int32_t* label,
-								  const uint32_t* islandFlag, uint32_t* flag)
+								  const uint32_t* islandFlag, uint32_t* flag, const uint32_t* active)
 {
 	int j = blockIdx.x * blockDim.x + threadIdx.x;
 	if (j >= count)
 	{
 		return;
 	}
-	const JointRec& jr = joints[j];
 	uint32_t f = 0;
-	if (jr.inUse)
+	const JointRec& jr = joints[j];
+	if (*active && jr.inUse)
 	{
 		int32_t dyn = cold[jr.bodyA].type == kDynamic ? jr.bodyA : jr.bodyB;
 		if (cold[dyn].type == kDynamic && islandFlag[label[dyn]])
@@ -219,7 +273,7 @@ __global__ void kJointIslandFlags(const JointRec* joints, int32_t count, const B
 }
 
 // (label, index) pairs of the flagged items, in index order
-__global__ void kLabelPairs(const uint32_t* flag, const uint32_t* offs, int32_t count, const int32_t* itemLabelOf,
+__global__ void kLabelPairs(const uint32_t* flag, const uint32_t* offs, int32_t count, const int32_t* label,
 							const int2* contactBodies, const JointRec* joints, const uint8_t* bFlags, const BodyCold* cold,
 							int mode, uint64_t* keys, uint32_t* vals)
 {
@@ -228,35 +282,20 @@ __global__ void kLabelPairs(const uint32_t* flag, const uint32_t* offs, int32_t 
 	{
 		return;
 	}
-	int32_t lab;
-	if (mode == 0)
-	{
-		lab = itemLabelOf[i]; // bodies
-	}
-	else if (mode == 1)
+	int32_t dyn;
+	if (mode == 1)
 	{
 		int2 ab = contactBodies[i];
-		int32_t dyn = (bFlags[ab.x] & kBFDynamic) ? ab.x : ab.y;
-		lab = itemLabelOf[dyn];
+		dyn = (bFlags[ab.x] & kBFDynamic) ? ab.x : ab.y;
 	}
 	else
 	{
 		const JointRec& jr = joints[i];
-		int32_t dyn = cold[jr.bodyA].type == kDynamic ? jr.bodyA : jr.bodyB;
-		lab = itemLabelOf[dyn];
+		dyn = cold[jr.bodyA].type == kDynamic ? jr.bodyA : jr.bodyB;
 	}
 	uint32_t o = offs[i];
-	keys[o] = (uint64_t)(uint32_t)lab;
+	keys[o] = (uint64_t)(uint32_t)label[dyn];
 	vals[o] = (uint32_t)i;
-}
-
-__global__ void kIslandStarts(const uint64_t* keys, int32_t n, uint32_t* flag)
-{
-	int i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i < n)
-	{
-		flag[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
-	}
 }
 
 __device__ __forceinline__ int32_t lowerBound64(const uint64_t* keys, int32_t n, uint64_t k)
@@ -273,35 +312,32 @@ __device__ __forceinline__ int32_t lowerBound64(const uint64_t* keys, int32_t n,
 	return lo;
 }
 
-__global__ void kIslandTable(const uint64_t* bodyKeys, int32_t nBodies, const uint32_t* startFlag,
-							 const uint32_t* startOffs, const uint64_t* contactKeys, int32_t nContacts,
-							 const uint64_t* jointKeys, int32_t nJoints, IslandRec* islands, int32_t nIslands,
-							 StepCounters* dc)
+__global__ void kIslandTable(const int32_t* islandLabels, int32_t maxIslands, const uint32_t* islandsDev,
+							 const uint32_t* labelStart, const uint32_t* labelCount, const uint64_t* contactKeys,
+							 const uint32_t* contactsDev, const uint64_t* jointKeys, const uint32_t* jointsDev,
+							 IslandRec* islands, int32_t* coloredList, StepCounters* dc)
 {
-	int i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= nBodies || !startFlag[i])
+	int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k >= maxIslands || k >= (int)*islandsDev)
 	{
 		return;
 	}
-	int32_t k = (int32_t)startOffs[i];
-	uint64_t key = bodyKeys[i];
-	int32_t end = i + 1;
-	while (end < nBodies && bodyKeys[end] == key)
-	{
-		++end;
-	}
+	int32_t lab = islandLabels[k];
+	uint64_t key = (uint64_t)(uint32_t)lab;
+	int32_t nc = (int32_t)*contactsDev;
+	int32_t nj = jointsDev != nullptr ? (int32_t)*jointsDev : 0;
 	IslandRec r;
-	r.label = (int32_t)key;
-	r.bodyStart = i;
-	r.bodyCount = end - i;
-	r.contactStart = lowerBound64(contactKeys, nContacts, key);
-	r.contactCount = lowerBound64(contactKeys, nContacts, key + 1) - r.contactStart;
-	r.jointStart = lowerBound64(jointKeys, nJoints, key);
-	r.jointCount = lowerBound64(jointKeys, nJoints, key + 1) - r.jointStart;
+	r.label = lab;
+	r.bodyStart = (int32_t)labelStart[lab];
+	r.bodyCount = (int32_t)labelCount[lab];
+	r.contactStart = lowerBound64(contactKeys, nc, key);
+	r.contactCount = lowerBound64(contactKeys, nc, key + 1) - r.contactStart;
+	r.jointStart = nj > 0 ? lowerBound64(jointKeys, nj, key) : 0;
+	r.jointCount = nj > 0 ? lowerBound64(jointKeys, nj, key + 1) - r.jointStart : 0;
 	if (r.contactCount >= kBigIslandContacts)
 	{
 		r.kind = 2;
-		atomicAdd(&dc->coloredIslands, 1u);
+		coloredList[atomicAdd(&dc->coloredIslands, 1u)] = k;
 	}
 	else if (r.contactCount > 0 || r.jointCount > 0)
 	{
@@ -314,108 +350,107 @@ __global__ void kIslandTable(const uint64_t* bodyKeys, int32_t nBodies, const ui
 		atomicAdd(&dc->freeIslands, 1u);
 	}
 	islands[k] = r;
-	(void)nIslands;
 }
 
-// flag scan + (label, index) pairs + stable sort by label
-static int32_t groupByLabel(DevWorld& w, int mode, int32_t count, DevBuf& flag, DevBuf& keys, DevBuf& vals,
-							uint32_t* totalDev, uint32_t* totalHost)
+static int bitsFor(int64_t n)
 {
-	DevBuf& offs = w.removeScan;
-	offs.ensure((size_t)(count + 1) * sizeof(uint32_t));
-	scanExclusive(flag.as<uint32_t>(), offs.as<uint32_t>(), count, totalDev, w.prim, w.stream);
-	readCounters(w);
-	int32_t total = (int32_t)*totalHost;
-	keys.ensure((size_t)(total + 1) * sizeof(uint64_t));
-	vals.ensure((size_t)(total + 1) * sizeof(uint32_t));
-	if (count > 0)
+	int b = 1;
+	while (b < 63 && (1ll << b) <= n)
 	{
-		M3G_LAUNCH(kLabelPairs, blocksFor(count, 256), 256, w.stream, 
-			flag.as<uint32_t>(), offs.as<uint32_t>(), count, w.label.as<int32_t>(), w.C.bodies,
-			w.joints.as<JointRec>(), w.B.bFlags, w.B.cold, mode, keys.as<uint64_t>(), vals.as<uint32_t>());
+		++b;
 	}
-	if (total > 1)
-	{
-		reduceKeyRange(keys.as<uint64_t>(), total, w.prim, w.stream);
-		cudaStreamSynchronize(w.stream);
-		radixSortPairs(keys.as<uint64_t>(), vals.as<uint32_t>(), total, w.prim.hostReduce[0] ^ w.prim.hostReduce[1],
-					   w.prim, w.stream);
-	}
-	return total;
+	return b;
 }
 
 void launchIslands(DevWorld& w, int32_t n)
 {
 	StepCounters* dc = devCounters(w);
 	cudaStream_t s = w.stream;
+	const uint32_t* active = &dc->anyAwakeDynamic;
+	int32_t M = w.contactMax;
 	size_t n4 = (size_t)(n + 1) * sizeof(uint32_t);
 	w.label.ensure(n4);
 	w.islandFlag.ensure(n4);
-	w.cellCountA.ensure(n4); // reused: per-body solve flag
+	w.labelCount.ensure(n4);
+	w.labelStart.ensure(n4);
+	w.labelCursor.ensure(n4);
+	w.islandListFlag.ensure(n4);
+	w.islandListOffs.ensure(n4);
+	w.islandLabels.ensure(n4);
+	w.bodyVals.ensure(n4);
+	w.islands.ensure((size_t)(n + 1) * sizeof(IslandRec));
+	w.coloredList.ensure(n4);
 	int32_t* parent = w.label.as<int32_t>();
-	M3G_LAUNCH(kInitParent, blocksFor(n, 256), 256, s, parent, n);
-	if (w.contactCount > 0)
+	M3G_LAUNCH(kInitParent, blocksFor(n, 256), 256, s, parent, n, active, w.labelCount.as<uint32_t>(),
+			   w.labelCursor.as<uint32_t>());
+	if (M > 0)
 	{
-		M3G_LAUNCH(kUnionContacts, blocksFor(w.contactCount, 256), 256, s, w.C, w.contactCount, w.B.bFlags, parent);
+		M3G_LAUNCH(kUnionContacts, blocksFor(M, 256), 256, s, w.C, M, &dc->contactCount, w.B.bFlags, parent, active);
 	}
 	if (w.jointCount > 0)
 	{
 		M3G_LAUNCH(kUnionJoints, blocksFor(w.jointCount, 128), 128, s, w.joints.as<JointRec>(), w.jointCount, w.B.cold,
-																   parent);
+				   parent, active);
 	}
-	cudaMemsetAsync(&dc->islandCount, 0, sizeof(uint32_t), s);
-	cudaMemsetAsync(&dc->touchingCount, 0, sizeof(uint32_t), s);
-	cudaMemsetAsync(&dc->coloredIslands, 0, 3 * sizeof(uint32_t), s);
-	M3G_LAUNCH(kLabels, blocksFor(n, 256), 256, s, parent, n, w.B.bFlags, w.label.as<int32_t>(), w.islandFlag.as<uint32_t>(),
-											  &dc->islandCount);
-	M3G_LAUNCH(kIslandAwake, blocksFor(n, 256), 256, s, w.B.bFlags, n, w.label.as<int32_t>(), w.islandFlag.as<uint32_t>());
-	M3G_LAUNCH(kIslandWakeBodies, blocksFor(n, 256), 256, s, w.B, n, w.label.as<int32_t>(), w.islandFlag.as<uint32_t>(),
-														 w.cellCountA.as<uint32_t>(), &dc->stableDirty);
-	int32_t cc = w.contactCount;
-	w.removeFlag.ensure((size_t)(cc + 1) * sizeof(uint32_t));
-	if (cc > 0)
-	{
-		M3G_LAUNCH(kContactIslandFlags, blocksFor(cc, 256), 256, s, w.C, cc, w.B.bFlags, w.label.as<int32_t>(),
-																 w.islandFlag.as<uint32_t>(), w.removeFlag.as<uint32_t>(),
-																 &dc->touchingCount);
-	}
-	w.overFlagS.ensure((size_t)(w.jointCount + 1) * sizeof(uint32_t));
-	if (w.jointCount > 0)
-	{
-		M3G_LAUNCH(kJointIslandFlags, blocksFor(w.jointCount, 128), 128, s, w.joints.as<JointRec>(), w.jointCount, w.B.cold,
-																		w.label.as<int32_t>(),
-																		w.islandFlag.as<uint32_t>(),
-																		w.overFlagS.as<uint32_t>());
-	}
+	M3G_LAUNCH(kLabels, blocksFor(n, 256), 256, s, parent, n, w.B.bFlags, w.label.as<int32_t>(),
+			   w.islandFlag.as<uint32_t>(), &dc->islandCount, active);
+	M3G_LAUNCH(kIslandAwake, blocksFor(n, 256), 256, s, w.B.bFlags, n, w.label.as<int32_t>(), w.islandFlag.as<uint32_t>(),
+			   active);
+	M3G_LAUNCH(kIslandBodies, blocksFor(n, 256), 256, s, w.B, n, w.label.as<int32_t>(), w.islandFlag.as<uint32_t>(),
+			   w.labelCount.as<uint32_t>(), &dc->stableDirty, active);
+	// bodies per island: label counts -> starts -> placement
+	scanExclusive(w.labelCount.as<uint32_t>(), w.labelStart.as<uint32_t>(), n, &dc->islandBodies, w.prim, s);
+	M3G_LAUNCH(kIslandListFlags, blocksFor(n, 256), 256, s, w.labelCount.as<uint32_t>(), n,
+			   w.islandListFlag.as<uint32_t>());
+	scanExclusive(w.islandListFlag.as<uint32_t>(), w.islandListOffs.as<uint32_t>(), n, &dc->awakeIslands, w.prim, s);
+	M3G_LAUNCH(kIslandListCompact, blocksFor(n, 256), 256, s, w.islandListFlag.as<uint32_t>(),
+			   w.islandListOffs.as<uint32_t>(), n, w.islandLabels.as<int32_t>());
+	M3G_LAUNCH(kPlaceBodies, blocksFor(n, 256), 256, s, w.B, n, w.label.as<int32_t>(), w.islandFlag.as<uint32_t>(),
+			   w.labelStart.as<uint32_t>(), w.labelCursor.as<uint32_t>(), w.bodyVals.as<uint32_t>(), active);
 
-	int32_t nb = groupByLabel(w, 0, n, w.cellCountA, w.bodyKeys, w.bodyVals, &dc->islandBodies,
-							  &w.hostCounters->islandBodies);
-	int32_t nc = groupByLabel(w, 1, cc, w.removeFlag, w.contactKeys, w.contactVals, &dc->islandContacts,
-							  &w.hostCounters->islandContacts);
-	int32_t nj = groupByLabel(w, 2, w.jointCount, w.overFlagS, w.jointKeys, w.jointVals, &dc->islandJoints,
-							  &w.hostCounters->islandJoints);
-
-	// island table
-	w.islandStartFlag.ensure((size_t)(nb + 1) * sizeof(uint32_t));
-	w.runPairCount.ensure((size_t)(nb + 1) * sizeof(uint32_t));
-	if (nb > 0)
+	// contacts per island, ascending contact index inside each island
+	uint64_t labelMask = (1ull << bitsFor(n)) - 1ull;
+	w.removeFlag.ensure((size_t)(M + 1) * sizeof(uint32_t));
+	w.removeScan.ensure((size_t)(M + 1) * sizeof(uint32_t));
+	w.contactKeys.ensure((size_t)(M + 1) * sizeof(uint64_t));
+	w.contactVals.ensure((size_t)(M + 1) * sizeof(uint32_t));
+	if (M > 0)
 	{
-		M3G_LAUNCH(kIslandStarts, blocksFor(nb, 256), 256, s, w.bodyKeys.as<uint64_t>(), nb,
-														  w.islandStartFlag.as<uint32_t>());
+		M3G_LAUNCH(kContactIslandFlags, blocksFor(M, 256), 256, s, w.C, M, &dc->contactCount, w.B.bFlags,
+				   w.label.as<int32_t>(), w.islandFlag.as<uint32_t>(), w.removeFlag.as<uint32_t>(), &dc->touchingCount,
+				   active);
 	}
-	scanExclusive(w.islandStartFlag.as<uint32_t>(), w.runPairCount.as<uint32_t>(), nb, &dc->awakeIslands, w.prim, s);
-	readCounters(w);
-	int32_t ni = (int32_t)w.hostCounters->awakeIslands;
-	w.islands.ensure((size_t)(ni + 1) * sizeof(IslandRec));
-	if (nb > 0)
+	scanExclusive(w.removeFlag.as<uint32_t>(), w.removeScan.as<uint32_t>(), M, &dc->islandContacts, w.prim, s);
+	if (M > 0)
 	{
-		M3G_LAUNCH(kIslandTable, blocksFor(nb, 256), 256, s, 
-			w.bodyKeys.as<uint64_t>(), nb, w.islandStartFlag.as<uint32_t>(), w.runPairCount.as<uint32_t>(),
-			w.contactKeys.as<uint64_t>(), nc, w.jointKeys.as<uint64_t>(), nj, w.islands.as<IslandRec>(), ni, dc);
+		M3G_LAUNCH(kLabelPairs, blocksFor(M, 256), 256, s, w.removeFlag.as<uint32_t>(), w.removeScan.as<uint32_t>(), M,
+				   w.label.as<int32_t>(), w.C.bodies, w.joints.as<JointRec>(), w.B.bFlags, w.B.cold, 1,
+				   w.contactKeys.as<uint64_t>(), w.contactVals.as<uint32_t>());
+		radixSortPairs(w.contactKeys.as<uint64_t>(), w.contactVals.as<uint32_t>(), M, labelMask, w.prim, s,
+					   &dc->islandContacts);
 	}
-	w.islandCount = ni;
-	w.islandsBuiltFor = n;
-	readCounters(w);
+	// joints per island
+	int32_t J = w.jointCount;
+	if (J > 0)
+	{
+		w.overFlagS.ensure((size_t)(J + 1) * sizeof(uint32_t));
+		w.jointScan.ensure((size_t)(J + 1) * sizeof(uint32_t));
+		w.jointKeys.ensure((size_t)(J + 1) * sizeof(uint64_t));
+		w.jointVals.ensure((size_t)(J + 1) * sizeof(uint32_t));
+		M3G_LAUNCH(kJointIslandFlags, blocksFor(J, 128), 128, s, w.joints.as<JointRec>(), J, w.B.cold,
+				   w.label.as<int32_t>(), w.islandFlag.as<uint32_t>(), w.overFlagS.as<uint32_t>(), active);
+		scanExclusive(w.overFlagS.as<uint32_t>(), w.jointScan.as<uint32_t>(), J, &dc->islandJoints, w.prim, s);
+		M3G_LAUNCH(kLabelPairs, blocksFor(J, 128), 128, s, w.overFlagS.as<uint32_t>(), w.jointScan.as<uint32_t>(), J,
+				   w.label.as<int32_t>(), w.C.bodies, w.joints.as<JointRec>(), w.B.bFlags, w.B.cold, 2,
+				   w.jointKeys.as<uint64_t>(), w.jointVals.as<uint32_t>());
+		radixSortPairs(w.jointKeys.as<uint64_t>(), w.jointVals.as<uint32_t>(), J, labelMask, w.prim, s,
+					   &dc->islandJoints);
+	}
+	M3G_LAUNCH(kIslandTable, blocksFor(n, 128), 128, s, w.islandLabels.as<int32_t>(), n, &dc->awakeIslands,
+			   w.labelStart.as<uint32_t>(), w.labelCount.as<uint32_t>(), w.contactKeys.as<uint64_t>(),
+			   &dc->islandContacts, w.jointKeys.as<uint64_t>(), J > 0 ? &dc->islandJoints : nullptr,
+			   w.islands.as<IslandRec>(), w.coloredList.as<int32_t>(), dc);
+	w.islandMax = n;
 }
 
 // ---------------------------------------------------------------------------
@@ -425,41 +460,43 @@ void launchIslands(DevWorld& w, int32_t n)
 // smallest timer reached kTimeToSleep.
 // ---------------------------------------------------------------------------
 
-__global__ void kSleepInit(const IslandRec* islands, int32_t ni, int32_t* firstNo, uint32_t* minBits)
+__global__ void kSleepInit(const int32_t* islandLabels, int32_t maxIslands, const uint32_t* islandsDev, int32_t* firstNo,
+						   uint32_t* minBits)
 {
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
-	if (k < ni)
+	if (k < maxIslands && k < (int)*islandsDev)
 	{
-		int32_t lab = islands[k].label;
+		int32_t lab = islandLabels[k];
 		firstNo[lab] = 0x7FFFFFFF;
 		minBits[lab] = __float_as_uint(FLT_MAX);
 	}
 }
 
-__global__ void kSleepNoFlags(const BodySoA B, const uint64_t* keys, const uint32_t* vals, int32_t nb, int32_t* firstNo)
+__global__ void kSleepNoFlags(const BodySoA B, const uint32_t* vals, int32_t maxBodies, const uint32_t* bodiesDev,
+							  const int32_t* label, int32_t* firstNo)
 {
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
-	if (k >= nb)
+	if (k >= maxBodies || k >= (int)*bodiesDev)
 	{
 		return;
 	}
 	int32_t i = (int32_t)vals[k];
 	if (!(B.state[i] & kStEnableSleep))
 	{
-		atomicMin(&firstNo[(int32_t)keys[k]], i);
+		atomicMin(&firstNo[label[i]], i);
 	}
 }
 
-__global__ void kSleepUpdate(BodySoA B, const uint64_t* keys, const uint32_t* vals, int32_t nb, const int32_t* firstNo,
-							 uint32_t* minBits, float dt)
+__global__ void kSleepUpdate(BodySoA B, const uint32_t* vals, int32_t maxBodies, const uint32_t* bodiesDev,
+							 const int32_t* label, const int32_t* firstNo, uint32_t* minBits, float dt)
 {
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
-	if (k >= nb)
+	if (k >= maxBodies || k >= (int)*bodiesDev)
 	{
 		return;
 	}
 	int32_t i = (int32_t)vals[k];
-	int32_t lab = (int32_t)keys[k];
+	int32_t lab = label[i];
 	if (i >= firstNo[lab])
 	{
 		return;
@@ -483,20 +520,21 @@ __global__ void kSleepUpdate(BodySoA B, const uint64_t* keys, const uint32_t* va
 	atomicMin(&minBits[lab], __float_as_uint(sl.x));
 }
 
-__global__ void kSleepApply(BodySoA B, const uint64_t* keys, const uint32_t* vals, int32_t nb, const int32_t* firstNo,
-							const uint32_t* minBits, uint32_t* stableDirty)
+__global__ void kSleepApply(BodySoA B, const uint32_t* vals, int32_t maxBodies, const uint32_t* bodiesDev,
+							const int32_t* label, const int32_t* firstNo, const uint32_t* minBits,
+							uint32_t* stableDirty)
 {
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
-	if (k >= nb)
-	{
-		return;
-	}
-	int32_t lab = (int32_t)keys[k];
-	if (firstNo[lab] != 0x7FFFFFFF || !(__uint_as_float(minBits[lab]) >= kTimeToSleep))
+	if (k >= maxBodies || k >= (int)*bodiesDev)
 	{
 		return;
 	}
 	int32_t i = (int32_t)vals[k];
+	int32_t lab = label[i];
+	if (firstNo[lab] != 0x7FFFFFFF || !(__uint_as_float(minBits[lab]) >= kTimeToSleep))
+	{
+		return;
+	}
 	B.state[i] &= (uint8_t)~kStAwake;
 	float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 	B.vel[i] = z;
@@ -508,9 +546,8 @@ __global__ void kSleepApply(BodySoA B, const uint64_t* keys, const uint32_t* val
 void launchSleep(DevWorld& w, float dt)
 {
 	StepCounters* dc = devCounters(w);
-	int32_t ni = w.islandCount;
-	int32_t nb = (int32_t)w.hostCounters->islandBodies;
-	if (ni <= 0 || nb <= 0)
+	int32_t nmax = w.islandMax;
+	if (nmax <= 0)
 	{
 		return;
 	}
@@ -518,15 +555,16 @@ void launchSleep(DevWorld& w, float dt)
 	w.sleepFirstNo.ensure(cap * sizeof(int32_t));
 	w.sleepMin.ensure(cap * sizeof(uint32_t));
 	cudaStream_t s = w.stream;
-	M3G_LAUNCH(kSleepInit, blocksFor(ni, 256), 256, s, w.islands.as<IslandRec>(), ni, w.sleepFirstNo.as<int32_t>(),
-												   w.sleepMin.as<uint32_t>());
-	M3G_LAUNCH(kSleepNoFlags, blocksFor(nb, 256), 256, s, w.B, w.bodyKeys.as<uint64_t>(), w.bodyVals.as<uint32_t>(), nb,
-													  w.sleepFirstNo.as<int32_t>());
-	M3G_LAUNCH(kSleepUpdate, blocksFor(nb, 256), 256, s, w.B, w.bodyKeys.as<uint64_t>(), w.bodyVals.as<uint32_t>(), nb,
-													 w.sleepFirstNo.as<int32_t>(), w.sleepMin.as<uint32_t>(), dt);
-	M3G_LAUNCH(kSleepApply, blocksFor(nb, 256), 256, s, w.B, w.bodyKeys.as<uint64_t>(), w.bodyVals.as<uint32_t>(), nb,
-													w.sleepFirstNo.as<int32_t>(), w.sleepMin.as<uint32_t>(),
-													&dc->stableDirty);
+	const uint32_t* vals = w.bodyVals.as<uint32_t>();
+	const int32_t* lab = w.label.as<int32_t>();
+	M3G_LAUNCH(kSleepInit, blocksFor(nmax, 256), 256, s, w.islandLabels.as<int32_t>(), nmax, &dc->awakeIslands,
+			   w.sleepFirstNo.as<int32_t>(), w.sleepMin.as<uint32_t>());
+	M3G_LAUNCH(kSleepNoFlags, blocksFor(nmax, 256), 256, s, w.B, vals, nmax, &dc->islandBodies, lab,
+			   w.sleepFirstNo.as<int32_t>());
+	M3G_LAUNCH(kSleepUpdate, blocksFor(nmax, 256), 256, s, w.B, vals, nmax, &dc->islandBodies, lab,
+			   w.sleepFirstNo.as<int32_t>(), w.sleepMin.as<uint32_t>(), dt);
+	M3G_LAUNCH(kSleepApply, blocksFor(nmax, 256), 256, s, w.B, vals, nmax, &dc->islandBodies, lab,
+			   w.sleepFirstNo.as<int32_t>(), w.sleepMin.as<uint32_t>(), &dc->stableDirty);
 }
 
 // kinematic integration, one-step force clear, profile counters

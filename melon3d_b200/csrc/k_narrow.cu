@@ -9,15 +9,20 @@
 namespace m3g
 {
 
-__global__ void kNarrowphase(BodySoA B, ContactSoA C, int32_t count, float dt, int8_t* transition)
+__global__ void kNarrowphase(BodySoA B, ContactSoA C, int32_t maxCount, const uint32_t* countDev, float dt,
+							 int8_t* transition)
 {
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
-	if (c >= count)
+	if (c >= maxCount)
+	{
+		return;
+	}
+	transition[c] = 0;
+	if (c >= (int)*countDev)
 	{
 		return;
 	}
 	int2 ab = C.bodies[c];
-	transition[c] = 0;
 	if (!(B.bFlags[ab.x] & kBFAwake) && !(B.bFlags[ab.y] & kBFAwake))
 	{
 		return; // sleeping pair: nothing changes
@@ -145,33 +150,33 @@ void launchNarrowphase(DevWorld& w, float dt)
 {
 	StepCounters* dc = devCounters(w);
 	cudaStream_t s = w.stream;
-	int32_t count = w.contactCount;
-	size_t c4 = (size_t)(count + 1) * sizeof(uint32_t);
-	w.transition.ensure((size_t)count + 1);
+	int32_t M = w.contactMax; // upper bound of the device contact count
+	size_t c4 = (size_t)(M + 1) * sizeof(uint32_t);
+	w.transition.ensure((size_t)M + 1);
 	w.evBeginFlag.ensure(c4);
 	w.evEndFlag.ensure(c4);
 	w.removeScan.ensure(c4);
 	w.moveSrc.ensure(c4);
-	w.evBegin.ensure((size_t)(count + 1) * sizeof(int4));
-	w.evEnd.ensure((size_t)(count + 1) * sizeof(int4));
-	if (count <= 0)
+	w.evBegin.ensure((size_t)(M + 1) * sizeof(int4));
+	w.evEnd.ensure((size_t)(M + 1) * sizeof(int4));
+	if (M <= 0)
 	{
 		cudaMemsetAsync(&dc->beginNP, 0, 2 * sizeof(uint32_t), s);
 		return;
 	}
 	int8_t* tr = w.transition.as<int8_t>();
-	M3G_LAUNCH(kNarrowphase, blocksFor(count, 128), 128, s, w.B, w.C, count, dt, tr);
-	M3G_LAUNCH(kTransitionFlags, blocksFor(count, 256), 256, s, tr, count, w.evBeginFlag.as<uint32_t>(),
-															 w.evEndFlag.as<uint32_t>());
+	M3G_LAUNCH(kNarrowphase, blocksFor(M, 128), 128, s, w.B, w.C, M, &dc->contactCount, dt, tr);
+	M3G_LAUNCH(kTransitionFlags, blocksFor(M, 256), 256, s, tr, M, w.evBeginFlag.as<uint32_t>(),
+			   w.evEndFlag.as<uint32_t>());
 	uint32_t* beginScan = w.removeScan.as<uint32_t>();
 	uint32_t* endScan = (uint32_t*)w.moveSrc.ptr;
-	scanExclusive(w.evBeginFlag.as<uint32_t>(), beginScan, count, &dc->beginNP, w.prim, s);
-	scanExclusive(w.evEndFlag.as<uint32_t>(), endScan, count, &dc->endNP, w.prim, s);
-	M3G_LAUNCH(kTransitionEvents, blocksFor(count, 256), 256, s, w.C, count, tr, beginScan, endScan, w.evBegin.as<int4>(),
-															  w.evEnd.as<int4>());
+	scanExclusive(w.evBeginFlag.as<uint32_t>(), beginScan, M, &dc->beginNP, w.prim, s);
+	scanExclusive(w.evEndFlag.as<uint32_t>(), endScan, M, &dc->endNP, w.prim, s);
+	M3G_LAUNCH(kTransitionEvents, blocksFor(M, 256), 256, s, w.C, M, tr, beginScan, endScan, w.evBegin.as<int4>(),
+			   w.evEnd.as<int4>());
 	int32_t* target = (int32_t*)w.evBeginFlag.ptr; // flags no longer needed
-	M3G_LAUNCH(kWakeDecide, blocksFor(count, 256), 256, s, w.B, w.C, count, tr, target);
-	M3G_LAUNCH(kWakeApply, blocksFor(count, 256), 256, s, w.B, count, target, &dc->stableDirty);
+	M3G_LAUNCH(kWakeDecide, blocksFor(M, 256), 256, s, w.B, w.C, M, tr, target);
+	M3G_LAUNCH(kWakeApply, blocksFor(M, 256), 256, s, w.B, M, target, &dc->stableDirty);
 }
 
 } // namespace m3g

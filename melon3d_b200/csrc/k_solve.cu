@@ -24,10 +24,11 @@ struct SolveParams
 	int iterations;
 };
 
-__global__ void kSolveFree(BodySoA B, const IslandRec* islands, int32_t ni, const uint32_t* bodyVals, SolveParams P)
+__global__ void kSolveFree(BodySoA B, const IslandRec* islands, int32_t ni, const uint32_t* islandsDev,
+						   const uint32_t* bodyVals, SolveParams P)
 {
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
-	if (k >= ni)
+	if (k >= ni || k >= (int)*islandsDev)
 	{
 		return;
 	}
@@ -72,11 +73,11 @@ __device__ __forceinline__ void jointReset(JointRec* J, int ji)
 }
 
 __global__ void kSolveSerial(BodySoA B, ContactSoA C, JointRec* J, const IslandRec* islands, int32_t ni,
-							 const uint32_t* bodyVals, const uint32_t* contactVals, const uint32_t* jointVals,
-							 SolveParams P)
+							 const uint32_t* islandsDev, const uint32_t* bodyVals, const uint32_t* contactVals,
+							 const uint32_t* jointVals, SolveParams P)
 {
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
-	if (k >= ni)
+	if (k >= ni || k >= (int)*islandsDev)
 	{
 		return;
 	}
@@ -145,23 +146,12 @@ __global__ void kSolveSerial(BodySoA B, ContactSoA C, JointRec* J, const IslandR
 
 constexpr int kColorThreads = 256;
 
-__global__ void __launch_bounds__(kColorThreads)
-	kSolveColored(BodySoA B, ContactSoA C, JointRec* J, const IslandRec* islands, int32_t ni, const uint32_t* bodyVals,
-				  const uint32_t* contactVals, const uint32_t* jointVals, uint32_t* colorMask, int32_t* colorOrder,
-				  int32_t* packetMax, int32_t* contactColor, SolveParams P)
+__device__ void colorIsland(BodySoA B, ContactSoA C, JointRec* J, const IslandRec r, const uint32_t* bodyVals,
+							const uint32_t* contactVals, const uint32_t* jointVals, uint32_t* colorMask,
+							int32_t* colorOrder, int32_t* packetMax, int32_t* contactColor, SolveParams P,
+							int32_t* bucketStart, int32_t* colorCountPtr)
 {
-	__shared__ int32_t bucketStart[kMaxGraphColors + 2];
-	__shared__ int32_t colorCount;
-	int k = blockIdx.x;
-	if (k >= ni)
-	{
-		return;
-	}
-	const IslandRec r = islands[k];
-	if (r.kind != 2)
-	{
-		return;
-	}
+	int32_t& colorCount = *colorCountPtr;
 	const int tid = threadIdx.x, nt = blockDim.x;
 	const uint32_t* bodies = bodyVals + r.bodyStart;
 	const uint32_t* contacts = contactVals + r.contactStart;
@@ -378,9 +368,26 @@ __global__ void __launch_bounds__(kColorThreads)
 	}
 }
 
+__global__ void __launch_bounds__(kColorThreads)
+	kSolveColored(BodySoA B, ContactSoA C, JointRec* J, const IslandRec* islands, const int32_t* coloredList,
+				  const uint32_t* coloredDev, const uint32_t* bodyVals, const uint32_t* contactVals,
+				  const uint32_t* jointVals, uint32_t* colorMask, int32_t* colorOrder, int32_t* packetMax,
+				  int32_t* contactColor, SolveParams P)
+{
+	__shared__ int32_t bucketStart[kMaxGraphColors + 2];
+	__shared__ int32_t colorCount;
+	for (int ci = blockIdx.x; ci < (int)*coloredDev; ci += gridDim.x)
+	{
+		colorIsland(B, C, J, islands[coloredList[ci]], bodyVals, contactVals, jointVals, colorMask, colorOrder,
+					packetMax, contactColor, P, bucketStart, &colorCount);
+		__syncthreads();
+	}
+}
+
 void launchSolve(DevWorld& w, float dt, int substeps, V3 gravity, int positionIterations)
 {
-	int32_t ni = w.islandCount;
+	StepCounters* dc = devCounters(w);
+	int32_t ni = w.islandMax; // upper bound; the exact island count is on the device
 	if (ni <= 0)
 	{
 		return;
@@ -395,28 +402,17 @@ void launchSolve(DevWorld& w, float dt, int substeps, V3 gravity, int positionIt
 	P.iterations = positionIterations > 0 ? positionIterations : 2;
 	cudaStream_t s = w.stream;
 	const IslandRec* isl = w.islands.as<IslandRec>();
-	const StepCounters* hc = w.hostCounters;
-	if (hc->freeIslands > 0)
-	{
-		M3G_LAUNCH(kSolveFree, blocksFor(ni, 128), 128, s, w.B, isl, ni, w.bodyVals.as<uint32_t>(), P);
-	}
-	if (hc->serialIslands > 0)
-	{
-		M3G_LAUNCH(kSolveSerial, blocksFor(ni, 64), 64, s, w.B, w.C, w.joints.as<JointRec>(), isl, ni,
-													   w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(),
-													   w.jointVals.as<uint32_t>(), P);
-	}
-	if (hc->coloredIslands > 0)
-	{
-		size_t nc = (size_t)hc->islandContacts + 1;
-		w.colorMask.ensure((size_t)(w.bodyCap + 1) * sizeof(uint32_t));
-		w.colorOrder.ensure(nc * sizeof(int32_t));
-		w.packetMax.ensure(nc * sizeof(int32_t));
-		M3G_LAUNCH(kSolveColored, ni, kColorThreads, s, w.B, w.C, w.joints.as<JointRec>(), isl, ni, w.bodyVals.as<uint32_t>(),
-													w.contactVals.as<uint32_t>(), w.jointVals.as<uint32_t>(),
-													w.colorMask.as<uint32_t>(), w.colorOrder.as<int32_t>(),
-													w.packetMax.as<int32_t>(), w.contactColor.as<int32_t>(), P);
-	}
+	M3G_LAUNCH(kSolveFree, blocksFor(ni, 128), 128, s, w.B, isl, ni, &dc->awakeIslands, w.bodyVals.as<uint32_t>(), P);
+	M3G_LAUNCH(kSolveSerial, blocksFor(ni, 64), 64, s, w.B, w.C, w.joints.as<JointRec>(), isl, ni, &dc->awakeIslands,
+			   w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(), w.jointVals.as<uint32_t>(), P);
+	size_t nc = (size_t)w.contactMax + 1;
+	w.colorMask.ensure((size_t)(w.bodyCap + 1) * sizeof(uint32_t));
+	w.colorOrder.ensure(nc * sizeof(int32_t));
+	w.packetMax.ensure(nc * sizeof(int32_t));
+	M3G_LAUNCH(kSolveColored, 2 * 148, kColorThreads, s, w.B, w.C, w.joints.as<JointRec>(), isl,
+			   w.coloredList.as<int32_t>(), &dc->coloredIslands, w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(),
+			   w.jointVals.as<uint32_t>(), w.colorMask.as<uint32_t>(), w.colorOrder.as<int32_t>(),
+			   w.packetMax.as<int32_t>(), w.contactColor.as<int32_t>(), P);
 }
 
 } // namespace m3g

@@ -40,7 +40,8 @@ struct StepCounters
 	uint32_t serialIslands;
 	uint32_t freeIslands;
 	uint32_t solveErrors;
-	uint32_t pad[5];
+	uint32_t contactCount; // live contacts (device-side count during the step)
+	uint32_t pad[4];
 };
 
 // Host -> device body update record (one per body touched by the API
@@ -114,11 +115,18 @@ struct DevWorld
 	DevBuf activeOver, stableOver;
 	int64_t activeEntries = 0, stableEntries = 0;
 	int32_t activeOverCount = 0, stableOverCount = 0;
-	DevBuf runStarts, runFlag;
-	int32_t runCount = 0;
+	DevBuf runStarts, runFlag, runOffs;
+	int32_t runCount = 0; // upper bound of the cell runs (exact count on the device)
+	DevBuf entryOffsA, entryOffsS, overOffsA, overOffsS;
+	DevBuf keyMasks;                        // OR / AND of the cell keys of both tiers
+	unsigned long long* hostMasks = nullptr; // pinned copy
 
 	// pair build
-	DevBuf runPairCount;          // u32 per run
+	DevBuf runPairCount, runPairOffs; // u32 per run
+	DevBuf overKeys;              // u64 per oversized candidate
+	DevBuf keepScan;
+	int64_t pairTotal = 0;        // admitted pairs (upper bound of new contacts)
+	int32_t contactMax = 0;       // upper bound of the device contact count
 	DevBuf pairKeys;              // u64 admitted candidates in emission order
 	DevBuf overFlag, overScan;    // oversized candidate flags
 	DevBuf existingSet;           // hash set of existing contact keys
@@ -141,6 +149,9 @@ struct DevWorld
 	DevBuf jointKeys, jointVals;
 	DevBuf islandStartFlag, islands; // IslandRec
 	DevBuf islandKinds;
+	DevBuf labelCount, labelStart, labelCursor; // per label: island bodies
+	DevBuf islandListFlag, islandListOffs, islandLabels, coloredList, jointScan;
+	int32_t islandMax = 0; // upper bound of the awake islands of the step
 	int32_t islandCount = 0;
 	int32_t islandsBuiltFor = 0; // body count of the last island build (0: never)
 	DevBuf colorOf;      // per island-contact position: colour 0..8
@@ -161,18 +172,21 @@ struct DevWorld
 bool growBodies(DevWorld& w, int32_t capacity);
 bool growContacts(DevWorld& w, int32_t capacity);
 void readCounters(DevWorld& w); // stream sync + D2H of StepCounters
+void setDeviceCount(DevWorld& w, uint32_t* p, uint32_t v); // stream-ordered store
 StepCounters* devCounters(DevWorld& w);
 
 void launchApplyUploads(DevWorld& w, const BodyUpload* hostRecs, int32_t count);
 void launchMaterialRefresh(DevWorld& w);
 
-// broadphase (k_broadphase.cu)
+// broadphase (k_broadphase.cu); the step's host syncs sit between
+// launchEmitGrid / launchSortGrid and launchPairCount / launchPairEmit
 void launchRefresh(DevWorld& w, int32_t n, float dt, bool rebuildStable, float cellSize);
-void launchBuildActiveGrid(DevWorld& w, int32_t n, float cellSize);
-void launchBuildStableGrid(DevWorld& w, int32_t n, float cellSize);
+void launchEmitGrid(DevWorld& w, int32_t n, float cellSize, bool rebuildStable);
+void launchSortGrid(DevWorld& w, bool rebuildStable);
 void launchFindRuns(DevWorld& w);
-void launchPairs(DevWorld& w, int32_t n, float cellSize);
-void launchCreateContacts(DevWorld& w, int32_t newCount);
+void launchPairCount(DevWorld& w, int32_t n, float cellSize);
+void launchPairEmit(DevWorld& w, int32_t n, float cellSize);
+void launchCreateContacts(DevWorld& w);
 void launchRemoval(DevWorld& w);
 // destroy-time swap-removes computed on the host: move (dst, src) pairs
 void launchContactMoves(DevWorld& w, const int2* hostMoves, int32_t count);

@@ -330,9 +330,21 @@ constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortThreads * kSortItems;
 constexpr int kRadix = 256;
 
-__global__ void kSortHistogram(const uint64_t* keys, int64_t n, int shift, uint32_t* counts, int tiles)
+__device__ __forceinline__ int64_t effectiveN(int64_t nMax, const uint32_t* nDev)
+{
+	if (nDev == nullptr)
+	{
+		return nMax;
+	}
+	int64_t d = (int64_t)*nDev;
+	return d < nMax ? d : nMax;
+}
+
+__global__ void kSortHistogram(const uint64_t* keys, int64_t nMax, const uint32_t* nDev, int shift, uint32_t* counts,
+							   int tiles)
 {
 	__shared__ uint32_t hist[kRadix];
+	const int64_t n = effectiveN(nMax, nDev);
 	for (int d = threadIdx.x; d < kRadix; d += kSortThreads)
 	{
 		hist[d] = 0;
@@ -355,9 +367,10 @@ __global__ void kSortHistogram(const uint64_t* keys, int64_t n, int shift, uint3
 }
 
 __global__ void kSortScatter(const uint64_t* keysIn, const uint32_t* valsIn, uint64_t* keysOut, uint32_t* valsOut,
-							 int64_t n, int shift, const uint32_t* offsets, int tiles)
+							 int64_t nMax, const uint32_t* nDev, int shift, const uint32_t* offsets, int tiles)
 {
 	__shared__ uint32_t warpHist[kSortWarps][kRadix];
+	const int64_t n = effectiveN(nMax, nDev);
 	int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	for (int d = threadIdx.x; d < kSortWarps * kRadix; d += kSortThreads)
 	{
@@ -416,8 +429,10 @@ __global__ void kSortScatter(const uint64_t* keysIn, const uint32_t* valsIn, uin
 	}
 }
 
-__global__ void kCopyPairs(const uint64_t* ks, const uint32_t* vs, uint64_t* kd, uint32_t* vd, int64_t n)
+__global__ void kCopyPairs(const uint64_t* ks, const uint32_t* vs, uint64_t* kd, uint32_t* vd, int64_t nMax,
+						   const uint32_t* nDev)
 {
+	const int64_t n = effectiveN(nMax, nDev);
 	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n)
 	{
@@ -427,7 +442,7 @@ __global__ void kCopyPairs(const uint64_t* ks, const uint32_t* vs, uint64_t* kd,
 }
 
 void radixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, uint64_t varyMask, PrimScratch& s,
-					cudaStream_t stream)
+					cudaStream_t stream, const uint32_t* nDev)
 {
 	if (n <= 1)
 	{
@@ -449,9 +464,9 @@ void radixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, uint64_t varyMask
 		{
 			continue;
 		}
-		M3G_LAUNCH(kSortHistogram, tiles, kSortThreads, stream, k0, n, shift, counts, tiles);
+		M3G_LAUNCH(kSortHistogram, tiles, kSortThreads, stream, k0, n, nDev, shift, counts, tiles);
 		scanExclusive(counts, counts, (int64_t)kRadix * tiles, nullptr, s, stream);
-		M3G_LAUNCH(kSortScatter, tiles, kSortThreads, stream, k0, v0, k1, v1, n, shift, counts, tiles);
+		M3G_LAUNCH(kSortScatter, tiles, kSortThreads, stream, k0, v0, k1, v1, n, nDev, shift, counts, tiles);
 		uint64_t* tk = k0;
 		k0 = k1;
 		k1 = tk;
@@ -462,7 +477,7 @@ void radixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, uint64_t varyMask
 	}
 	if (passes & 1)
 	{
-		M3G_LAUNCH(kCopyPairs, blocksFor(n, 256), 256, stream, k0, v0, keys, vals, n);
+		M3G_LAUNCH(kCopyPairs, blocksFor(n, 256), 256, stream, k0, v0, keys, vals, n, nDev);
 	}
 }
 

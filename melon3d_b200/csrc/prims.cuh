@@ -44,11 +44,12 @@ void scanExclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total
 				   cudaStream_t stream);
 
 // Stable sort of n (key, val) pairs by key.  Only the key bits in `varyMask`
-// are examined: 8-bit digits whose bits are all outside the mask are skipped
-// (the caller passes keyOr ^ keyAnd from reduceKeyRange, or ~0ull).
-// Result lands back in keys/vals.
+// are examined: 8-bit digits whose bits are all outside the mask are skipped.
+// When nDev is given, the element count is min(n, *nDev) read on the device
+// (n is then the host-side upper bound that sizes the grid).  Result lands
+// back in keys/vals.
 void radixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, uint64_t varyMask, PrimScratch& s,
-					cudaStream_t stream);
+					cudaStream_t stream, const uint32_t* nDev = nullptr);
 
 // Device-side OR / AND of n keys into s.reduce (two u64 words), then copied
 // to the pinned host words s.hostReduce[0..1] (stream-ordered, no sync).

@@ -80,13 +80,17 @@ struct m3d_world
 	bool stableForce = false;
 	int32_t stepsSinceStableBuild = 1000;
 	bool anyForcesApplied = false;
-	bool mirrorStale = false;
+	bool mirrorStale = false; // device bodies newer than the host records
+	bool awakeStale = false;  // device awake bits newer than the host records
 
 	// contact sidecar (valid between a step and the next flush)
 	bool contactMirrorValid = false;
 	std::vector<int2> cBodies;
 	std::vector<uint8_t> cFlags;
-	std::vector<int32_t> cPerm; // original device index of each host-side slot
+	std::vector<int32_t> cPerm;   // original device index of each host-side slot
+	std::vector<int32_t> cPos;    // current slot of each original contact (-1: removed)
+	std::vector<int32_t> adjStart; // per body: contacts touching it (original indices), CSR
+	std::vector<int32_t> adjList;
 	bool contactsEdited = false;
 
 	std::vector<m3d_contact_event> beginEvents;
@@ -216,21 +220,33 @@ void syncMirror(m3d_world* w)
 		for (int32_t i = 0; i < n; ++i)
 		{
 			HostBody& b = w->bodies[i];
-			// a body created since the step has no device state yet
-			if (!b.inUse || (anyDirty && i < (int32_t)w->dirtyMask.size() && (w->dirtyMask[i] & kUpAll)))
+			// fields changed through the API since the step are newer on the
+			// host; a body created since the step has no device state yet
+			uint32_t dm = (anyDirty && i < (int32_t)w->dirtyMask.size()) ? w->dirtyMask[i] : 0u;
+			if (!b.inUse || (dm & kUpAll))
 			{
 				continue;
 			}
-			b.position = m3d_v3(w->pinPos[i].x, w->pinPos[i].y, w->pinPos[i].z);
-			b.rotation = { w->pinRot[i].x, w->pinRot[i].y, w->pinRot[i].z, w->pinRot[i].w };
-			b.linearVelocity = m3d_v3(w->pinVel[i].x, w->pinVel[i].y, w->pinVel[i].z);
-			b.angularVelocity = m3d_v3(w->pinAng[i].x, w->pinAng[i].y, w->pinAng[i].z);
-			b.isAwake = (w->pinState[i] & kStAwake) != 0;
-			b.sleepTime = w->pinSleep[i].x;
-			b.smoothedEnergy = w->pinSleep[i].y;
+			if (!(dm & kUpPose))
+			{
+				b.position = m3d_v3(w->pinPos[i].x, w->pinPos[i].y, w->pinPos[i].z);
+				b.rotation = { w->pinRot[i].x, w->pinRot[i].y, w->pinRot[i].z, w->pinRot[i].w };
+			}
+			if (!(dm & kUpVel))
+			{
+				b.linearVelocity = m3d_v3(w->pinVel[i].x, w->pinVel[i].y, w->pinVel[i].z);
+				b.angularVelocity = m3d_v3(w->pinAng[i].x, w->pinAng[i].y, w->pinAng[i].z);
+			}
+			if (!(dm & kUpState))
+			{
+				b.isAwake = (w->pinState[i] & kStAwake) != 0;
+				b.sleepTime = w->pinSleep[i].x;
+				b.smoothedEnergy = w->pinSleep[i].y;
+			}
 		}
 	}
 	w->mirrorStale = false;
+	w->awakeStale = false;
 }
 
 void ensureContactMirror(m3d_world* w)
@@ -251,9 +267,30 @@ void ensureContactMirror(m3d_world* w)
 		cudaStreamSynchronize(d.stream);
 		checkCuda(w, "contact sidecar download");
 	}
+	w->cPos.resize(c);
 	for (int32_t i = 0; i < c; ++i)
 	{
 		w->cPerm[i] = i;
+		w->cPos[i] = i;
+	}
+	// per-body adjacency (CSR over original contact indices)
+	int32_t n = (int32_t)w->bodies.size();
+	w->adjStart.assign((size_t)n + 1, 0);
+	for (int32_t i = 0; i < c; ++i)
+	{
+		++w->adjStart[w->cBodies[i].x + 1];
+		++w->adjStart[w->cBodies[i].y + 1];
+	}
+	for (int32_t b = 0; b < n; ++b)
+	{
+		w->adjStart[b + 1] += w->adjStart[b];
+	}
+	w->adjList.resize((size_t)2 * c);
+	std::vector<int32_t> fill(w->adjStart.begin(), w->adjStart.end() - 1);
+	for (int32_t i = 0; i < c; ++i)
+	{
+		w->adjList[fill[w->cBodies[i].x]++] = i;
+		w->adjList[fill[w->cBodies[i].y]++] = i;
 	}
 	w->contactMirrorValid = true;
 	w->contactsEdited = false;
@@ -263,16 +300,46 @@ void ensureContactMirror(m3d_world* w)
 void removeContactAt(m3d_world* w, int32_t i)
 {
 	int32_t last = (int32_t)w->cBodies.size() - 1;
+	w->cPos[w->cPerm[i]] = -1;
 	if (i != last)
 	{
 		w->cBodies[i] = w->cBodies[last];
 		w->cFlags[i] = w->cFlags[last];
 		w->cPerm[i] = w->cPerm[last];
+		w->cPos[w->cPerm[i]] = i;
 	}
 	w->cBodies.pop_back();
 	w->cFlags.pop_back();
 	w->cPerm.pop_back();
 	w->contactsEdited = true;
+}
+
+// Refresh only the awake bits of the host records (what a destroy needs).
+void syncAwake(m3d_world* w)
+{
+	if (!w->awakeStale)
+	{
+		return;
+	}
+	int32_t n = (int32_t)w->bodies.size();
+	if (n > 0)
+	{
+		ensurePinned(w, n);
+		cudaMemcpyAsync(w->pinState, w->dev.B.state, sizeof(uint8_t) * n, cudaMemcpyDeviceToHost, w->dev.stream);
+		cudaStreamSynchronize(w->dev.stream);
+		bool anyDirty = !w->dirtyList.empty();
+		for (int32_t i = 0; i < n; ++i)
+		{
+			HostBody& b = w->bodies[i];
+			uint32_t dm = (anyDirty && i < (int32_t)w->dirtyMask.size()) ? w->dirtyMask[i] : 0u;
+			if (!b.inUse || (dm & (kUpAll | kUpState)))
+			{
+				continue;
+			}
+			b.isAwake = (w->pinState[i] & kStAwake) != 0;
+		}
+	}
+	w->awakeStale = false;
 }
 
 void wakeBodyHost(m3d_world* w, int32_t index)
@@ -467,10 +534,11 @@ void refreshBroadphase(m3d_world* w, float dt)
 	int32_t n = (int32_t)w->bodies.size();
 	bool rebuildStable = w->stableForce || (w->stableDirty && w->stepsSinceStableBuild >= 4);
 	launchRefresh(d, n, dt, rebuildStable, w->def.gridCellSize);
-	launchBuildActiveGrid(d, n, w->def.gridCellSize);
+	launchEmitGrid(d, n, w->def.gridCellSize, rebuildStable);
+	readCounters(d); // sync: tier sizes and cell-key masks
+	launchSortGrid(d, rebuildStable);
 	if (rebuildStable)
 	{
-		launchBuildStableGrid(d, n, w->def.gridCellSize);
 		w->stableDirty = false;
 		w->stableForce = false;
 		w->stepsSinceStableBuild = 0;
@@ -482,22 +550,13 @@ void refreshBroadphase(m3d_world* w, float dt)
 	w->gridDirty = false;
 }
 
-void appendEvents(m3d_world* w, std::vector<m3d_contact_event>& out, const int4* dev, int32_t count)
+// copy `count` device events to the host list (stream-ordered; the caller syncs)
+void fetchEvents(m3d_world* w, std::vector<int4>& tmp, const int4* dev, int32_t count)
 {
-	if (count <= 0)
+	tmp.resize((size_t)(count > 0 ? count : 0));
+	if (count > 0)
 	{
-		return;
-	}
-	std::vector<int4> tmp((size_t)count);
-	cudaMemcpyAsync(tmp.data(), dev, sizeof(int4) * count, cudaMemcpyDeviceToHost, w->dev.stream);
-	cudaStreamSynchronize(w->dev.stream);
-	for (int32_t k = 0; k < count; ++k)
-	{
-		m3d_contact_event e;
-		e.bodyA = makeId(w, tmp[k].x);
-		e.bodyB = makeId(w, tmp[k].y);
-		e.isSensor = tmp[k].z != 0;
-		out.push_back(e);
+		cudaMemcpyAsync(tmp.data(), dev, sizeof(int4) * count, cudaMemcpyDeviceToHost, w->dev.stream);
 	}
 }
 
@@ -723,35 +782,50 @@ m3d_body_id m3d_body_create(m3d_world* world, const m3d_body_def* bodyDef, const
 
 void m3d_body_destroy(m3d_world* world, m3d_body_id id)
 {
-	syncMirror(world);
 	HostBody* b = getBody(world, id);
 	if (b == nullptr)
 	{
 		return;
 	}
+	syncAwake(world);
 	int32_t index = id.index;
 	ensureContactMirror(world);
-	for (int32_t i = (int32_t)world->cBodies.size() - 1; i >= 0; --i)
+	// The reference scans every contact in descending index order
+	// (src/world.cpp:578-594).  Its matches never move before they are
+	// reached (only non-matching survivors from the tail are swapped down),
+	// so visiting this body's live contacts in descending current slot order
+	// removes the same contacts in the same order.
+	std::vector<int32_t> slots;
+	if (index + 1 < (int32_t)world->adjStart.size())
+	{
+		for (int32_t k = world->adjStart[index]; k < world->adjStart[index + 1]; ++k)
+		{
+			int32_t p = world->cPos[world->adjList[k]];
+			if (p >= 0)
+			{
+				slots.push_back(p);
+			}
+		}
+	}
+	std::sort(slots.begin(), slots.end(), [](int32_t a, int32_t c) { return a > c; });
+	for (int32_t i : slots)
 	{
 		int2 ab = world->cBodies[i];
-		if (ab.x == index || ab.y == index)
+		int32_t other = ab.x == index ? ab.y : ab.x;
+		uint8_t fl = world->cFlags[i];
+		if (fl & kCFTouching)
 		{
-			int32_t other = ab.x == index ? ab.y : ab.x;
-			uint8_t fl = world->cFlags[i];
-			if (fl & kCFTouching)
+			if (!(fl & kCFSensor))
 			{
-				if (!(fl & kCFSensor))
-				{
-					wakeBodyHost(world, other);
-				}
-				m3d_contact_event e;
-				e.bodyA = makeId(world, ab.x);
-				e.bodyB = makeId(world, ab.y);
-				e.isSensor = (fl & kCFSensor) != 0;
-				world->endEvents.push_back(e);
+				wakeBodyHost(world, other);
 			}
-			removeContactAt(world, i);
+			m3d_contact_event e;
+			e.bodyA = makeId(world, ab.x);
+			e.bodyB = makeId(world, ab.y);
+			e.isSensor = (fl & kCFSensor) != 0;
+			world->endEvents.push_back(e);
 		}
+		removeContactAt(world, i);
 	}
 	for (int32_t i = 0; i < (int32_t)world->joints.size(); ++i)
 	{
@@ -1356,54 +1430,76 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	flushHostChanges(world);
 	StepCounters* dc = devCounters(d);
 	cudaMemsetAsync(dc, 0, sizeof(StepCounters), d.stream);
+	setDeviceCount(d, &dc->contactCount, (uint32_t)d.contactCount);
 
-	// broadphase and pair bookkeeping
+	// broadphase and pair bookkeeping: sync 1 inside (tier sizes), sync 2
+	// after counting the admitted pairs (buffer sizes)
 	refreshBroadphase(world, dt);
 	launchFindRuns(d);
-	launchPairs(d, n, world->def.gridCellSize);
-	int32_t newContacts = (int32_t)d.hostCounters->newContacts;
+	launchPairCount(d, n, world->def.gridCellSize);
+	readCounters(d);
 	if (d.hostCounters->hashFail != 0)
 	{
 		setError(world, M3D_GPU_ERR_HASH, "pair hash table overflow");
 	}
-	if (!growContacts(d, d.contactCount + newContacts + 1))
+	int64_t admitted = (int64_t)d.hostCounters->gridPairs + d.hostCounters->overPairs;
+	if (!growContacts(d, (int32_t)(d.contactCount + admitted + 1)))
 	{
 		setError(world, M3D_GPU_ERR_ALLOC, "contact arena growth failed");
 		return;
 	}
-	launchCreateContacts(d, newContacts);
-	int32_t preRemoval = d.contactCount;
+	launchPairEmit(d, n, world->def.gridCellSize);
+	launchCreateContacts(d);
 	launchRemoval(d);
-	(void)preRemoval;
-	appendEvents(world, world->endEvents, d.evRemoval.as<int4>(), (int32_t)d.hostCounters->endRemoval);
 	checkCuda(world, "broadphase");
 	auto tBroad = Clock::now();
 
-	// narrowphase
+	// narrowphase, islands, solve, sleep: no host round trip until the end
 	launchNarrowphase(d, dt);
 	launchAnyAwakeDynamic(d, n);
-	readCounters(d);
-	appendEvents(world, world->beginEvents, d.evBegin.as<int4>(), (int32_t)d.hostCounters->beginNP);
-	appendEvents(world, world->endEvents, d.evEnd.as<int4>(), (int32_t)d.hostCounters->endNP);
-	checkCuda(world, "narrowphase");
 	auto tNarrow = Clock::now();
-
-	int32_t islandCount = 0, touchingCount = 0;
-	if (d.hostCounters->anyAwakeDynamic)
-	{
-		d.contactColor.ensure((size_t)(d.contactCap + 1) * sizeof(int32_t));
-		cudaMemsetAsync(d.contactColor.ptr, 0xFF, (size_t)(d.contactCount + 1) * sizeof(int32_t), d.stream);
-		launchIslands(d, n);
-		islandCount = (int32_t)d.hostCounters->islandCount;
-		touchingCount = (int32_t)d.hostCounters->touchingCount;
-		launchSolve(d, dt, substepCount, hv(world->def.gravity), world->def.positionIterations);
-		launchSleep(d, dt);
-	}
+	d.contactColor.ensure((size_t)(d.contactCap + 1) * sizeof(int32_t));
+	cudaMemsetAsync(d.contactColor.ptr, 0xFF, (size_t)(d.contactMax + 1) * sizeof(int32_t), d.stream);
+	launchIslands(d, n);
+	launchSolve(d, dt, substepCount, hv(world->def.gravity), world->def.positionIterations);
+	launchSleep(d, dt);
 	launchFinish(d, n, dt, world->anyForcesApplied);
 	cudaEventRecord(world->evStop, d.stream);
+
+	// sync 3: counters, then the step's events in one batch
 	readCounters(d);
-	checkCuda(world, "solve");
-	if (d.hostCounters->stableDirty)
+	const StepCounters* hc = d.hostCounters;
+	std::vector<int4> evR, evB, evE;
+	fetchEvents(world, evR, d.evRemoval.as<int4>(), (int32_t)hc->endRemoval);
+	fetchEvents(world, evB, d.evBegin.as<int4>(), (int32_t)hc->beginNP);
+	fetchEvents(world, evE, d.evEnd.as<int4>(), (int32_t)hc->endNP);
+	cudaStreamSynchronize(d.stream);
+	checkCuda(world, "step");
+	auto toEvent = [&](const int4& e) {
+		m3d_contact_event ev;
+		ev.bodyA = makeId(world, e.x);
+		ev.bodyB = makeId(world, e.y);
+		ev.isSensor = e.z != 0;
+		return ev;
+	};
+	for (const int4& e : evR)
+	{
+		world->endEvents.push_back(toEvent(e));
+	}
+	for (const int4& e : evB)
+	{
+		world->beginEvents.push_back(toEvent(e));
+	}
+	for (const int4& e : evE)
+	{
+		world->endEvents.push_back(toEvent(e));
+	}
+	d.contactCount = (int32_t)hc->contactCount;
+	if (hc->anyAwakeDynamic)
+	{
+		d.islandsBuiltFor = n;
+	}
+	if (hc->stableDirty)
 	{
 		world->stableDirty = true;
 	}
@@ -1421,6 +1517,7 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	}
 	cudaEventElapsedTime(&world->lastDeviceMs, world->evStart, world->evStop);
 	world->mirrorStale = true;
+	world->awakeStale = true;
 	world->contactMirrorValid = false;
 
 	auto tEnd = Clock::now();
@@ -1428,11 +1525,11 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	world->profile.narrowphaseMs = toMs(tBroad, tNarrow);
 	world->profile.solverMs = toMs(tNarrow, tEnd);
 	world->profile.stepMs = toMs(tStart, tEnd);
-	world->profile.bodyCount = (int32_t)d.hostCounters->bodyCount;
-	world->profile.awakeBodyCount = (int32_t)d.hostCounters->awakeBodyCount;
+	world->profile.bodyCount = (int32_t)hc->bodyCount;
+	world->profile.awakeBodyCount = (int32_t)hc->awakeBodyCount;
 	world->profile.contactCount = d.contactCount;
-	world->profile.touchingContactCount = touchingCount;
-	world->profile.islandCount = islandCount;
+	world->profile.touchingContactCount = (int32_t)hc->touchingCount;
+	world->profile.islandCount = (int32_t)hc->islandCount;
 }
 
 // ---- GPU extensions ------------------------------------------------------------
@@ -1450,8 +1547,14 @@ void m3d_gpu_read_poses(m3d_world* world, float* positions, float* rotations, in
 	}
 	ensurePinned(world, n);
 	DevWorld& d = world->dev;
-	cudaMemcpyAsync(world->pinPos, d.B.pos, sizeof(float4) * n, cudaMemcpyDeviceToHost, d.stream);
-	cudaMemcpyAsync(world->pinRot, d.B.rot, sizeof(float4) * n, cudaMemcpyDeviceToHost, d.stream);
+	if (positions != nullptr)
+	{
+		cudaMemcpyAsync(world->pinPos, d.B.pos, sizeof(float4) * n, cudaMemcpyDeviceToHost, d.stream);
+	}
+	if (rotations != nullptr)
+	{
+		cudaMemcpyAsync(world->pinRot, d.B.rot, sizeof(float4) * n, cudaMemcpyDeviceToHost, d.stream);
+	}
 	cudaStreamSynchronize(d.stream);
 	for (int32_t i = 0; i < n; ++i)
 	{

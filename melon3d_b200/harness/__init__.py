@@ -47,6 +47,10 @@ def _load():
         _lib.scn_run.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_float)]
         _lib.scn_dynamic_ids.restype = C.c_int32
         _lib.scn_dynamic_ids.argtypes = [C.c_void_p, C.POINTER(api.BodyId), C.c_int32]
+        _lib.scn_churn.restype = None
+        _lib.scn_churn.argtypes = [C.c_void_p]
+        _lib.scn_step_only.restype = None
+        _lib.scn_step_only.argtypes = [C.c_void_p, C.c_int]
         _lib.scn_destroy.restype = None
         _lib.scn_destroy.argtypes = [C.c_void_p]
     return _lib
@@ -84,6 +88,12 @@ class Scene:
         ms = (C.c_float * steps)() if per_step else None
         bs = self.sl.scn_run(self.handle, steps, substeps, C.byref(wall), ms)
         return bs, wall.value, (list(ms) if per_step else None)
+
+    def churn(self):
+        self.sl.scn_churn(self.handle)
+
+    def step_only(self, substeps=4):
+        self.sl.scn_step_only(self.handle, substeps)
 
     def dynamic_ids(self):
         n = self.sl.scn_dynamic_count(self.handle)

@@ -342,6 +342,16 @@ int64_t scn_run(void* scene, int steps, int substeps, double* wallMs, float* ste
 	return bodySubsteps;
 }
 
+// the streaming scene's destroy/spawn of one step, without stepping
+void scn_churn(void* scene) { churnStep(*(Scene*)scene); }
+
+// one step without the churn
+void scn_step_only(void* scene, int substeps)
+{
+	Scene& s = *(Scene*)scene;
+	s.api.world_step(s.world, 1.0f / 60.0f, substeps);
+}
+
 // ids of the live dynamic bodies (creation order)
 int32_t scn_dynamic_ids(void* scene, m3d_body_id* out, int32_t cap)
 {
