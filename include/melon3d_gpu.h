@@ -27,6 +27,9 @@ extern "C" {
 #define M3D_GPU_ERR_CUDA (-1)    /* a CUDA call failed; see m3d_gpu_last_error_string */
 #define M3D_GPU_ERR_ALLOC (-2)   /* device memory could not be grown */
 #define M3D_GPU_ERR_HASH (-3)    /* a pair hash table overflowed (internal sizing bug) */
+#define M3D_GPU_ERR_LIMIT (-4)   /* input larger than a fixed scratch block allows */
+#define M3D_GPU_ERR_PENDING (-5) /* API edits not yet uploaded to the device */
+#define M3D_GPU_ERR_ARGUMENT (-6) /* a required pointer was NULL */
 
 /* Number of body slots (live or free); slot i is body index i. */
 M3D_API int32_t m3d_gpu_body_capacity(m3d_world* world);
@@ -52,6 +55,38 @@ M3D_API int32_t m3d_gpu_step_counters(m3d_world* world, uint32_t* out, int32_t c
 /* 0 when healthy, else the first M3D_GPU_ERR_* seen since creation. */
 M3D_API int32_t m3d_gpu_status(m3d_world* world);
 M3D_API const char* m3d_gpu_last_error_string(m3d_world* world);
+
+/* Sphere cast that allocates nothing.  It has no counterpart in the
+ * reference.  Same result as m3d_world_sphere_cast (melon3d.h), written to
+ * *out; returns M3D_GPU_OK or an M3D_GPU_ERR_* code.
+ *
+ * Why: m3d_world_sphere_cast keeps one candidate record per body slot in a
+ * device buffer that grows with the world, and first uploads any pending API
+ * edits, which can grow other device buffers.  Callers that cannot allocate
+ * device memory at query time need a path that never does: code that runs
+ * under a fixed device-memory budget with the rest of HBM owned by another
+ * allocator, and latency-critical callers (a frame's gameplay queries) for
+ * which a cudaMalloc or cudaFree would stall on the device.  This entry point
+ * uses one block of device memory built into the library (about 1.8 MB per
+ * device) and calls no cudaMalloc, cudaFree or other allocating routine.
+ *
+ * Limits and rules:
+ *  - worlds of at most 65536 body slots (m3d_gpu_body_capacity); larger ones
+ *    are rejected with M3D_GPU_ERR_LIMIT and a message on stderr;
+ *  - edits made through melon3d.h since the last step or query are not
+ *    uploaded here: the call returns M3D_GPU_ERR_PENDING until the world is
+ *    stepped or queried through m3d_world_* once;
+ *  - the first call on a device looks up the block's device address
+ *    (cudaGetSymbolAddress, with the world's device made current) and caches
+ *    it; make that first call before any stream capture on that device;
+ *  - the block is shared by every world and every call on the device and
+ *    keeps the last call's contents (each call resets the parts it reads
+ *    before use); each call waits for its own work, but calls whose work
+ *    overlaps on the GPU (made at the same time from different host threads,
+ *    for different worlds) race on the block: serialise them.
+ * On M3D_GPU_ERR_* returns, *out (when non-NULL) holds a no-hit result. */
+M3D_API int32_t m3d_gpu_sphere_cast_noalloc(m3d_world* world, m3d_vec3 origin, float radius, m3d_vec3 translation,
+                                            uint32_t maskBits, m3d_ray_result* out);
 
 /* Launch accounting (process-wide).  Every kernel launch of the library is
  * counted; the kernel named in m3d_gpu_profiler_reset (its source name, e.g.

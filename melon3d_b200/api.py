@@ -203,7 +203,17 @@ _GPU_PROTOS = {
     "m3d_gpu_profiler_launches": (C.c_longlong, []),
     "m3d_gpu_profiler_kernel": (None, [C.POINTER(C.c_float), C.POINTER(C.c_int32)]),
     "m3d_gpu_profiler_bytes": (None, [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "m3d_gpu_sphere_cast_noalloc": (C.c_int32, [W, Vec3, C.c_float, Vec3, C.c_uint32, C.POINTER(RayResult)]),
 }
+
+# status codes of melon3d_gpu.h
+GPU_OK = 0
+GPU_ERR_CUDA = -1
+GPU_ERR_ALLOC = -2
+GPU_ERR_HASH = -3
+GPU_ERR_LIMIT = -4
+GPU_ERR_PENDING = -5
+GPU_ERR_ARGUMENT = -6
 
 API_SYMBOLS = sorted(_PROTOS)
 GPU_SYMBOLS = sorted(_GPU_PROTOS)

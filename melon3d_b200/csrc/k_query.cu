@@ -408,6 +408,32 @@ void launchSphereCast(DevWorld& w, int32_t n, V3 origin, float radius, V3 transl
 	cudaStreamSynchronize(w.stream);
 }
 
+static_assert(sizeof(CastRec) == kCastRecBytes, "scratch sizing of the fixed-buffer sphere cast");
+
+size_t sphereCastScratchBytes(int32_t n) { return 128 + sizeof(CastRec) * (size_t)(n + 1); }
+
+// The same two kernels over a caller-provided scratch block laid out as
+// above (result at 0, the two pick keys at 64, per-body records at 128).
+// Only the keys need a defined start value; a record is read only for the
+// body whose key won, which this call wrote.
+void launchSphereCastInto(DevWorld& w, int32_t n, V3 origin, float radius, V3 translation, uint32_t maskBits,
+						  void* scratch, RayQueryOut* hostOut)
+{
+	radius = radius > 0.0f ? radius : 0.0f;
+	char* base = (char*)scratch;
+	RayQueryOut* out = (RayQueryOut*)base;
+	unsigned long long* keys = (unsigned long long*)(base + 64);
+	CastRec* recs = (CastRec*)(base + 128);
+	cudaMemsetAsync(keys, 0xFF, 2 * sizeof(unsigned long long), w.stream);
+	if (n > 0)
+	{
+		M3G_LAUNCH(kSphereCast, blocksFor(n, 128), 128, w.stream, w.B, n, origin, radius, translation, maskBits, recs, keys);
+	}
+	M3G_LAUNCH(kSphereCastPick, 1, 1, w.stream, recs, keys, origin, translation, out);
+	cudaMemcpyAsync(hostOut, out, sizeof(RayQueryOut), cudaMemcpyDeviceToHost, w.stream);
+	cudaStreamSynchronize(w.stream);
+}
+
 __global__ void kOverlap(BodySoA B, int32_t n, Box box, uint8_t* flags)
 {
 	int bi = blockIdx.x * blockDim.x + threadIdx.x;

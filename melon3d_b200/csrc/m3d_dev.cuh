@@ -218,4 +218,11 @@ void launchSphereCast(DevWorld& w, int32_t n, V3 origin, float radius, V3 transl
 					  RayQueryOut* hostOut);
 void launchOverlap(DevWorld& w, int32_t n, Box box, uint8_t* hostFlags);
 
+// sphere cast into a caller-provided device scratch block of
+// sphereCastScratchBytes(n) bytes, 16-byte aligned
+constexpr size_t kCastRecBytes = 28;
+size_t sphereCastScratchBytes(int32_t n);
+void launchSphereCastInto(DevWorld& w, int32_t n, V3 origin, float radius, V3 translation, uint32_t maskBits,
+						  void* scratch, RayQueryOut* hostOut);
+
 } // namespace m3g

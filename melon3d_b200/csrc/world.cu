@@ -22,6 +22,7 @@
 #include <stdio.h>
 #include <string.h>
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 using namespace m3g;
@@ -561,6 +562,42 @@ void fetchEvents(m3d_world* w, std::vector<int4>& tmp, const int4* dev, int32_t 
 }
 
 } // namespace
+
+// ---- fixed scratch of m3d_gpu_sphere_cast_noalloc --------------------------------
+// One block of device memory in the library image, sized for worlds of up to
+// kNoAllocCastSlots body slots: the result record, the two pick keys and one
+// candidate record per body slot.  It is shared by every world and every call
+// on a device and keeps the last call's contents.
+constexpr int32_t kNoAllocCastSlots = 65536;
+constexpr size_t kNoAllocCastBytes = 128 + kCastRecBytes * (size_t)(kNoAllocCastSlots + 1);
+static __device__ __align__(256) unsigned char g_noAllocCastScratch[kNoAllocCastBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+static void* g_noAllocCastPtr[kNoAllocMaxDevices] = {};
+static std::mutex g_noAllocCastMutex;
+
+// Device address of the scratch block on `device`, which must be current.
+// Looked up on the first call per device and cached.
+static cudaError_t noAllocCastScratch(int device, void** out)
+{
+	if (device < 0 || device >= kNoAllocMaxDevices)
+	{
+		return cudaErrorInvalidDevice;
+	}
+	std::lock_guard<std::mutex> lock(g_noAllocCastMutex);
+	if (g_noAllocCastPtr[device] == nullptr)
+	{
+		void* ptr = nullptr;
+		cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_noAllocCastScratch);
+		if (e != cudaSuccess)
+		{
+			return e;
+		}
+		g_noAllocCastPtr[device] = ptr;
+	}
+	*out = g_noAllocCastPtr[device];
+	return cudaSuccess;
+}
 
 extern "C"
 {
@@ -1588,6 +1625,91 @@ int32_t m3d_gpu_step_counters(m3d_world* world, uint32_t* out, int32_t capacity)
 }
 int32_t m3d_gpu_status(m3d_world* world) { return world->status; }
 const char* m3d_gpu_last_error_string(m3d_world* world) { return world->errorText; }
+
+int32_t m3d_gpu_sphere_cast_noalloc(m3d_world* world, m3d_vec3 origin, float radius, m3d_vec3 translation,
+									uint32_t maskBits, m3d_ray_result* out)
+{
+	if (world == nullptr || out == nullptr)
+	{
+		fprintf(stderr, "melon3d_gpu: m3d_gpu_sphere_cast_noalloc: world and out must not be NULL\n");
+		return M3D_GPU_ERR_ARGUMENT;
+	}
+	RayQueryOut miss;
+	miss.body = -1;
+	miss.hit = 0;
+	miss.fraction = 2.0f;
+	m3d_vec3 end = m3d_add(origin, translation);
+	miss.point[0] = end.x;
+	miss.point[1] = end.y;
+	miss.point[2] = end.z;
+	miss.normal[0] = miss.normal[1] = miss.normal[2] = 0.0f;
+	*out = toRayResult(world, miss);
+
+	const int32_t n = (int32_t)world->bodies.size();
+	if (n > kNoAllocCastSlots)
+	{
+		fprintf(stderr,
+				"melon3d_gpu: m3d_gpu_sphere_cast_noalloc: the world has %d body slots; the fixed scratch holds %d\n", n,
+				kNoAllocCastSlots);
+		return M3D_GPU_ERR_LIMIT;
+	}
+	// edits made through the API since the last step or query must be uploaded
+	// first, and uploading may grow device buffers
+	if (!world->dirtyList.empty() || (world->contactMirrorValid && world->contactsEdited) ||
+		world->anyMaterialChange || world->jointsDirty || world->jointedPairsDirty || n + 1 > world->dev.bodyCap)
+	{
+		fprintf(stderr, "melon3d_gpu: m3d_gpu_sphere_cast_noalloc: the world has edits not yet on the device; "
+						"step it or run any other query first\n");
+		return M3D_GPU_ERR_PENDING;
+	}
+
+	cudaPointerAttributes attr;
+	int current = 0;
+	if (cudaPointerGetAttributes(&attr, world->dev.B.state) != cudaSuccess || cudaGetDevice(&current) != cudaSuccess)
+	{
+		checkCuda(world, "sphere cast (fixed scratch): device lookup");
+		return M3D_GPU_ERR_CUDA;
+	}
+	const bool switched = attr.device != current;
+	if (switched && cudaSetDevice(attr.device) != cudaSuccess)
+	{
+		checkCuda(world, "sphere cast (fixed scratch): cudaSetDevice");
+		return M3D_GPU_ERR_CUDA;
+	}
+	int32_t rc = M3D_GPU_OK;
+	void* scratch = nullptr;
+	cudaError_t e = noAllocCastScratch(attr.device, &scratch);
+	if (e != cudaSuccess)
+	{
+		char buf[256];
+		snprintf(buf, sizeof(buf), "sphere cast (fixed scratch): cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+		cudaGetLastError();
+		setError(world, M3D_GPU_ERR_CUDA, buf);
+		rc = M3D_GPU_ERR_CUDA;
+	}
+	else
+	{
+		RayQueryOut q;
+		launchSphereCastInto(world->dev, n, hv(origin), radius, hv(translation), maskBits, scratch, &q);
+		cudaError_t le = cudaGetLastError();
+		if (le != cudaSuccess)
+		{
+			char buf[256];
+			snprintf(buf, sizeof(buf), "sphere cast (fixed scratch): %s", cudaGetErrorString(le));
+			setError(world, M3D_GPU_ERR_CUDA, buf);
+			rc = M3D_GPU_ERR_CUDA;
+		}
+		else
+		{
+			*out = toRayResult(world, q);
+		}
+	}
+	if (switched)
+	{
+		cudaSetDevice(current);
+	}
+	return rc;
+}
 
 // ---- snapshots (include/melon3d_debug.h) ----------------------------------------
 
