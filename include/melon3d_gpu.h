@@ -30,6 +30,7 @@ extern "C" {
 #define M3D_GPU_ERR_LIMIT (-4)   /* input larger than a fixed scratch block allows */
 #define M3D_GPU_ERR_PENDING (-5) /* API edits not yet uploaded to the device */
 #define M3D_GPU_ERR_ARGUMENT (-6) /* a required pointer was NULL */
+#define M3D_GPU_ERR_WAIT (-7)    /* a bounded device-side wait ran out (the step's results are suspect) */
 
 /* Number of body slots (live or free); slot i is body index i. */
 M3D_API int32_t m3d_gpu_body_capacity(m3d_world* world);
@@ -90,11 +91,14 @@ M3D_API int32_t m3d_gpu_sphere_cast_noalloc(m3d_world* world, m3d_vec3 origin, f
 
 /* Launch accounting (process-wide).  Every kernel launch of the library is
  * counted; the kernel named in m3d_gpu_profiler_reset (its source name, e.g.
- * "kNarrowphase"; NULL for none) is also bracketed by CUDA events on its
- * stream, so its average device duration can be read while the world runs. */
+ * "kNarrowphase"; "*" for every kernel; NULL for none) is also bracketed by
+ * CUDA events on its stream, so its average device duration can be read while
+ * the world runs.  m3d_gpu_profiler_table writes one line per timed kernel,
+ * "<name> <launches> <total ms>", and returns the table's full length. */
 M3D_API void m3d_gpu_profiler_reset(const char* kernelName);
 M3D_API long long m3d_gpu_profiler_launches(void);
 M3D_API void m3d_gpu_profiler_kernel(float* totalMs, int32_t* launches);
+M3D_API int32_t m3d_gpu_profiler_table(char* out, int32_t capacity);
 /* Host->device and device->host bytes the library copied since the reset. */
 M3D_API void m3d_gpu_profiler_bytes(long long* h2d, long long* d2h);
 

@@ -203,6 +203,7 @@ _GPU_PROTOS = {
     "m3d_gpu_profiler_launches": (C.c_longlong, []),
     "m3d_gpu_profiler_kernel": (None, [C.POINTER(C.c_float), C.POINTER(C.c_int32)]),
     "m3d_gpu_profiler_bytes": (None, [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "m3d_gpu_profiler_table": (C.c_int32, [C.c_char_p, C.c_int32]),
     "m3d_gpu_sphere_cast_noalloc": (C.c_int32, [W, Vec3, C.c_float, Vec3, C.c_uint32, C.POINTER(RayResult)]),
 }
 
@@ -214,6 +215,7 @@ GPU_ERR_HASH = -3
 GPU_ERR_LIMIT = -4
 GPU_ERR_PENDING = -5
 GPU_ERR_ARGUMENT = -6
+GPU_ERR_WAIT = -7
 
 API_SYMBOLS = sorted(_PROTOS)
 GPU_SYMBOLS = sorted(_GPU_PROTOS)

@@ -146,6 +146,7 @@ StepCounters* devCounters(DevWorld& w)
 		cudaMemsetAsync(w.counters.ptr, 0, sizeof(StepCounters), w.stream);
 		cudaMallocHost((void**)&w.hostCounters, sizeof(StepCounters));
 		memset(w.hostCounters, 0, sizeof(StepCounters));
+		w.prim.errorWord = &w.counters.as<StepCounters>()->waitErrors;
 	}
 	return w.counters.as<StepCounters>();
 }

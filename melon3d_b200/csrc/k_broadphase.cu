@@ -184,10 +184,10 @@ void launchRefresh(DevWorld& w, int32_t n, float dt, bool rebuildStable, float c
 // ---------------------------------------------------------------------------
 
 __global__ void kEmitEntries(BodySoA B, int32_t n, float inv, const uint32_t* cnt, const uint32_t* offs,
-							 uint64_t* keys, uint32_t* vals, unsigned long long* masks)
+							 uint64_t* keys, uint32_t* vals, uint32_t* ranges)
 {
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
-	uint64_t kor = 0ull, kand = ~0ull;
+	uint32_t lo[3] = { 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu }, hi[3] = { 0u, 0u, 0u };
 	if (i < n && cnt[i] != 0)
 	{
 		Box b = loadFat(B, i);
@@ -203,23 +203,36 @@ __global__ void kEmitEntries(BodySoA B, int32_t n, float inv, const uint32_t* cn
 					uint64_t k = packCell(x, y, z);
 					keys[o] = k;
 					vals[o] = (uint32_t)i;
-					kor |= k;
-					kand &= k;
+					uint32_t f[3] = { (uint32_t)(k >> 42) & 0x1FFFFFu, (uint32_t)(k >> 21) & 0x1FFFFFu,
+									  (uint32_t)k & 0x1FFFFFu };
+#pragma unroll
+					for (int a = 0; a < 3; ++a)
+					{
+						lo[a] = f[a] < lo[a] ? f[a] : lo[a];
+						hi[a] = f[a] > hi[a] ? f[a] : hi[a];
+					}
 					++o;
 				}
 			}
 		}
 	}
-	// key bits that vary across the tier decide which radix passes run
-	for (int off = 16; off > 0; off >>= 1)
+	// the range of each key field decides which radix passes run
+#pragma unroll
+	for (int a = 0; a < 3; ++a)
 	{
-		kor |= __shfl_xor_sync(0xffffffffu, kor, off);
-		kand &= __shfl_xor_sync(0xffffffffu, kand, off);
-	}
-	if ((threadIdx.x & 31) == 0)
-	{
-		atomicOr(&masks[0], (unsigned long long)kor);
-		atomicAnd(&masks[1], (unsigned long long)kand);
+		uint32_t l = lo[a], h = hi[a];
+		for (int off = 16; off > 0; off >>= 1)
+		{
+			uint32_t lt = __shfl_xor_sync(0xffffffffu, l, off);
+			uint32_t ht = __shfl_xor_sync(0xffffffffu, h, off);
+			l = lt < l ? lt : l;
+			h = ht > h ? ht : h;
+		}
+		if ((threadIdx.x & 31) == 0 && l <= h)
+		{
+			atomicMin(&ranges[a], l);
+			atomicMax(&ranges[3 + a], h);
+		}
 	}
 }
 
@@ -232,12 +245,42 @@ __global__ void kCompactIndices(const uint32_t* flags, const uint32_t* offs, int
 	}
 }
 
-__global__ void kInitMasks(unsigned long long* masks)
+__global__ void kInitRanges(uint32_t* ranges)
 {
-	masks[0] = 0ull;
-	masks[1] = ~0ull;
-	masks[2] = 0ull;
-	masks[3] = ~0ull;
+	for (int t = 0; t < 2; ++t)
+	{
+		for (int a = 0; a < 3; ++a)
+		{
+			ranges[6 * t + a] = 0xFFFFFFFFu;
+			ranges[6 * t + 3 + a] = 0u;
+		}
+	}
+}
+
+// Radix-sort parameters of one tier from its key-field ranges: subtracting
+// each field's minimum keeps the key order (no field borrows from the next)
+// and leaves only the low bits of each field varying.
+static void tierSortBias(const uint32_t* r, uint64_t* bias, uint64_t* vary)
+{
+	uint64_t b = 0ull, v = 0ull;
+	for (int a = 0; a < 3; ++a)
+	{
+		const int shift = 42 - 21 * a;
+		if (r[a] > r[3 + a])
+		{
+			continue; // no entries
+		}
+		uint32_t d = r[3 + a] - r[a];
+		int bits = 0;
+		while (bits < 21 && (d >> bits) != 0)
+		{
+			++bits;
+		}
+		b |= (uint64_t)r[a] << shift;
+		v |= ((1ull << bits) - 1ull) << shift;
+	}
+	*bias = b;
+	*vary = v;
 }
 
 // One tier: counts -> offsets -> (key, body) entries in body order and the
@@ -245,7 +288,7 @@ __global__ void kInitMasks(unsigned long long* masks)
 // so nothing waits for the host; the sort runs after the step's first sync.
 static void emitTier(DevWorld& w, int32_t n, float inv, DevBuf& cnt, DevBuf& over, DevBuf& offs, DevBuf& ooffs,
 					 DevBuf& keys, DevBuf& vals, DevBuf& overList, uint32_t* entryTotal, uint32_t* overTotal,
-					 unsigned long long* masks)
+					 uint32_t* ranges)
 {
 	size_t bound = (size_t)n * kOversizedCellSpan + 1;
 	offs.ensure((size_t)(n + 1) * sizeof(uint32_t));
@@ -258,7 +301,7 @@ static void emitTier(DevWorld& w, int32_t n, float inv, DevBuf& cnt, DevBuf& ove
 	if (n > 0)
 	{
 		M3G_LAUNCH(kEmitEntries, blocksFor(n, 128), 128, w.stream, w.B, n, inv, cnt.as<uint32_t>(), offs.as<uint32_t>(),
-				   keys.as<uint64_t>(), vals.as<uint32_t>(), masks);
+				   keys.as<uint64_t>(), vals.as<uint32_t>(), ranges);
 		M3G_LAUNCH(kCompactIndices, blocksFor(n, 256), 256, w.stream, over.as<uint32_t>(), ooffs.as<uint32_t>(), n,
 				   overList.as<int32_t>());
 	}
@@ -267,34 +310,36 @@ static void emitTier(DevWorld& w, int32_t n, float inv, DevBuf& cnt, DevBuf& ove
 void launchEmitGrid(DevWorld& w, int32_t n, float cellSize, bool rebuildStable)
 {
 	StepCounters* dc = devCounters(w);
-	w.keyMasks.ensure(4 * sizeof(unsigned long long));
-	unsigned long long* masks = w.keyMasks.as<unsigned long long>();
-	M3G_LAUNCH(kInitMasks, 1, 1, w.stream, masks);
+	w.keyRanges.ensure(12 * sizeof(uint32_t));
+	uint32_t* ranges = w.keyRanges.as<uint32_t>();
+	M3G_LAUNCH(kInitRanges, 1, 1, w.stream, ranges);
 	float inv = 1.0f / cellSize;
 	emitTier(w, n, inv, w.cellCountA, w.overFlagA, w.entryOffsA, w.overOffsA, w.activeKeys, w.activeVals, w.activeOver,
-			 &dc->activeEntries, &dc->activeOversized, masks);
+			 &dc->activeEntries, &dc->activeOversized, ranges);
 	if (rebuildStable)
 	{
 		emitTier(w, n, inv, w.cellCountS, w.overFlagS, w.entryOffsS, w.overOffsS, w.stableKeys, w.stableVals,
-				 w.stableOver, &dc->stableEntries, &dc->stableOversized, masks + 2);
+				 w.stableOver, &dc->stableEntries, &dc->stableOversized, ranges + 6);
 	}
-	if (w.hostMasks == nullptr)
+	if (w.hostRanges == nullptr)
 	{
-		cudaMallocHost((void**)&w.hostMasks, 4 * sizeof(unsigned long long));
+		cudaMallocHost((void**)&w.hostRanges, 12 * sizeof(uint32_t));
 	}
-	cudaMemcpyAsync(w.hostMasks, masks, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, w.stream);
+	cudaMemcpyAsync(w.hostRanges, ranges, 12 * sizeof(uint32_t), cudaMemcpyDeviceToHost, w.stream);
 }
 
-// after the first sync of the step: sizes and key masks are on the host
+// after the first sync of the step: sizes and key ranges are on the host
 void launchSortGrid(DevWorld& w, bool rebuildStable)
 {
 	const StepCounters* hc = w.hostCounters;
+	uint64_t bias, vary;
 	w.activeEntries = hc->activeEntries;
 	w.activeOverCount = (int32_t)hc->activeOversized;
 	if (w.activeEntries > 1)
 	{
-		radixSortPairs(w.activeKeys.as<uint64_t>(), w.activeVals.as<uint32_t>(), w.activeEntries,
-					   w.hostMasks[0] ^ w.hostMasks[1], w.prim, w.stream);
+		tierSortBias(w.hostRanges, &bias, &vary);
+		radixSortPairs(w.activeKeys.as<uint64_t>(), w.activeVals.as<uint32_t>(), w.activeEntries, vary, w.prim,
+					   w.stream, nullptr, bias);
 	}
 	if (rebuildStable)
 	{
@@ -302,8 +347,9 @@ void launchSortGrid(DevWorld& w, bool rebuildStable)
 		w.stableOverCount = (int32_t)hc->stableOversized;
 		if (w.stableEntries > 1)
 		{
-			radixSortPairs(w.stableKeys.as<uint64_t>(), w.stableVals.as<uint32_t>(), w.stableEntries,
-						   w.hostMasks[2] ^ w.hostMasks[3], w.prim, w.stream);
+			tierSortBias(w.hostRanges + 6, &bias, &vary);
+			radixSortPairs(w.stableKeys.as<uint64_t>(), w.stableVals.as<uint32_t>(), w.stableEntries, vary, w.prim,
+						   w.stream, nullptr, bias);
 		}
 	}
 }

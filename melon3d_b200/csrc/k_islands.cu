@@ -315,7 +315,7 @@ __device__ __forceinline__ int32_t lowerBound64(const uint64_t* keys, int32_t n,
 __global__ void kIslandTable(const int32_t* islandLabels, int32_t maxIslands, const uint32_t* islandsDev,
 							 const uint32_t* labelStart, const uint32_t* labelCount, const uint64_t* contactKeys,
 							 const uint32_t* contactsDev, const uint64_t* jointKeys, const uint32_t* jointsDev,
-							 IslandRec* islands, int32_t* coloredList, StepCounters* dc)
+							 IslandRec* islands, int32_t* coloredList, int32_t* serialList, StepCounters* dc)
 {
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= maxIslands || k >= (int)*islandsDev)
@@ -342,7 +342,7 @@ __global__ void kIslandTable(const int32_t* islandLabels, int32_t maxIslands, co
 	else if (r.contactCount > 0 || r.jointCount > 0)
 	{
 		r.kind = 1;
-		atomicAdd(&dc->serialIslands, 1u);
+		serialList[atomicAdd(&dc->serialIslands, 1u)] = k;
 	}
 	else
 	{
@@ -380,6 +380,7 @@ void launchIslands(DevWorld& w, int32_t n)
 	w.bodyVals.ensure(n4);
 	w.islands.ensure((size_t)(n + 1) * sizeof(IslandRec));
 	w.coloredList.ensure(n4);
+	w.serialList.ensure(n4);
 	int32_t* parent = w.label.as<int32_t>();
 	M3G_LAUNCH(kInitParent, blocksFor(n, 256), 256, s, parent, n, active, w.labelCount.as<uint32_t>(),
 			   w.labelCursor.as<uint32_t>());
@@ -449,7 +450,7 @@ void launchIslands(DevWorld& w, int32_t n)
 	M3G_LAUNCH(kIslandTable, blocksFor(n, 128), 128, s, w.islandLabels.as<int32_t>(), n, &dc->awakeIslands,
 			   w.labelStart.as<uint32_t>(), w.labelCount.as<uint32_t>(), w.contactKeys.as<uint64_t>(),
 			   &dc->islandContacts, w.jointKeys.as<uint64_t>(), J > 0 ? &dc->islandJoints : nullptr,
-			   w.islands.as<IslandRec>(), w.coloredList.as<int32_t>(), dc);
+			   w.islands.as<IslandRec>(), w.coloredList.as<int32_t>(), w.serialList.as<int32_t>(), dc);
 	w.islandMax = n;
 }
 

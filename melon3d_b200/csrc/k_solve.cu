@@ -3,7 +3,7 @@
 //  - free islands (one body, no contacts, no joints): integrate and
 //    reconstruct per substep, one thread per body;
 //  - small islands (< 300 contacts): the reference's serial Gauss-Seidel in
-//    ascending contact order (src/xpbd.cpp:898-974), one thread per island;
+//    ascending contact order (src/xpbd.cpp:898-974), one warp per island;
 //  - big islands (>= 300 contacts): the reference's graph-coloured solve
 //    (src/xpbd.cpp:1167-1369), one CTA per island: greedy first-fit colouring
 //    in contact order, colour buckets solved in parallel (bodies in a bucket
@@ -72,74 +72,97 @@ __device__ __forceinline__ void jointReset(JointRec* J, int ji)
 	J[ji].motorLambda = 0.0f;
 }
 
-__global__ void kSolveSerial(BodySoA B, ContactSoA C, JointRec* J, const IslandRec* islands, int32_t ni,
-							 const uint32_t* islandsDev, const uint32_t* bodyVals, const uint32_t* contactVals,
-							 const uint32_t* jointVals, SolveParams P)
+// One warp per small island.  The per-element stages of a substep whose
+// elements are independent - integration and velocity reconstruction of each
+// body, preparation of each contact (which reads only body state and writes
+// only its own contact) - run across the lanes; the Gauss-Seidel sweeps,
+// whose order is the result, run on lane 0 in ascending contact order.
+// __syncwarp() orders the global-memory writes of one stage before the reads
+// of the next.
+constexpr int kSerialWarpsPerBlock = 8;
+
+__global__ void __launch_bounds__(32 * kSerialWarpsPerBlock)
+	kSolveSerial(BodySoA B, ContactSoA C, JointRec* J, const IslandRec* islands, const int32_t* serialList,
+				 const uint32_t* serialDev, const uint32_t* bodyVals, const uint32_t* contactVals,
+				 const uint32_t* jointVals, SolveParams P)
 {
-	int k = blockIdx.x * blockDim.x + threadIdx.x;
-	if (k >= ni || k >= (int)*islandsDev)
+	const int lane = threadIdx.x & 31;
+	const int warps = gridDim.x * kSerialWarpsPerBlock;
+	const int count = (int)*serialDev;
+	for (int si = blockIdx.x * kSerialWarpsPerBlock + (threadIdx.x >> 5); si < count; si += warps)
 	{
-		return;
-	}
-	const IslandRec r = islands[k];
-	if (r.kind != 1)
-	{
-		return;
-	}
-	const uint32_t* bodies = bodyVals + r.bodyStart;
-	const uint32_t* contacts = contactVals + r.contactStart;
-	const uint32_t* joints = jointVals + r.jointStart;
-	if (r.jointCount > 0)
-	{
-		for (int b = 0; b < r.bodyCount; ++b)
+		const IslandRec r = islands[serialList[si]];
+		const uint32_t* bodies = bodyVals + r.bodyStart;
+		const uint32_t* contacts = contactVals + r.contactStart;
+		const uint32_t* joints = jointVals + r.jointStart;
+		if (r.jointCount > 0)
 		{
-			refreshInvInertia(B, (int)bodies[b]);
-		}
-		for (int j = 0; j < r.jointCount; ++j)
-		{
-			jointPrepare(B, J, (int)joints[j]);
-		}
-	}
-	for (int sub = 0; sub < P.substeps; ++sub)
-	{
-		for (int b = 0; b < r.bodyCount; ++b)
-		{
-			integrateBody(B, (int)bodies[b], P.h, P.gravity);
-		}
-		for (int c = 0; c < r.contactCount; ++c)
-		{
-			prepareContact(B, C, (int)contacts[c], P.h);
-		}
-		for (int j = 0; j < r.jointCount; ++j)
-		{
-			jointReset(J, (int)joints[j]);
-		}
-		for (int it = 0; it < P.iterations; ++it)
-		{
-			for (int j = 0; j < r.jointCount; ++j)
+			for (int b = lane; b < r.bodyCount; b += 32)
 			{
-				jointPosition(B, J, (int)joints[j], P.h);
+				refreshInvInertia(B, (int)bodies[b]);
 			}
-			for (int c = 0; c < r.contactCount; ++c)
+			__syncwarp();
+			if (lane == 0)
 			{
-				solveContactNormals(B, C, (int)contacts[c], P.maxCorrection);
+				for (int j = 0; j < r.jointCount; ++j)
+				{
+					jointPrepare(B, J, (int)joints[j]);
+				}
 			}
+			__syncwarp();
 		}
-		for (int c = 0; c < r.contactCount; ++c)
+		for (int sub = 0; sub < P.substeps; ++sub)
 		{
-			applyContactFriction(B, C, (int)contacts[c]);
-		}
-		for (int b = 0; b < r.bodyCount; ++b)
-		{
-			reconstructBody(B, (int)bodies[b], P.invH);
-		}
-		for (int c = 0; c < r.contactCount; ++c)
-		{
-			solveContactVelocity(B, C, (int)contacts[c], P.h, P.gravityLen);
-		}
-		for (int j = 0; j < r.jointCount; ++j)
-		{
-			jointVelocity(B, J, (int)joints[j], P.h);
+			for (int b = lane; b < r.bodyCount; b += 32)
+			{
+				integrateBody(B, (int)bodies[b], P.h, P.gravity);
+			}
+			__syncwarp();
+			for (int c = lane; c < r.contactCount; c += 32)
+			{
+				prepareContact(B, C, (int)contacts[c], P.h);
+			}
+			__syncwarp();
+			if (lane == 0)
+			{
+				for (int j = 0; j < r.jointCount; ++j)
+				{
+					jointReset(J, (int)joints[j]);
+				}
+				for (int it = 0; it < P.iterations; ++it)
+				{
+					for (int j = 0; j < r.jointCount; ++j)
+					{
+						jointPosition(B, J, (int)joints[j], P.h);
+					}
+					for (int c = 0; c < r.contactCount; ++c)
+					{
+						solveContactNormals(B, C, (int)contacts[c], P.maxCorrection);
+					}
+				}
+				for (int c = 0; c < r.contactCount; ++c)
+				{
+					applyContactFriction(B, C, (int)contacts[c]);
+				}
+			}
+			__syncwarp();
+			for (int b = lane; b < r.bodyCount; b += 32)
+			{
+				reconstructBody(B, (int)bodies[b], P.invH);
+			}
+			__syncwarp();
+			if (lane == 0)
+			{
+				for (int c = 0; c < r.contactCount; ++c)
+				{
+					solveContactVelocity(B, C, (int)contacts[c], P.h, P.gravityLen);
+				}
+				for (int j = 0; j < r.jointCount; ++j)
+				{
+					jointVelocity(B, J, (int)joints[j], P.h);
+				}
+			}
+			__syncwarp();
 		}
 	}
 }
@@ -403,8 +426,12 @@ void launchSolve(DevWorld& w, float dt, int substeps, V3 gravity, int positionIt
 	cudaStream_t s = w.stream;
 	const IslandRec* isl = w.islands.as<IslandRec>();
 	M3G_LAUNCH(kSolveFree, blocksFor(ni, 128), 128, s, w.B, isl, ni, &dc->awakeIslands, w.bodyVals.as<uint32_t>(), P);
-	M3G_LAUNCH(kSolveSerial, blocksFor(ni, 64), 64, s, w.B, w.C, w.joints.as<JointRec>(), isl, ni, &dc->awakeIslands,
-			   w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(), w.jointVals.as<uint32_t>(), P);
+	// enough warps for every serial island of a rain or pile step to start at once
+	int serialBlocks = (ni + kSerialWarpsPerBlock - 1) / kSerialWarpsPerBlock;
+	serialBlocks = serialBlocks < 148 * 8 ? serialBlocks : 148 * 8;
+	M3G_LAUNCH(kSolveSerial, serialBlocks, 32 * kSerialWarpsPerBlock, s, w.B, w.C, w.joints.as<JointRec>(), isl,
+			   w.serialList.as<int32_t>(), &dc->serialIslands, w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(),
+			   w.jointVals.as<uint32_t>(), P);
 	size_t nc = (size_t)w.contactMax + 1;
 	w.colorMask.ensure((size_t)(w.bodyCap + 1) * sizeof(uint32_t));
 	w.colorOrder.ensure(nc * sizeof(int32_t));

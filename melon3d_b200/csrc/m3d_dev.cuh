@@ -39,7 +39,7 @@ struct StepCounters
 	uint32_t coloredIslands;
 	uint32_t serialIslands;
 	uint32_t freeIslands;
-	uint32_t solveErrors;
+	uint32_t waitErrors; // bounded device waits that ran out (non-zero: results of the step are suspect)
 	uint32_t contactCount; // live contacts (device-side count during the step)
 	uint32_t pad[4];
 };
@@ -118,8 +118,8 @@ struct DevWorld
 	DevBuf runStarts, runFlag, runOffs;
 	int32_t runCount = 0; // upper bound of the cell runs (exact count on the device)
 	DevBuf entryOffsA, entryOffsS, overOffsA, overOffsS;
-	DevBuf keyMasks;                        // OR / AND of the cell keys of both tiers
-	unsigned long long* hostMasks = nullptr; // pinned copy
+	DevBuf keyRanges;               // per tier: min x, y, z then max x, y, z of the key fields (u32)
+	uint32_t* hostRanges = nullptr; // pinned copy, 12 words
 
 	// pair build
 	DevBuf runPairCount, runPairOffs; // u32 per run
@@ -150,7 +150,7 @@ struct DevWorld
 	DevBuf islandStartFlag, islands; // IslandRec
 	DevBuf islandKinds;
 	DevBuf labelCount, labelStart, labelCursor; // per label: island bodies
-	DevBuf islandListFlag, islandListOffs, islandLabels, coloredList, jointScan;
+	DevBuf islandListFlag, islandListOffs, islandLabels, coloredList, serialList, jointScan;
 	int32_t islandMax = 0; // upper bound of the awake islands of the step
 	int32_t islandCount = 0;
 	int32_t islandsBuiltFor = 0; // body count of the last island build (0: never)

@@ -3,8 +3,10 @@
 #include "prims.cuh"
 
 #include <atomic>
+#include <map>
 #include <mutex>
 #include <stdio.h>
+#include <string.h>
 #include <string>
 #include <utility>
 #include <vector>
@@ -20,10 +22,18 @@ std::atomic<long long> gLaunches{ 0 };
 std::mutex gMu;
 std::string gTarget;
 std::vector<cudaEvent_t> gPool;
-std::vector<std::pair<cudaEvent_t, cudaEvent_t>> gPairs;
+struct TimedLaunch
+{
+	const char* name;
+	cudaEvent_t start, stop;
+};
+std::vector<TimedLaunch> gPairs;
 cudaEvent_t gOpen = nullptr;
 double gTimedMs = 0.0;
 long long gTimedLaunches = 0;
+std::map<std::string, std::pair<double, long long>> gPerKernel; // "*" target: every kernel
+
+bool timed(const char* name) { return gTarget == "*" || gTarget == name; }
 
 cudaEvent_t takeEvent()
 {
@@ -44,12 +54,15 @@ void drainPairs()
 	for (auto& p : gPairs)
 	{
 		float ms = 0.0f;
-		cudaEventSynchronize(p.second);
-		cudaEventElapsedTime(&ms, p.first, p.second);
+		cudaEventSynchronize(p.stop);
+		cudaEventElapsedTime(&ms, p.start, p.stop);
 		gTimedMs += ms;
 		++gTimedLaunches;
-		gPool.push_back(p.first);
-		gPool.push_back(p.second);
+		auto& k = gPerKernel[p.name];
+		k.first += ms;
+		++k.second;
+		gPool.push_back(p.start);
+		gPool.push_back(p.stop);
 	}
 	gPairs.clear();
 }
@@ -81,7 +94,7 @@ void launchBegin(const char* name, cudaStream_t s)
 		return;
 	}
 	std::lock_guard<std::mutex> lock(gMu);
-	if (gTarget == name)
+	if (timed(name))
 	{
 		gOpen = takeEvent();
 		cudaEventRecord(gOpen, s);
@@ -95,11 +108,11 @@ void launchEnd(const char* name, cudaStream_t s)
 		return;
 	}
 	std::lock_guard<std::mutex> lock(gMu);
-	if (gOpen != nullptr && gTarget == name)
+	if (gOpen != nullptr && timed(name))
 	{
 		cudaEvent_t stop = takeEvent();
 		cudaEventRecord(stop, s);
-		gPairs.emplace_back(gOpen, stop);
+		gPairs.push_back({ name, gOpen, stop });
 		gOpen = nullptr;
 		if (gPairs.size() >= 4096)
 		{
@@ -159,9 +172,9 @@ void DevBuf::release()
 
 void PrimScratch::release()
 {
-	scanA.release();
-	scanB.release();
-	scanC.release();
+	scanStatus.release();
+	scanTicket.release();
+	waitError.release();
 	sortKeys.release();
 	sortVals.release();
 	sortCounts.release();
@@ -174,12 +187,21 @@ void PrimScratch::release()
 }
 
 // ---------------------------------------------------------------------------
-// scan: 256 threads x 8 items per block; block totals are scanned recursively
+// scan: one pass with decoupled look-back.  Each CTA takes the next 2048-word
+// tile from a ticket counter (so a CTA only ever waits on tiles whose CTAs
+// are already running), publishes its tile total, then its warp 0 walks back
+// over the predecessors' published words, 32 at a time, until it meets an
+// inclusive prefix.  Status words carry the call's epoch, so words left by
+// earlier calls read as "not yet published" and nothing is cleared between
+// calls.  Waits are bounded: a wait that runs out counts as a zero
+// contribution and raises the caller's error word.
 // ---------------------------------------------------------------------------
 
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
+constexpr uint32_t kLookbackSpinLimit = 1u << 22;
+constexpr uint32_t kEpochLimit = 1u << 30;
 
 __device__ __forceinline__ uint32_t warpInclusive(uint32_t v)
 {
@@ -196,7 +218,18 @@ __device__ __forceinline__ uint32_t warpInclusive(uint32_t v)
 	return v;
 }
 
-// exclusive scan of one tile in place; returns the tile total to thread 0..N
+__device__ __forceinline__ uint32_t warpSum(uint32_t v)
+{
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+	{
+		v += __shfl_xor_sync(0xffffffffu, v, o);
+	}
+	return v;
+}
+
+// exclusive scan of one value per thread across the CTA; the CTA total is
+// left in warpSums[kScanThreads / 32]
 __device__ uint32_t blockExclusive(uint32_t v, uint32_t* warpSums)
 {
 	int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -224,10 +257,26 @@ __device__ uint32_t blockExclusive(uint32_t v, uint32_t* warpSums)
 	return r;
 }
 
-__global__ void kScanTiles(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* tileSums)
+// status word: epoch (30 bits) << 34 | flag (1 aggregate, 2 inclusive) << 32 | value
+__device__ __forceinline__ uint64_t statusWord(uint32_t epoch, uint32_t flag, uint32_t value)
+{
+	return ((uint64_t)epoch << 34) | ((uint64_t)flag << 32) | value;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+	kScanLookback(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total, uint64_t* status,
+				  uint32_t* ticket, uint32_t epoch, uint32_t* error)
 {
 	__shared__ uint32_t warpSums[kScanThreads / 32 + 1];
-	int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+	__shared__ uint32_t sTile, sPrefix;
+	const int tiles = (int)((n + kScanTile - 1) / kScanTile);
+	if (threadIdx.x == 0)
+	{
+		sTile = atomicAdd(&ticket[0], 1u);
+	}
+	__syncthreads();
+	const int t = (int)sTile;
+	const int64_t base = (int64_t)t * kScanTile + (int64_t)threadIdx.x * kScanItems;
 	uint32_t vals[kScanItems];
 	uint32_t sum = 0;
 #pragma unroll
@@ -238,6 +287,70 @@ __global__ void kScanTiles(const uint32_t* in, uint32_t* out, int64_t n, uint32_
 		sum += vals[k];
 	}
 	uint32_t pre = blockExclusive(sum, warpSums);
+	const uint32_t agg = warpSums[kScanThreads / 32];
+	volatile uint64_t* vs = status;
+	if (threadIdx.x < 32)
+	{
+		const int lane = threadIdx.x;
+		uint32_t excl = 0;
+		if (t == 0)
+		{
+			if (lane == 0)
+			{
+				vs[0] = statusWord(epoch, 2u, agg);
+			}
+		}
+		else
+		{
+			if (lane == 0)
+			{
+				vs[t] = statusWord(epoch, 1u, agg);
+			}
+			int idx = t - 1;
+			while (true)
+			{
+				const int j = idx - lane;
+				uint32_t flag = 2u, value = 0u; // lanes before tile 0 contribute nothing
+				if (j >= 0)
+				{
+					flag = 0u;
+					for (uint32_t it = 0; flag == 0u; ++it)
+					{
+						uint64_t w = vs[j];
+						if ((uint32_t)(w >> 34) == epoch)
+						{
+							flag = (uint32_t)(w >> 32) & 3u;
+							value = (uint32_t)w;
+						}
+						else if (it >= kLookbackSpinLimit)
+						{
+							atomicOr(error, 1u);
+							flag = 2u;
+						}
+					}
+				}
+				const uint32_t inclusive = __ballot_sync(0xffffffffu, flag == 2u);
+				if (inclusive != 0u)
+				{
+					const int stop = __ffs((int)inclusive) - 1;
+					excl += warpSum(lane <= stop ? value : 0u);
+					break;
+				}
+				excl += warpSum(value);
+				idx -= 32;
+			}
+			if (lane == 0)
+			{
+				vs[t] = statusWord(epoch, 2u, excl + agg);
+			}
+		}
+		if (lane == 0)
+		{
+			sPrefix = excl;
+		}
+	}
+	__syncthreads();
+	pre += sPrefix;
 #pragma unroll
 	for (int k = 0; k < kScanItems; ++k)
 	{
@@ -248,46 +361,19 @@ __global__ void kScanTiles(const uint32_t* in, uint32_t* out, int64_t n, uint32_
 		}
 		pre += vals[k];
 	}
-	if (threadIdx.x == 0 && tileSums != nullptr)
+	if (threadIdx.x == 0)
 	{
-		tileSums[blockIdx.x] = warpSums[kScanThreads / 32];
-	}
-}
-
-__global__ void kScanAdd(uint32_t* out, int64_t n, const uint32_t* tileOffsets)
-{
-	int64_t base = (int64_t)blockIdx.x * kScanTile;
-	uint32_t add = tileOffsets[blockIdx.x];
-	for (int k = threadIdx.x; k < kScanTile; k += kScanThreads)
-	{
-		int64_t i = base + k;
-		if (i < n)
+		if (t == tiles - 1 && total != nullptr)
 		{
-			out[i] += add;
+			*total = sPrefix + agg;
+		}
+		// the last CTA to finish rewinds the ticket for the next call
+		if (atomicAdd(&ticket[1], 1u) == (uint32_t)tiles - 1u)
+		{
+			ticket[0] = 0u;
+			ticket[1] = 0u;
 		}
 	}
-}
-
-__global__ void kScanTotal(const uint32_t* in, const uint32_t* out, int64_t n, uint32_t* total)
-{
-	*total = n > 0 ? out[n - 1] + in[n - 1] : 0u;
-}
-
-// total of a single-tile scan is produced by kScanTiles into tileSums
-static void scanLevel(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total, DevBuf* levels, int level,
-					  cudaStream_t stream)
-{
-	int64_t tiles = (n + kScanTile - 1) / kScanTile;
-	if (tiles <= 1)
-	{
-		M3G_LAUNCH(kScanTiles, 1, kScanThreads, stream, in, out, n, total);
-		return;
-	}
-	levels[level].ensure((size_t)tiles * sizeof(uint32_t));
-	uint32_t* sums = levels[level].as<uint32_t>();
-	M3G_LAUNCH(kScanTiles, (unsigned)tiles, kScanThreads, stream, in, out, n, sums);
-	scanLevel(sums, sums, tiles, total, levels, level + 1, stream);
-	M3G_LAUNCH(kScanAdd, (unsigned)tiles, kScanThreads, stream, out, n, sums);
 }
 
 void scanExclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total, PrimScratch& s,
@@ -301,22 +387,23 @@ void scanExclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total
 		}
 		return;
 	}
-	DevBuf levels[3] = {};
-	levels[0] = s.scanA;
-	levels[1] = s.scanB;
-	levels[2] = s.scanC;
-	// the in-place aliasing is fine: each tile reads all its inputs before
-	// writing, and tiles are disjoint
-	if (total == nullptr)
+	const int64_t tiles = (n + kScanTile - 1) / kScanTile;
+	s.scanTicket.ensureZeroed(4 * sizeof(uint32_t), stream);
+	s.waitError.ensureZeroed(4 * sizeof(uint32_t), stream);
+	void* before = s.scanStatus.ptr;
+	s.scanStatus.ensureZeroed((size_t)(tiles + 1) * sizeof(uint64_t), stream);
+	if (s.scanStatus.ptr != before || ++s.scanEpoch >= kEpochLimit)
 	{
-		// scan the tile sums without a total: reuse a scratch word
-		levels[2].ensure(sizeof(uint32_t) * 4);
+		// fresh (zeroed) status words, or the epoch wrapped: restart at 1
+		if (s.scanStatus.ptr == before)
+		{
+			cudaMemsetAsync(s.scanStatus.ptr, 0, s.scanStatus.bytes, stream);
+		}
+		s.scanEpoch = 1;
 	}
-	uint32_t* tot = total != nullptr ? total : levels[2].as<uint32_t>();
-	scanLevel(in, out, n, tot, levels, 0, stream);
-	s.scanA = levels[0];
-	s.scanB = levels[1];
-	s.scanC = levels[2];
+	uint32_t* err = s.errorWord != nullptr ? s.errorWord : s.waitError.as<uint32_t>();
+	M3G_LAUNCH(kScanLookback, (unsigned)tiles, kScanThreads, stream, in, out, n, total, s.scanStatus.as<uint64_t>(),
+			   s.scanTicket.as<uint32_t>(), s.scanEpoch, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -340,8 +427,8 @@ __device__ __forceinline__ int64_t effectiveN(int64_t nMax, const uint32_t* nDev
 	return d < nMax ? d : nMax;
 }
 
-__global__ void kSortHistogram(const uint64_t* keys, int64_t nMax, const uint32_t* nDev, int shift, uint32_t* counts,
-							   int tiles)
+__global__ void kSortHistogram(const uint64_t* keys, int64_t nMax, const uint32_t* nDev, int shift, uint64_t bias,
+							   uint32_t* counts, int tiles)
 {
 	__shared__ uint32_t hist[kRadix];
 	const int64_t n = effectiveN(nMax, nDev);
@@ -356,7 +443,7 @@ __global__ void kSortHistogram(const uint64_t* keys, int64_t nMax, const uint32_
 		int64_t i = base + k;
 		if (i < n)
 		{
-			atomicAdd(&hist[(uint32_t)(keys[i] >> shift) & 0xFFu], 1u);
+			atomicAdd(&hist[(uint32_t)((keys[i] - bias) >> shift) & 0xFFu], 1u);
 		}
 	}
 	__syncthreads();
@@ -367,7 +454,8 @@ __global__ void kSortHistogram(const uint64_t* keys, int64_t nMax, const uint32_
 }
 
 __global__ void kSortScatter(const uint64_t* keysIn, const uint32_t* valsIn, uint64_t* keysOut, uint32_t* valsOut,
-							 int64_t nMax, const uint32_t* nDev, int shift, const uint32_t* offsets, int tiles)
+							 int64_t nMax, const uint32_t* nDev, int shift, uint64_t bias, const uint32_t* offsets,
+							 int tiles)
 {
 	__shared__ uint32_t warpHist[kSortWarps][kRadix];
 	const int64_t n = effectiveN(nMax, nDev);
@@ -385,7 +473,7 @@ __global__ void kSortScatter(const uint64_t* keysIn, const uint32_t* valsIn, uin
 	{
 		int64_t i = base + r * 32 + lane;
 		bool valid = i < n;
-		uint32_t d = valid ? ((uint32_t)(keysIn[i] >> shift) & 0xFFu) : 0x100u;
+		uint32_t d = valid ? ((uint32_t)((keysIn[i] - bias) >> shift) & 0xFFu) : 0x100u;
 		uint32_t peers = __match_any_sync(0xffffffffu, d);
 		if (valid && (peers & lt) == 0)
 		{
@@ -412,7 +500,7 @@ __global__ void kSortScatter(const uint64_t* keysIn, const uint32_t* valsIn, uin
 		int64_t i = base + r * 32 + lane;
 		bool valid = i < n;
 		uint64_t key = valid ? keysIn[i] : 0ull;
-		uint32_t d = valid ? ((uint32_t)(key >> shift) & 0xFFu) : 0x100u;
+		uint32_t d = valid ? ((uint32_t)((key - bias) >> shift) & 0xFFu) : 0x100u;
 		uint32_t peers = __match_any_sync(0xffffffffu, d);
 		if (valid)
 		{
@@ -442,7 +530,7 @@ __global__ void kCopyPairs(const uint64_t* ks, const uint32_t* vs, uint64_t* kd,
 }
 
 void radixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, uint64_t varyMask, PrimScratch& s,
-					cudaStream_t stream, const uint32_t* nDev)
+					cudaStream_t stream, const uint32_t* nDev, uint64_t bias)
 {
 	if (n <= 1)
 	{
@@ -457,16 +545,20 @@ void radixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, uint64_t varyMask
 	uint64_t* k1 = s.sortKeys.as<uint64_t>();
 	uint32_t* v1 = s.sortVals.as<uint32_t>();
 	uint32_t* counts = s.sortCounts.as<uint32_t>();
+	// 8-bit digit windows placed greedily on the bits that vary among the keys
+	// (constant bits need no pass): each window starts at the lowest varying
+	// bit not yet covered, clamped so it stays inside the key.  Windows rise
+	// monotonically, which keeps the LSD sort exact even where two overlap.
 	int passes = 0;
-	for (int shift = 0; shift < 64; shift += 8)
+	uint64_t remaining = varyMask;
+	while (remaining != 0)
 	{
-		if (((varyMask >> shift) & 0xFFull) == 0)
-		{
-			continue;
-		}
-		M3G_LAUNCH(kSortHistogram, tiles, kSortThreads, stream, k0, n, nDev, shift, counts, tiles);
+		int shift = __builtin_ctzll(remaining);
+		shift = shift > 56 ? 56 : shift;
+		remaining &= ~(0xFFull << shift);
+		M3G_LAUNCH(kSortHistogram, tiles, kSortThreads, stream, k0, n, nDev, shift, bias, counts, tiles);
 		scanExclusive(counts, counts, (int64_t)kRadix * tiles, nullptr, s, stream);
-		M3G_LAUNCH(kSortScatter, tiles, kSortThreads, stream, k0, v0, k1, v1, n, nDev, shift, counts, tiles);
+		M3G_LAUNCH(kSortScatter, tiles, kSortThreads, stream, k0, v0, k1, v1, n, nDev, shift, bias, counts, tiles);
 		uint64_t* tk = k0;
 		k0 = k1;
 		k1 = tk;
@@ -530,7 +622,8 @@ void reduceKeyRange(const uint64_t* keys, int64_t n, PrimScratch& s, cudaStream_
 extern "C"
 {
 
-// Select the kernel to time ("" or NULL: none) and zero the counters.
+// Select the kernel to time ("" or NULL: none; "*": every kernel) and zero
+// the counters.
 void m3d_gpu_profiler_reset(const char* kernelName)
 {
 	std::lock_guard<std::mutex> lock(m3g::gMu);
@@ -538,6 +631,7 @@ void m3d_gpu_profiler_reset(const char* kernelName)
 	m3g::gTarget = kernelName != nullptr ? kernelName : "";
 	m3g::gTimedMs = 0.0;
 	m3g::gTimedLaunches = 0;
+	m3g::gPerKernel.clear();
 	m3g::gOpen = nullptr;
 	m3g::gLaunches.store(0);
 	m3g::gH2D.store(0);
@@ -574,6 +668,29 @@ void m3d_gpu_profiler_kernel(float* totalMs, int32_t* launches)
 	{
 		*launches = (int32_t)m3g::gTimedLaunches;
 	}
+}
+
+// Per-kernel table of the timed launches since the last reset, one line per
+// kernel: "<name> <launches> <total ms>\n".  Returns the length of the whole
+// table; writes at most capacity-1 characters and a terminating NUL.
+int32_t m3d_gpu_profiler_table(char* out, int32_t capacity)
+{
+	std::lock_guard<std::mutex> lock(m3g::gMu);
+	m3g::drainPairs();
+	std::string t;
+	char line[160];
+	for (const auto& k : m3g::gPerKernel)
+	{
+		snprintf(line, sizeof(line), "%s %lld %.6f\n", k.first.c_str(), k.second.second, k.second.first);
+		t += line;
+	}
+	if (out != nullptr && capacity > 0)
+	{
+		size_t n = t.size() < (size_t)capacity - 1 ? t.size() : (size_t)capacity - 1;
+		memcpy(out, t.data(), n);
+		out[n] = 0;
+	}
+	return (int32_t)t.size();
 }
 
 } // extern "C"

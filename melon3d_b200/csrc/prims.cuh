@@ -29,7 +29,11 @@ struct DevBuf
 // Scratch owned by the caller of the primitives.
 struct PrimScratch
 {
-	DevBuf scanA, scanB, scanC;   // block sums for up to three scan levels
+	DevBuf scanStatus;           // u64 per scan tile: epoch | flag | value
+	DevBuf scanTicket;           // tile ticket + finished-CTA count (rewound by each scan)
+	uint32_t scanEpoch = 0;      // epoch of the last scan launched
+	DevBuf waitError;            // fallback error word when errorWord is not set
+	uint32_t* errorWord = nullptr; // device word raised when a bounded wait runs out
 	DevBuf sortKeys, sortVals;   // ping-pong partner of a radix sort
 	DevBuf sortCounts;           // per-tile digit histograms
 	DevBuf reduce;               // 2 x u64: OR and AND of the keys
@@ -43,13 +47,15 @@ struct PrimScratch
 void scanExclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total, PrimScratch& s,
 				   cudaStream_t stream);
 
-// Stable sort of n (key, val) pairs by key.  Only the key bits in `varyMask`
-// are examined: 8-bit digits whose bits are all outside the mask are skipped.
-// When nDev is given, the element count is min(n, *nDev) read on the device
-// (n is then the host-side upper bound that sizes the grid).  Result lands
-// back in keys/vals.
+// Stable sort of n (key, val) pairs by key.  Digits are taken from
+// (key - bias), which must preserve the key order over the keys sorted (every
+// key >= bias field by field, no borrows); only the bits of (key - bias) in
+// `varyMask` are examined, by 8-bit windows placed on them.  When nDev is
+// given, the element count is min(n, *nDev) read on the device (n is then the
+// host-side upper bound that sizes the grid).  Result lands back in
+// keys/vals, with the original keys.
 void radixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, uint64_t varyMask, PrimScratch& s,
-					cudaStream_t stream, const uint32_t* nDev = nullptr);
+					cudaStream_t stream, const uint32_t* nDev = nullptr, uint64_t bias = 0ull);
 
 // Device-side OR / AND of n keys into s.reduce (two u64 words), then copied
 // to the pinned host words s.hostReduce[0..1] (stream-ordered, no sync).

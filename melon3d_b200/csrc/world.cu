@@ -1506,6 +1506,10 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	// sync 3: counters, then the step's events in one batch
 	readCounters(d);
 	const StepCounters* hc = d.hostCounters;
+	if (hc->waitErrors != 0)
+	{
+		setError(world, M3D_GPU_ERR_WAIT, "a bounded device wait ran out during the step");
+	}
 	std::vector<int4> evR, evB, evE;
 	fetchEvents(world, evR, d.evRemoval.as<int4>(), (int32_t)hc->endRemoval);
 	fetchEvents(world, evB, d.evBegin.as<int4>(), (int32_t)hc->beginNP);

@@ -76,6 +76,13 @@ def test_dense_rain_bit_exact():
     lockstep(U.oracle_cr(), harness.RAIN, 12, seed=5, a=20000, b=200)
 
 
+def test_large_rain_bit_exact():
+    # 150k bodies: per-body scans span 74 tiles and the grid sort ~120, so the
+    # look-back walks several 32-tile windows; cell keys straddle the key
+    # offset in every field, which the bias-subtracted sort digits cover
+    lockstep(U.oracle_cr(), harness.RAIN, 4, seed=9, a=150000, b=500)
+
+
 def test_small_pile_bit_exact():
     lockstep(U.oracle_cr(), harness.PILE, 40, seed=3, a=6, b=8, c=6)
 
