@@ -75,18 +75,94 @@ __device__ __forceinline__ void jointReset(JointRec* J, int ji)
 // One warp per small island.  The per-element stages of a substep whose
 // elements are independent - integration and velocity reconstruction of each
 // body, preparation of each contact (which reads only body state and writes
-// only its own contact) - run across the lanes; the Gauss-Seidel sweeps,
-// whose order is the result, run on lane 0 in ascending contact order.
-// __syncwarp() orders the global-memory writes of one stage before the reads
-// of the next.
+// only its own contact) - run across the lanes.
+//
+// The Gauss-Seidel sweeps follow the reference's ascending contact order
+// exactly, but not one contact at a time: a contact reads and writes only its
+// own records and the two bodies it joins, and only bodies with non-zero
+// inverse mass are ever written, so two contacts that share no island body
+// commute.  Each contact gets the level 1 + max(level of the previous contact
+// on each of its island bodies); a sweep runs level by level, the contacts of
+// one level in parallel.  Every contact still sees each body exactly as the
+// serial sweep leaves it.  Islands with joints, or larger than the shared
+// tables, sweep serially on lane 0.  __syncwarp() orders the global-memory
+// writes of one stage or level before the reads of the next.
 constexpr int kSerialWarpsPerBlock = 8;
+constexpr int kLevelTable = 320; // contacts and bodies per island for the level schedule
+constexpr uint32_t kNotIsland = 0xFFFFu;
+
+struct LevelTables
+{
+	uint32_t contact[kLevelTable]; // contact index per island position
+	uint32_t ends[kLevelTable];    // island-local body of each end (kNotIsland: static / kinematic / other)
+	uint16_t level[kLevelTable];   // 1-based sweep level per island position
+	uint16_t last[kLevelTable];    // per island body: level of its latest contact
+};
+
+enum SweepOp
+{
+	kSweepNormals,
+	kSweepFriction,
+	kSweepVelocity
+};
+
+__device__ __forceinline__ void sweepContact(SweepOp op, const BodySoA& B, const ContactSoA& C, int c,
+											 const SolveParams& P)
+{
+	if (op == kSweepNormals)
+	{
+		solveContactNormals(B, C, c, P.maxCorrection);
+	}
+	else if (op == kSweepFriction)
+	{
+		applyContactFriction(B, C, c);
+	}
+	else
+	{
+		solveContactVelocity(B, C, c, P.h, P.gravityLen);
+	}
+}
+
+// one Gauss-Seidel sweep over the island's contacts in reference order
+__device__ __forceinline__ void sweepIsland(SweepOp op, const BodySoA& B, const ContactSoA& C, const IslandRec& r,
+											const uint32_t* contacts, const LevelTables& T, int levels, int lane,
+											const SolveParams& P)
+{
+	if (levels > 0)
+	{
+		for (int L = 1; L <= levels; ++L)
+		{
+			for (int p = lane; p < r.contactCount; p += 32)
+			{
+				if (T.level[p] == L)
+				{
+					sweepContact(op, B, C, (int)T.contact[p], P);
+				}
+			}
+			__syncwarp();
+		}
+	}
+	else
+	{
+		if (lane == 0)
+		{
+			for (int c = 0; c < r.contactCount; ++c)
+			{
+				sweepContact(op, B, C, (int)contacts[c], P);
+			}
+		}
+		__syncwarp();
+	}
+}
 
 __global__ void __launch_bounds__(32 * kSerialWarpsPerBlock)
 	kSolveSerial(BodySoA B, ContactSoA C, JointRec* J, const IslandRec* islands, const int32_t* serialList,
 				 const uint32_t* serialDev, const uint32_t* bodyVals, const uint32_t* contactVals,
-				 const uint32_t* jointVals, SolveParams P)
+				 const uint32_t* jointVals, uint32_t* localIndex, SolveParams P)
 {
+	__shared__ LevelTables tables[kSerialWarpsPerBlock];
 	const int lane = threadIdx.x & 31;
+	LevelTables& T = tables[threadIdx.x >> 5];
 	const int warps = gridDim.x * kSerialWarpsPerBlock;
 	const int count = (int)*serialDev;
 	for (int si = blockIdx.x * kSerialWarpsPerBlock + (threadIdx.x >> 5); si < count; si += warps)
@@ -95,6 +171,61 @@ __global__ void __launch_bounds__(32 * kSerialWarpsPerBlock)
 		const uint32_t* bodies = bodyVals + r.bodyStart;
 		const uint32_t* contacts = contactVals + r.contactStart;
 		const uint32_t* joints = jointVals + r.jointStart;
+
+		// level schedule of the island's contacts (fixed for the whole step)
+		int levels = 0;
+		if (r.jointCount == 0 && r.contactCount <= kLevelTable && r.bodyCount <= kLevelTable)
+		{
+			for (int b = lane; b < r.bodyCount; b += 32)
+			{
+				localIndex[bodies[b]] = (uint32_t)b;
+				T.last[b] = 0;
+			}
+			__syncwarp();
+			for (int p = lane; p < r.contactCount; p += 32)
+			{
+				const uint32_t c = contacts[p];
+				const int2 ab = C.bodies[c];
+				uint32_t la = localIndex[ab.x], lb = localIndex[ab.y];
+				la = la < (uint32_t)r.bodyCount && bodies[la] == (uint32_t)ab.x ? la : kNotIsland;
+				lb = lb < (uint32_t)r.bodyCount && bodies[lb] == (uint32_t)ab.y ? lb : kNotIsland;
+				T.contact[p] = c;
+				T.ends[p] = la | (lb << 16);
+			}
+			__syncwarp();
+			if (lane == 0)
+			{
+				int maxLevel = 0;
+				for (int p = 0; p < r.contactCount; ++p)
+				{
+					const uint32_t la = T.ends[p] & 0xFFFFu, lb = T.ends[p] >> 16;
+					int l = 0;
+					if (la != kNotIsland)
+					{
+						l = T.last[la];
+					}
+					if (lb != kNotIsland && T.last[lb] > l)
+					{
+						l = T.last[lb];
+					}
+					++l;
+					T.level[p] = (uint16_t)l;
+					if (la != kNotIsland)
+					{
+						T.last[la] = (uint16_t)l;
+					}
+					if (lb != kNotIsland)
+					{
+						T.last[lb] = (uint16_t)l;
+					}
+					maxLevel = l > maxLevel ? l : maxLevel;
+				}
+				levels = maxLevel;
+			}
+			levels = __shfl_sync(0xffffffffu, levels, 0);
+			__syncwarp();
+		}
+
 		if (r.jointCount > 0)
 		{
 			for (int b = lane; b < r.bodyCount; b += 32)
@@ -123,40 +254,45 @@ __global__ void __launch_bounds__(32 * kSerialWarpsPerBlock)
 				prepareContact(B, C, (int)contacts[c], P.h);
 			}
 			__syncwarp();
-			if (lane == 0)
+			if (r.jointCount > 0)
 			{
-				for (int j = 0; j < r.jointCount; ++j)
-				{
-					jointReset(J, (int)joints[j]);
-				}
-				for (int it = 0; it < P.iterations; ++it)
+				// joints interleave with the contact sweeps: serial on lane 0
+				if (lane == 0)
 				{
 					for (int j = 0; j < r.jointCount; ++j)
 					{
-						jointPosition(B, J, (int)joints[j], P.h);
+						jointReset(J, (int)joints[j]);
 					}
-					for (int c = 0; c < r.contactCount; ++c)
+					for (int it = 0; it < P.iterations; ++it)
 					{
-						solveContactNormals(B, C, (int)contacts[c], P.maxCorrection);
+						for (int j = 0; j < r.jointCount; ++j)
+						{
+							jointPosition(B, J, (int)joints[j], P.h);
+						}
+						for (int c = 0; c < r.contactCount; ++c)
+						{
+							solveContactNormals(B, C, (int)contacts[c], P.maxCorrection);
+						}
 					}
 				}
-				for (int c = 0; c < r.contactCount; ++c)
+				__syncwarp();
+			}
+			else
+			{
+				for (int it = 0; it < P.iterations; ++it)
 				{
-					applyContactFriction(B, C, (int)contacts[c]);
+					sweepIsland(kSweepNormals, B, C, r, contacts, T, levels, lane, P);
 				}
 			}
-			__syncwarp();
+			sweepIsland(kSweepFriction, B, C, r, contacts, T, levels, lane, P);
 			for (int b = lane; b < r.bodyCount; b += 32)
 			{
 				reconstructBody(B, (int)bodies[b], P.invH);
 			}
 			__syncwarp();
+			sweepIsland(kSweepVelocity, B, C, r, contacts, T, levels, lane, P);
 			if (lane == 0)
 			{
-				for (int c = 0; c < r.contactCount; ++c)
-				{
-					solveContactVelocity(B, C, (int)contacts[c], P.h, P.gravityLen);
-				}
 				for (int j = 0; j < r.jointCount; ++j)
 				{
 					jointVelocity(B, J, (int)joints[j], P.h);
@@ -429,11 +565,11 @@ void launchSolve(DevWorld& w, float dt, int substeps, V3 gravity, int positionIt
 	// enough warps for every serial island of a rain or pile step to start at once
 	int serialBlocks = (ni + kSerialWarpsPerBlock - 1) / kSerialWarpsPerBlock;
 	serialBlocks = serialBlocks < 148 * 8 ? serialBlocks : 148 * 8;
+	w.colorMask.ensure((size_t)(w.bodyCap + 1) * sizeof(uint32_t)); // also the serial islands' local body index
 	M3G_LAUNCH(kSolveSerial, serialBlocks, 32 * kSerialWarpsPerBlock, s, w.B, w.C, w.joints.as<JointRec>(), isl,
 			   w.serialList.as<int32_t>(), &dc->serialIslands, w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(),
-			   w.jointVals.as<uint32_t>(), P);
+			   w.jointVals.as<uint32_t>(), w.colorMask.as<uint32_t>(), P);
 	size_t nc = (size_t)w.contactMax + 1;
-	w.colorMask.ensure((size_t)(w.bodyCap + 1) * sizeof(uint32_t));
 	w.colorOrder.ensure(nc * sizeof(int32_t));
 	w.packetMax.ensure(nc * sizeof(int32_t));
 	M3G_LAUNCH(kSolveColored, 2 * 148, kColorThreads, s, w.B, w.C, w.joints.as<JointRec>(), isl,
