@@ -53,6 +53,12 @@ M3D_API float m3d_gpu_last_step_device_ms(m3d_world* world);
  * freeIslands.  Returns how many counters exist (writes at most capacity). */
 M3D_API int32_t m3d_gpu_step_counters(m3d_world* world, uint32_t* out, int32_t capacity);
 
+/* Coloured islands (>= 300 contacts, solved with the reference's greedy
+ * colouring) with at least `contacts` contacts are solved by all SMs in one
+ * cooperative launch instead of one CTA each (default 8192; values below 300
+ * mean 300).  Results are identical either way; only the speed differs. */
+M3D_API void m3d_gpu_set_giant_island_contacts(m3d_world* world, int32_t contacts);
+
 /* 0 when healthy, else the first M3D_GPU_ERR_* seen since creation. */
 M3D_API int32_t m3d_gpu_status(m3d_world* world);
 M3D_API const char* m3d_gpu_last_error_string(m3d_world* world);

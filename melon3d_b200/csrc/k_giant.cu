@@ -1,0 +1,693 @@
+// Graph-coloured solve of giant islands on the whole GPU.
+//
+// The reference solves an island of >= 300 contacts with a greedy first-fit
+// colouring in contact order and colour-parallel projection
+// (src/xpbd.cpp:1167-1369).  One CTA per island (k_solve.cu) follows it
+// step for step; an island of tens of thousands of contacts (a settled pile)
+// needs every SM, so islands above the giant threshold run here, in one
+// cooperative launch whose CTAs meet at a bounded grid barrier between the
+// stages the reference separates:
+//
+//  - colouring: contact p takes the first colour free on both of its dynamic
+//    bodies among the contacts before it in island order.  Only the previous
+//    contact on each of its two bodies matters (it already folded everything
+//    earlier into the body's colour mask), so each contact waits for those two
+//    predecessors - found from per-body incidence lists sorted by position -
+//    and the colouring runs as a dataflow over the whole grid.  Every thread
+//    takes its positions in ascending order; the lowest uncoloured position
+//    can always proceed, so the waits end.  Result: the reference's colours.
+//  - buckets: a stable counting sort of positions by colour (chunk
+//    histograms, one scan, ranked placement), i.e. contact order inside each
+//    colour, as the reference regroups them.
+//  - the overflow bucket (colour 8), solved serially by the reference, runs
+//    on CTA 0 level by level: overflow contacts that share no dynamic body
+//    commute, so each level's contacts run at once and every contact sees its
+//    bodies exactly as the serial order leaves them.
+//  - joints stay serial on one thread, as in the reference.
+// Every wait (dataflow or barrier) is bounded; one that runs out raises the
+// error word and lets the kernel finish.
+#include "m3d_dev.cuh"
+#include "m3d_solve.cuh"
+
+namespace m3g
+{
+
+constexpr int kGiantThreads = 256;
+constexpr int kGiantChunk = 256; // positions per colour-histogram chunk
+constexpr uint32_t kGiantSpinLimit = 1u << 22;
+constexpr uint32_t kNoEnd = 0xFFFFFFFFu;
+
+struct GiantArgs
+{
+	BodySoA B;
+	ContactSoA C;
+	JointRec* J;
+	const IslandRec* islands;
+	const int32_t* giantList;
+	const uint32_t* giantDev;
+	const uint32_t* bodyVals;
+	const uint32_t* contactVals;
+	const uint32_t* jointVals;
+	uint32_t* colorMask;  // per body: colours taken so far
+	uint32_t* localIndex; // per body: index in its island's body list
+	uint32_t* bodyOffs;   // per island body + 1: incidence counts, then CSR offsets
+	uint32_t* bodyCursor; // per island body: fill cursor, then overflow levels
+	uint32_t* incidence;  // 2 per island contact: positions, ascending per body
+	int32_t* pred;        // 2 per island contact position: previous position on end A / B; then overflow levels
+	uint32_t* done;       // per island contact position: == epoch once coloured
+	int32_t* order;       // per island contact position: contact of the bucket order
+	int32_t* pmax;        // per position: colour during colouring, then the packet's point count
+	int32_t* contactColor;
+	uint32_t* chunkHist;  // colour-major chunk histograms, then their offsets
+	uint32_t* misc;       // [0..9] bucket starts, [10] colour count, [11] overflow levels
+	uint32_t* barrier;    // [0] arrivals, [1] generation
+	uint32_t* error;
+	uint32_t epoch;
+	SolveParams P;
+};
+
+__device__ __forceinline__ uint32_t ldAcquire(const uint32_t* p) { return *(const volatile uint32_t*)p; }
+
+// island-local index of a contact end that the solve writes (non-zero inverse
+// mass) and that belongs to the island's body list; kNoEnd otherwise
+__device__ __forceinline__ uint32_t islandEnd(const GiantArgs& a, const uint32_t* bodies, int nb, int body)
+{
+	if (a.B.massInv[body].x == 0.0f)
+	{
+		return kNoEnd;
+	}
+	const uint32_t l = a.localIndex[body];
+	return l < (uint32_t)nb && bodies[l] == (uint32_t)body ? l : kNoEnd;
+}
+
+// All CTAs meet here; writes before it are visible to reads after it.
+__device__ void gridSync(const GiantArgs& a, uint32_t* gen)
+{
+	__syncthreads();
+	if (threadIdx.x == 0)
+	{
+		const uint32_t g = *gen;
+		__threadfence();
+		if (atomicAdd(&a.barrier[0], 1u) == gridDim.x - 1)
+		{
+			atomicExch(&a.barrier[0], 0u);
+			__threadfence();
+			atomicExch(&a.barrier[1], g + 1u);
+		}
+		else
+		{
+			uint32_t it = 0;
+			while (ldAcquire(&a.barrier[1]) == g)
+			{
+				if (++it > kGiantSpinLimit)
+				{
+					atomicOr(a.error, 1u);
+					break;
+				}
+				__nanosleep(32);
+			}
+		}
+		__threadfence();
+		*gen = g + 1u;
+	}
+	__syncthreads();
+}
+
+// exclusive scan of v[0..n) in place by the calling CTA; returns the total
+// to every thread of the CTA
+__device__ uint32_t ctaScan(uint32_t* v, int n, uint32_t* warpSums)
+{
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	uint32_t carry = 0;
+	for (int base = 0; base < n; base += kGiantThreads)
+	{
+		const int i = base + threadIdx.x;
+		const uint32_t x = i < n ? v[i] : 0u;
+		uint32_t inc = x;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1)
+		{
+			uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+			if (lane >= o)
+			{
+				inc += t;
+			}
+		}
+		if (lane == 31)
+		{
+			warpSums[warp] = inc;
+		}
+		__syncthreads();
+		if (threadIdx.x == 0)
+		{
+			uint32_t run = 0;
+			for (int w = 0; w < kGiantThreads / 32; ++w)
+			{
+				uint32_t t = warpSums[w];
+				warpSums[w] = run;
+				run += t;
+			}
+			warpSums[kGiantThreads / 32] = run;
+		}
+		__syncthreads();
+		if (i < n)
+		{
+			v[i] = carry + warpSums[warp] + inc - x;
+		}
+		carry += warpSums[kGiantThreads / 32];
+		__syncthreads();
+	}
+	return carry;
+}
+
+enum GiantOp
+{
+	kGiantNormals,
+	kGiantFriction,
+	kGiantVelocity
+};
+
+__device__ __forceinline__ void giantContactOp(GiantOp op, const GiantArgs& a, int c)
+{
+	if (op == kGiantNormals)
+	{
+		solveContactNormals(a.B, a.C, c, a.P.maxCorrection);
+	}
+	else if (op == kGiantFriction)
+	{
+		applyContactFriction(a.B, a.C, c);
+	}
+	else
+	{
+		solveContactVelocity(a.B, a.C, c, a.P.h, a.P.gravityLen);
+	}
+}
+
+// the overflow bucket in reference order, level by level on CTA 0
+__device__ void overflowSweep(GiantOp op, const GiantArgs& a, const int32_t* order, const int32_t* level, int o0,
+							  int o1, int levels)
+{
+	if (blockIdx.x != 0)
+	{
+		return;
+	}
+	for (int L = 1; L <= levels; ++L)
+	{
+		for (int q = o0 + threadIdx.x; q < o1; q += kGiantThreads)
+		{
+			if (level[q] == L)
+			{
+				giantContactOp(op, a, order[q]);
+			}
+		}
+		__syncthreads();
+	}
+}
+
+__global__ void __launch_bounds__(kGiantThreads) kSolveGiant(GiantArgs a)
+{
+	__shared__ uint32_t gen;
+	__shared__ uint32_t warpSums[kGiantThreads / 32 + 1];
+	__shared__ int32_t bucket[kMaxGraphColors + 2];
+	__shared__ uint32_t chunkCount[kMaxGraphColors + 1];
+	__shared__ uint32_t warpColor[kGiantThreads / 32][kMaxGraphColors + 1];
+	if (threadIdx.x == 0)
+	{
+		gen = ldAcquire(&a.barrier[1]);
+	}
+	__syncthreads();
+	const int gtid = blockIdx.x * kGiantThreads + threadIdx.x;
+	const int gthreads = gridDim.x * kGiantThreads;
+	const BodySoA& B = a.B;
+	const ContactSoA& C = a.C;
+	const SolveParams& P = a.P;
+	const int islandsHere = (int)*a.giantDev;
+
+	for (int gi = 0; gi < islandsHere; ++gi)
+	{
+		const IslandRec r = a.islands[a.giantList[gi]];
+		const uint32_t* bodies = a.bodyVals + r.bodyStart;
+		const uint32_t* contacts = a.contactVals + r.contactStart;
+		const uint32_t* joints = a.jointVals + r.jointStart;
+		int32_t* order = a.order + r.contactStart;
+		int32_t* pmax = a.pmax + r.contactStart;
+		int32_t* pred = a.pred + 2 * (int64_t)r.contactStart;
+		uint32_t* done = a.done + r.contactStart;
+		uint32_t* incidence = a.incidence + 2 * (int64_t)r.contactStart;
+		const int nb = r.bodyCount, nc = r.contactCount;
+
+		// ---- incidence lists: island contacts per dynamic body, ascending position
+		for (int b = gtid; b < nb; b += gthreads)
+		{
+			const uint32_t body = bodies[b];
+			a.localIndex[body] = (uint32_t)b;
+			a.colorMask[body] = 0u;
+			a.bodyOffs[b] = 0u;
+			a.bodyCursor[b] = 0u;
+		}
+		if (gtid == 0)
+		{
+			a.bodyOffs[nb] = 0u;
+		}
+		gridSync(a, &gen);
+		for (int p = gtid; p < nc; p += gthreads)
+		{
+			const int2 ab = C.bodies[contacts[p]];
+			pred[2 * p] = -1;
+			pred[2 * p + 1] = -1;
+			const uint32_t la = islandEnd(a, bodies, nb, ab.x), lb = islandEnd(a, bodies, nb, ab.y);
+			if (la != kNoEnd)
+			{
+				atomicAdd(&a.bodyOffs[la], 1u);
+			}
+			if (lb != kNoEnd)
+			{
+				atomicAdd(&a.bodyOffs[lb], 1u);
+			}
+		}
+		gridSync(a, &gen);
+		if (blockIdx.x == 0)
+		{
+			uint32_t total = ctaScan(a.bodyOffs, nb, warpSums);
+			if (threadIdx.x == 0)
+			{
+				a.bodyOffs[nb] = total;
+			}
+		}
+		gridSync(a, &gen);
+		for (int p = gtid; p < nc; p += gthreads)
+		{
+			const int2 ab = C.bodies[contacts[p]];
+			const uint32_t la = islandEnd(a, bodies, nb, ab.x), lb = islandEnd(a, bodies, nb, ab.y);
+			if (la != kNoEnd)
+			{
+				incidence[a.bodyOffs[la] + atomicAdd(&a.bodyCursor[la], 1u)] = (uint32_t)p;
+			}
+			if (lb != kNoEnd)
+			{
+				incidence[a.bodyOffs[lb] + atomicAdd(&a.bodyCursor[lb], 1u)] = (uint32_t)p;
+			}
+		}
+		gridSync(a, &gen);
+		for (int b = gtid; b < nb; b += gthreads)
+		{
+			const uint32_t s0 = a.bodyOffs[b], s1 = a.bodyOffs[b + 1];
+			for (uint32_t i = s0 + 1; i < s1; ++i) // insertion sort: a body has a handful of contacts
+			{
+				const uint32_t v = incidence[i];
+				uint32_t j = i;
+				while (j > s0 && incidence[j - 1] > v)
+				{
+					incidence[j] = incidence[j - 1];
+					--j;
+				}
+				incidence[j] = v;
+			}
+			const uint32_t body = bodies[b];
+			for (uint32_t i = s0 + 1; i < s1; ++i)
+			{
+				const uint32_t p = incidence[i];
+				const int2 ab = C.bodies[contacts[p]];
+				pred[2 * p + ((uint32_t)ab.x == body ? 0 : 1)] = (int32_t)incidence[i - 1];
+			}
+		}
+		gridSync(a, &gen);
+
+		// ---- greedy first-fit colouring as a dataflow (src/xpbd.cpp:1179-1235)
+		for (int p = gtid; p < nc; p += gthreads)
+		{
+			const int32_t pa = pred[2 * p], pb = pred[2 * p + 1];
+			for (uint32_t it = 0; (pa >= 0 && ldAcquire(&done[pa]) != a.epoch) || (pb >= 0 && ldAcquire(&done[pb]) != a.epoch);
+				 ++it)
+			{
+				if (it > kGiantSpinLimit)
+				{
+					atomicOr(a.error, 1u);
+					break;
+				}
+				__nanosleep(20);
+			}
+			__threadfence();
+			const int c = (int)contacts[p];
+			const int2 ab = C.bodies[c];
+			const bool dynA = B.massInv[ab.x].x > 0.0f;
+			const bool dynB = B.massInv[ab.y].x > 0.0f;
+			const uint32_t ma = dynA ? __ldcg(&a.colorMask[ab.x]) : 0u;
+			const uint32_t mb = dynB ? __ldcg(&a.colorMask[ab.y]) : 0u;
+			const uint32_t freeBits = ~(ma | mb);
+			int color = freeBits != 0 ? __ffs((int)freeBits) - 1 : kMaxGraphColors;
+			if (color >= kMaxGraphColors)
+			{
+				color = kMaxGraphColors;
+			}
+			else
+			{
+				const uint32_t bit = 1u << color;
+				if (dynA)
+				{
+					__stcg(&a.colorMask[ab.x], ma | bit);
+				}
+				if (dynB)
+				{
+					__stcg(&a.colorMask[ab.y], mb | bit);
+				}
+			}
+			a.contactColor[c] = color;
+			pmax[p] = color;
+			__threadfence();
+			*(volatile uint32_t*)&done[p] = a.epoch;
+		}
+		gridSync(a, &gen);
+
+		// ---- buckets: stable counting sort of positions by colour
+		const int chunks = (nc + kGiantChunk - 1) / kGiantChunk;
+		for (int k = blockIdx.x; k < chunks; k += gridDim.x)
+		{
+			if (threadIdx.x <= kMaxGraphColors)
+			{
+				chunkCount[threadIdx.x] = 0u;
+			}
+			__syncthreads();
+			const int p = k * kGiantChunk + threadIdx.x;
+			if (p < nc)
+			{
+				atomicAdd(&chunkCount[pmax[p]], 1u);
+			}
+			__syncthreads();
+			if (threadIdx.x <= kMaxGraphColors)
+			{
+				a.chunkHist[threadIdx.x * chunks + k] = chunkCount[threadIdx.x];
+			}
+			__syncthreads();
+		}
+		gridSync(a, &gen);
+		if (blockIdx.x == 0)
+		{
+			ctaScan(a.chunkHist, (kMaxGraphColors + 1) * chunks, warpSums);
+			if (threadIdx.x <= kMaxGraphColors)
+			{
+				a.misc[threadIdx.x] = a.chunkHist[threadIdx.x * chunks];
+			}
+			if (threadIdx.x == 0)
+			{
+				a.misc[kMaxGraphColors + 1] = (uint32_t)nc;
+			}
+		}
+		gridSync(a, &gen);
+		if (threadIdx.x <= kMaxGraphColors + 1)
+		{
+			bucket[threadIdx.x] = (int32_t)a.misc[threadIdx.x];
+		}
+		__syncthreads();
+		int ncol = 0;
+		for (int c = 0; c < kMaxGraphColors; ++c)
+		{
+			ncol = bucket[c + 1] > bucket[c] ? c + 1 : ncol;
+		}
+		for (int k = blockIdx.x; k < chunks; k += gridDim.x)
+		{
+			const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+			for (int i = threadIdx.x; i < (kGiantThreads / 32) * (kMaxGraphColors + 1); i += kGiantThreads)
+			{
+				(&warpColor[0][0])[i] = 0u;
+			}
+			__syncthreads();
+			const int p = k * kGiantChunk + threadIdx.x;
+			const bool valid = p < nc;
+			const int color = valid ? pmax[p] : kMaxGraphColors + 1;
+			const uint32_t peers = __match_any_sync(0xffffffffu, color);
+			const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+			if (valid && rank == 0)
+			{
+				warpColor[warp][color] = __popc(peers);
+			}
+			__syncthreads();
+			if (threadIdx.x <= kMaxGraphColors)
+			{
+				uint32_t run = 0;
+				for (int w = 0; w < kGiantThreads / 32; ++w)
+				{
+					uint32_t t = warpColor[w][threadIdx.x];
+					warpColor[w][threadIdx.x] = run;
+					run += t;
+				}
+			}
+			__syncthreads();
+			if (valid)
+			{
+				order[a.chunkHist[color * chunks + k] + warpColor[warp][color] + rank] = (int32_t)contacts[p];
+			}
+			__syncthreads();
+		}
+		gridSync(a, &gen);
+
+		// ---- overflow levels (serial order of the overflow bucket)
+		const int o0 = bucket[kMaxGraphColors], o1 = bucket[kMaxGraphColors + 1];
+		int32_t* level = pred; // the predecessor table is free again
+		if (gtid == 0 && o1 > o0)
+		{
+			for (int q = o0; q < o1; ++q)
+			{
+				const int2 ab = C.bodies[order[q]];
+				const uint32_t la = islandEnd(a, bodies, nb, ab.x), lb = islandEnd(a, bodies, nb, ab.y);
+				if (la != kNoEnd)
+				{
+					a.bodyCursor[la] = 0u;
+				}
+				if (lb != kNoEnd)
+				{
+					a.bodyCursor[lb] = 0u;
+				}
+			}
+			uint32_t maxLevel = 0;
+			for (int q = o0; q < o1; ++q)
+			{
+				const int2 ab = C.bodies[order[q]];
+				const uint32_t la = islandEnd(a, bodies, nb, ab.x), lb = islandEnd(a, bodies, nb, ab.y);
+				uint32_t l = 0;
+				if (la != kNoEnd)
+				{
+					l = a.bodyCursor[la];
+				}
+				if (lb != kNoEnd && a.bodyCursor[lb] > l)
+				{
+					l = a.bodyCursor[lb];
+				}
+				++l;
+				level[q] = (int32_t)l;
+				if (la != kNoEnd)
+				{
+					a.bodyCursor[la] = l;
+				}
+				if (lb != kNoEnd)
+				{
+					a.bodyCursor[lb] = l;
+				}
+				maxLevel = l > maxLevel ? l : maxLevel;
+			}
+			a.misc[kMaxGraphColors + 3] = maxLevel;
+		}
+		if (r.jointCount > 0)
+		{
+			for (int b = gtid; b < nb; b += gthreads)
+			{
+				refreshInvInertia(B, (int)bodies[b]);
+			}
+		}
+		gridSync(a, &gen);
+		const int overLevels = o1 > o0 ? (int)a.misc[kMaxGraphColors + 3] : 0;
+		if (r.jointCount > 0)
+		{
+			if (gtid == 0)
+			{
+				for (int j = 0; j < r.jointCount; ++j)
+				{
+					jointPrepare(B, a.J, (int)joints[j]);
+				}
+			}
+			gridSync(a, &gen);
+		}
+
+		// ---- substeps (src/xpbd.cpp:1237-1369)
+		const int colored = bucket[kMaxGraphColors];
+		for (int sub = 0; sub < P.substeps; ++sub)
+		{
+			for (int b = gtid; b < nb; b += gthreads)
+			{
+				integrateBody(B, (int)bodies[b], P.h, P.gravity);
+			}
+			gridSync(a, &gen);
+			for (int p = gtid; p < nc; p += gthreads)
+			{
+				prepareContact(B, C, (int)contacts[p], P.h);
+			}
+			if (gtid == 0)
+			{
+				for (int j = 0; j < r.jointCount; ++j)
+				{
+					jointReset(a.J, (int)joints[j]);
+				}
+			}
+			gridSync(a, &gen);
+			// packets of 8 consecutive bucket entries share the largest point count
+			for (int q = gtid; q < colored; q += gthreads)
+			{
+				int color = 0;
+				while (q >= bucket[color + 1])
+				{
+					++color;
+				}
+				const int bs = bucket[color], be = bucket[color + 1];
+				const int p0 = bs + ((q - bs) & ~7);
+				const int p1 = p0 + 8 < be ? p0 + 8 : be;
+				int m = 0;
+				for (int p = p0; p < p1; ++p)
+				{
+					const int pc = C.pointCount[order[p]];
+					m = pc > m ? pc : m;
+				}
+				pmax[q] = m;
+			}
+			gridSync(a, &gen);
+			for (int it = 0; it < P.iterations; ++it)
+			{
+				if (r.jointCount > 0)
+				{
+					if (gtid == 0)
+					{
+						for (int j = 0; j < r.jointCount; ++j)
+						{
+							jointPosition(B, a.J, (int)joints[j], P.h);
+						}
+					}
+					gridSync(a, &gen);
+				}
+				for (int color = 0; color < ncol; ++color)
+				{
+					for (int q = bucket[color] + gtid; q < bucket[color + 1]; q += gthreads)
+					{
+						solvePacketLane(B, C, order[q], pmax[q], P.maxCorrection);
+					}
+					gridSync(a, &gen);
+				}
+				if (overLevels > 0)
+				{
+					overflowSweep(kGiantNormals, a, order, level, o0, o1, overLevels);
+					gridSync(a, &gen);
+				}
+			}
+			for (int color = 0; color < ncol; ++color)
+			{
+				for (int q = bucket[color] + gtid; q < bucket[color + 1]; q += gthreads)
+				{
+					applyContactFriction(B, C, order[q]);
+				}
+				gridSync(a, &gen);
+			}
+			if (overLevels > 0)
+			{
+				overflowSweep(kGiantFriction, a, order, level, o0, o1, overLevels);
+				gridSync(a, &gen);
+			}
+			for (int b = gtid; b < nb; b += gthreads)
+			{
+				reconstructBody(B, (int)bodies[b], P.invH);
+			}
+			gridSync(a, &gen);
+			for (int color = 0; color < ncol; ++color)
+			{
+				for (int q = bucket[color] + gtid; q < bucket[color + 1]; q += gthreads)
+				{
+					solveContactVelocity(B, C, order[q], P.h, P.gravityLen);
+				}
+				gridSync(a, &gen);
+			}
+			if (overLevels > 0 || r.jointCount > 0)
+			{
+				overflowSweep(kGiantVelocity, a, order, level, o0, o1, overLevels);
+				if (gtid == 0)
+				{
+					for (int j = 0; j < r.jointCount; ++j)
+					{
+						jointVelocity(B, a.J, (int)joints[j], P.h);
+					}
+				}
+				gridSync(a, &gen);
+			}
+		}
+	}
+}
+
+void launchSolveGiant(DevWorld& w, const SolveParams& P)
+{
+	if (w.contactMax < w.giantIslandContacts)
+	{
+		return; // no island can reach the threshold this step
+	}
+	StepCounters* dc = devCounters(w);
+	const size_t nc = (size_t)w.contactMax + 1;
+	const size_t nb = (size_t)w.bodyCap + 1;
+	const size_t chunks = nc / kGiantChunk + 2;
+	w.giantLocal.ensure(nb * sizeof(uint32_t));
+	w.giantBodyOffs.ensure((nb + 1) * sizeof(uint32_t));
+	w.giantBodyCursor.ensure(nb * sizeof(uint32_t));
+	w.giantIncidence.ensure(2 * nc * sizeof(uint32_t));
+	w.giantPred.ensure(2 * nc * sizeof(int32_t));
+	void* doneBefore = w.giantDone.ptr;
+	w.giantDone.ensureZeroed(nc * sizeof(uint32_t), w.stream);
+	w.giantChunkHist.ensure((kMaxGraphColors + 1) * chunks * sizeof(uint32_t));
+	w.giantMisc.ensure(16 * sizeof(uint32_t));
+	w.giantBarrier.ensureZeroed(4 * sizeof(uint32_t), w.stream);
+	if (w.giantDone.ptr != doneBefore || ++w.giantEpoch == 0u)
+	{
+		if (w.giantDone.ptr == doneBefore)
+		{
+			cudaMemsetAsync(w.giantDone.ptr, 0, w.giantDone.bytes, w.stream);
+		}
+		w.giantEpoch = 1u;
+	}
+	if (w.giantGrid == 0)
+	{
+		int dev = 0, sms = 0, perSm = 0;
+		cudaGetDevice(&dev);
+		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kSolveGiant, kGiantThreads, 0);
+		perSm = perSm > 2 ? 2 : perSm;
+		w.giantGrid = (perSm > 0 ? perSm : 1) * (sms > 0 ? sms : 1);
+	}
+	GiantArgs a;
+	a.B = w.B;
+	a.C = w.C;
+	a.J = w.joints.as<JointRec>();
+	a.islands = w.islands.as<IslandRec>();
+	a.giantList = w.giantList.as<int32_t>();
+	a.giantDev = &dc->giantIslands;
+	a.bodyVals = w.bodyVals.as<uint32_t>();
+	a.contactVals = w.contactVals.as<uint32_t>();
+	a.jointVals = w.jointVals.as<uint32_t>();
+	a.colorMask = w.colorMask.as<uint32_t>();
+	a.localIndex = w.giantLocal.as<uint32_t>();
+	a.bodyOffs = w.giantBodyOffs.as<uint32_t>();
+	a.bodyCursor = w.giantBodyCursor.as<uint32_t>();
+	a.incidence = w.giantIncidence.as<uint32_t>();
+	a.pred = w.giantPred.as<int32_t>();
+	a.done = w.giantDone.as<uint32_t>();
+	a.order = w.colorOrder.as<int32_t>();
+	a.pmax = w.packetMax.as<int32_t>();
+	a.contactColor = w.contactColor.as<int32_t>();
+	a.chunkHist = w.giantChunkHist.as<uint32_t>();
+	a.misc = w.giantMisc.as<uint32_t>();
+	a.barrier = w.giantBarrier.as<uint32_t>();
+	a.error = &dc->waitErrors;
+	a.epoch = w.giantEpoch;
+	a.P = P;
+	// arrivals start from zero even if an earlier launch gave up on a wait
+	cudaMemsetAsync(w.giantBarrier.ptr, 0, sizeof(uint32_t), w.stream);
+	void* args[] = { &a };
+	launchBegin("kSolveGiant", w.stream);
+	cudaLaunchCooperativeKernel((const void*)kSolveGiant, dim3((unsigned)w.giantGrid), dim3(kGiantThreads), args, 0,
+								w.stream);
+	launchEnd("kSolveGiant", w.stream);
+}
+
+} // namespace m3g

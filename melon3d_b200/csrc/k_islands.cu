@@ -75,6 +75,21 @@ __device__ __forceinline__ int32_t ufFind(int32_t* parent, int32_t x)
 	return x;
 }
 
+// Root of x without writing: the labelling pass stores each body's root into
+// the same array, and a halving write there could replace a label already
+// written with an intermediate ancestor.
+__device__ __forceinline__ int32_t ufRoot(const int32_t* parent, int32_t x)
+{
+	const volatile int32_t* p = parent;
+	int32_t px = p[x];
+	while (px != x)
+	{
+		x = px;
+		px = p[x];
+	}
+	return x;
+}
+
 __device__ void ufUnite(int32_t* parent, int32_t a, int32_t b)
 {
 	for (;;)
@@ -145,7 +160,9 @@ __global__ void kLabels(int32_t* parent, int32_t n, const uint8_t* bFlags, int32
 	islandFlag[i] = 0;
 	if (bFlags[i] & kBFDynamic)
 	{
-		int32_t r = ufFind(parent, i);
+		// label and parent are one array: only roots are written here, which
+		// keeps every value any thread can read an ancestor of its body
+		int32_t r = ufRoot(parent, i);
 		label[i] = r;
 		if (r == i)
 		{
@@ -315,7 +332,8 @@ __device__ __forceinline__ int32_t lowerBound64(const uint64_t* keys, int32_t n,
 __global__ void kIslandTable(const int32_t* islandLabels, int32_t maxIslands, const uint32_t* islandsDev,
 							 const uint32_t* labelStart, const uint32_t* labelCount, const uint64_t* contactKeys,
 							 const uint32_t* contactsDev, const uint64_t* jointKeys, const uint32_t* jointsDev,
-							 IslandRec* islands, int32_t* coloredList, int32_t* serialList, StepCounters* dc)
+							 IslandRec* islands, int32_t* coloredList, int32_t* serialList, int32_t* giantList,
+							 int32_t giantContacts, StepCounters* dc)
 {
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= maxIslands || k >= (int)*islandsDev)
@@ -334,7 +352,12 @@ __global__ void kIslandTable(const int32_t* islandLabels, int32_t maxIslands, co
 	r.contactCount = lowerBound64(contactKeys, nc, key + 1) - r.contactStart;
 	r.jointStart = nj > 0 ? lowerBound64(jointKeys, nj, key) : 0;
 	r.jointCount = nj > 0 ? lowerBound64(jointKeys, nj, key + 1) - r.jointStart : 0;
-	if (r.contactCount >= kBigIslandContacts)
+	if (r.contactCount >= giantContacts && r.contactCount >= kBigIslandContacts)
+	{
+		r.kind = 3;
+		giantList[atomicAdd(&dc->giantIslands, 1u)] = k;
+	}
+	else if (r.contactCount >= kBigIslandContacts)
 	{
 		r.kind = 2;
 		coloredList[atomicAdd(&dc->coloredIslands, 1u)] = k;
@@ -381,6 +404,7 @@ void launchIslands(DevWorld& w, int32_t n)
 	w.islands.ensure((size_t)(n + 1) * sizeof(IslandRec));
 	w.coloredList.ensure(n4);
 	w.serialList.ensure(n4);
+	w.giantList.ensure(n4);
 	int32_t* parent = w.label.as<int32_t>();
 	M3G_LAUNCH(kInitParent, blocksFor(n, 256), 256, s, parent, n, active, w.labelCount.as<uint32_t>(),
 			   w.labelCursor.as<uint32_t>());
@@ -450,7 +474,8 @@ void launchIslands(DevWorld& w, int32_t n)
 	M3G_LAUNCH(kIslandTable, blocksFor(n, 128), 128, s, w.islandLabels.as<int32_t>(), n, &dc->awakeIslands,
 			   w.labelStart.as<uint32_t>(), w.labelCount.as<uint32_t>(), w.contactKeys.as<uint64_t>(),
 			   &dc->islandContacts, w.jointKeys.as<uint64_t>(), J > 0 ? &dc->islandJoints : nullptr,
-			   w.islands.as<IslandRec>(), w.coloredList.as<int32_t>(), w.serialList.as<int32_t>(), dc);
+			   w.islands.as<IslandRec>(), w.coloredList.as<int32_t>(), w.serialList.as<int32_t>(),
+			   w.giantList.as<int32_t>(), w.giantIslandContacts, dc);
 	w.islandMax = n;
 }
 

@@ -4,6 +4,7 @@
 //    reconstruct per substep, one thread per body;
 //  - small islands (< 300 contacts): the reference's serial Gauss-Seidel in
 //    ascending contact order (src/xpbd.cpp:898-974), one warp per island;
+//  - giant islands (k_giant.cu) take the whole GPU;
 //  - big islands (>= 300 contacts): the reference's graph-coloured solve
 //    (src/xpbd.cpp:1167-1369), one CTA per island: greedy first-fit colouring
 //    in contact order, colour buckets solved in parallel (bodies in a bucket
@@ -16,13 +17,6 @@
 namespace m3g
 {
 
-struct SolveParams
-{
-	float h, invH, maxCorrection, gravityLen;
-	V3 gravity;
-	int substeps;
-	int iterations;
-};
 
 __global__ void kSolveFree(BodySoA B, const IslandRec* islands, int32_t ni, const uint32_t* islandsDev,
 						   const uint32_t* bodyVals, SolveParams P)
@@ -46,30 +40,6 @@ __global__ void kSolveFree(BodySoA B, const IslandRec* islands, int32_t ni, cons
 			reconstructBody(B, i, P.invH);
 		}
 	}
-}
-
-__device__ __forceinline__ void jointPosition(const BodySoA& B, JointRec* J, int ji, float h)
-{
-	JointRec jr = J[ji];
-	solveJointPosition(B, jr, h);
-	J[ji] = jr;
-}
-__device__ __forceinline__ void jointVelocity(const BodySoA& B, JointRec* J, int ji, float h)
-{
-	JointRec jr = J[ji];
-	solveJointVelocity(B, jr, h);
-	J[ji] = jr;
-}
-__device__ __forceinline__ void jointPrepare(const BodySoA& B, JointRec* J, int ji)
-{
-	JointRec jr = J[ji];
-	prepareJoint(B, jr);
-	J[ji] = jr;
-}
-__device__ __forceinline__ void jointReset(JointRec* J, int ji)
-{
-	J[ji].lambda = 0.0f;
-	J[ji].motorLambda = 0.0f;
 }
 
 // One warp per small island.  The per-element stages of a substep whose
@@ -576,6 +546,7 @@ void launchSolve(DevWorld& w, float dt, int substeps, V3 gravity, int positionIt
 			   w.coloredList.as<int32_t>(), &dc->coloredIslands, w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(),
 			   w.jointVals.as<uint32_t>(), w.colorMask.as<uint32_t>(), w.colorOrder.as<int32_t>(),
 			   w.packetMax.as<int32_t>(), w.contactColor.as<int32_t>(), P);
+	launchSolveGiant(w, P);
 }
 
 } // namespace m3g

@@ -41,7 +41,8 @@ struct StepCounters
 	uint32_t freeIslands;
 	uint32_t waitErrors; // bounded device waits that ran out (non-zero: results of the step are suspect)
 	uint32_t contactCount; // live contacts (device-side count during the step)
-	uint32_t pad[4];
+	uint32_t giantIslands; // islands solved by the whole-GPU coloured kernel
+	uint32_t pad[3];
 };
 
 // Host -> device body update record (one per body touched by the API
@@ -79,7 +80,7 @@ struct IslandRec
 	int32_t contactStart, contactCount;
 	int32_t jointStart, jointCount;
 	int32_t label;
-	int32_t kind; // 0 free bodies, 1 serial Gauss-Seidel, 2 graph coloured
+	int32_t kind; // 0 free bodies, 1 serial Gauss-Seidel, 2 graph coloured (one CTA), 3 giant (whole GPU)
 };
 
 struct DevWorld
@@ -150,7 +151,7 @@ struct DevWorld
 	DevBuf islandStartFlag, islands; // IslandRec
 	DevBuf islandKinds;
 	DevBuf labelCount, labelStart, labelCursor; // per label: island bodies
-	DevBuf islandListFlag, islandListOffs, islandLabels, coloredList, serialList, jointScan;
+	DevBuf islandListFlag, islandListOffs, islandLabels, coloredList, serialList, giantList, jointScan;
 	int32_t islandMax = 0; // upper bound of the awake islands of the step
 	int32_t islandCount = 0;
 	int32_t islandsBuiltFor = 0; // body count of the last island build (0: never)
@@ -159,6 +160,13 @@ struct DevWorld
 	DevBuf colorStart;   // per island: 10 offsets into colorOrder
 	DevBuf packetMax;    // per colorOrder position: max points of its packet
 	DevBuf contactColor; // per contact: colour for introspection
+
+	// giant islands (k_giant.cu): coloured across the whole GPU
+	int32_t giantIslandContacts = 8192; // islands with at least this many contacts
+	DevBuf giantLocal, giantBodyOffs, giantBodyCursor, giantIncidence, giantPred, giantDone, giantChunkHist;
+	DevBuf giantMisc, giantBarrier;
+	uint32_t giantEpoch = 0;
+	int giantGrid = 0;
 
 	DevBuf uploads;      // BodyUpload staging (device)
 	DevBuf counters;     // StepCounters
@@ -200,8 +208,10 @@ void launchIslands(DevWorld& w, int32_t n);
 void launchSleep(DevWorld& w, float dt);
 void launchFinish(DevWorld& w, int32_t n, float dt, bool clearForces);
 
-// solver (k_solve.cu)
+// solver (k_solve.cu, k_giant.cu)
+struct SolveParams;
 void launchSolve(DevWorld& w, float dt, int substeps, V3 gravity, int positionIterations);
+void launchSolveGiant(DevWorld& w, const SolveParams& P);
 
 // queries (k_query.cu)
 struct RayQueryOut

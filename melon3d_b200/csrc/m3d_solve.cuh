@@ -944,4 +944,38 @@ M3G_D void solveJointVelocity(const BodySoA& B, JointRec& j, float h)
 	}
 }
 
+// ---- shared by the island solve kernels ---------------------------------------
+
+struct SolveParams
+{
+	float h, invH, maxCorrection, gravityLen;
+	V3 gravity;
+	int substeps;
+	int iterations;
+};
+
+__device__ __forceinline__ void jointPosition(const BodySoA& B, JointRec* J, int ji, float h)
+{
+	JointRec jr = J[ji];
+	solveJointPosition(B, jr, h);
+	J[ji] = jr;
+}
+__device__ __forceinline__ void jointVelocity(const BodySoA& B, JointRec* J, int ji, float h)
+{
+	JointRec jr = J[ji];
+	solveJointVelocity(B, jr, h);
+	J[ji] = jr;
+}
+__device__ __forceinline__ void jointPrepare(const BodySoA& B, JointRec* J, int ji)
+{
+	JointRec jr = J[ji];
+	prepareJoint(B, jr);
+	J[ji] = jr;
+}
+__device__ __forceinline__ void jointReset(JointRec* J, int ji)
+{
+	J[ji].lambda = 0.0f;
+	J[ji].motorLambda = 0.0f;
+}
+
 } // namespace m3g

@@ -6,6 +6,7 @@
 #include <map>
 #include <mutex>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 #include <string>
 #include <utility>
@@ -121,6 +122,19 @@ void launchEnd(const char* name, cudaStream_t s)
 	}
 }
 
+// Test aid: with M3D_GPU_POISON_ALLOCATIONS=1 in the environment, every
+// scratch buffer the library allocates starts filled with 0xA5 bytes instead
+// of whatever the allocator hands back, so a kernel that reads memory it never
+// wrote fails the same way on every run.
+static bool poisonAllocations()
+{
+	static const bool on = [] {
+		const char* v = getenv("M3D_GPU_POISON_ALLOCATIONS");
+		return v != nullptr && v[0] == '1';
+	}();
+	return on;
+}
+
 bool DevBuf::ensure(size_t need)
 {
 	if (need <= bytes && ptr != nullptr)
@@ -136,6 +150,10 @@ bool DevBuf::ensure(size_t need)
 	if (cudaMalloc(&p, nb) != cudaSuccess)
 	{
 		return false;
+	}
+	if (poisonAllocations())
+	{
+		cudaMemset(p, 0xA5, nb);
 	}
 	if (ptr != nullptr)
 	{

@@ -1628,6 +1628,11 @@ int32_t m3d_gpu_step_counters(m3d_world* world, uint32_t* out, int32_t capacity)
 	return n;
 }
 int32_t m3d_gpu_status(m3d_world* world) { return world->status; }
+
+void m3d_gpu_set_giant_island_contacts(m3d_world* world, int32_t contacts)
+{
+	world->dev.giantIslandContacts = contacts < kBigIslandContacts ? kBigIslandContacts : contacts;
+}
 const char* m3d_gpu_last_error_string(m3d_world* world) { return world->errorText; }
 
 int32_t m3d_gpu_sphere_cast_noalloc(m3d_world* world, m3d_vec3 origin, float radius, m3d_vec3 translation,

@@ -24,10 +24,12 @@ from . import _util as U
 pytestmark = pytest.mark.gpu
 
 
-def lockstep(ref, kind, steps, seed=1, a=0, b=0, c=0, substeps=4, check_colors=True):
+def lockstep(ref, kind, steps, seed=1, a=0, b=0, c=0, substeps=4, check_colors=True, giant=None):
     g = U.gpu()
     sr = harness.Scene(ref, kind, seed, a, b, c)
     sg = harness.Scene(g, kind, seed, a, b, c)
+    if giant is not None:
+        g.m3d_gpu_set_giant_island_contacts(sg.world, giant)
     coloured_steps = 0
     try:
         for step in range(steps):
@@ -66,6 +68,21 @@ def test_pyramid_bit_exact_until_asleep():
 
 def test_raft_coloured_path_bit_exact():
     assert lockstep(U.oracle(), harness.RAFT, 90) > 0
+
+
+def test_pyramid_whole_gpu_coloured_path_bit_exact():
+    # every coloured island through the cooperative whole-GPU kernel
+    assert lockstep(U.oracle(), harness.PYRAMID, 80, giant=300) > 0
+
+
+def test_raft_whole_gpu_coloured_path_bit_exact():
+    assert lockstep(U.oracle(), harness.RAFT, 90, giant=300) > 0
+
+
+def test_large_pile_whole_gpu_coloured_path_bit_exact():
+    # 16,000 boxes: one island of ~38k touching contacts (above the default
+    # giant threshold), 8 colours and a small overflow bucket
+    assert lockstep(U.oracle_cr(), harness.PILE, 5, seed=3, a=20, b=40, c=20) > 0
 
 
 def test_rain_with_churn_bit_exact():
@@ -115,3 +132,34 @@ def test_pyramid_pose_gate_60_steps():
         ss.close()
         sg.close()
     print("pyramid, GPU vs reference release build (FMA): max %.3g m, %.3g" % worst_stock)
+
+
+def _gpu_twins(kind, steps, seed, a=0, b=0, c=0, giant=None):
+    """Two GPU worlds built from the same seed and stepped alternately must
+    agree bit for bit after every step (run-to-run determinism: no float
+    atomics, fixed-order reductions, exact reorderings only)."""
+    g = U.gpu()
+    s1 = harness.Scene(g, kind, seed, a, b, c)
+    s2 = harness.Scene(g, kind, seed, a, b, c)
+    if giant is not None:
+        g.m3d_gpu_set_giant_island_contacts(s1.world, giant)
+        g.m3d_gpu_set_giant_island_contacts(s2.world, giant)
+    try:
+        for step in range(steps):
+            s1.run(1)
+            s2.run(1)
+            d = U.diff_contacts(U.contacts(g, s1.world), U.contacts(g, s2.world))
+            assert d is None, "step %d: %s" % (step, d)
+            d = U.diff_bodies(U.bodies(g, s1.world), U.bodies(g, s2.world))
+            assert d is None, "step %d: %s" % (step, d)
+    finally:
+        s1.close()
+        s2.close()
+
+
+def test_runs_are_bit_identical_rain():
+    _gpu_twins(harness.RAIN, 40, 7, a=40000, b=400)
+
+
+def test_runs_are_bit_identical_pile():
+    _gpu_twins(harness.PILE, 6, 3, a=20, b=40, c=20)
