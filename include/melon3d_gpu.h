@@ -59,6 +59,25 @@ M3D_API int32_t m3d_gpu_step_counters(m3d_world* world, uint32_t* out, int32_t c
  * mean 300).  Results are identical either way; only the speed differs. */
 M3D_API void m3d_gpu_set_giant_island_contacts(m3d_world* world, int32_t contacts);
 
+/* Batch of worlds (no counterpart in the reference).  Packs `count` worlds
+ * built with melon3d.h and not stepped yet (same gravity, iterations, cell
+ * size and sleep setting) into one new world whose step advances all of them
+ * at once.  Each world's result is the one its own step would give: its
+ * contacts keep their own order, its stable tier its own schedule, and no
+ * pair spans two worlds.  Body i of world k is body slot
+ * m3d_gpu_batch_first_body(batch, k) + i of the batch, with the generation it
+ * had; getters, setters, poses, profile and m3d_gpu_* work on the batch.
+ * Bodies and joints cannot be created or destroyed in a batch and the
+ * world queries return no hit; contact events are the narrowphase begin/end
+ * events of all worlds together.  The source worlds stay valid and
+ * independent.  Limits: 2^24 worlds; cell coordinates within +-2^(b-1) cells
+ * where b = floor((63 - ceil(log2 count)) / 3) (17 bits for 4096 worlds).
+ * Returns NULL on failure (message on stderr). */
+M3D_API m3d_world* m3d_gpu_batch_create(m3d_world* const* worlds, int32_t count);
+M3D_API int32_t m3d_gpu_batch_world_count(m3d_world* batch);
+/* first body slot of world k; k == count gives the total slot count */
+M3D_API int32_t m3d_gpu_batch_first_body(m3d_world* batch, int32_t k);
+
 /* 0 when healthy, else the first M3D_GPU_ERR_* seen since creation. */
 M3D_API int32_t m3d_gpu_status(m3d_world* world);
 M3D_API const char* m3d_gpu_last_error_string(m3d_world* world);

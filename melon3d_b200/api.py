@@ -198,6 +198,9 @@ _GPU_PROTOS = {
     "m3d_gpu_last_step_device_ms": (C.c_float, [W]),
     "m3d_gpu_status": (C.c_int32, [W]),
     "m3d_gpu_set_giant_island_contacts": (None, [W, C.c_int32]),
+    "m3d_gpu_batch_create": (W, [C.POINTER(W), C.c_int32]),
+    "m3d_gpu_batch_world_count": (C.c_int32, [W]),
+    "m3d_gpu_batch_first_body": (C.c_int32, [W, C.c_int32]),
     "m3d_gpu_last_error_string": (C.c_char_p, [W]),
     "m3d_gpu_step_counters": (C.c_int32, [W, C.POINTER(C.c_uint32), C.c_int32]),
     "m3d_gpu_profiler_reset": (None, [C.c_char_p]),

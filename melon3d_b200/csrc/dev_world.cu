@@ -135,6 +135,30 @@ bool growContacts(DevWorld& w, int32_t capacity)
 	ok &= growPointArray(C.pJB, o, nc, s);
 	C.capacity = nc;
 	w.contactCap = nc;
+	if (w.batched)
+	{
+		// the re-layout target: same capacity, no contents to keep
+		ContactSoA& D = w.C2;
+		ok &= growArray(D.bodies, 0, nc, s);
+		ok &= growArray(D.pointCount, 0, nc, s);
+		ok &= growArray(D.flags, 0, nc, s);
+		ok &= growArray(D.normal, 0, nc, s);
+		ok &= growArray(D.mat, 0, nc, s);
+		ok &= growArray(D.cachePosA, 0, nc, s);
+		ok &= growArray(D.cacheRotA, 0, nc, s);
+		ok &= growArray(D.cachePosB, 0, nc, s);
+		ok &= growArray(D.cacheRotB, 0, nc, s);
+		ok &= growPointArray(D.pAnchorA, 0, nc, s);
+		ok &= growPointArray(D.pAnchorB, 0, nc, s);
+		ok &= growPointArray(D.pFricA, 0, nc, s);
+		ok &= growPointArray(D.pFricB, 0, nc, s);
+		ok &= growPointArray(D.pSlip, 0, nc, s);
+		ok &= growPointArray(D.pRA, 0, nc, s);
+		ok &= growPointArray(D.pRB, 0, nc, s);
+		ok &= growPointArray(D.pJA, 0, nc, s);
+		ok &= growPointArray(D.pJB, 0, nc, s);
+		D.capacity = nc;
+	}
 	return ok;
 }
 
@@ -149,6 +173,15 @@ StepCounters* devCounters(DevWorld& w)
 		w.prim.errorWord = &w.counters.as<StepCounters>()->waitErrors;
 	}
 	return w.counters.as<StepCounters>();
+}
+
+uint32_t* stableDirtyWords(DevWorld& w)
+{
+	if (w.batched)
+	{
+		return w.worldStableDirty.as<uint32_t>();
+	}
+	return &devCounters(w)->stableDirty;
 }
 
 __global__ void kSetU32(uint32_t* p, uint32_t v) { *p = v; }

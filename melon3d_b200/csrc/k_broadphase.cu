@@ -20,18 +20,25 @@ namespace m3g
 
 __device__ __forceinline__ int64_t cellCoord(float v, float inv) { return (int64_t)floorf(v * inv); }
 
-__device__ __forceinline__ uint64_t packCell(int64_t x, int64_t y, int64_t z)
+// PackCell (reference src/grid.cpp:19-37): each coordinate offset by half its
+// range and masked to `bits` bits, x above y above z, so keys order cells as
+// (x, y, z).  One world uses 21 bits per coordinate, as the reference; a
+// batch of worlds puts the world index above the coordinates (fewer bits
+// each), which orders entries world-major and, inside a world, exactly as the
+// world's own keys do while its cells stay within the narrower range.
+__device__ __forceinline__ uint64_t packCell(int64_t x, int64_t y, int64_t z, uint32_t world, int bits)
 {
-	const int64_t offset = 1 << 20;
-	uint64_t ux = (uint64_t)(x + offset) & 0x1FFFFFull;
-	uint64_t uy = (uint64_t)(y + offset) & 0x1FFFFFull;
-	uint64_t uz = (uint64_t)(z + offset) & 0x1FFFFFull;
-	return (ux << 42) | (uy << 21) | uz;
+	const int64_t offset = (int64_t)1 << (bits - 1);
+	const uint64_t mask = (1ull << bits) - 1ull;
+	uint64_t ux = (uint64_t)(x + offset) & mask;
+	uint64_t uy = (uint64_t)(y + offset) & mask;
+	uint64_t uz = (uint64_t)(z + offset) & mask;
+	return ((uint64_t)world << (3 * bits)) | (ux << (2 * bits)) | (uy << bits) | uz;
 }
 
-__device__ __forceinline__ uint64_t cellKeyOf(V3 p, float inv)
+__device__ __forceinline__ uint64_t cellKeyOf(V3 p, float inv, uint32_t world, int bits)
 {
-	return packCell(cellCoord(p.x, inv), cellCoord(p.y, inv), cellCoord(p.z, inv));
+	return packCell(cellCoord(p.x, inv), cellCoord(p.y, inv), cellCoord(p.z, inv), world, bits);
 }
 
 __device__ __forceinline__ uint64_t pairKey(int32_t lo, int32_t hi)
@@ -59,14 +66,17 @@ __device__ __forceinline__ int64_t cellSpan(const Box& b, float inv)
 // fat AABB refresh (reference src/world.cpp:143-211)
 // ---------------------------------------------------------------------------
 
-__global__ void kRefresh(BodySoA B, int32_t n, float dt, int rebuildStable, float inv, uint32_t* cntA, uint32_t* overA,
-						 uint32_t* cntS, uint32_t* overS, uint8_t* inActiveCells)
+// rebuildAny: the stable tier is emitted this step; worldRebuild (batch only)
+// says which worlds rebuild theirs, the others keep their entries.
+__global__ void kRefresh(BodySoA B, int32_t n, float dt, int rebuildAny, const uint8_t* worldRebuild, float inv,
+						 uint32_t* cntA, uint32_t* overA, uint32_t* cntS, uint32_t* overS, uint8_t* inActiveCells)
 {
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
 	{
 		return;
 	}
+	const bool rebuildStable = rebuildAny && (worldRebuild == nullptr || worldRebuild[worldOfBody(B, i)] != 0);
 	uint8_t st = B.state[i];
 	bool inUse = (st & kStInUse) != 0;
 	bool awake = (st & kStAwake) != 0;
@@ -135,6 +145,11 @@ __global__ void kRefresh(BodySoA B, int32_t n, float dt, int rebuildStable, floa
 	cntA[i] = ca;
 	overA[i] = oa;
 	inActiveCells[i] = inCellsA;
+	if (rebuildAny && !rebuildStable)
+	{
+		cntS[i] = 0; // this body's world keeps its stable entries
+		overS[i] = 0;
+	}
 	if (rebuildStable)
 	{
 		uint32_t cs = 0, os = 0;
@@ -172,7 +187,8 @@ void launchRefresh(DevWorld& w, int32_t n, float dt, bool rebuildStable, float c
 	{
 		return;
 	}
-	M3G_LAUNCH(kRefresh, blocksFor(n, 256), 256, w.stream, w.B, n, dt, rebuildStable ? 1 : 0, inv,
+	M3G_LAUNCH(kRefresh, blocksFor(n, 256), 256, w.stream, w.B, n, dt, rebuildStable ? 1 : 0,
+			   w.batched ? w.worldRebuild.as<uint8_t>() : nullptr, inv,
 													   w.cellCountA.as<uint32_t>(), w.overFlagA.as<uint32_t>(),
 													   w.cellCountS.as<uint32_t>(), w.overFlagS.as<uint32_t>(),
 													   w.inActiveCells.as<uint8_t>());
@@ -183,30 +199,32 @@ void launchRefresh(DevWorld& w, int32_t n, float dt, bool rebuildStable, float c
 // key, which yields the unique (key, body) order (reference src/grid.cpp:39-95)
 // ---------------------------------------------------------------------------
 
-__global__ void kEmitEntries(BodySoA B, int32_t n, float inv, const uint32_t* cnt, const uint32_t* offs,
+__global__ void kEmitEntries(BodySoA B, int32_t n, float inv, int bits, const uint32_t* cnt, const uint32_t* offs,
 							 uint64_t* keys, uint32_t* vals, uint32_t* ranges)
 {
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
-	uint32_t lo[3] = { 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu }, hi[3] = { 0u, 0u, 0u };
+	uint32_t lo[4] = { 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu }, hi[4] = { 0u, 0u, 0u, 0u };
+	const uint64_t mask = (1ull << bits) - 1ull;
 	if (i < n && cnt[i] != 0)
 	{
 		Box b = loadFat(B, i);
 		int64_t x0 = cellCoord(b.lo.x, inv), y0 = cellCoord(b.lo.y, inv), z0 = cellCoord(b.lo.z, inv);
 		int64_t x1 = cellCoord(b.hi.x, inv), y1 = cellCoord(b.hi.y, inv), z1 = cellCoord(b.hi.z, inv);
 		uint32_t o = offs[i];
+		const uint32_t world = worldOfBody(B, i);
 		for (int64_t x = x0; x <= x1; ++x)
 		{
 			for (int64_t y = y0; y <= y1; ++y)
 			{
 				for (int64_t z = z0; z <= z1; ++z)
 				{
-					uint64_t k = packCell(x, y, z);
+					uint64_t k = packCell(x, y, z, world, bits);
 					keys[o] = k;
 					vals[o] = (uint32_t)i;
-					uint32_t f[3] = { (uint32_t)(k >> 42) & 0x1FFFFFu, (uint32_t)(k >> 21) & 0x1FFFFFu,
-									  (uint32_t)k & 0x1FFFFFu };
+					uint32_t f[4] = { world, (uint32_t)((k >> (2 * bits)) & mask), (uint32_t)((k >> bits) & mask),
+									  (uint32_t)(k & mask) };
 #pragma unroll
-					for (int a = 0; a < 3; ++a)
+					for (int a = 0; a < 4; ++a)
 					{
 						lo[a] = f[a] < lo[a] ? f[a] : lo[a];
 						hi[a] = f[a] > hi[a] ? f[a] : hi[a];
@@ -218,7 +236,7 @@ __global__ void kEmitEntries(BodySoA B, int32_t n, float inv, const uint32_t* cn
 	}
 	// the range of each key field decides which radix passes run
 #pragma unroll
-	for (int a = 0; a < 3; ++a)
+	for (int a = 0; a < 4; ++a)
 	{
 		uint32_t l = lo[a], h = hi[a];
 		for (int off = 16; off > 0; off >>= 1)
@@ -231,7 +249,7 @@ __global__ void kEmitEntries(BodySoA B, int32_t n, float inv, const uint32_t* cn
 		if ((threadIdx.x & 31) == 0 && l <= h)
 		{
 			atomicMin(&ranges[a], l);
-			atomicMax(&ranges[3 + a], h);
+			atomicMax(&ranges[4 + a], h);
 		}
 	}
 }
@@ -245,14 +263,15 @@ __global__ void kCompactIndices(const uint32_t* flags, const uint32_t* offs, int
 	}
 }
 
+// per tier: min of (world, x, y, z) fields, then their max
 __global__ void kInitRanges(uint32_t* ranges)
 {
 	for (int t = 0; t < 2; ++t)
 	{
-		for (int a = 0; a < 3; ++a)
+		for (int a = 0; a < 4; ++a)
 		{
-			ranges[6 * t + a] = 0xFFFFFFFFu;
-			ranges[6 * t + 3 + a] = 0u;
+			ranges[8 * t + a] = 0xFFFFFFFFu;
+			ranges[8 * t + 4 + a] = 0u;
 		}
 	}
 }
@@ -260,24 +279,24 @@ __global__ void kInitRanges(uint32_t* ranges)
 // Radix-sort parameters of one tier from its key-field ranges: subtracting
 // each field's minimum keeps the key order (no field borrows from the next)
 // and leaves only the low bits of each field varying.
-static void tierSortBias(const uint32_t* r, uint64_t* bias, uint64_t* vary)
+static void tierSortBias(const uint32_t* r, int keyBits, uint64_t* bias, uint64_t* vary)
 {
 	uint64_t b = 0ull, v = 0ull;
-	for (int a = 0; a < 3; ++a)
+	for (int a = 0; a < 4; ++a)
 	{
-		const int shift = 42 - 21 * a;
-		if (r[a] > r[3 + a])
+		const int shift = keyBits * (3 - a);
+		if (r[a] > r[4 + a])
 		{
 			continue; // no entries
 		}
-		uint32_t d = r[3 + a] - r[a];
+		uint32_t d = r[4 + a] - r[a];
 		int bits = 0;
-		while (bits < 21 && (d >> bits) != 0)
+		while (bits < 32 && (d >> bits) != 0)
 		{
 			++bits;
 		}
 		b |= (uint64_t)r[a] << shift;
-		v |= ((1ull << bits) - 1ull) << shift;
+		v |= (bits >= 64 ? ~0ull : ((1ull << bits) - 1ull)) << shift;
 	}
 	*bias = b;
 	*vary = v;
@@ -288,9 +307,9 @@ static void tierSortBias(const uint32_t* r, uint64_t* bias, uint64_t* vary)
 // so nothing waits for the host; the sort runs after the step's first sync.
 static void emitTier(DevWorld& w, int32_t n, float inv, DevBuf& cnt, DevBuf& over, DevBuf& offs, DevBuf& ooffs,
 					 DevBuf& keys, DevBuf& vals, DevBuf& overList, uint32_t* entryTotal, uint32_t* overTotal,
-					 uint32_t* ranges)
+					 uint32_t* ranges, size_t extra = 0)
 {
-	size_t bound = (size_t)n * kOversizedCellSpan + 1;
+	size_t bound = (size_t)n * kOversizedCellSpan + 1 + extra;
 	offs.ensure((size_t)(n + 1) * sizeof(uint32_t));
 	ooffs.ensure((size_t)(n + 1) * sizeof(uint32_t));
 	keys.ensure(bound * sizeof(uint64_t));
@@ -300,8 +319,8 @@ static void emitTier(DevWorld& w, int32_t n, float inv, DevBuf& cnt, DevBuf& ove
 	scanExclusive(over.as<uint32_t>(), ooffs.as<uint32_t>(), n, overTotal, w.prim, w.stream);
 	if (n > 0)
 	{
-		M3G_LAUNCH(kEmitEntries, blocksFor(n, 128), 128, w.stream, w.B, n, inv, cnt.as<uint32_t>(), offs.as<uint32_t>(),
-				   keys.as<uint64_t>(), vals.as<uint32_t>(), ranges);
+		M3G_LAUNCH(kEmitEntries, blocksFor(n, 128), 128, w.stream, w.B, n, inv, w.keyBits, cnt.as<uint32_t>(),
+				   offs.as<uint32_t>(), keys.as<uint64_t>(), vals.as<uint32_t>(), ranges);
 		M3G_LAUNCH(kCompactIndices, blocksFor(n, 256), 256, w.stream, over.as<uint32_t>(), ooffs.as<uint32_t>(), n,
 				   overList.as<int32_t>());
 	}
@@ -310,7 +329,7 @@ static void emitTier(DevWorld& w, int32_t n, float inv, DevBuf& cnt, DevBuf& ove
 void launchEmitGrid(DevWorld& w, int32_t n, float cellSize, bool rebuildStable)
 {
 	StepCounters* dc = devCounters(w);
-	w.keyRanges.ensure(12 * sizeof(uint32_t));
+	w.keyRanges.ensure(16 * sizeof(uint32_t));
 	uint32_t* ranges = w.keyRanges.as<uint32_t>();
 	M3G_LAUNCH(kInitRanges, 1, 1, w.stream, ranges);
 	float inv = 1.0f / cellSize;
@@ -318,14 +337,22 @@ void launchEmitGrid(DevWorld& w, int32_t n, float cellSize, bool rebuildStable)
 			 &dc->activeEntries, &dc->activeOversized, ranges);
 	if (rebuildStable)
 	{
+		size_t extra = 0;
+		if (w.batched)
+		{
+			// worlds that keep their stable tier: entries set aside before the
+			// fresh ones overwrite the arrays, appended back after the sync
+			launchKeepStable(w, ranges + 8);
+			extra = (size_t)w.stableEntries;
+		}
 		emitTier(w, n, inv, w.cellCountS, w.overFlagS, w.entryOffsS, w.overOffsS, w.stableKeys, w.stableVals,
-				 w.stableOver, &dc->stableEntries, &dc->stableOversized, ranges + 6);
+				 w.stableOver, &dc->stableEntries, &dc->stableOversized, ranges + 8, extra);
 	}
 	if (w.hostRanges == nullptr)
 	{
-		cudaMallocHost((void**)&w.hostRanges, 12 * sizeof(uint32_t));
+		cudaMallocHost((void**)&w.hostRanges, 16 * sizeof(uint32_t));
 	}
-	cudaMemcpyAsync(w.hostRanges, ranges, 12 * sizeof(uint32_t), cudaMemcpyDeviceToHost, w.stream);
+	cudaMemcpyAsync(w.hostRanges, ranges, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, w.stream);
 }
 
 // after the first sync of the step: sizes and key ranges are on the host
@@ -337,7 +364,7 @@ void launchSortGrid(DevWorld& w, bool rebuildStable)
 	w.activeOverCount = (int32_t)hc->activeOversized;
 	if (w.activeEntries > 1)
 	{
-		tierSortBias(w.hostRanges, &bias, &vary);
+		tierSortBias(w.hostRanges, w.keyBits, &bias, &vary);
 		radixSortPairs(w.activeKeys.as<uint64_t>(), w.activeVals.as<uint32_t>(), w.activeEntries, vary, w.prim,
 					   w.stream, nullptr, bias);
 	}
@@ -345,9 +372,13 @@ void launchSortGrid(DevWorld& w, bool rebuildStable)
 	{
 		w.stableEntries = hc->stableEntries;
 		w.stableOverCount = (int32_t)hc->stableOversized;
+		if (w.batched)
+		{
+			launchAppendKeptStable(w, hc->stableEntries, (int32_t)hc->stableOversized);
+		}
 		if (w.stableEntries > 1)
 		{
-			tierSortBias(w.hostRanges + 6, &bias, &vary);
+			tierSortBias(w.hostRanges + 8, w.keyBits, &bias, &vary);
 			radixSortPairs(w.stableKeys.as<uint64_t>(), w.stableVals.as<uint32_t>(), w.stableEntries, vary, w.prim,
 						   w.stream, nullptr, bias);
 		}
@@ -412,6 +443,7 @@ struct PairCtx
 	const uint64_t* jointed;
 	int32_t jointedCount;
 	float inv;
+	int keyBits;
 };
 
 __device__ __forceinline__ bool jointedContains(const uint64_t* keys, int32_t n, uint64_t k)
@@ -435,7 +467,7 @@ __device__ __forceinline__ bool jointedContains(const uint64_t* keys, int32_t n,
 // every read-only admission filter of the reference (src/world.cpp:1486-1538)
 __device__ bool admissible(const PairCtx& P, int32_t a, int32_t b, uint64_t* keyOut)
 {
-	if (a == b)
+	if (a == b || worldOfBody(P.B, a) != worldOfBody(P.B, b))
 	{
 		return false;
 	}
@@ -538,7 +570,7 @@ __global__ void kRunPairs(PairCtx P, const uint64_t* actKeys, const uint32_t* ac
 			int32_t b = (int32_t)actVals[j];
 			V3 lo2 = vmax(la, ld3(P.B.fatLo[b]));
 			uint64_t pk;
-			if (cellKeyOf(lo2, P.inv) == key && admissible(P, a, b, &pk))
+			if (cellKeyOf(lo2, P.inv, worldOfBody(P.B, a), P.keyBits) == key && admissible(P, a, b, &pk))
 			{
 				if (EMIT)
 				{
@@ -561,7 +593,7 @@ __global__ void kRunPairs(PairCtx P, const uint64_t* actKeys, const uint32_t* ac
 			}
 			V3 lo2 = vmax(ld3(P.B.fatLo[a]), lb);
 			uint64_t pk;
-			if (cellKeyOf(lo2, P.inv) == key && admissible(P, a, b, &pk))
+			if (cellKeyOf(lo2, P.inv, worldOfBody(P.B, a), P.keyBits) == key && admissible(P, a, b, &pk))
 			{
 				if (EMIT)
 				{
@@ -769,6 +801,7 @@ static PairCtx pairCtx(DevWorld& w, float cellSize)
 	P.jointed = w.jointedPairs.as<uint64_t>();
 	P.jointedCount = w.jointedCount;
 	P.inv = 1.0f / cellSize;
+	P.keyBits = w.keyBits;
 	return P;
 }
 
@@ -783,6 +816,158 @@ static OverCtx overCtx(DevWorld& w, int32_t n, int64_t* total)
 	O.inActiveCells = w.inActiveCells.as<uint8_t>();
 	*total = (int64_t)O.nAO * ((int64_t)n + O.nSO) + (int64_t)O.nAO * (O.nAO - 1) / 2 + (int64_t)O.nSO * n;
 	return O;
+}
+
+// ---- oversized pairs, world by world ---------------------------------------------
+// The reference's oversized loops (src/world.cpp:1663-1702) pair an oversized
+// body with every body of its world.  In a batch the candidate stream is cut
+// into one block per oversized body - in the order of the single-world loops
+// (active oversized bodies, then stable ones) - holding only its own world's
+// bodies, so the stream of each world is the one its own step produces.
+
+__device__ __forceinline__ int32_t lowerBoundI32(const int32_t* a, int32_t n, int32_t v)
+{
+	int32_t lo = 0, hi = n;
+	while (lo < hi)
+	{
+		int32_t mid = (lo + hi) >> 1;
+		if (a[mid] < v)
+			lo = mid + 1;
+		else
+			hi = mid;
+	}
+	return lo;
+}
+
+struct OverBatch
+{
+	const int32_t* actOver;
+	int32_t nAO;
+	const int32_t* stabOver;
+	int32_t nSO;
+	const uint32_t* first; // per world + 1: first body slot
+	const uint8_t* inActiveCells;
+	const uint32_t* blockOffs;
+};
+
+__global__ void kOverBlocks(const BodySoA B, OverBatch O, uint32_t* blocks)
+{
+	int o = blockIdx.x * blockDim.x + threadIdx.x;
+	if (o >= O.nAO + O.nSO)
+	{
+		return;
+	}
+	const int32_t a = o < O.nAO ? O.actOver[o] : O.stabOver[o - O.nAO];
+	const uint32_t w = worldOfBody(B, a);
+	const int32_t f0 = (int32_t)O.first[w], f1 = (int32_t)O.first[w + 1];
+	uint32_t size = (uint32_t)(f1 - f0);
+	if (o < O.nAO)
+	{
+		const int32_t aEnd = lowerBoundI32(O.actOver, O.nAO, f1);
+		const int32_t s0 = lowerBoundI32(O.stabOver, O.nSO, f0), s1 = lowerBoundI32(O.stabOver, O.nSO, f1);
+		size += (uint32_t)(aEnd - o - 1) + (uint32_t)(s1 - s0);
+	}
+	blocks[o] = size;
+}
+
+__global__ void kOverPairsBatch(PairCtx P, OverBatch O, int64_t maxTotal, const uint32_t* totalDev, uint32_t* flags,
+								uint64_t* keys)
+{
+	const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= maxTotal)
+	{
+		return;
+	}
+	uint32_t ok = 0;
+	uint64_t pk = 0;
+	if (idx < (int64_t)*totalDev)
+	{
+		// the block holding idx: the last o with blockOffs[o] <= idx
+		int32_t lo = 0, hi = O.nAO + O.nSO;
+		while (hi - lo > 1)
+		{
+			int32_t mid = (lo + hi) >> 1;
+			if ((int64_t)O.blockOffs[mid] <= idx)
+				lo = mid;
+			else
+				hi = mid;
+		}
+		const int32_t o = lo;
+		int64_t local = idx - (int64_t)O.blockOffs[o];
+		const int32_t a = o < O.nAO ? O.actOver[o] : O.stabOver[o - O.nAO];
+		const uint32_t w = worldOfBody(P.B, a);
+		const int32_t f0 = (int32_t)O.first[w], f1 = (int32_t)O.first[w + 1];
+		const int64_t nw = f1 - f0;
+		int32_t b = -1;
+		bool inGrid = true;
+		if (o < O.nAO)
+		{
+			if (local < nw)
+			{
+				b = f0 + (int32_t)local;
+				inGrid = O.inActiveCells[b] || P.B.inStableCells[b];
+			}
+			else
+			{
+				local -= nw;
+				const int32_t aEnd = lowerBoundI32(O.actOver, O.nAO, f1);
+				if (local < aEnd - o - 1)
+				{
+					b = O.actOver[o + 1 + local];
+				}
+				else
+				{
+					local -= aEnd - o - 1;
+					b = O.stabOver[lowerBoundI32(O.stabOver, O.nSO, f0) + local];
+				}
+			}
+		}
+		else
+		{
+			b = f0 + (int32_t)local;
+			inGrid = O.inActiveCells[b] != 0;
+		}
+		if (b >= 0 && b != a && inGrid && admissible(P, a, b, &pk))
+		{
+			ok = 1;
+		}
+	}
+	flags[idx] = ok;
+	keys[idx] = pk;
+}
+
+int64_t launchOverPairsBatch(DevWorld& w, const PairCtx& P)
+{
+	StepCounters* dc = devCounters(w);
+	cudaStream_t s = w.stream;
+	const int32_t nAO = w.activeOverCount, nSO = w.stableOverCount, nO = nAO + nSO;
+	if (nO == 0)
+	{
+		setDeviceCount(w, &dc->overPairs, 0u);
+		return 0;
+	}
+	const int64_t maxN = w.maxWorldBodies;
+	const int64_t maxTotal = (int64_t)nO * (maxN + (nO < maxN ? nO : maxN));
+	w.overBlockOffs.ensure((size_t)(nO + 2) * sizeof(uint32_t));
+	w.overFlag.ensure((size_t)(maxTotal + 1) * sizeof(uint32_t));
+	w.overScan.ensure((size_t)(maxTotal + 1) * sizeof(uint32_t));
+	w.overKeys.ensure((size_t)(maxTotal + 1) * sizeof(uint64_t));
+	OverBatch O;
+	O.actOver = w.activeOver.as<int32_t>();
+	O.nAO = nAO;
+	O.stabOver = w.stableOver.as<int32_t>();
+	O.nSO = nSO;
+	O.first = w.worldFirstBody.as<uint32_t>();
+	O.inActiveCells = w.inActiveCells.as<uint8_t>();
+	O.blockOffs = w.overBlockOffs.as<uint32_t>();
+	uint32_t* blocks = w.overBlockOffs.as<uint32_t>();
+	M3G_LAUNCH(kOverBlocks, blocksFor(nO, 256), 256, s, w.B, O, blocks);
+	uint32_t* total = blocks + nO;
+	scanExclusive(blocks, blocks, nO, total, w.prim, s);
+	M3G_LAUNCH(kOverPairsBatch, blocksFor(maxTotal, 256), 256, s, P, O, maxTotal, total, w.overFlag.as<uint32_t>(),
+			   w.overKeys.as<uint64_t>());
+	scanExclusive(w.overFlag.as<uint32_t>(), w.overScan.as<uint32_t>(), maxTotal, &dc->overPairs, w.prim, s);
+	return maxTotal;
 }
 
 // Count the admitted pairs of every cell run and of the oversized loops; the
@@ -816,8 +1001,14 @@ void launchPairCount(DevWorld& w, int32_t n, float cellSize)
 	}
 	scanExclusive(w.runPairCount.as<uint32_t>(), w.runPairOffs.as<uint32_t>(), runMax, &dc->gridPairs, w.prim, s);
 
+	if (w.batched)
+	{
+		w.overTotal = launchOverPairsBatch(w, P);
+		return;
+	}
 	int64_t overTotal;
 	OverCtx O = overCtx(w, n, &overTotal);
+	w.overTotal = overTotal;
 	w.overFlag.ensure((size_t)(overTotal + 1) * sizeof(uint32_t));
 	w.overScan.ensure((size_t)(overTotal + 1) * sizeof(uint32_t));
 	w.overKeys.ensure((size_t)(overTotal + 1) * sizeof(uint64_t));
@@ -851,8 +1042,7 @@ void launchPairEmit(DevWorld& w, int32_t n, float cellSize)
 				   w.stableKeys.as<uint64_t>(), w.stableVals.as<uint32_t>(), w.stableEntries, nullptr,
 				   w.runPairOffs.as<uint32_t>(), pk);
 	}
-	int64_t overTotal;
-	overCtx(w, n, &overTotal);
+	const int64_t overTotal = w.overTotal;
 	if (overPairs > 0)
 	{
 		M3G_LAUNCH(kScatterKeys, blocksFor(overTotal, 256), 256, s, w.overFlag.as<uint32_t>(),

@@ -422,7 +422,7 @@ void launchIslands(DevWorld& w, int32_t n)
 	M3G_LAUNCH(kIslandAwake, blocksFor(n, 256), 256, s, w.B.bFlags, n, w.label.as<int32_t>(), w.islandFlag.as<uint32_t>(),
 			   active);
 	M3G_LAUNCH(kIslandBodies, blocksFor(n, 256), 256, s, w.B, n, w.label.as<int32_t>(), w.islandFlag.as<uint32_t>(),
-			   w.labelCount.as<uint32_t>(), &dc->stableDirty, active);
+			   w.labelCount.as<uint32_t>(), stableDirtyWords(w), active);
 	// bodies per island: label counts -> starts -> placement
 	scanExclusive(w.labelCount.as<uint32_t>(), w.labelStart.as<uint32_t>(), n, &dc->islandBodies, w.prim, s);
 	M3G_LAUNCH(kIslandListFlags, blocksFor(n, 256), 256, s, w.labelCount.as<uint32_t>(), n,
@@ -566,7 +566,7 @@ __global__ void kSleepApply(BodySoA B, const uint32_t* vals, int32_t maxBodies, 
 	B.vel[i] = z;
 	B.angVel[i] = z;
 	B.bFlags[i] &= (uint8_t)~kBFAwake;
-	*stableDirty = 1;
+	stableDirty[worldOfBody(B, i)] = 1;
 }
 
 void launchSleep(DevWorld& w, float dt)
@@ -590,7 +590,7 @@ void launchSleep(DevWorld& w, float dt)
 	M3G_LAUNCH(kSleepUpdate, blocksFor(nmax, 256), 256, s, w.B, vals, nmax, &dc->islandBodies, lab,
 			   w.sleepFirstNo.as<int32_t>(), w.sleepMin.as<uint32_t>(), dt);
 	M3G_LAUNCH(kSleepApply, blocksFor(nmax, 256), 256, s, w.B, vals, nmax, &dc->islandBodies, lab,
-			   w.sleepFirstNo.as<int32_t>(), w.sleepMin.as<uint32_t>(), &dc->stableDirty);
+			   w.sleepFirstNo.as<int32_t>(), w.sleepMin.as<uint32_t>(), stableDirtyWords(w));
 }
 
 // kinematic integration, one-step force clear, profile counters

@@ -176,7 +176,7 @@ void launchNarrowphase(DevWorld& w, float dt)
 			   w.evEnd.as<int4>());
 	int32_t* target = (int32_t*)w.evBeginFlag.ptr; // flags no longer needed
 	M3G_LAUNCH(kWakeDecide, blocksFor(M, 256), 256, s, w.B, w.C, M, tr, target);
-	M3G_LAUNCH(kWakeApply, blocksFor(M, 256), 256, s, w.B, M, target, &dc->stableDirty);
+	M3G_LAUNCH(kWakeApply, blocksFor(M, 256), 256, s, w.B, M, target, stableDirtyWords(w));
 }
 
 } // namespace m3g

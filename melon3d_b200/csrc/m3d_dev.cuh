@@ -42,7 +42,9 @@ struct StepCounters
 	uint32_t waitErrors; // bounded device waits that ran out (non-zero: results of the step are suspect)
 	uint32_t contactCount; // live contacts (device-side count during the step)
 	uint32_t giantIslands; // islands solved by the whole-GPU coloured kernel
-	uint32_t pad[3];
+	uint32_t keptStable;     // batch: stable entries of worlds that keep their tier
+	uint32_t keptStableOver; // batch: their oversized bodies
+	uint32_t keptContacts;   // batch: contacts after the world-major re-layout
 };
 
 // Host -> device body update record (one per body touched by the API
@@ -130,6 +132,7 @@ struct DevWorld
 	int32_t contactMax = 0;       // upper bound of the device contact count
 	DevBuf pairKeys;              // u64 admitted candidates in emission order
 	DevBuf overFlag, overScan;    // oversized candidate flags
+	int64_t overTotal = 0;        // length of the oversized candidate stream
 	DevBuf existingSet;           // hash set of existing contact keys
 	uint32_t existingMask = 0;
 	DevBuf newSet, newSetPos;     // first-occurrence dedupe
@@ -173,7 +176,31 @@ struct DevWorld
 	StepCounters* hostCounters = nullptr; // pinned
 
 	DevBuf queryOut;     // query results
+
+	// batch of worlds packed into this arena (m3d_gpu_batch_create): bodies of
+	// world w are contiguous, cell keys carry the world above the cell
+	// coordinates, contacts are kept world-major (each world's contacts in its
+	// own reference order) and the stable tier is rebuilt per world
+	bool batched = false;
+	int32_t worldCount = 1;
+	int keyBits = 21;            // bits per cell coordinate in a cell key
+	DevBuf worldOf;              // u32 per body (B.world)
+	DevBuf worldFirstBody;       // u32 per world + 1: first body slot of each world
+	int32_t maxWorldBodies = 0;  // largest world (body slots)
+	DevBuf overBlockOffs;        // oversized candidate blocks, world by world
+	DevBuf worldRebuild;         // u8 per world: stable tier rebuilt this step
+	DevBuf worldStableDirty;     // u32 per world: stable tier made dirty on the device
+	DevBuf worldContactCount;    // u32 per world: contacts at the start of the step
+	DevBuf worldContactStart;    // u32 per world + 1
+	DevBuf worldNewCount, worldNewStart, worldVStart, worldRemoved, worldFinalStart; // u32 per world + 1
+	DevBuf newByWorldKeys, newByWorldVals; // new contacts grouped by world (emission order inside)
+	DevBuf vFlag, vScan, vSrc;   // per virtual contact (old then new, world-major)
+	DevBuf keptKeys, keptVals, keptOver; // stable-tier entries of worlds that keep their tier
+	ContactSoA C2 = {};          // second contact arena: target of the world-major re-layout
 };
+
+// one stable-dirty word per world (StepCounters::stableDirty for one world)
+uint32_t* stableDirtyWords(DevWorld& w);
 
 // ---- launchers (defined in k_*.cu) -----------------------------------------
 
@@ -198,6 +225,11 @@ void launchCreateContacts(DevWorld& w);
 void launchRemoval(DevWorld& w);
 // destroy-time swap-removes computed on the host: move (dst, src) pairs
 void launchContactMoves(DevWorld& w, const int2* hostMoves, int32_t count);
+
+// batch of worlds (k_batch.cu)
+void launchKeepStable(DevWorld& w, uint32_t* ranges);
+void launchAppendKeptStable(DevWorld& w, int64_t fresh, int32_t freshOver);
+void launchBatchRelayout(DevWorld& w);
 
 // narrowphase (k_narrow.cu)
 void launchNarrowphase(DevWorld& w, float dt);

@@ -174,8 +174,13 @@ struct BodySoA
 	uint8_t* inStableTier;  // stable at the last stable-tier build
 	uint8_t* inStableCells; // binned into stable-tier cells at that build
 	uint8_t* bFlags;
+	// world of each body when the arena packs several worlds (a batch); null
+	// when it holds one world
+	uint32_t* world;
 	int32_t capacity;
 };
+
+M3G_D uint32_t worldOfBody(const BodySoA& B, int i) { return B.world != nullptr ? B.world[i] : 0u; }
 
 struct ContactSoA
 {
@@ -277,6 +282,7 @@ M3G_D Xf bodyXf(const BodySoA& B, int i)
 
 // WakeBodyInternal (reference src/world.cpp:121-140): awake, timers reset,
 // stable tier dirty when the body was asleep; static bodies never wake.
+// stableDirty holds one word per world (one word for a single world).
 M3G_D void wakeBody(const BodySoA& B, int i, uint32_t* stableDirty)
 {
 	if (B.cold[i].type == kStatic)
@@ -285,7 +291,7 @@ M3G_D void wakeBody(const BodySoA& B, int i, uint32_t* stableDirty)
 	}
 	if (!(B.state[i] & kStAwake))
 	{
-		*stableDirty = 1;
+		stableDirty[worldOfBody(B, i)] = 1;
 	}
 	B.state[i] |= kStAwake;
 	B.sleep[i] = make_float2(0.0f, 4.0f * kSleepEnergyThresh);

@@ -10,11 +10,15 @@
 namespace m3g
 {
 
-// Grow-only device buffer.
+// Grow-only device buffer, freed with its owner.
 struct DevBuf
 {
 	void* ptr = nullptr;
 	size_t bytes = 0;
+	DevBuf() = default;
+	DevBuf(const DevBuf&) = delete;
+	DevBuf& operator=(const DevBuf&) = delete;
+	~DevBuf() { release(); }
 	bool ensure(size_t need);
 	// like ensure(), but a fresh allocation is zero-filled on `stream`
 	bool ensureZeroed(size_t need, cudaStream_t stream);

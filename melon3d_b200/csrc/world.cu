@@ -103,6 +103,15 @@ struct m3d_world
 	int32_t status = M3D_GPU_OK;
 	char errorText[256] = { 0 };
 
+	// a batch of worlds packed into this one (m3d_gpu_batch_create): per world,
+	// its first body slot and its own stable-tier schedule; empty otherwise
+	std::vector<int32_t> batchFirstBody; // worlds + 1 entries
+	std::vector<uint32_t> bodyWorld;     // world of each body slot
+	std::vector<uint8_t> batchStableDirty, batchStableForce, batchRebuild;
+	std::vector<int32_t> batchStepsSinceStableBuild;
+	std::vector<uint32_t> batchDirtyRead;
+	bool stepped = false;
+
 	// pinned staging
 	std::vector<BodyUpload> uploadRecs;
 	float4* pinPos = nullptr;
@@ -165,6 +174,29 @@ void markDirty(m3d_world* w, int32_t index, uint32_t mask)
 		w->dirtyList.push_back(index);
 	}
 	w->dirtyMask[index] |= mask;
+}
+
+bool isBatch(const m3d_world* w) { return !w->batchFirstBody.empty(); }
+
+// the stable tier of the body's world is out of date (and, with force, is
+// rebuilt at the next step whatever its schedule)
+void markStableDirty(m3d_world* w, int32_t index, bool force = false)
+{
+	if (isBatch(w))
+	{
+		const uint32_t k = w->bodyWorld[index];
+		w->batchStableDirty[k] = 1;
+		if (force)
+		{
+			w->batchStableForce[k] = 1;
+		}
+		return;
+	}
+	w->stableDirty = true;
+	if (force)
+	{
+		w->stableForce = true;
+	}
 }
 
 uint32_t stateBits(const HostBody& b)
@@ -352,7 +384,7 @@ void wakeBodyHost(m3d_world* w, int32_t index)
 	}
 	if (!b.isAwake)
 	{
-		w->stableDirty = true;
+		markStableDirty(w, index);
 	}
 	b.isAwake = true;
 	b.sleepTime = 0.0f;
@@ -534,6 +566,29 @@ void refreshBroadphase(m3d_world* w, float dt)
 	DevWorld& d = w->dev;
 	int32_t n = (int32_t)w->bodies.size();
 	bool rebuildStable = w->stableForce || (w->stableDirty && w->stepsSinceStableBuild >= 4);
+	if (isBatch(w))
+	{
+		// each world on its own schedule (reference src/world.cpp:167-229)
+		rebuildStable = false;
+		const size_t worlds = w->batchRebuild.size();
+		for (size_t k = 0; k < worlds; ++k)
+		{
+			const bool rb = w->batchStableForce[k] || (w->batchStableDirty[k] && w->batchStepsSinceStableBuild[k] >= 4);
+			w->batchRebuild[k] = rb ? 1 : 0;
+			rebuildStable |= rb;
+			if (rb)
+			{
+				w->batchStableDirty[k] = 0;
+				w->batchStableForce[k] = 0;
+				w->batchStepsSinceStableBuild[k] = 0;
+			}
+			else
+			{
+				++w->batchStepsSinceStableBuild[k];
+			}
+		}
+		cudaMemcpyAsync(d.worldRebuild.ptr, w->batchRebuild.data(), worlds, cudaMemcpyHostToDevice, d.stream);
+	}
 	launchRefresh(d, n, dt, rebuildStable, w->def.gridCellSize);
 	launchEmitGrid(d, n, w->def.gridCellSize, rebuildStable);
 	readCounters(d); // sync: tier sizes and cell-key masks
@@ -732,6 +787,14 @@ void m3d_world_destroy(m3d_world* world)
 	{
 		cudaFree(p);
 	}
+	ContactSoA& C2 = d.C2;
+	void* cp2[] = { C2.bodies, C2.pointCount, C2.flags, C2.normal, C2.mat, C2.cachePosA, C2.cacheRotA, C2.cachePosB,
+					C2.cacheRotB, C2.pAnchorA, C2.pAnchorB, C2.pFricA, C2.pFricB, C2.pSlip, C2.pRA, C2.pRB, C2.pJA,
+					C2.pJB };
+	for (void* p : cp2)
+	{
+		cudaFree(p);
+	}
 	DevBuf* bufs[] = { &d.joints, &d.jointedPairs, &d.inActiveCells, &d.inStableCells, &d.cellCountA, &d.cellCountS,
 					   &d.overFlagA, &d.overFlagS, &d.label, &d.islandFlag, &d.colorMask, &d.matDirty, &d.sleepFirstNo,
 					   &d.sleepMin, &d.bodyKeys, &d.bodyVals, &d.activeKeys, &d.activeVals, &d.stableKeys,
@@ -767,6 +830,11 @@ void m3d_world_destroy(m3d_world* world)
 
 m3d_body_id m3d_body_create(m3d_world* world, const m3d_body_def* bodyDef, const m3d_shape_def* shapeDef)
 {
+	if (isBatch(world))
+	{
+		fprintf(stderr, "melon3d_gpu: %s is not available on a batch of worlds\n", __func__);
+		return m3d_body_id_null();
+	}
 	int32_t index;
 	if (!world->freeBodies.empty())
 	{
@@ -819,6 +887,11 @@ m3d_body_id m3d_body_create(m3d_world* world, const m3d_body_def* bodyDef, const
 
 void m3d_body_destroy(m3d_world* world, m3d_body_id id)
 {
+	if (isBatch(world))
+	{
+		fprintf(stderr, "melon3d_gpu: %s is not available on a batch of worlds\n", __func__);
+		return;
+	}
 	HostBody* b = getBody(world, id);
 	if (b == nullptr)
 	{
@@ -926,7 +999,7 @@ void m3d_body_set_transform(m3d_world* world, m3d_body_id id, m3d_vec3 position,
 	updateInvInertiaWorld(*b);
 	markDirty(world, id.index, kUpPose | kUpIW | kUpFatReset);
 	world->gridDirty = true;
-	world->stableDirty = true;
+	markStableDirty(world, id.index);
 	wakeBodyHost(world, id.index);
 }
 
@@ -1159,6 +1232,11 @@ static m3d_vec3 mv(V3 v) { return m3d_v3(v.x, v.y, v.z); }
 
 m3d_joint_id m3d_joint_create_distance(m3d_world* world, const m3d_distance_joint_def* def)
 {
+	if (isBatch(world))
+	{
+		fprintf(stderr, "melon3d_gpu: %s is not available on a batch of worlds\n", __func__);
+		return { -1, 0 };
+	}
 	syncMirror(world);
 	HostBody* a = getBody(world, def->bodyA);
 	HostBody* b = getBody(world, def->bodyB);
@@ -1194,6 +1272,11 @@ m3d_joint_id m3d_joint_create_distance(m3d_world* world, const m3d_distance_join
 
 m3d_joint_id m3d_joint_create_ball(m3d_world* world, const m3d_ball_joint_def* def)
 {
+	if (isBatch(world))
+	{
+		fprintf(stderr, "melon3d_gpu: %s is not available on a batch of worlds\n", __func__);
+		return { -1, 0 };
+	}
 	syncMirror(world);
 	HostBody* a = getBody(world, def->bodyA);
 	HostBody* b = getBody(world, def->bodyB);
@@ -1217,6 +1300,11 @@ m3d_joint_id m3d_joint_create_ball(m3d_world* world, const m3d_ball_joint_def* d
 
 m3d_joint_id m3d_joint_create_hinge(m3d_world* world, const m3d_hinge_joint_def* def)
 {
+	if (isBatch(world))
+	{
+		fprintf(stderr, "melon3d_gpu: %s is not available on a batch of worlds\n", __func__);
+		return { -1, 0 };
+	}
 	syncMirror(world);
 	HostBody* a = getBody(world, def->bodyA);
 	HostBody* b = getBody(world, def->bodyB);
@@ -1269,6 +1357,11 @@ m3d_joint_id m3d_joint_create_hinge(m3d_world* world, const m3d_hinge_joint_def*
 
 m3d_joint_id m3d_joint_create_weld(m3d_world* world, const m3d_weld_joint_def* def)
 {
+	if (isBatch(world))
+	{
+		fprintf(stderr, "melon3d_gpu: %s is not available on a batch of worlds\n", __func__);
+		return { -1, 0 };
+	}
 	syncMirror(world);
 	HostBody* a = getBody(world, def->bodyA);
 	HostBody* b = getBody(world, def->bodyB);
@@ -1373,8 +1466,27 @@ static m3d_ray_result toRayResult(m3d_world* world, const RayQueryOut& q)
 	return r;
 }
 
+static m3d_ray_result noHit(m3d_world* world, m3d_vec3 origin, m3d_vec3 translation)
+{
+	RayQueryOut q;
+	q.body = -1;
+	q.hit = 0;
+	q.fraction = 2.0f;
+	m3d_vec3 end = m3d_add(origin, translation);
+	q.point[0] = end.x;
+	q.point[1] = end.y;
+	q.point[2] = end.z;
+	q.normal[0] = q.normal[1] = q.normal[2] = 0.0f;
+	return toRayResult(world, q);
+}
+
 static m3d_ray_result rayCastInternal(m3d_world* world, m3d_vec3 origin, m3d_vec3 translation, uint32_t maskBits)
 {
+	if (isBatch(world))
+	{
+		fprintf(stderr, "melon3d_gpu: queries are not available on a batch of worlds\n");
+		return noHit(world, origin, translation);
+	}
 	syncMirror(world);
 	flushHostChanges(world);
 	if (world->gridDirty || world->stableDirty)
@@ -1401,6 +1513,11 @@ m3d_ray_result m3d_world_ray_cast_filtered(m3d_world* world, m3d_vec3 origin, m3
 m3d_ray_result m3d_world_sphere_cast(m3d_world* world, m3d_vec3 origin, float radius, m3d_vec3 translation,
 									 uint32_t maskBits)
 {
+	if (isBatch(world))
+	{
+		fprintf(stderr, "melon3d_gpu: queries are not available on a batch of worlds\n");
+		return noHit(world, origin, translation);
+	}
 	syncMirror(world);
 	flushHostChanges(world);
 	RayQueryOut q;
@@ -1411,7 +1528,7 @@ m3d_ray_result m3d_world_sphere_cast(m3d_world* world, m3d_vec3 origin, float ra
 
 void m3d_world_overlap_aabb(m3d_world* world, m3d_aabb aabb, m3d_overlap_fn fn, void* context)
 {
-	if (fn == NULL)
+	if (fn == NULL || isBatch(world))
 	{
 		return;
 	}
@@ -1467,6 +1584,10 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	flushHostChanges(world);
 	StepCounters* dc = devCounters(d);
 	cudaMemsetAsync(dc, 0, sizeof(StepCounters), d.stream);
+	if (isBatch(world))
+	{
+		cudaMemsetAsync(d.worldStableDirty.ptr, 0, sizeof(uint32_t) * (size_t)d.worldCount, d.stream);
+	}
 	setDeviceCount(d, &dc->contactCount, (uint32_t)d.contactCount);
 
 	// broadphase and pair bookkeeping: sync 1 inside (tier sizes), sync 2
@@ -1487,7 +1608,14 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	}
 	launchPairEmit(d, n, world->def.gridCellSize);
 	launchCreateContacts(d);
-	launchRemoval(d);
+	if (isBatch(world))
+	{
+		launchBatchRelayout(d); // per-world swap-remove, worlds packed again
+	}
+	else
+	{
+		launchRemoval(d);
+	}
 	checkCuda(world, "broadphase");
 	auto tBroad = Clock::now();
 
@@ -1516,6 +1644,20 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	fetchEvents(world, evE, d.evEnd.as<int4>(), (int32_t)hc->endNP);
 	cudaStreamSynchronize(d.stream);
 	checkCuda(world, "step");
+	if (isBatch(world))
+	{
+		world->batchDirtyRead.resize((size_t)d.worldCount);
+		cudaMemcpy(world->batchDirtyRead.data(), d.worldStableDirty.ptr, sizeof(uint32_t) * (size_t)d.worldCount,
+				   cudaMemcpyDeviceToHost);
+		for (int32_t k = 0; k < d.worldCount; ++k)
+		{
+			if (world->batchDirtyRead[k] != 0)
+			{
+				world->batchStableDirty[k] = 1;
+			}
+		}
+	}
+	world->stepped = true;
 	auto toEvent = [&](const int4& e) {
 		m3d_contact_event ev;
 		ev.bodyA = makeId(world, e.x);
@@ -1629,6 +1771,149 @@ int32_t m3d_gpu_step_counters(m3d_world* world, uint32_t* out, int32_t capacity)
 }
 int32_t m3d_gpu_status(m3d_world* world) { return world->status; }
 
+// ---- batch of worlds ----------------------------------------------------------
+
+m3d_world* m3d_gpu_batch_create(m3d_world* const* worlds, int32_t count)
+{
+	if (worlds == nullptr || count < 1)
+	{
+		fprintf(stderr, "melon3d_gpu: m3d_gpu_batch_create: no worlds\n");
+		return nullptr;
+	}
+	const m3d_world_def& def0 = worlds[0] != nullptr ? worlds[0]->def : m3d_world_def();
+	for (int32_t k = 0; k < count; ++k)
+	{
+		const m3d_world* w = worlds[k];
+		if (w == nullptr || w->stepped || isBatch(w))
+		{
+			fprintf(stderr, "melon3d_gpu: m3d_gpu_batch_create: world %d is missing, was already stepped or is a batch\n",
+					k);
+			return nullptr;
+		}
+		const m3d_world_def& d = w->def;
+		if (d.gravity.x != def0.gravity.x || d.gravity.y != def0.gravity.y || d.gravity.z != def0.gravity.z ||
+			d.positionIterations != def0.positionIterations || d.gridCellSize != def0.gridCellSize ||
+			d.enableSleep != def0.enableSleep)
+		{
+			fprintf(stderr, "melon3d_gpu: m3d_gpu_batch_create: world %d has a different world definition\n", k);
+			return nullptr;
+		}
+	}
+	int worldBits = 0;
+	while (worldBits < 31 && ((int64_t)1 << worldBits) < count)
+	{
+		++worldBits;
+	}
+	const int keyBits = (63 - worldBits) / 3;
+	if (keyBits < 12)
+	{
+		fprintf(stderr, "melon3d_gpu: m3d_gpu_batch_create: %d worlds leave too few cell-key bits\n", count);
+		return nullptr;
+	}
+	m3d_world_def def = def0;
+	m3d_world* b = m3d_world_create(&def);
+	if (b == nullptr)
+	{
+		return nullptr;
+	}
+	const int32_t worldCount = count;
+	b->batchStableDirty.resize(worldCount);
+	b->batchStableForce.resize(worldCount);
+	b->batchStepsSinceStableBuild.resize(worldCount);
+	b->batchRebuild.assign(worldCount, 0);
+	for (int32_t k = 0; k < worldCount; ++k)
+	{
+		m3d_world* src = worlds[k];
+		syncMirror(src);
+		const int32_t base = (int32_t)b->bodies.size();
+		b->batchFirstBody.push_back(base);
+		for (const HostBody& hb : src->bodies)
+		{
+			b->bodies.push_back(hb);
+			b->bodyWorld.push_back((uint32_t)k);
+		}
+		for (const JointRec& j : src->joints)
+		{
+			JointRec jr = j;
+			jr.bodyA += base;
+			jr.bodyB += base;
+			b->joints.push_back(jr);
+		}
+		b->batchStableDirty[k] = src->stableDirty ? 1 : 0;
+		b->batchStableForce[k] = src->stableForce ? 1 : 0;
+		b->batchStepsSinceStableBuild[k] = src->stepsSinceStableBuild;
+		b->anyForcesApplied |= src->anyForcesApplied;
+		b->anyMaterialChange |= src->anyMaterialChange;
+	}
+	const int32_t n = (int32_t)b->bodies.size();
+	b->batchFirstBody.push_back(n);
+	for (int32_t i = 0; i < n; ++i)
+	{
+		markDirty(b, i, kUpAll);
+	}
+	b->jointsDirty = true;
+	b->jointedPairsDirty = true;
+	b->gridDirty = true;
+
+	DevWorld& d = b->dev;
+	d.batched = true;
+	d.worldCount = worldCount;
+	d.keyBits = keyBits;
+	bool ok = growBodies(d, n + 1);
+	ok = ok && d.worldOf.ensureZeroed(sizeof(uint32_t) * (size_t)d.bodyCap, d.stream);
+	ok = ok && d.worldRebuild.ensureZeroed((size_t)worldCount + 1, d.stream);
+	ok = ok && d.worldStableDirty.ensureZeroed(sizeof(uint32_t) * (size_t)(worldCount + 1), d.stream);
+	ok = ok && d.worldContactCount.ensureZeroed(sizeof(uint32_t) * (size_t)(worldCount + 1), d.stream);
+	ok = ok && d.worldContactStart.ensureZeroed(sizeof(uint32_t) * (size_t)(worldCount + 1), d.stream);
+	ok = ok && d.worldFirstBody.ensure(sizeof(uint32_t) * (size_t)(worldCount + 1));
+	if (ok && n > 0)
+	{
+		cudaMemcpyAsync(d.worldOf.ptr, b->bodyWorld.data(), sizeof(uint32_t) * (size_t)n, cudaMemcpyHostToDevice,
+						d.stream);
+	}
+	if (ok)
+	{
+		cudaMemcpyAsync(d.worldFirstBody.ptr, b->batchFirstBody.data(), sizeof(uint32_t) * (size_t)(worldCount + 1),
+						cudaMemcpyHostToDevice, d.stream);
+	}
+	for (int32_t k = 0; k < worldCount; ++k)
+	{
+		const int32_t nk = b->batchFirstBody[k + 1] - b->batchFirstBody[k];
+		d.maxWorldBodies = nk > d.maxWorldBodies ? nk : d.maxWorldBodies;
+	}
+	d.B.world = d.worldOf.as<uint32_t>();
+	// the second contact arena at the current capacity
+	const int32_t cap = d.contactCap;
+	d.contactCap = 0;
+	ok = ok && growContacts(d, cap);
+	cudaStreamSynchronize(d.stream);
+	if (!ok || cudaGetLastError() != cudaSuccess)
+	{
+		fprintf(stderr, "melon3d_gpu: m3d_gpu_batch_create: device allocation failed\n");
+		m3d_world_destroy(b);
+		return nullptr;
+	}
+	return b;
+}
+
+int32_t m3d_gpu_batch_world_count(m3d_world* batch)
+{
+	return isBatch(batch) ? (int32_t)batch->batchFirstBody.size() - 1 : 1;
+}
+
+int32_t m3d_gpu_batch_first_body(m3d_world* batch, int32_t worldIndex)
+{
+	if (!isBatch(batch))
+	{
+		return worldIndex == 0 ? 0 : (worldIndex == 1 ? (int32_t)batch->bodies.size() : -1);
+	}
+	if (worldIndex < 0 || worldIndex >= (int32_t)batch->batchFirstBody.size())
+	{
+		return -1;
+	}
+	return batch->batchFirstBody[worldIndex];
+}
+
 void m3d_gpu_set_giant_island_contacts(m3d_world* world, int32_t contacts)
 {
 	world->dev.giantIslandContacts = contacts < kBigIslandContacts ? kBigIslandContacts : contacts;
@@ -1641,6 +1926,12 @@ int32_t m3d_gpu_sphere_cast_noalloc(m3d_world* world, m3d_vec3 origin, float rad
 	if (world == nullptr || out == nullptr)
 	{
 		fprintf(stderr, "melon3d_gpu: m3d_gpu_sphere_cast_noalloc: world and out must not be NULL\n");
+		return M3D_GPU_ERR_ARGUMENT;
+	}
+	if (isBatch(world))
+	{
+		fprintf(stderr, "melon3d_gpu: queries are not available on a batch of worlds\n");
+		*out = noHit(world, origin, translation);
 		return M3D_GPU_ERR_ARGUMENT;
 	}
 	RayQueryOut miss;

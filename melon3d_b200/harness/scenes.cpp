@@ -15,6 +15,11 @@
 //   2  settled pile: nx x ny x nz lattice of boxes he 0.5 spaced 1.02 m with
 //      +-0.01 m positional and +-1 deg rotational jitter, mu 0.6
 //   3  raft: 15x15 touching boxes plus 5 droppers (one island > 300 contacts)
+//   4  one world of the batched-worlds config (its index is the seed): its
+//      own 12x1x12 m ground box, floor(exp(U[ln16, ln512])) bodies drawn from
+//      the rain distributions inside a 10x10x10 m volume above it, and 0-4
+//      ball or hinge joints between random body pairs, anchored at the pair's
+//      midpoint (a > 0 fixes the body count, b > 0 leaves the joints out)
 #include "melon3d.h"
 
 #include <algorithm>
@@ -41,6 +46,10 @@ struct M3dApi
 	m3d_profile (*world_profile)(m3d_world*);
 	// optional: batch pose readback of the GPU library (NULL elsewhere)
 	void (*read_poses)(m3d_world*, float*, float*, int32_t);
+	// joints (scene 4)
+	m3d_joint_id (*joint_create_ball)(m3d_world*, const m3d_ball_joint_def*);
+	m3d_joint_id (*joint_create_hinge)(m3d_world*, const m3d_hinge_joint_def*);
+	m3d_hinge_joint_def (*hinge_joint_def_default)(void);
 };
 
 } // extern "C"
@@ -88,6 +97,8 @@ struct Scene
 	int churn = 0;
 	Rng rng{ 0 };
 	std::vector<m3d_body_id> dynamic; // live dynamic bodies, creation order
+	std::vector<m3d_vec3> positions;  // creation pose of each entry of `dynamic` (scene 4)
+	std::vector<m3d_quat> orientations;
 	std::vector<float> pos, rot;
 	double lastHostMs = 0.0;
 };
@@ -118,12 +129,13 @@ m3d_body_id addBox(Scene& s, m3d_vec3 p, m3d_quat q, m3d_vec3 he, float mu)
 	return id;
 }
 
-m3d_body_id spawnRain(Scene& s, int kind)
+// a body from the rain distributions at a uniform position in [lo, hi]
+m3d_body_id spawnShape(Scene& s, int kind, m3d_vec3 lo, m3d_vec3 hi)
 {
 	Rng& r = s.rng;
 	m3d_body_def bd = s.api.body_def_default();
 	bd.type = M3D_BODY_DYNAMIC;
-	bd.position = m3d_v3(r.range(-50.0, 50.0), r.range(1.0, 61.0), r.range(-50.0, 50.0));
+	bd.position = m3d_v3(r.range(lo.x, hi.x), r.range(lo.y, hi.y), r.range(lo.z, hi.z));
 	bd.orientation = r.quat();
 	bd.linearVelocity = m3d_v3((float)(2.0 * r.normal()), (float)(2.0 * r.normal()), (float)(2.0 * r.normal()));
 	m3d_shape_def sd = s.api.shape_def_default();
@@ -147,7 +159,57 @@ m3d_body_id spawnRain(Scene& s, int kind)
 	sd.restitution = r.range(0.0, 0.3);
 	m3d_body_id id = s.api.body_create(s.world, &bd, &sd);
 	s.dynamic.push_back(id);
+	s.positions.push_back(bd.position);
+	s.orientations.push_back(bd.orientation);
 	return id;
+}
+
+m3d_body_id spawnRain(Scene& s, int kind)
+{
+	return spawnShape(s, kind, m3d_v3(-50.0f, 1.0f, -50.0f), m3d_v3(50.0f, 61.0f, 50.0f));
+}
+
+// joints of scene 4: pairs of distinct bodies, anchored at their midpoint
+void addBatchJoints(Scene& s, int count)
+{
+	size_t n = s.dynamic.size();
+	if (n < 2 || s.api.joint_create_ball == nullptr || s.api.joint_create_hinge == nullptr)
+	{
+		return;
+	}
+	std::vector<float> pos(n * 3), rot(n * 4);
+	for (int j = 0; j < count; ++j)
+	{
+		size_t ia = (size_t)(s.rng.next() % n), ib = (size_t)(s.rng.next() % (n - 1));
+		ib = ib >= ia ? ib + 1 : ib;
+		bool hinge = (s.rng.next() & 1) != 0;
+		m3d_body_id a = s.dynamic[ia], b = s.dynamic[ib];
+		m3d_vec3 pa = s.positions[ia], pb = s.positions[ib];
+		m3d_quat qa = s.orientations[ia], qb = s.orientations[ib];
+		m3d_vec3 mid = m3d_scale(0.5f, m3d_add(pa, pb));
+		m3d_vec3 la = m3d_inv_rotate(qa, m3d_sub(mid, pa)), lb = m3d_inv_rotate(qb, m3d_sub(mid, pb));
+		if (hinge)
+		{
+			m3d_hinge_joint_def d = s.api.hinge_joint_def_default();
+			d.bodyA = a;
+			d.bodyB = b;
+			d.localAnchorA = la;
+			d.localAnchorB = lb;
+			d.localAxisA = m3d_inv_rotate(qa, m3d_v3(0.0f, 1.0f, 0.0f));
+			d.localAxisB = m3d_inv_rotate(qb, m3d_v3(0.0f, 1.0f, 0.0f));
+			s.api.joint_create_hinge(s.world, &d);
+		}
+		else
+		{
+			m3d_ball_joint_def d;
+			memset(&d, 0, sizeof(d));
+			d.bodyA = a;
+			d.bodyB = b;
+			d.localAnchorA = la;
+			d.localAnchorB = lb;
+			s.api.joint_create_ball(s.world, &d);
+		}
+	}
 }
 
 // destroy the `churn` lowest dynamic bodies (ties by index), spawn as many
@@ -291,6 +353,18 @@ void* scn_create(const M3dApi* api, int kind, uint64_t seed, int a, int b, int c
 				}
 			}
 		}
+	}
+	else if (kind == 4)
+	{
+		addGround(*s, m3d_v3(0.0f, -0.5f, 0.0f), m3d_v3(6.0f, 0.5f, 6.0f));
+		double u = s->rng.uniform();
+		int count = a > 0 ? a : (int)floor(exp(log(16.0) + u * (log(512.0) - log(16.0))));
+		for (int i = 0; i < count; ++i)
+		{
+			spawnShape(*s, i % 3, m3d_v3(-5.0f, 0.5f, -5.0f), m3d_v3(5.0f, 10.5f, 5.0f));
+		}
+		int joints = (int)(s->rng.next() % 5);
+		addBatchJoints(*s, b > 0 ? 0 : joints); // b > 0: no joints
 	}
 	else if (kind == 3)
 	{
