@@ -55,7 +55,7 @@ M3D_API int32_t m3d_gpu_step_counters(m3d_world* world, uint32_t* out, int32_t c
 
 /* Coloured islands (>= 300 contacts, solved with the reference's greedy
  * colouring) with at least `contacts` contacts are solved by all SMs in one
- * cooperative launch instead of one CTA each (default 8192; values below 300
+ * cooperative launch instead of one CTA each (default 32768; values below 300
  * mean 300).  Results are identical either way; only the speed differs. */
 M3D_API void m3d_gpu_set_giant_island_contacts(m3d_world* world, int32_t contacts);
 

@@ -332,8 +332,8 @@ __device__ __forceinline__ int32_t lowerBound64(const uint64_t* keys, int32_t n,
 __global__ void kIslandTable(const int32_t* islandLabels, int32_t maxIslands, const uint32_t* islandsDev,
 							 const uint32_t* labelStart, const uint32_t* labelCount, const uint64_t* contactKeys,
 							 const uint32_t* contactsDev, const uint64_t* jointKeys, const uint32_t* jointsDev,
-							 IslandRec* islands, int32_t* coloredList, int32_t* serialList, int32_t* giantList,
-							 int32_t giantContacts, StepCounters* dc)
+							 IslandRec* islands, int32_t* coloredList, int32_t* serialList, int32_t* tinyList,
+							 int32_t* giantList, int32_t giantContacts, int32_t tinyContacts, StepCounters* dc)
 {
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= maxIslands || k >= (int)*islandsDev)
@@ -365,7 +365,15 @@ __global__ void kIslandTable(const int32_t* islandLabels, int32_t maxIslands, co
 	else if (r.contactCount > 0 || r.jointCount > 0)
 	{
 		r.kind = 1;
-		serialList[atomicAdd(&dc->serialIslands, 1u)] = k;
+		atomicAdd(&dc->serialIslands, 1u);
+		if (r.contactCount <= tinyContacts && r.jointCount == 0)
+		{
+			tinyList[atomicAdd(&dc->tinyIslands, 1u)] = k;
+		}
+		else
+		{
+			serialList[atomicAdd(&dc->warpIslands, 1u)] = k;
+		}
 	}
 	else
 	{
@@ -404,6 +412,7 @@ void launchIslands(DevWorld& w, int32_t n)
 	w.islands.ensure((size_t)(n + 1) * sizeof(IslandRec));
 	w.coloredList.ensure(n4);
 	w.serialList.ensure(n4);
+	w.tinyList.ensure(n4);
 	w.giantList.ensure(n4);
 	int32_t* parent = w.label.as<int32_t>();
 	M3G_LAUNCH(kInitParent, blocksFor(n, 256), 256, s, parent, n, active, w.labelCount.as<uint32_t>(),
@@ -475,7 +484,8 @@ void launchIslands(DevWorld& w, int32_t n)
 			   w.labelStart.as<uint32_t>(), w.labelCount.as<uint32_t>(), w.contactKeys.as<uint64_t>(),
 			   &dc->islandContacts, w.jointKeys.as<uint64_t>(), J > 0 ? &dc->islandJoints : nullptr,
 			   w.islands.as<IslandRec>(), w.coloredList.as<int32_t>(), w.serialList.as<int32_t>(),
-			   w.giantList.as<int32_t>(), w.giantIslandContacts, dc);
+			   w.tinyList.as<int32_t>(), w.giantList.as<int32_t>(), w.giantIslandContacts,
+			   w.lastSerialIslands > kTinyModeIslands ? kTinyIslandContacts : 0, dc);
 	w.islandMax = n;
 }
 

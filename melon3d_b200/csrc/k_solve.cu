@@ -3,7 +3,8 @@
 //  - free islands (one body, no contacts, no joints): integrate and
 //    reconstruct per substep, one thread per body;
 //  - small islands (< 300 contacts): the reference's serial Gauss-Seidel in
-//    ascending contact order (src/xpbd.cpp:898-974), one warp per island;
+//    ascending contact order (src/xpbd.cpp:898-974), one thread per island
+//    for the smallest (up to 8 contacts, no joints), one warp otherwise;
 //  - giant islands (k_giant.cu) take the whole GPU;
 //  - big islands (>= 300 contacts): the reference's graph-coloured solve
 //    (src/xpbd.cpp:1167-1369), one CTA per island: greedy first-fit colouring
@@ -273,6 +274,52 @@ __global__ void __launch_bounds__(32 * kSerialWarpsPerBlock)
 	}
 }
 
+// Small serial islands without joints, one thread each: the whole substep
+// loop in the reference's order (src/xpbd.cpp:898-974), 32 islands per warp.
+__global__ void __launch_bounds__(128)
+	kSolveTiny(BodySoA B, ContactSoA C, const IslandRec* islands, const int32_t* tinyList, const uint32_t* tinyDev,
+			   const uint32_t* bodyVals, const uint32_t* contactVals, SolveParams P)
+{
+	const int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k >= (int)*tinyDev)
+	{
+		return;
+	}
+	const IslandRec r = islands[tinyList[k]];
+	const uint32_t* bodies = bodyVals + r.bodyStart;
+	const uint32_t* contacts = contactVals + r.contactStart;
+	for (int sub = 0; sub < P.substeps; ++sub)
+	{
+		for (int b = 0; b < r.bodyCount; ++b)
+		{
+			integrateBody(B, (int)bodies[b], P.h, P.gravity);
+		}
+		for (int c = 0; c < r.contactCount; ++c)
+		{
+			prepareContact(B, C, (int)contacts[c], P.h);
+		}
+		for (int it = 0; it < P.iterations; ++it)
+		{
+			for (int c = 0; c < r.contactCount; ++c)
+			{
+				solveContactNormals(B, C, (int)contacts[c], P.maxCorrection);
+			}
+		}
+		for (int c = 0; c < r.contactCount; ++c)
+		{
+			applyContactFriction(B, C, (int)contacts[c]);
+		}
+		for (int b = 0; b < r.bodyCount; ++b)
+		{
+			reconstructBody(B, (int)bodies[b], P.invH);
+		}
+		for (int c = 0; c < r.contactCount; ++c)
+		{
+			solveContactVelocity(B, C, (int)contacts[c], P.h, P.gravityLen);
+		}
+	}
+}
+
 constexpr int kColorThreads = 256;
 
 __device__ void colorIsland(BodySoA B, ContactSoA C, JointRec* J, const IslandRec r, const uint32_t* bodyVals,
@@ -536,8 +583,13 @@ void launchSolve(DevWorld& w, float dt, int substeps, V3 gravity, int positionIt
 	int serialBlocks = (ni + kSerialWarpsPerBlock - 1) / kSerialWarpsPerBlock;
 	serialBlocks = serialBlocks < 148 * 8 ? serialBlocks : 148 * 8;
 	w.colorMask.ensure((size_t)(w.bodyCap + 1) * sizeof(uint32_t)); // also the serial islands' local body index
+	if (w.lastSerialIslands > kTinyModeIslands) // the island table listed tiny islands this step
+	{
+		M3G_LAUNCH(kSolveTiny, blocksFor(ni, 128), 128, s, w.B, w.C, isl, w.tinyList.as<int32_t>(), &dc->tinyIslands,
+				   w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(), P);
+	}
 	M3G_LAUNCH(kSolveSerial, serialBlocks, 32 * kSerialWarpsPerBlock, s, w.B, w.C, w.joints.as<JointRec>(), isl,
-			   w.serialList.as<int32_t>(), &dc->serialIslands, w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(),
+			   w.serialList.as<int32_t>(), &dc->warpIslands, w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(),
 			   w.jointVals.as<uint32_t>(), w.colorMask.as<uint32_t>(), P);
 	size_t nc = (size_t)w.contactMax + 1;
 	w.colorOrder.ensure(nc * sizeof(int32_t));

@@ -45,6 +45,8 @@ struct StepCounters
 	uint32_t keptStable;     // batch: stable entries of worlds that keep their tier
 	uint32_t keptStableOver; // batch: their oversized bodies
 	uint32_t keptContacts;   // batch: contacts after the world-major re-layout
+	uint32_t tinyIslands;    // serial islands small enough for one thread each
+	uint32_t warpIslands;    // the other serial islands (one warp each)
 };
 
 // Host -> device body update record (one per body touched by the API
@@ -154,8 +156,9 @@ struct DevWorld
 	DevBuf islandStartFlag, islands; // IslandRec
 	DevBuf islandKinds;
 	DevBuf labelCount, labelStart, labelCursor; // per label: island bodies
-	DevBuf islandListFlag, islandListOffs, islandLabels, coloredList, serialList, giantList, jointScan;
+	DevBuf islandListFlag, islandListOffs, islandLabels, coloredList, serialList, tinyList, giantList, jointScan;
 	int32_t islandMax = 0; // upper bound of the awake islands of the step
+	uint32_t lastSerialIslands = 0; // serial islands of the previous step (kernel choice)
 	int32_t islandCount = 0;
 	int32_t islandsBuiltFor = 0; // body count of the last island build (0: never)
 	DevBuf colorOf;      // per island-contact position: colour 0..8
@@ -165,7 +168,7 @@ struct DevWorld
 	DevBuf contactColor; // per contact: colour for introspection
 
 	// giant islands (k_giant.cu): coloured across the whole GPU
-	int32_t giantIslandContacts = 8192; // islands with at least this many contacts
+	int32_t giantIslandContacts = 32768; // islands with at least this many contacts
 	DevBuf giantLocal, giantBodyOffs, giantBodyCursor, giantIncidence, giantPred, giantDone, giantChunkHist;
 	DevBuf giantMisc, giantBarrier;
 	uint32_t giantEpoch = 0;

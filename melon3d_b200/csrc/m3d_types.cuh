@@ -30,6 +30,12 @@ constexpr float kSleepWakeFactor = 3.0f;
 constexpr int32_t kOversizedCellSpan = 64;
 constexpr int32_t kBigIslandContacts = 300;
 constexpr int32_t kMaxGraphColors = 8;
+// Serial islands up to kTinyIslandContacts contacts (no joints) take one
+// thread each when the previous step had more than kTinyModeIslands serial
+// islands (throughput-bound: 32 islands per warp); with fewer, every serial
+// island takes a warp (latency-bound: no divergence between islands).
+constexpr int32_t kTinyIslandContacts = 8;
+constexpr uint32_t kTinyModeIslands = 16384;
 
 // body sidecar bits (reference src/m3d_internal.h:271-274)
 constexpr uint8_t kBFDynamic = 1;

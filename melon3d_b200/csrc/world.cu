@@ -1678,6 +1678,7 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 		world->endEvents.push_back(toEvent(e));
 	}
 	d.contactCount = (int32_t)hc->contactCount;
+	d.lastSerialIslands = hc->serialIslands;
 	if (hc->anyAwakeDynamic)
 	{
 		d.islandsBuiltFor = n;

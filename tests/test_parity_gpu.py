@@ -81,7 +81,7 @@ def test_raft_whole_gpu_coloured_path_bit_exact():
 
 def test_large_pile_whole_gpu_coloured_path_bit_exact():
     # 16,000 boxes: one island of ~38k touching contacts (above the default
-    # giant threshold), 8 colours and a small overflow bucket
+    # giant threshold of 32768), 8 colours and a small overflow bucket
     assert lockstep(U.oracle_cr(), harness.PILE, 5, seed=3, a=20, b=40, c=20) > 0
 
 
