@@ -70,6 +70,11 @@ def parse():
     p.add_argument("--roofline-kernel", default="kSolveFree")
     p.add_argument("--cpu-baseline-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-variants", action="store_true",
+                   help="skip the batched-worlds and large-pile measurements")
+    p.add_argument("--batch-worlds", type=int, default=4096)
+    p.add_argument("--batch-steps", type=int, default=40)
+    p.add_argument("--pile-steps", type=int, default=12)
     return p.parse_args()
 
 
@@ -180,6 +185,96 @@ def run_reference_sample(steps, warmup, args, seconds_cap=None):
                       "workerCount=%d" % (done, warmup, cores), "ms_per_step": wall_total / max(done, 1)}, None
 
 
+def _device_steps(lib, world, steps, substeps, bodies):
+    """Steps through the C API: device time (CUDA events on the world's
+    stream) and host wall time, in ms."""
+    dev = 0.0
+    t = time.perf_counter()
+    for _ in range(steps):
+        lib.m3d_world_step(world, 1.0 / 60.0, substeps)
+        dev += lib.m3d_gpu_last_step_device_ms(world)
+    wall = (time.perf_counter() - t) * 1000.0
+    return dev, wall
+
+
+def measure_pile(lib, args, ref_lib):
+    """250,000-box settled pile (50x100x50 lattice), one giant island: the
+    whole-GPU coloured solve.  Step 0 (3.1M contacts created) is untimed."""
+    sc = harness.Scene(lib, harness.PILE, 3, 50, 100, 50)
+    n = sc.sl.scn_dynamic_count(sc.handle)
+    lib.m3d_world_step(sc.world, 1.0 / 60.0, args.substeps)
+    lib.m3d_world_step(sc.world, 1.0 / 60.0, args.substeps)
+    dev, wall = _device_steps(lib, sc.world, args.pile_steps, args.substeps, n)
+    pr = lib.m3d_world_profile(sc.world)
+    out = {"workload": "settled pile, 250,000 boxes (50x100x50 lattice, 1.02 m spacing, jitter), one giant island",
+           "bodies": n, "steps": args.pile_steps, "value": n * args.substeps * args.pile_steps / (dev / 1000.0),
+           "unit": "body-substeps/s", "ms_per_step": dev / args.pile_steps,
+           "e2e": {"value": n * args.substeps * args.pile_steps / (wall / 1000.0), "ms_per_step": wall / args.pile_steps},
+           "contacts": pr.contactCount, "touching": pr.touchingContactCount, "status": lib.m3d_gpu_status(sc.world)}
+    sc.close()
+    if ref_lib is not None and not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        rs = harness.Scene(ref_lib, harness.PILE, 3, 50, 100, 50, workers=cores)
+        rs.run(1, args.substeps)  # contact creation
+        bs, wall_ms, _ = rs.run(2, args.substeps)
+        rs.close()
+        out["cpu_baseline"] = {"value": bs / (wall_ms / 1000.0), "unit": "body-substeps/s", "cores": cores,
+                               "kind": "reference", "sample": "2 steps after the first, reference release build, "
+                                                               "workerCount=%d" % cores}
+    return out
+
+
+def measure_batch(lib, args, ref_lib):
+    """4096 independent worlds (own ground, 16-512 bodies, 0-4 joints) in one
+    batch, against the same worlds stepped one at a time."""
+    W = args.batch_worlds
+    scenes = [harness.Scene(lib, harness.BATCH_WORLD, k) for k in range(W)]
+    bodies = sum(s.sl.scn_dynamic_count(s.handle) for s in scenes)
+    arr = (C.c_void_p * W)(*[s.world for s in scenes])
+    batch = lib.m3d_gpu_batch_create(arr, W)
+    # one at a time: the first worlds stepped through the plain path
+    solo_n, solo_steps = min(64, W), 10
+    t = time.perf_counter()
+    solo_bs = 0
+    for s in scenes[:solo_n]:
+        bs, _, _ = s.run(solo_steps, args.substeps)
+        solo_bs += bs
+    solo_rate = solo_bs / (time.perf_counter() - t)
+    for s in scenes:
+        s.close()
+    lib.m3d_world_step(batch, 1.0 / 60.0, args.substeps)
+    launches0 = lib.m3d_gpu_profiler_launches()
+    dev, wall = _device_steps(lib, batch, args.batch_steps, args.substeps, bodies)
+    launches = lib.m3d_gpu_profiler_launches() - launches0
+    pos = (C.c_float * (3 * lib.m3d_gpu_body_capacity(batch)))()
+    lib.m3d_gpu_read_poses(batch, pos, None, lib.m3d_gpu_body_capacity(batch))
+    value = bodies * args.substeps * args.batch_steps / (dev / 1000.0)
+    e2e = bodies * args.substeps * args.batch_steps / (wall / 1000.0)
+    out = {"workload": "%d worlds, log-uniform 16-512 bodies each (rain shapes, own ground box, 0-4 ball/hinge "
+                       "joints)" % W, "bodies": bodies, "steps": args.batch_steps, "value": value,
+           "unit": "body-substeps/s", "ms_per_step": dev / args.batch_steps,
+           "e2e": {"value": e2e, "ms_per_step": wall / args.batch_steps},
+           "one_at_a_time": {"value": solo_rate, "unit": "body-substeps/s",
+                             "sample": "%d worlds x %d steps through the plain GPU path" % (solo_n, solo_steps)},
+           "speedup_vs_one_at_a_time": e2e / solo_rate, "gpu_launches_per_step": launches / args.batch_steps,
+           "status": lib.m3d_gpu_status(batch)}
+    lib.m3d_world_destroy(batch)
+    if ref_lib is not None and not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        rn, rsteps = min(256, W), 5
+        t = time.perf_counter()
+        rbs = 0
+        for k in range(rn):
+            rs = harness.Scene(ref_lib, harness.BATCH_WORLD, k, workers=cores)
+            bs, _, _ = rs.run(rsteps, args.substeps)
+            rbs += bs
+            rs.close()
+        out["cpu_baseline"] = {"value": rbs / (time.perf_counter() - t), "unit": "body-substeps/s", "cores": cores,
+                               "kind": "reference", "sample": "%d worlds x %d steps one after another (world "
+                                                              "creation included), workerCount=%d" % (rn, rsteps, cores)}
+    return out
+
+
 def main():
     args = parse()
     d = Dist(args.gpus)
@@ -266,6 +361,10 @@ def main():
                 "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
                 "bytes_per_launch": per_launch, "avg_launch_us": avg_s * 1e6, "launches": kl.value,
                 "model": model[0], "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+    variants = None
+    if d.rank == 0 and d.world == 1 and not args.no_variants:
+        ref_lib = api.bind(C.CDLL(REF_RELEASE_LIB)) if os.path.exists(REF_RELEASE_LIB) else None
+        variants = {"batched": measure_batch(lib, args, ref_lib), "pile": measure_pile(lib, args, ref_lib)}
     if d.rank == 0:
         line = {"metric": "body-substeps/s", "value": total_bs / (dev_ms_max / 1000.0), "unit": "body-substeps/s",
                 "n_gpus": d.world, "steps": args.steps, "warmup": args.warmup,
@@ -280,7 +379,7 @@ def main():
                         "d2h_bytes_per_step": d2h.value // max(args.steps, 1),
                         "ms_per_step": wall_ms_max / args.steps},
                 "roofline": roof, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk,
-                "status": status}
+                "status": status, "variants": variants}
         print(json.dumps(line))
     scene.close()
     d.barrier()
