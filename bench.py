@@ -43,18 +43,30 @@ COUNTER_NAMES = ["activeEntries", "stableEntries", "activeOversized", "stableOve
                  "overPairs", "newContacts", "removed", "endRemoval", "beginNP", "endNP", "anyAwakeDynamic",
                  "islandCount", "touchingCount", "awakeIslands", "islandContacts", "islandJoints", "islandBodies",
                  "stableDirty", "bodyCount", "awakeBodyCount", "hashFail", "coloredIslands", "serialIslands",
-                 "freeIslands"]
+                 "freeIslands", "waitErrors", "contactCount", "giantIslands", "keptStable", "keptStableOver",
+                 "keptContacts", "tinyIslands", "warpIslands", "islandPoints", "serialBodies", "serialContacts"]
 
-# Algorithmic bytes per launch of the kernels that can be named as the
-# roofline kernel: each field a kernel must read or write, counted once
-# (fp32 SoA; per body-substep 300 B = integrate 220 + reconstruct 80).
+
+def _serial_bytes(c, sub):
+    # per substep 300 B per body (integrate 220 + reconstruct 80), 320 B per
+    # manifold point and 884 B per contact (prepare, two normal iterations,
+    # friction, velocity pass), the serial islands' share of the points
+    # taken in proportion to their contacts
+    pts = c["islandPoints"] * c["serialContacts"] / max(c["islandContacts"], 1)
+    return sub * (300.0 * c["serialBodies"] + 884.0 * c["serialContacts"] + 320.0 * pts)
+
+
+# Algorithmic bytes per step of the kernels reported against the roofline:
+# each field a kernel must read or write, counted once (fp32 SoA).
 ROOFLINE_MODELS = {
+    # serial islands: the whole substep loop of every serial island
+    "kSolveSerial": ("HBM bytes per serial-island body, contact and point per substep", _serial_bytes),
     # free-body islands: every substep integrates and reconstructs each body
-    "kSolveFree": ("HBM bytes per free body per step", lambda c, sub: c["freeIslands"] * 300 * sub),
+    "kSolveFree": ("HBM bytes per free body per substep", lambda c, sub: c["freeIslands"] * 300.0 * sub),
     # narrowphase: per live contact the two body indices, flags, two poses,
     # two cached poses, point count (~150 B); regenerated pairs also write
     # their manifold (~4 x 132 B) - counted as the cached case (a floor)
-    "kNarrowphase": ("HBM bytes per contact", lambda c, sub: (c["_contacts"]) * 150),
+    "kNarrowphase": ("HBM bytes per contact", lambda c, sub: c["contactCount"] * 150.0),
 }
 
 
@@ -67,7 +79,7 @@ def parse():
     p.add_argument("--bodies", type=int, default=20000)
     p.add_argument("--churn", type=int, default=200)
     p.add_argument("--substeps", type=int, default=4)
-    p.add_argument("--roofline-kernel", default="kSolveFree")
+    p.add_argument("--roofline-kernels", default="kSolveSerial,kSolveFree,kNarrowphase")
     p.add_argument("--cpu-baseline-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-variants", action="store_true",
@@ -156,6 +168,21 @@ class Clocks:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def read_traffic():
+    """DRAM bytes per launch (read + write) of kernels captured with ncu on
+    this workload, from profiles/dram_traffic.txt ("<kernel> <bytes>" lines);
+    empty when the file is absent."""
+    out = {}
+    try:
+        for line in open(os.path.join(ROOT, "profiles", "dram_traffic.txt")):
+            parts = line.split()
+            if len(parts) >= 2 and not line.startswith("#"):
+                out[parts[0]] = float(parts[1])
+    except OSError:
+        pass
+    return out
 
 
 def flush_l2(buf):
@@ -309,12 +336,12 @@ def main():
     clocks = Clocks(d.local)
     d.barrier()
     torch.cuda.synchronize()
-    lib.m3d_gpu_profiler_reset(args.roofline_kernel.encode())
+    names = [k for k in args.roofline_kernels.split(",") if k in ROOFLINE_MODELS]
+    lib.m3d_gpu_profiler_reset(",".join(names).encode())
     clocks.start()
     dev_ms = wall_ms = 0.0
     body_substeps = 0
-    alg_bytes = 0.0
-    model = ROOFLINE_MODELS.get(args.roofline_kernel)
+    alg_bytes = {k: 0.0 for k in names}
     for _ in range(args.steps):
         flush_l2(flush_buf)
         torch.cuda.synchronize()
@@ -322,18 +349,21 @@ def main():
         dev_ms += lib.m3d_gpu_last_step_device_ms(world)
         wall_ms += wall
         body_substeps += bs
-        if model is not None:
-            n = lib.m3d_gpu_step_counters(world, counters, 64)
-            c = {name: counters[i] for i, name in enumerate(COUNTER_NAMES[:n])}
-            c["_contacts"] = lib.m3d_world_profile(world).contactCount
-            alg_bytes += model[1](c, args.substeps)
+        n = lib.m3d_gpu_step_counters(world, counters, 64)
+        c = {name: counters[i] for i, name in enumerate(COUNTER_NAMES[:n])}
+        for k in names:
+            alg_bytes[k] += ROOFLINE_MODELS[k][1](c, args.substeps)
     torch.cuda.synchronize()
     clk = clocks.stop()
     launches = lib.m3d_gpu_profiler_launches()
     h2d, d2h = C.c_longlong(0), C.c_longlong(0)
     lib.m3d_gpu_profiler_bytes(C.byref(h2d), C.byref(d2h))
-    kms, kl = C.c_float(0.0), C.c_int32(0)
-    lib.m3d_gpu_profiler_kernel(C.byref(kms), C.byref(kl))
+    table = C.create_string_buffer(1 << 14)
+    lib.m3d_gpu_profiler_table(table, 1 << 14)
+    timed = {}
+    for row in table.value.decode().splitlines():
+        kname, kl, kms = row.split()
+        timed[kname] = (int(kl), float(kms))
     status = lib.m3d_gpu_status(world)
     d.barrier()
     dev_ms_max = d.reduce(dev_ms, "MAX")
@@ -352,15 +382,22 @@ def main():
     except (OSError, ValueError):
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-    roof = None
-    if model is not None and kl.value > 0:
-        avg_s = kms.value / 1000.0 / kl.value
-        per_launch = alg_bytes / kl.value
+    traffic = read_traffic()
+    roofs = []
+    for k in names:
+        if k not in timed or timed[k][0] == 0:
+            continue
+        kl, kms = timed[k]
+        avg_s = kms / 1000.0 / kl
+        per_launch = alg_bytes[k] / kl
         achieved = per_launch / avg_s / 1e9
-        roof = {"bound": "hbm", "kernel": args.roofline_kernel, "achieved": achieved, "peak": hbm_peak,
-                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
-                "bytes_per_launch": per_launch, "avg_launch_us": avg_s * 1e6, "launches": kl.value,
-                "model": model[0], "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+        roofs.append({"bound": "hbm", "kernel": k, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                      "frac": achieved / hbm_peak, "traffic": traffic.get(k),
+                      "bytes_per_launch": per_launch, "avg_launch_us": avg_s * 1e6, "launches": kl,
+                      "share_of_step": kms / max(dev_ms, 1e-9), "model": ROOFLINE_MODELS[k][0],
+                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"})
+    roofs.sort(key=lambda r: -r["share_of_step"])
+    roof = roofs[0] if roofs else None
     variants = None
     if d.rank == 0 and d.world == 1 and not args.no_variants:
         ref_lib = api.bind(C.CDLL(REF_RELEASE_LIB)) if os.path.exists(REF_RELEASE_LIB) else None
@@ -378,7 +415,8 @@ def main():
                         "h2d_bytes_per_step": h2d.value // max(args.steps, 1),
                         "d2h_bytes_per_step": d2h.value // max(args.steps, 1),
                         "ms_per_step": wall_ms_max / args.steps},
-                "roofline": roof, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk,
+                "roofline": roof, "roofline_others": roofs[1:], "cpu_baseline": cpu, "gpu_launches": launches,
+                "clocks": clk,
                 "status": status, "variants": variants}
         print(json.dumps(line))
     scene.close()

@@ -50,7 +50,10 @@ M3D_API float m3d_gpu_last_step_device_ms(m3d_world* world);
  * beginEvents, endEvents, anyAwakeDynamic, islandCount, touchingContacts,
  * awakeIslands, islandContacts, islandJoints, islandBodies, stableDirty,
  * bodyCount, awakeBodyCount, hashFailures, colouredIslands, serialIslands,
- * freeIslands.  Returns how many counters exist (writes at most capacity). */
+ * freeIslands, waitErrors, contactCount, giantIslands, keptStable,
+ * keptStableOversized, keptContacts, tinyIslands, warpIslands, islandPoints,
+ * serialBodies, serialContacts.  Returns how many counters exist (writes at
+ * most capacity). */
 M3D_API int32_t m3d_gpu_step_counters(m3d_world* world, uint32_t* out, int32_t capacity);
 
 /* Coloured islands (>= 300 contacts, solved with the reference's greedy
@@ -115,11 +118,12 @@ M3D_API int32_t m3d_gpu_sphere_cast_noalloc(m3d_world* world, m3d_vec3 origin, f
                                             uint32_t maskBits, m3d_ray_result* out);
 
 /* Launch accounting (process-wide).  Every kernel launch of the library is
- * counted; the kernel named in m3d_gpu_profiler_reset (its source name, e.g.
- * "kNarrowphase"; "*" for every kernel; NULL for none) is also bracketed by
- * CUDA events on its stream, so its average device duration can be read while
- * the world runs.  m3d_gpu_profiler_table writes one line per timed kernel,
- * "<name> <launches> <total ms>", and returns the table's full length. */
+ * counted; the kernels named in m3d_gpu_profiler_reset (source names, e.g.
+ * "kNarrowphase" or "kSolveSerial,kSolveFree"; "*" for every kernel; NULL for
+ * none) are also bracketed by CUDA events on their stream, so their average
+ * device duration can be read while the world runs.  m3d_gpu_profiler_table
+ * writes one line per timed kernel, "<name> <launches> <total ms>", and
+ * returns the table's full length. */
 M3D_API void m3d_gpu_profiler_reset(const char* kernelName);
 M3D_API long long m3d_gpu_profiler_launches(void);
 M3D_API void m3d_gpu_profiler_kernel(float* totalMs, int32_t* launches);

@@ -240,15 +240,11 @@ __global__ void kPlaceBodies(const BodySoA B, int32_t n, const int32_t* label, c
 
 __global__ void kContactIslandFlags(const ContactSoA C, int32_t maxCount, const uint32_t* countDev,
 									const uint8_t* bFlags, const int32_t* label, const uint32_t* islandFlag,
-									uint32_t* flag, uint32_t* touchingCount, const uint32_t* active)
+									uint32_t* flag, uint32_t* touchingCount, uint32_t* pointCount, const uint32_t* active)
 {
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
-	if (c >= maxCount)
-	{
-		return;
-	}
-	uint32_t f = 0;
-	if (c < (int)*countDev && *active)
+	uint32_t f = 0, points = 0;
+	if (c < maxCount && c < (int)*countDev && *active)
 	{
 		uint8_t fl = C.flags[c];
 		if (fl & kCFTouching)
@@ -261,11 +257,21 @@ __global__ void kContactIslandFlags(const ContactSoA C, int32_t maxCount, const 
 				if ((bFlags[dyn] & kBFDynamic) && islandFlag[label[dyn]])
 				{
 					f = 1;
+					points = (uint32_t)C.pointCount[c];
 				}
 			}
 		}
 	}
-	flag[c] = f;
+	if (c < maxCount)
+	{
+		flag[c] = f;
+	}
+	// warp total of the island points, one atomic per warp
+	points = __reduce_add_sync(0xffffffffu, points);
+	if ((threadIdx.x & 31) == 0 && points != 0)
+	{
+		atomicAdd(pointCount, points);
+	}
 }
 
 __global__ void kJointIslandFlags(const JointRec* joints, int32_t count, const BodyCold* cold, const int32_t* label,
@@ -366,6 +372,8 @@ __global__ void kIslandTable(const int32_t* islandLabels, int32_t maxIslands, co
 	{
 		r.kind = 1;
 		atomicAdd(&dc->serialIslands, 1u);
+		atomicAdd(&dc->serialBodies, (uint32_t)r.bodyCount);
+		atomicAdd(&dc->serialContacts, (uint32_t)r.contactCount);
 		if (r.contactCount <= tinyContacts && r.jointCount == 0)
 		{
 			tinyList[atomicAdd(&dc->tinyIslands, 1u)] = k;
@@ -452,7 +460,7 @@ void launchIslands(DevWorld& w, int32_t n)
 	{
 		M3G_LAUNCH(kContactIslandFlags, blocksFor(M, 256), 256, s, w.C, M, &dc->contactCount, w.B.bFlags,
 				   w.label.as<int32_t>(), w.islandFlag.as<uint32_t>(), w.removeFlag.as<uint32_t>(), &dc->touchingCount,
-				   active);
+				   &dc->islandPoints, active);
 	}
 	scanExclusive(w.removeFlag.as<uint32_t>(), w.removeScan.as<uint32_t>(), M, &dc->islandContacts, w.prim, s);
 	if (M > 0)

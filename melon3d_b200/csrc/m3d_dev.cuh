@@ -47,6 +47,9 @@ struct StepCounters
 	uint32_t keptContacts;   // batch: contacts after the world-major re-layout
 	uint32_t tinyIslands;    // serial islands small enough for one thread each
 	uint32_t warpIslands;    // the other serial islands (one warp each)
+	uint32_t islandPoints;   // manifold points of the island contacts (before the solve)
+	uint32_t serialBodies;   // bodies of the serial islands
+	uint32_t serialContacts; // contacts of the serial islands
 };
 
 // Host -> device body update record (one per body touched by the API

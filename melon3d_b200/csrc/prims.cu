@@ -34,7 +34,27 @@ double gTimedMs = 0.0;
 long long gTimedLaunches = 0;
 std::map<std::string, std::pair<double, long long>> gPerKernel; // "*" target: every kernel
 
-bool timed(const char* name) { return gTarget == "*" || gTarget == name; }
+// the selection: "*" (every kernel) or a comma-separated list of names
+bool timed(const char* name)
+{
+	if (gTarget == "*")
+	{
+		return true;
+	}
+	const size_t len = strlen(name);
+	size_t pos = 0;
+	while (pos <= gTarget.size())
+	{
+		size_t end = gTarget.find(',', pos);
+		end = end == std::string::npos ? gTarget.size() : end;
+		if (end - pos == len && gTarget.compare(pos, len, name) == 0)
+		{
+			return true;
+		}
+		pos = end + 1;
+	}
+	return false;
+}
 
 cudaEvent_t takeEvent()
 {
