@@ -1,0 +1,1995 @@
+// Differentiable substep: forward and reverse (adjoint) of the XPBD substep
+// operations, templated on the scalar type.
+//
+// The forward functions restate the engine's element routines
+// (m3d_solve.cuh; reference src/xpbd.cpp) with the same float operations in
+// the same order, so with T = float they reproduce the engine bit for bit
+// (the replay test checks that); with T = double the same code is the FP64
+// host reference.  Each reverse function takes the adjoints of an
+// operation's outputs and accumulates the adjoints of its inputs, recomputing
+// the forward temporaries it needs.
+//
+// What is held fixed (the "frozen tape"): the contact set, every manifold
+// (normal, anchors, separation offsets, point count) as the forward's contact
+// preparation left it in each substep, the stiction anchors and slip
+// directions, the solve order, and every branch the forward took (contact
+// gates, caps, stiction and coherence tests).  Derivatives flow through body
+// states, inverse masses and inertias, friction and restitution coefficients.
+//
+// Scope: spheres and boxes with isotropic inertia (cubes); no joints, no
+// external forces; serial islands.  For an isotropic body the world inverse
+// inertia R d R^T equals d I, so its derivative with respect to the rotation
+// is zero and is not propagated.
+#pragma once
+
+#include <math.h>
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define M3D_DIFF_HD __host__ __device__ __forceinline__
+#else
+#define M3D_DIFF_HD inline
+#endif
+
+namespace m3d_diff
+{
+
+// ---- scalar functions with the engine's rounding for float -------------------
+
+M3D_DIFF_HD float dsqrt(float x) { return sqrtf(x); }
+M3D_DIFF_HD double dsqrt(double x) { return sqrt(x); }
+// the engine evaluates these in double and rounds once
+M3D_DIFF_HD float dsin(float x) { return (float)sin((double)x); }
+M3D_DIFF_HD double dsin(double x) { return sin(x); }
+M3D_DIFF_HD float dcos(float x) { return (float)cos((double)x); }
+M3D_DIFF_HD double dcos(double x) { return cos(x); }
+M3D_DIFF_HD float datan2(float y, float x) { return (float)atan2((double)y, (double)x); }
+M3D_DIFF_HD double datan2(double y, double x) { return atan2(y, x); }
+M3D_DIFF_HD float dabs(float x) { return fabsf(x); }
+M3D_DIFF_HD double dabs(double x) { return fabs(x); }
+
+template <typename T>
+struct V
+{
+	T x, y, z;
+};
+template <typename T>
+struct Q
+{
+	T x, y, z, w;
+};
+template <typename T>
+struct M
+{
+	V<T> cx, cy, cz;
+};
+
+template <typename T>
+M3D_DIFF_HD V<T> v3(T x, T y, T z)
+{
+	V<T> r;
+	r.x = x;
+	r.y = y;
+	r.z = z;
+	return r;
+}
+template <typename T>
+M3D_DIFF_HD Q<T> q4(T x, T y, T z, T w)
+{
+	Q<T> r;
+	r.x = x;
+	r.y = y;
+	r.z = z;
+	r.w = w;
+	return r;
+}
+template <typename T>
+M3D_DIFF_HD V<T> vzero()
+{
+	return v3<T>(T(0), T(0), T(0));
+}
+template <typename T>
+M3D_DIFF_HD Q<T> qzero()
+{
+	return q4<T>(T(0), T(0), T(0), T(0));
+}
+template <typename T>
+M3D_DIFF_HD V<T> add(V<T> a, V<T> b)
+{
+	return v3<T>(a.x + b.x, a.y + b.y, a.z + b.z);
+}
+template <typename T>
+M3D_DIFF_HD V<T> sub(V<T> a, V<T> b)
+{
+	return v3<T>(a.x - b.x, a.y - b.y, a.z - b.z);
+}
+template <typename T>
+M3D_DIFF_HD V<T> neg(V<T> a)
+{
+	return v3<T>(-a.x, -a.y, -a.z);
+}
+template <typename T>
+M3D_DIFF_HD V<T> scale(T s, V<T> v)
+{
+	return v3<T>(s * v.x, s * v.y, s * v.z);
+}
+template <typename T>
+M3D_DIFF_HD V<T> madd(V<T> a, T s, V<T> b)
+{
+	return v3<T>(a.x + s * b.x, a.y + s * b.y, a.z + s * b.z);
+}
+template <typename T>
+M3D_DIFF_HD T dot(V<T> a, V<T> b)
+{
+	return a.x * b.x + a.y * b.y + a.z * b.z;
+}
+template <typename T>
+M3D_DIFF_HD V<T> cross(V<T> a, V<T> b)
+{
+	return v3<T>(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+template <typename T>
+M3D_DIFF_HD T len(V<T> v)
+{
+	return dsqrt(dot(v, v));
+}
+template <typename T>
+M3D_DIFF_HD Q<T> qadd(Q<T> a, Q<T> b)
+{
+	return q4<T>(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+template <typename T>
+M3D_DIFF_HD Q<T> qscale(T s, Q<T> a)
+{
+	return q4<T>(s * a.x, s * a.y, s * a.z, s * a.w);
+}
+template <typename T>
+M3D_DIFF_HD T qdot(Q<T> a, Q<T> b)
+{
+	return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w;
+}
+template <typename T>
+M3D_DIFF_HD Q<T> qmul(Q<T> a, Q<T> b)
+{
+	Q<T> q;
+	q.x = a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y;
+	q.y = a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x;
+	q.z = a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w;
+	q.w = a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z;
+	return q;
+}
+template <typename T>
+M3D_DIFF_HD Q<T> qconj(Q<T> q)
+{
+	return q4<T>(-q.x, -q.y, -q.z, q.w);
+}
+template <typename T>
+M3D_DIFF_HD V<T> rotate(Q<T> q, V<T> v)
+{
+	V<T> u = v3<T>(q.x, q.y, q.z);
+	V<T> t = scale(T(2), cross(u, v));
+	return add(add(v, scale(q.w, t)), cross(u, t));
+}
+template <typename T>
+M3D_DIFF_HD Q<T> renormFast(Q<T> q)
+{
+	T s = T(1.5) - T(0.5) * (q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+	return q4<T>(q.x * s, q.y * s, q.z * s, q.w * s);
+}
+template <typename T>
+M3D_DIFF_HD V<T> mulv(const M<T>& m, V<T> v)
+{
+	return add(add(scale(v.x, m.cx), scale(v.y, m.cy)), scale(v.z, m.cz));
+}
+// I^-1_world = R diag(d) R^T, element order of the engine
+template <typename T>
+M3D_DIFF_HD M<T> invInertiaWorld(Q<T> q, V<T> d)
+{
+	T x = q.x, y = q.y, z = q.z, w = q.w;
+	T x2 = x + x, y2 = y + y, z2 = z + z;
+	T xx = x * x2, xy = x * y2, xz = x * z2;
+	T yy = y * y2, yz = y * z2, zz = z * z2;
+	T wx = w * x2, wy = w * y2, wz = w * z2;
+	M<T> r;
+	r.cx = v3<T>(T(1) - (yy + zz), xy + wz, xz - wy);
+	r.cy = v3<T>(xy - wz, T(1) - (xx + zz), yz + wx);
+	r.cz = v3<T>(xz + wy, yz - wx, T(1) - (xx + yy));
+	M<T> rd;
+	rd.cx = scale(d.x, r.cx);
+	rd.cy = scale(d.y, r.cy);
+	rd.cz = scale(d.z, r.cz);
+	M<T> m;
+	m.cx = v3<T>(rd.cx.x * r.cx.x + rd.cy.x * r.cy.x + rd.cz.x * r.cz.x, rd.cx.y * r.cx.x + rd.cy.y * r.cy.x + rd.cz.y * r.cz.x,
+				 rd.cx.z * r.cx.x + rd.cy.z * r.cy.x + rd.cz.z * r.cz.x);
+	m.cy = v3<T>(rd.cx.x * r.cx.y + rd.cy.x * r.cy.y + rd.cz.x * r.cz.y, rd.cx.y * r.cx.y + rd.cy.y * r.cy.y + rd.cz.y * r.cz.y,
+				 rd.cx.z * r.cx.y + rd.cy.z * r.cy.y + rd.cz.z * r.cz.y);
+	m.cz = v3<T>(rd.cx.x * r.cx.z + rd.cy.x * r.cy.z + rd.cz.x * r.cz.z, rd.cx.y * r.cx.z + rd.cy.y * r.cy.z + rd.cz.y * r.cz.z,
+				 rd.cx.z * r.cx.z + rd.cy.z * r.cy.z + rd.cz.z * r.cz.z);
+	return m;
+}
+
+// ---- reverse of the primitives ------------------------------------------------
+// Each *_rev accumulates (+=) the adjoints of the inputs given the output's.
+
+template <typename T>
+M3D_DIFF_HD void cross_rev(V<T> a, V<T> b, V<T> o, V<T>& ab, V<T>& bb)
+{
+	// o . (da x b) = da . (b x o);  o . (a x db) = db . (o x a)
+	ab = add(ab, cross(b, o));
+	bb = add(bb, cross(o, a));
+}
+template <typename T>
+M3D_DIFF_HD void qmul_rev(Q<T> a, Q<T> b, Q<T> o, Q<T>& ab, Q<T>& bb)
+{
+	// o = a (x) b is bilinear; the transposed rows of the product formula
+	ab.x += o.x * b.w - o.y * b.z + o.z * b.y - o.w * b.x;
+	ab.y += o.x * b.z + o.y * b.w - o.z * b.x - o.w * b.y;
+	ab.z += -o.x * b.y + o.y * b.x + o.z * b.w - o.w * b.z;
+	ab.w += o.x * b.x + o.y * b.y + o.z * b.z + o.w * b.w;
+	bb.x += o.x * a.w + o.y * a.z - o.z * a.y - o.w * a.x;
+	bb.y += -o.x * a.z + o.y * a.w + o.z * a.x - o.w * a.y;
+	bb.z += o.x * a.y - o.y * a.x + o.z * a.w - o.w * a.z;
+	bb.w += o.x * a.x + o.y * a.y + o.z * a.z + o.w * a.w;
+}
+template <typename T>
+M3D_DIFF_HD void renormFast_rev(Q<T> q, Q<T> o, Q<T>& qb)
+{
+	// out = s q, s = 1.5 - 0.5 |q|^2:  d out = s dq - q (q . dq)
+	T s = T(1.5) - T(0.5) * qdot(q, q);
+	T k = qdot(o, q);
+	qb.x += s * o.x - q.x * k;
+	qb.y += s * o.y - q.y * k;
+	qb.z += s * o.z - q.z * k;
+	qb.w += s * o.w - q.w * k;
+}
+// rotate(q, v) with v constant: adjoint of q
+template <typename T>
+M3D_DIFF_HD void rotate_rev_q(Q<T> q, V<T> v, V<T> o, Q<T>& qb)
+{
+	V<T> u = v3<T>(q.x, q.y, q.z);
+	V<T> t = scale(T(2), cross(u, v));
+	// out = v + w t + u x t
+	qb.w += dot(o, t);
+	V<T> tb = scale(q.w, o);
+	V<T> ub = vzero<T>();
+	cross_rev(u, t, o, ub, tb);
+	// t = 2 u x v
+	V<T> vb = vzero<T>();
+	cross_rev(u, v, scale(T(2), tb), ub, vb);
+	qb.x += ub.x;
+	qb.y += ub.y;
+	qb.z += ub.z;
+}
+// y = m v: adjoints of m (outer product) and v
+template <typename T>
+M3D_DIFF_HD void mulv_rev(const M<T>& m, V<T> v, V<T> o, M<T>& mb, V<T>& vb)
+{
+	mb.cx = madd(mb.cx, v.x, o);
+	mb.cy = madd(mb.cy, v.y, o);
+	mb.cz = madd(mb.cz, v.z, o);
+	vb.x += dot(m.cx, o);
+	vb.y += dot(m.cy, o);
+	vb.z += dot(m.cz, o);
+}
+// len(v): adjoint of v
+template <typename T>
+M3D_DIFF_HD void len_rev(V<T> v, T l, T ob, V<T>& vb)
+{
+	if (l > T(0))
+	{
+		vb = madd(vb, ob / l, v);
+	}
+}
+// I^-1_world of an isotropic body: d (m) / d d = R R^T, taken as the identity
+template <typename T>
+M3D_DIFF_HD T iw_rev_isotropic(const M<T>& mb)
+{
+	return mb.cx.x + mb.cy.y + mb.cz.z;
+}
+
+// ---- per-body state ---------------------------------------------------------
+
+template <typename T>
+struct Body
+{
+	V<T> x;
+	Q<T> q;
+	V<T> v;
+	V<T> w;
+};
+template <typename T>
+M3D_DIFF_HD Body<T> bodyZero()
+{
+	Body<T> b;
+	b.x = vzero<T>();
+	b.q = qzero<T>();
+	b.v = vzero<T>();
+	b.w = vzero<T>();
+	return b;
+}
+// constants of a body during the step (the isotropic inverse inertia `il` is
+// one value; the engine stores it per axis, all three equal)
+template <typename T>
+struct BodyConst
+{
+	T invMass;
+	T il;
+	T gravityScale;
+	T linearDamping;
+	T angularDamping;
+	int dynamic;
+};
+template <typename T>
+struct BodyConstBar
+{
+	T invMass;
+	T il;
+};
+
+// ---- integration (reference src/xpbd.cpp:587-705; isotropic: no gyroscopic
+// term, no external force) ---------------------------------------------------
+
+template <typename T>
+M3D_DIFF_HD void integrate(const Body<T>& s0, const BodyConst<T>& c, T h, V<T> g, Body<T>& s1, M<T>& iw)
+{
+	V<T> v = madd(s0.v, h * c.gravityScale, g);
+	V<T> w = s0.w;
+	v = scale(T(1) / (T(1) + h * c.linearDamping), v);
+	w = scale(T(1) / (T(1) + h * c.angularDamping), w);
+	Q<T> q = s0.q;
+	V<T> x = madd(s0.x, h, v);
+	T wlen = len(w);
+	if (wlen > T(1e-9))
+	{
+		T half = T(0.5) * h * wlen;
+		T sinHalf, cosHalf;
+		if (half < T(0.02))
+		{
+			T h2 = half * half;
+			sinHalf = half * (T(1) - h2 * (T(1) / T(6)));
+			cosHalf = T(1) - h2 * T(0.5);
+		}
+		else
+		{
+			sinHalf = dsin(half);
+			cosHalf = dcos(half);
+		}
+		T s = sinHalf / wlen;
+		Q<T> dq = q4<T>(w.x * s, w.y * s, w.z * s, cosHalf);
+		q = renormFast(qmul(dq, q));
+	}
+	s1.x = x;
+	s1.q = q;
+	s1.v = v;
+	s1.w = w;
+	iw = invInertiaWorld(q, v3<T>(c.il, c.il, c.il));
+}
+
+// given the adjoints of s1 and iw, accumulate those of s0 and of il
+template <typename T>
+M3D_DIFF_HD void integrate_rev(const Body<T>& s0, const BodyConst<T>& c, T h, V<T> g, const Body<T>& s1b,
+							   const M<T>& iwb, Body<T>& s0b, BodyConstBar<T>& cb)
+{
+	const T cl = T(1) / (T(1) + h * c.linearDamping);
+	const T ca = T(1) / (T(1) + h * c.angularDamping);
+	V<T> w = scale(ca, s0.w);
+	// x1 = x0 + h v1, v1 = cl (v0 + h gs g)
+	V<T> vb = madd(s1b.v, h, s1b.x);
+	s0b.x = add(s0b.x, s1b.x);
+	s0b.v = madd(s0b.v, cl, vb);
+	V<T> wb = s1b.w;
+	T wlen = len(w);
+	if (wlen > T(1e-9))
+	{
+		T half = T(0.5) * h * wlen;
+		T sinHalf, cosHalf, dsin_dh, dcos_dh;
+		if (half < T(0.02))
+		{
+			T h2 = half * half;
+			sinHalf = half * (T(1) - h2 * (T(1) / T(6)));
+			cosHalf = T(1) - h2 * T(0.5);
+			dsin_dh = T(1) - half * half * T(0.5);
+			dcos_dh = -half;
+		}
+		else
+		{
+			sinHalf = dsin(half);
+			cosHalf = dcos(half);
+			dsin_dh = cosHalf;
+			dcos_dh = -sinHalf;
+		}
+		T s = sinHalf / wlen;
+		Q<T> dq = q4<T>(w.x * s, w.y * s, w.z * s, cosHalf);
+		Q<T> p = qmul(dq, s0.q);
+		Q<T> pb = qzero<T>();
+		renormFast_rev(p, s1b.q, pb);
+		Q<T> dqb = qzero<T>();
+		qmul_rev(dq, s0.q, pb, dqb, s0b.q);
+		// dq = (w s, cosHalf)
+		wb = madd(wb, s, v3<T>(dqb.x, dqb.y, dqb.z));
+		T sb = w.x * dqb.x + w.y * dqb.y + w.z * dqb.z;
+		T halfb = dqb.w * dcos_dh + (sb / wlen) * dsin_dh;
+		T wlenb = -sb * sinHalf / (wlen * wlen) + T(0.5) * h * halfb;
+		len_rev(w, wlen, wlenb, wb);
+	}
+	else
+	{
+		s0b.q = qadd(s0b.q, s1b.q);
+	}
+	s0b.w = madd(s0b.w, ca, wb);
+	cb.il += iw_rev_isotropic(iwb);
+}
+
+// ---- contacts -------------------------------------------------------------
+
+enum ShapeKind
+{
+	kShapeSphere = 0,
+	kShapeBox = 2
+};
+
+// the frozen manifold of one contact in one substep (as left by contact
+// preparation), with its materials
+template <typename T>
+struct Contact
+{
+	int a, b;          // body indices (island-local or global, as the caller uses them)
+	int pointCount;
+	int curved;        // not box-box: the velocity pass recomputes arms
+	int shapeA, shapeB;
+	T radiusA, radiusB;
+	V<T> n;
+	T mu, e, rolling;
+	V<T> la[4], lb[4]; // local anchors
+	T off[4];          // separation offsets
+	V<T> fa[4], fb[4]; // stiction anchors
+	V<T> slip[4];      // slip directions of the last velocity pass
+};
+
+// contact quantities frozen at preparation (reference src/xpbd.cpp:733-863)
+template <typename T>
+struct Prepared
+{
+	V<T> rA[4], rB[4], jA[4], jB[4];
+	T wN[4];
+};
+template <typename T>
+M3D_DIFF_HD void preparedZero(Prepared<T>& p)
+{
+	for (int s = 0; s < 4; ++s)
+	{
+		p.rA[s] = p.rB[s] = p.jA[s] = p.jB[s] = vzero<T>();
+		p.wN[s] = T(0);
+	}
+}
+
+// contact arm: geometric for a sphere, the rotated anchor for a box
+template <typename T>
+M3D_DIFF_HD V<T> arm(int shape, T radius, Q<T> q, V<T> l, V<T> n, T sign)
+{
+	return shape == kShapeSphere ? scale(sign * radius, n) : rotate(q, l);
+}
+template <typename T>
+M3D_DIFF_HD void arm_rev(int shape, Q<T> q, V<T> l, V<T> rb, Q<T>& qb)
+{
+	if (shape != kShapeSphere)
+	{
+		rotate_rev_q(q, l, rb, qb);
+	}
+}
+
+template <typename T>
+M3D_DIFF_HD void prepare(const Contact<T>& c, Q<T> qA, Q<T> qB, T imA, T imB, const M<T>& iwA, const M<T>& iwB,
+						 Prepared<T>& p)
+{
+	for (int s = 0; s < c.pointCount; ++s)
+	{
+		V<T> rA = arm(c.shapeA, c.radiusA, qA, c.la[s], c.n, T(1));
+		V<T> rB = arm(c.shapeB, c.radiusB, qB, c.lb[s], c.n, T(-1));
+		V<T> crossA = cross(rA, c.n);
+		V<T> crossB = cross(rB, c.n);
+		V<T> jA = mulv(iwA, crossA);
+		V<T> jB = mulv(iwB, crossB);
+		p.rA[s] = rA;
+		p.rB[s] = rB;
+		p.jA[s] = jA;
+		p.jB[s] = jB;
+		p.wN[s] = imA + imB + dot(crossA, jA) + dot(crossB, jB);
+	}
+}
+
+template <typename T>
+M3D_DIFF_HD void prepare_rev(const Contact<T>& c, Q<T> qA, Q<T> qB, const M<T>& iwA, const M<T>& iwB,
+							 const Prepared<T>& p, const Prepared<T>& pb, Q<T>& qAb, Q<T>& qBb, T& imAb, T& imBb,
+							 M<T>& iwAb, M<T>& iwBb)
+{
+	for (int s = 0; s < c.pointCount; ++s)
+	{
+		V<T> crossA = cross(p.rA[s], c.n);
+		V<T> crossB = cross(p.rB[s], c.n);
+		T wb = pb.wN[s];
+		imAb += wb;
+		imBb += wb;
+		V<T> cAb = scale(wb, p.jA[s]);
+		V<T> cBb = scale(wb, p.jB[s]);
+		V<T> jAb = madd(pb.jA[s], wb, crossA);
+		V<T> jBb = madd(pb.jB[s], wb, crossB);
+		mulv_rev(iwA, crossA, jAb, iwAb, cAb);
+		mulv_rev(iwB, crossB, jBb, iwBb, cBb);
+		V<T> rAb = pb.rA[s], rBb = pb.rB[s], nb = vzero<T>();
+		cross_rev(p.rA[s], c.n, cAb, rAb, nb);
+		cross_rev(p.rB[s], c.n, cBb, rBb, nb);
+		arm_rev(c.shapeA, qA, c.la[s], rAb, qAb);
+		arm_rev(c.shapeB, qB, c.lb[s], rBb, qBb);
+	}
+}
+
+// ApplyAxisCorrection (reference src/xpbd.cpp:45-58)
+template <typename T>
+M3D_DIFF_HD void axisCorrection(V<T>& p, Q<T>& q, T im, T dl, V<T> n, V<T> j)
+{
+	if (im == T(0))
+	{
+		return;
+	}
+	p = madd(p, dl * im, n);
+	V<T> dw = scale(dl, j);
+	Q<T> dq = qmul(q4<T>(dw.x, dw.y, dw.z, T(0)), q);
+	q = renormFast(q4<T>(q.x + T(0.5) * dq.x, q.y + T(0.5) * dq.y, q.z + T(0.5) * dq.z, q.w + T(0.5) * dq.w));
+}
+// inputs p, q (before); adjoints pb, qb of the outputs in, of the inputs out
+template <typename T>
+M3D_DIFF_HD void axisCorrection_rev(Q<T> q, T im, T dl, V<T> n, V<T> j, V<T>& pb, Q<T>& qb, T& dlb, T& imb, V<T>& jb)
+{
+	if (im == T(0))
+	{
+		return;
+	}
+	T s1b = dot(pb, n);
+	dlb += s1b * im;
+	imb += s1b * dl;
+	V<T> dw = scale(dl, j);
+	Q<T> wq = q4<T>(dw.x, dw.y, dw.z, T(0));
+	Q<T> dq = qmul(wq, q);
+	Q<T> P = q4<T>(q.x + T(0.5) * dq.x, q.y + T(0.5) * dq.y, q.z + T(0.5) * dq.z, q.w + T(0.5) * dq.w);
+	Q<T> Pb = qzero<T>();
+	renormFast_rev(P, qb, Pb);
+	Q<T> wqb = qzero<T>();
+	Q<T> qin = Pb;
+	qmul_rev(wq, q, qscale(T(0.5), Pb), wqb, qin);
+	qb = qin;
+	V<T> dwb = v3<T>(wqb.x, wqb.y, wqb.z);
+	dlb += dot(dwb, j);
+	jb = madd(jb, dl, dwb);
+}
+
+// SolveContactNormals, serial form (reference src/xpbd.cpp:122-163): the
+// points in order, each against the poses the previous one left
+template <typename T>
+M3D_DIFF_HD void normals(const Contact<T>& c, const Prepared<T>& p, T imA, T imB, T maxCorrection, V<T>& pA, Q<T>& qA,
+						 V<T>& pB, Q<T>& qB, T* lambdaN)
+{
+	for (int s = 0; s < c.pointCount; ++s)
+	{
+		T wN = p.wN[s];
+		if (wN <= T(0))
+		{
+			continue;
+		}
+		V<T> rA = rotate(qA, c.la[s]);
+		V<T> rB = rotate(qB, c.lb[s]);
+		T sep = c.off[s] + dot(sub(add(pB, rB), add(pA, rA)), c.n);
+		if (sep >= T(0))
+		{
+			continue;
+		}
+		if (sep < -maxCorrection)
+		{
+			sep = -maxCorrection;
+		}
+		T dl = -sep / wN;
+		lambdaN[s] += dl;
+		axisCorrection(pB, qB, imB, dl, c.n, p.jB[s]);
+		axisCorrection(pA, qA, imA, -dl, c.n, p.jA[s]);
+	}
+}
+
+// adjoints of the poses after the op in (pAb ...), of the poses before out;
+// lambdaNb: adjoint of each point's accumulated lambda (passes through)
+template <typename T>
+M3D_DIFF_HD void normals_rev(const Contact<T>& c, const Prepared<T>& p, T imA, T imB, T maxCorrection, V<T> pA0, Q<T> qA0,
+							 V<T> pB0, Q<T> qB0, V<T>& pAb, Q<T>& qAb, V<T>& pBb, Q<T>& qBb, const T* lambdaNb,
+							 Prepared<T>& pb, T& imAb, T& imBb)
+{
+	// poses before each point
+	V<T> sA[4], sB[4];
+	Q<T> tA[4], tB[4];
+	V<T> pA = pA0, pB = pB0;
+	Q<T> qA = qA0, qB = qB0;
+	for (int s = 0; s < c.pointCount; ++s)
+	{
+		sA[s] = pA;
+		tA[s] = qA;
+		sB[s] = pB;
+		tB[s] = qB;
+		T wN = p.wN[s];
+		if (wN <= T(0))
+		{
+			continue;
+		}
+		V<T> rA = rotate(qA, c.la[s]);
+		V<T> rB = rotate(qB, c.lb[s]);
+		T sep = c.off[s] + dot(sub(add(pB, rB), add(pA, rA)), c.n);
+		if (sep >= T(0))
+		{
+			continue;
+		}
+		if (sep < -maxCorrection)
+		{
+			sep = -maxCorrection;
+		}
+		T dl = -sep / wN;
+		axisCorrection(pB, qB, imB, dl, c.n, p.jB[s]);
+		axisCorrection(pA, qA, imA, -dl, c.n, p.jA[s]);
+	}
+	for (int s = c.pointCount - 1; s >= 0; --s)
+	{
+		T wN = p.wN[s];
+		if (wN <= T(0))
+		{
+			continue;
+		}
+		pA = sA[s];
+		qA = tA[s];
+		pB = sB[s];
+		qB = tB[s];
+		V<T> rA = rotate(qA, c.la[s]);
+		V<T> rB = rotate(qB, c.lb[s]);
+		T sep = c.off[s] + dot(sub(add(pB, rB), add(pA, rA)), c.n);
+		if (sep >= T(0))
+		{
+			continue;
+		}
+		bool capped = sep < -maxCorrection;
+		if (capped)
+		{
+			sep = -maxCorrection;
+		}
+		T dl = -sep / wN;
+		// B was corrected first, A second: reverse A, then B
+		T dlAb = T(0), dlBb = T(0);
+		axisCorrection_rev(qA, imA, -dl, c.n, p.jA[s], pAb, qAb, dlAb, imAb, pb.jA[s]);
+		axisCorrection_rev(qB, imB, dl, c.n, p.jB[s], pBb, qBb, dlBb, imBb, pb.jB[s]);
+		T dlb = dlBb - dlAb + lambdaNb[s];
+		T sepb = T(0);
+		if (capped)
+		{
+			pb.wN[s] += -dlb * maxCorrection / (wN * wN);
+		}
+		else
+		{
+			sepb = -dlb / wN;
+			pb.wN[s] += dlb * sep / (wN * wN);
+		}
+		V<T> gb = scale(sepb, c.n);
+		pBb = add(pBb, gb);
+		pAb = sub(pAb, gb);
+		rotate_rev_q(qB, c.lb[s], gb, qBb);
+		rotate_rev_q(qA, c.la[s], neg(gb), qAb);
+	}
+}
+
+// ReconstructBodyVelocity (reference src/xpbd.cpp:865-892)
+template <typename T>
+M3D_DIFF_HD void reconstruct(V<T> x, Q<T> q, V<T> x0, Q<T> q0, T invH, V<T>& v, V<T>& w)
+{
+	v = scale(invH, sub(x, x0));
+	Q<T> dq = qmul(q, qconj(q0));
+	T sign = dq.w >= T(0) ? T(1) : T(-1);
+	T v2 = dq.x * dq.x + dq.y * dq.y + dq.z * dq.z;
+	if (v2 > T(4e-4))
+	{
+		T vl = dsqrt(v2);
+		T angle = T(2) * datan2(vl, dabs(dq.w));
+		w = scale(sign * invH * angle / vl, v3<T>(dq.x, dq.y, dq.z));
+	}
+	else
+	{
+		T corr = T(1) + v2 * (T(1) / T(6));
+		w = scale(T(2) * invH * sign * corr, v3<T>(dq.x, dq.y, dq.z));
+	}
+}
+
+template <typename T>
+M3D_DIFF_HD void reconstruct_rev(V<T> x, Q<T> q, V<T> x0, Q<T> q0, T invH, V<T> vb, V<T> wb, V<T>& xb, Q<T>& qb,
+								 V<T>& x0b, Q<T>& q0b)
+{
+	xb = madd(xb, invH, vb);
+	x0b = madd(x0b, -invH, vb);
+	Q<T> c0 = qconj(q0);
+	Q<T> dq = qmul(q, c0);
+	V<T> dv = v3<T>(dq.x, dq.y, dq.z);
+	T sign = dq.w >= T(0) ? T(1) : T(-1);
+	T v2 = dot(dv, dv);
+	V<T> dvb = vzero<T>();
+	T dwb = T(0);
+	if (v2 > T(4e-4))
+	{
+		T vl = dsqrt(v2);
+		T aw = dabs(dq.w);
+		T angle = T(2) * datan2(vl, aw);
+		T k = sign * invH * angle / vl;
+		dvb = scale(k, wb);
+		T kb = dot(wb, dv);
+		T angleb = kb * sign * invH / vl;
+		T vlb = -kb * sign * invH * angle / (vl * vl);
+		T den = vl * vl + aw * aw;
+		vlb += angleb * T(2) * aw / den;
+		T awb = -angleb * T(2) * vl / den;
+		dwb += awb * sign;
+		T v2b = vlb / (T(2) * vl);
+		dvb = madd(dvb, T(2) * v2b, dv);
+	}
+	else
+	{
+		T corr = T(1) + v2 * (T(1) / T(6));
+		T k = T(2) * invH * sign * corr;
+		dvb = scale(k, wb);
+		T kb = dot(wb, dv);
+		T corrb = kb * T(2) * invH * sign;
+		T v2b = corrb / T(6);
+		dvb = madd(dvb, T(2) * v2b, dv);
+	}
+	Q<T> dqb = q4<T>(dvb.x, dvb.y, dvb.z, dwb);
+	Q<T> c0b = qzero<T>();
+	qmul_rev(q, c0, dqb, qb, c0b);
+	q0b.x -= c0b.x;
+	q0b.y -= c0b.y;
+	q0b.z -= c0b.z;
+	q0b.w += c0b.w;
+}
+
+// generalised inverse mass along an axis: im + (r x a) . I^-1 (r x a)
+template <typename T>
+M3D_DIFF_HD T genInvMass(T im, const M<T>& iw, V<T> r, V<T> a)
+{
+	V<T> rn = cross(r, a);
+	return im + dot(rn, mulv(iw, rn));
+}
+template <typename T>
+M3D_DIFF_HD void genInvMass_rev(const M<T>& iw, V<T> r, V<T> a, T ob, T& imb, M<T>& iwb, V<T>& rb, V<T>& ab)
+{
+	V<T> rn = cross(r, a);
+	V<T> y = mulv(iw, rn);
+	imb += ob;
+	V<T> rnb = scale(ob, y);
+	mulv_rev(iw, rn, scale(ob, rn), iwb, rnb);
+	cross_rev(r, a, rnb, rb, ab);
+}
+
+// ApplyPositionCorrection (reference src/xpbd.cpp:28-41)
+template <typename T>
+M3D_DIFF_HD void positionCorrection(V<T>& p, Q<T>& q, T im, const M<T>& iw, V<T> imp, V<T> r)
+{
+	if (im == T(0))
+	{
+		return;
+	}
+	p = madd(p, im, imp);
+	V<T> dw = mulv(iw, cross(r, imp));
+	Q<T> dq = qmul(q4<T>(dw.x, dw.y, dw.z, T(0)), q);
+	q = renormFast(q4<T>(q.x + T(0.5) * dq.x, q.y + T(0.5) * dq.y, q.z + T(0.5) * dq.z, q.w + T(0.5) * dq.w));
+}
+template <typename T>
+M3D_DIFF_HD void positionCorrection_rev(Q<T> q, T im, const M<T>& iw, V<T> imp, V<T> r, V<T>& pb, Q<T>& qb, T& imb,
+										M<T>& iwb, V<T>& impb, V<T>& rb)
+{
+	if (im == T(0))
+	{
+		return;
+	}
+	impb = madd(impb, im, pb);
+	imb += dot(pb, imp);
+	V<T> c = cross(r, imp);
+	V<T> dw = mulv(iw, c);
+	Q<T> wq = q4<T>(dw.x, dw.y, dw.z, T(0));
+	Q<T> dq = qmul(wq, q);
+	Q<T> P = q4<T>(q.x + T(0.5) * dq.x, q.y + T(0.5) * dq.y, q.z + T(0.5) * dq.z, q.w + T(0.5) * dq.w);
+	Q<T> Pb = qzero<T>();
+	renormFast_rev(P, qb, Pb);
+	Q<T> wqb = qzero<T>();
+	Q<T> qin = Pb;
+	qmul_rev(wq, q, qscale(T(0.5), Pb), wqb, qin);
+	qb = qin;
+	V<T> cb = vzero<T>();
+	mulv_rev(iw, c, v3<T>(wqb.x, wqb.y, wqb.z), iwb, cb);
+	cross_rev(r, imp, cb, rb, impb);
+}
+
+// ApplyContactFriction, positional stiction toward the anchors, box-box
+// only (reference src/xpbd.cpp:172-269).  Returns false when the speed gate
+// re-anchored the contact instead (nothing moves).
+template <typename T>
+M3D_DIFF_HD bool frictionGate(const Contact<T>& c, const Prepared<T>& p, V<T> va, V<T> wa, V<T> vb, V<T> wb)
+{
+	if (c.shapeA != kShapeBox || c.shapeB != kShapeBox || c.pointCount == 0)
+	{
+		return false;
+	}
+	V<T> vrel = sub(add(vb, cross(wb, p.rB[0])), add(va, cross(wa, p.rA[0])));
+	V<T> vt = sub(vrel, scale(dot(vrel, c.n), c.n));
+	return !(dot(vt, vt) > T(0.1) * T(0.1));
+}
+
+template <typename T>
+M3D_DIFF_HD void friction(const Contact<T>& c, T imA, T imB, const M<T>& iwA, const M<T>& iwB, const T* lambdaN,
+						  V<T>& pA, Q<T>& qA, V<T>& pB, Q<T>& qB, T* lambdaT)
+{
+	for (int s = 0; s < c.pointCount; ++s)
+	{
+		T lN = lambdaN[s];
+		if (lN <= T(0))
+		{
+			continue;
+		}
+		V<T> rA = rotate(qA, c.fa[s]);
+		V<T> rB = rotate(qB, c.fb[s]);
+		V<T> gap = sub(add(pB, rB), add(pA, rA));
+		V<T> dpt = sub(gap, scale(dot(gap, c.n), c.n));
+		T lt = len(dpt);
+		if (lt <= T(1e-9))
+		{
+			continue;
+		}
+		V<T> t = scale(T(1) / lt, dpt);
+		T wt = genInvMass(imA, iwA, rA, t) + genInvMass(imB, iwB, rB, t);
+		if (wt <= T(0))
+		{
+			continue;
+		}
+		T needed = T(0.5) * (lt / wt);
+		T allowed = c.mu * lN - lambdaT[s];
+		if (allowed <= T(0))
+		{
+			continue;
+		}
+		T dL = needed < allowed ? needed : allowed;
+		lambdaT[s] += dL;
+		V<T> pt = scale(dL, t);
+		positionCorrection(pB, qB, imB, iwB, neg(pt), rB);
+		positionCorrection(pA, qA, imA, iwA, pt, rA);
+	}
+}
+
+template <typename T>
+M3D_DIFF_HD void friction_rev(const Contact<T>& c, T imA, T imB, const M<T>& iwA, const M<T>& iwB, const T* lambdaN,
+							  V<T> pA0, Q<T> qA0, V<T> pB0, Q<T> qB0, const T* lambdaT0, V<T>& pAb, Q<T>& qAb,
+							  V<T>& pBb, Q<T>& qBb, T* lambdaNb, T* lambdaTb, T& muB, T& imAb, T& imBb, M<T>& iwAb,
+							  M<T>& iwBb)
+{
+	V<T> sA[4], sB[4];
+	Q<T> tA[4], tB[4];
+	T lT[4];
+	V<T> pA = pA0, pB = pB0;
+	Q<T> qA = qA0, qB = qB0;
+	for (int s = 0; s < 4; ++s)
+	{
+		lT[s] = lambdaT0[s];
+	}
+	for (int s = 0; s < c.pointCount; ++s)
+	{
+		sA[s] = pA;
+		tA[s] = qA;
+		sB[s] = pB;
+		tB[s] = qB;
+		T lN = lambdaN[s];
+		if (lN <= T(0))
+		{
+			continue;
+		}
+		V<T> rA = rotate(qA, c.fa[s]);
+		V<T> rB = rotate(qB, c.fb[s]);
+		V<T> gap = sub(add(pB, rB), add(pA, rA));
+		V<T> dpt = sub(gap, scale(dot(gap, c.n), c.n));
+		T lt = len(dpt);
+		if (lt <= T(1e-9))
+		{
+			continue;
+		}
+		V<T> t = scale(T(1) / lt, dpt);
+		T wt = genInvMass(imA, iwA, rA, t) + genInvMass(imB, iwB, rB, t);
+		if (wt <= T(0))
+		{
+			continue;
+		}
+		T needed = T(0.5) * (lt / wt);
+		T allowed = c.mu * lN - lT[s];
+		if (allowed <= T(0))
+		{
+			continue;
+		}
+		T dL = needed < allowed ? needed : allowed;
+		lT[s] += dL;
+		V<T> pt = scale(dL, t);
+		positionCorrection(pB, qB, imB, iwB, neg(pt), rB);
+		positionCorrection(pA, qA, imA, iwA, pt, rA);
+	}
+	for (int s = c.pointCount - 1; s >= 0; --s)
+	{
+		T lN = lambdaN[s];
+		if (lN <= T(0))
+		{
+			continue;
+		}
+		pA = sA[s];
+		qA = tA[s];
+		pB = sB[s];
+		qB = tB[s];
+		T lT0 = lambdaT0[s];
+		V<T> rA = rotate(qA, c.fa[s]);
+		V<T> rB = rotate(qB, c.fb[s]);
+		V<T> gap = sub(add(pB, rB), add(pA, rA));
+		T gn = dot(gap, c.n);
+		V<T> dpt = sub(gap, scale(gn, c.n));
+		T lt = len(dpt);
+		if (lt <= T(1e-9))
+		{
+			continue;
+		}
+		T inv = T(1) / lt;
+		V<T> t = scale(inv, dpt);
+		T wt = genInvMass(imA, iwA, rA, t) + genInvMass(imB, iwB, rB, t);
+		if (wt <= T(0))
+		{
+			continue;
+		}
+		T needed = T(0.5) * (lt / wt);
+		T allowed = c.mu * lN - lT0;
+		if (allowed <= T(0))
+		{
+			continue;
+		}
+		bool takeNeeded = needed < allowed;
+		T dL = takeNeeded ? needed : allowed;
+		V<T> pt = scale(dL, t);
+		// reverse: A's correction (last), then B's
+		V<T> ptb = vzero<T>(), rAb = vzero<T>(), rBb = vzero<T>();
+		positionCorrection_rev(qA, imA, iwA, pt, rA, pAb, qAb, imAb, iwAb, ptb, rAb);
+		V<T> nptb = vzero<T>();
+		positionCorrection_rev(qB, imB, iwB, neg(pt), rB, pBb, qBb, imBb, iwBb, nptb, rBb);
+		ptb = sub(ptb, nptb);
+		T dLb = dot(ptb, t) + lambdaTb[s];
+		V<T> tb = scale(dL, ptb);
+		T neededb = T(0), allowedb = T(0);
+		if (takeNeeded)
+			neededb = dLb;
+		else
+			allowedb = dLb;
+		muB += allowedb * lN;
+		lambdaNb[s] += allowedb * c.mu;
+		lambdaTb[s] -= allowedb;
+		T ltb = neededb * T(0.5) / wt;
+		T wtb = -neededb * T(0.5) * lt / (wt * wt);
+		genInvMass_rev(iwA, rA, t, wtb, imAb, iwAb, rAb, tb);
+		genInvMass_rev(iwB, rB, t, wtb, imBb, iwBb, rBb, tb);
+		// t = inv dpt, inv = 1/lt
+		V<T> dptb = scale(inv, tb);
+		ltb += -dot(tb, dpt) * inv * inv;
+		len_rev(dpt, lt, ltb, dptb);
+		V<T> gapb = sub(dptb, scale(dot(dptb, c.n), c.n));
+		pBb = add(pBb, gapb);
+		pAb = sub(pAb, gapb);
+		rBb = add(rBb, gapb);
+		rAb = sub(rAb, gapb);
+		rotate_rev_q(qA, c.fa[s], rAb, qAb);
+		rotate_rev_q(qB, c.fb[s], rBb, qBb);
+	}
+}
+
+// SolveContactVelocity (reference src/xpbd.cpp:275-407): dynamic friction
+// with the coherence test, restitution against the pre-substep normal
+// velocity, the normal-velocity fix, rolling resistance.  Velocities in/out;
+// qA, qB are the current rotations (curved arms); pv*, pw* the velocities at
+// the start of the substep.
+template <typename T>
+struct VelocityIn
+{
+	T imA, imB;
+	M<T> iwA, iwB;
+	Q<T> qA, qB;
+	V<T> pva, pwa, pvb, pwb;
+	T h, gravityLen;
+};
+
+template <typename T>
+M3D_DIFF_HD void velocity(const Contact<T>& c, const Prepared<T>& p, const VelocityIn<T>& in, const T* lambdaN, V<T>& va,
+						  V<T>& wa, V<T>& vb, V<T>& wb)
+{
+	const T invH = in.h > T(0) ? T(1) / in.h : T(0);
+	T lambdaNTotal = T(0);
+	for (int s = 0; s < c.pointCount; ++s)
+	{
+		T lN = lambdaN[s];
+		if (lN <= T(0))
+		{
+			continue;
+		}
+		V<T> rAf, rBf;
+		if (c.curved)
+		{
+			rAf = arm(c.shapeA, c.radiusA, in.qA, c.la[s], c.n, T(1));
+			rBf = arm(c.shapeB, c.radiusB, in.qB, c.lb[s], c.n, T(-1));
+		}
+		else
+		{
+			rAf = p.rA[s];
+			rBf = p.rB[s];
+		}
+		V<T> vrel = sub(add(vb, cross(wb, rBf)), add(va, cross(wa, rAf)));
+		T vn = dot(vrel, c.n);
+		V<T> vt = sub(vrel, scale(vn, c.n));
+		T vtLen = len(vt);
+		if (vtLen > T(1e-9))
+		{
+			V<T> t = scale(T(1) / vtLen, vt);
+			T wt = genInvMass(in.imA, in.iwA, rAf, t) + genInvMass(in.imB, in.iwB, rBf, t);
+			if (wt > T(0))
+			{
+				bool coherent = dot(t, c.slip[s]) > T(0.7);
+				T pStop = vtLen / wt;
+				T pMax = c.mu * lN * invH;
+				T P = !coherent && vtLen < T(0.08) ? pStop : (pStop < pMax ? pStop : pMax);
+				V<T> imp = scale(-P, t);
+				if (in.imB != T(0))
+				{
+					vb = madd(vb, in.imB, imp);
+					wb = add(wb, mulv(in.iwB, cross(rBf, imp)));
+				}
+				if (in.imA != T(0))
+				{
+					V<T> pn = neg(imp);
+					va = madd(va, in.imA, pn);
+					wa = add(wa, mulv(in.iwA, cross(rAf, pn)));
+				}
+			}
+		}
+		V<T> vrelPrev = sub(add(in.pvb, cross(in.pwb, rBf)), add(in.pva, cross(in.pwa, rAf)));
+		T vnPrev = dot(vrelPrev, c.n);
+		T e = dabs(vnPrev) > T(2) * in.gravityLen * in.h ? c.e : T(0);
+		vrel = sub(add(vb, cross(wb, rBf)), add(va, cross(wa, rAf)));
+		vn = dot(vrel, c.n);
+		T target = -e * vnPrev;
+		target = target > T(0) ? target : T(0);
+		T wN = p.wN[s];
+		if (wN > T(0))
+		{
+			T j = (target - vn) / wN;
+			if (in.imB != T(0))
+			{
+				vb = madd(vb, j * in.imB, c.n);
+				wb = madd(wb, j, p.jB[s]);
+			}
+			if (in.imA != T(0))
+			{
+				T mj = -j;
+				va = madd(va, mj * in.imA, c.n);
+				wa = madd(wa, mj, p.jA[s]);
+			}
+		}
+		lambdaNTotal += lN > T(0) ? lN : T(0);
+	}
+	if (c.rolling > T(0) && lambdaNTotal > T(0))
+	{
+		V<T> wrel = sub(wb, wa);
+		V<T> wroll = sub(wrel, scale(dot(wrel, c.n), c.n));
+		T wl = len(wroll);
+		if (wl > T(1e-6))
+		{
+			V<T> axis = scale(T(1) / wl, wroll);
+			T kk = dot(axis, mulv(in.iwA, axis)) + dot(axis, mulv(in.iwB, axis));
+			if (kk > T(1e-12))
+			{
+				T maxDw = c.rolling * lambdaNTotal * invH * kk;
+				T dw = maxDw < wl ? maxDw : wl;
+				V<T> angImp = scale(dw / kk, axis);
+				wb = sub(wb, mulv(in.iwB, angImp));
+				wa = add(wa, mulv(in.iwA, angImp));
+			}
+		}
+	}
+}
+
+// adjoints accumulated by the velocity pass of one contact
+template <typename T>
+struct VelocityBar
+{
+	T imA, imB, mu, e;
+	M<T> iwA, iwB;
+	Q<T> qA, qB;
+	V<T> pva, pwa, pvb, pwb;
+};
+
+template <typename T>
+M3D_DIFF_HD void velocity_rev(const Contact<T>& c, const Prepared<T>& p, const VelocityIn<T>& in, const T* lambdaN,
+							  V<T> va0, V<T> wa0, V<T> vb0, V<T> wb0, V<T>& vab, V<T>& wab, V<T>& vbb, V<T>& wbb,
+							  Prepared<T>& pb, T* lambdaNb, VelocityBar<T>& b)
+{
+	const T invH = in.h > T(0) ? T(1) / in.h : T(0);
+	// forward, keeping the velocities before each point
+	V<T> sva[4], swa[4], svb[4], swb[4];
+	V<T> va = va0, wa = wa0, vb = vb0, wb = wb0;
+	T lambdaNTotal = T(0);
+	for (int s = 0; s < c.pointCount; ++s)
+	{
+		sva[s] = va;
+		swa[s] = wa;
+		svb[s] = vb;
+		swb[s] = wb;
+		T lN = lambdaN[s];
+		if (lN <= T(0))
+		{
+			continue;
+		}
+		V<T> rAf, rBf;
+		if (c.curved)
+		{
+			rAf = arm(c.shapeA, c.radiusA, in.qA, c.la[s], c.n, T(1));
+			rBf = arm(c.shapeB, c.radiusB, in.qB, c.lb[s], c.n, T(-1));
+		}
+		else
+		{
+			rAf = p.rA[s];
+			rBf = p.rB[s];
+		}
+		V<T> vrel = sub(add(vb, cross(wb, rBf)), add(va, cross(wa, rAf)));
+		T vn = dot(vrel, c.n);
+		V<T> vt = sub(vrel, scale(vn, c.n));
+		T vtLen = len(vt);
+		if (vtLen > T(1e-9))
+		{
+			V<T> t = scale(T(1) / vtLen, vt);
+			T wt = genInvMass(in.imA, in.iwA, rAf, t) + genInvMass(in.imB, in.iwB, rBf, t);
+			if (wt > T(0))
+			{
+				bool coherent = dot(t, c.slip[s]) > T(0.7);
+				T pStop = vtLen / wt;
+				T pMax = c.mu * lN * invH;
+				T P = !coherent && vtLen < T(0.08) ? pStop : (pStop < pMax ? pStop : pMax);
+				V<T> imp = scale(-P, t);
+				if (in.imB != T(0))
+				{
+					vb = madd(vb, in.imB, imp);
+					wb = add(wb, mulv(in.iwB, cross(rBf, imp)));
+				}
+				if (in.imA != T(0))
+				{
+					V<T> pn = neg(imp);
+					va = madd(va, in.imA, pn);
+					wa = add(wa, mulv(in.iwA, cross(rAf, pn)));
+				}
+			}
+		}
+		V<T> vrelPrev = sub(add(in.pvb, cross(in.pwb, rBf)), add(in.pva, cross(in.pwa, rAf)));
+		T vnPrev = dot(vrelPrev, c.n);
+		T e = dabs(vnPrev) > T(2) * in.gravityLen * in.h ? c.e : T(0);
+		vrel = sub(add(vb, cross(wb, rBf)), add(va, cross(wa, rAf)));
+		vn = dot(vrel, c.n);
+		T target = -e * vnPrev;
+		target = target > T(0) ? target : T(0);
+		T wN = p.wN[s];
+		if (wN > T(0))
+		{
+			T j = (target - vn) / wN;
+			if (in.imB != T(0))
+			{
+				vb = madd(vb, j * in.imB, c.n);
+				wb = madd(wb, j, p.jB[s]);
+			}
+			if (in.imA != T(0))
+			{
+				T mj = -j;
+				va = madd(va, mj * in.imA, c.n);
+				wa = madd(wa, mj, p.jA[s]);
+			}
+		}
+		lambdaNTotal += lN > T(0) ? lN : T(0);
+	}
+	// rolling resistance, applied last: reverse first
+	if (c.rolling > T(0) && lambdaNTotal > T(0))
+	{
+		V<T> wrel = sub(wb, wa);
+		T wn = dot(wrel, c.n);
+		V<T> wroll = sub(wrel, scale(wn, c.n));
+		T wl = len(wroll);
+		if (wl > T(1e-6))
+		{
+			T inv = T(1) / wl;
+			V<T> axis = scale(inv, wroll);
+			V<T> ya = mulv(in.iwA, axis), yb = mulv(in.iwB, axis);
+			T kk = dot(axis, ya) + dot(axis, yb);
+			if (kk > T(1e-12))
+			{
+				T maxDw = c.rolling * lambdaNTotal * invH * kk;
+				bool takeMax = maxDw < wl;
+				T dw = takeMax ? maxDw : wl;
+				V<T> angImp = scale(dw / kk, axis);
+				// wb' = wb - IwB angImp, wa' = wa + IwA angImp
+				V<T> angImpb = vzero<T>();
+				mulv_rev(in.iwB, angImp, neg(wbb), b.iwB, angImpb);
+				mulv_rev(in.iwA, angImp, wab, b.iwA, angImpb);
+				V<T> axisb = scale(dw / kk, angImpb);
+				T sb = dot(angImpb, axis);
+				T dwb = sb / kk;
+				T kkb = -sb * dw / (kk * kk);
+				T maxDwb = T(0), wlb = T(0);
+				if (takeMax)
+					maxDwb = dwb;
+				else
+					wlb = dwb;
+				T lambdaTotb = maxDwb * c.rolling * invH * kk;
+				kkb += maxDwb * c.rolling * lambdaNTotal * invH;
+				axisb = madd(axisb, kkb, ya);
+				axisb = madd(axisb, kkb, yb);
+				mulv_rev(in.iwA, axis, scale(kkb, axis), b.iwA, axisb);
+				mulv_rev(in.iwB, axis, scale(kkb, axis), b.iwB, axisb);
+				V<T> wrollb = scale(inv, axisb);
+				wlb += -dot(axisb, wroll) * inv * inv;
+				len_rev(wroll, wl, wlb, wrollb);
+				V<T> wrelb = sub(wrollb, scale(dot(wrollb, c.n), c.n));
+				wbb = add(wbb, wrelb);
+				wab = sub(wab, wrelb);
+				for (int s = 0; s < c.pointCount; ++s)
+				{
+					if (lambdaN[s] > T(0))
+					{
+						lambdaNb[s] += lambdaTotb;
+					}
+				}
+			}
+		}
+	}
+	for (int s = c.pointCount - 1; s >= 0; --s)
+	{
+		T lN = lambdaN[s];
+		if (lN <= T(0))
+		{
+			continue;
+		}
+		va = sva[s];
+		wa = swa[s];
+		vb = svb[s];
+		wb = swb[s];
+		V<T> rAf, rBf;
+		if (c.curved)
+		{
+			rAf = arm(c.shapeA, c.radiusA, in.qA, c.la[s], c.n, T(1));
+			rBf = arm(c.shapeB, c.radiusB, in.qB, c.lb[s], c.n, T(-1));
+		}
+		else
+		{
+			rAf = p.rA[s];
+			rBf = p.rB[s];
+		}
+		V<T> rAfb = vzero<T>(), rBfb = vzero<T>();
+		// friction stage forward
+		V<T> vrel = sub(add(vb, cross(wb, rBf)), add(va, cross(wa, rAf)));
+		T vn = dot(vrel, c.n);
+		V<T> vt = sub(vrel, scale(vn, c.n));
+		T vtLen = len(vt);
+		bool fric = false, takeStop = false, useMaxBranch = false;
+		T wt = T(0), pStop = T(0), P = T(0);
+		V<T> t = vzero<T>(), imp = vzero<T>();
+		if (vtLen > T(1e-9))
+		{
+			t = scale(T(1) / vtLen, vt);
+			wt = genInvMass(in.imA, in.iwA, rAf, t) + genInvMass(in.imB, in.iwB, rBf, t);
+			if (wt > T(0))
+			{
+				fric = true;
+				bool coherent = dot(t, c.slip[s]) > T(0.7);
+				pStop = vtLen / wt;
+				T pMax = c.mu * lN * invH;
+				if (!coherent && vtLen < T(0.08))
+				{
+					takeStop = true;
+				}
+				else
+				{
+					takeStop = pStop < pMax;
+					useMaxBranch = !takeStop;
+				}
+				P = takeStop ? pStop : pMax;
+				imp = scale(-P, t);
+			}
+		}
+		V<T> va1 = va, wa1 = wa, vb1 = vb, wb1 = wb;
+		if (fric)
+		{
+			if (in.imB != T(0))
+			{
+				vb1 = madd(vb, in.imB, imp);
+				wb1 = add(wb, mulv(in.iwB, cross(rBf, imp)));
+			}
+			if (in.imA != T(0))
+			{
+				V<T> pn = neg(imp);
+				va1 = madd(va, in.imA, pn);
+				wa1 = add(wa, mulv(in.iwA, cross(rAf, pn)));
+			}
+		}
+		V<T> vrelPrev = sub(add(in.pvb, cross(in.pwb, rBf)), add(in.pva, cross(in.pwa, rAf)));
+		T vnPrev = dot(vrelPrev, c.n);
+		bool useE = dabs(vnPrev) > T(2) * in.gravityLen * in.h;
+		T e = useE ? c.e : T(0);
+		V<T> vrel2 = sub(add(vb1, cross(wb1, rBf)), add(va1, cross(wa1, rAf)));
+		T vn2 = dot(vrel2, c.n);
+		T target = -e * vnPrev;
+		bool targetPos = target > T(0);
+		target = targetPos ? target : T(0);
+		T wN = p.wN[s];
+		// normal impulse stage reverse
+		V<T> va1b = vab, wa1b = wab, vb1b = vbb, wb1b = wbb;
+		if (wN > T(0))
+		{
+			T j = (target - vn2) / wN;
+			T jb = T(0);
+			if (in.imB != T(0))
+			{
+				T d = dot(vbb, c.n);
+				jb += in.imB * d + dot(wbb, p.jB[s]);
+				b.imB += j * d;
+				pb.jB[s] = madd(pb.jB[s], j, wbb);
+			}
+			if (in.imA != T(0))
+			{
+				T mj = -j;
+				T d = dot(vab, c.n);
+				T mjb = in.imA * d + dot(wab, p.jA[s]);
+				b.imA += mj * d;
+				pb.jA[s] = madd(pb.jA[s], mj, wab);
+				jb -= mjb;
+			}
+			T targetb = jb / wN;
+			T vn2b = -jb / wN;
+			pb.wN[s] += -jb * j / wN;
+			if (targetPos)
+			{
+				T eb = -targetb * vnPrev;
+				T vnPrevb = -targetb * e;
+				if (useE)
+				{
+					b.e += eb;
+				}
+				V<T> vrelPrevb = scale(vnPrevb, c.n);
+				b.pvb = add(b.pvb, vrelPrevb);
+				cross_rev(in.pwb, rBf, vrelPrevb, b.pwb, rBfb);
+				b.pva = sub(b.pva, vrelPrevb);
+				cross_rev(in.pwa, rAf, neg(vrelPrevb), b.pwa, rAfb);
+			}
+			V<T> vrel2b = scale(vn2b, c.n);
+			vb1b = add(vb1b, vrel2b);
+			cross_rev(wb1, rBf, vrel2b, wb1b, rBfb);
+			va1b = sub(va1b, vrel2b);
+			cross_rev(wa1, rAf, neg(vrel2b), wa1b, rAfb);
+		}
+		// friction stage reverse
+		V<T> vab0 = va1b, wab0 = wa1b, vbb0 = vb1b, wbb0 = wb1b;
+		if (fric)
+		{
+			V<T> impb = vzero<T>();
+			if (in.imB != T(0))
+			{
+				impb = madd(impb, in.imB, vb1b);
+				b.imB += dot(vb1b, imp);
+				V<T> cB = cross(rBf, imp);
+				V<T> cBb = vzero<T>();
+				mulv_rev(in.iwB, cB, wb1b, b.iwB, cBb);
+				cross_rev(rBf, imp, cBb, rBfb, impb);
+			}
+			if (in.imA != T(0))
+			{
+				V<T> pn = neg(imp);
+				V<T> pnb = scale(in.imA, va1b);
+				b.imA += dot(va1b, pn);
+				V<T> cA = cross(rAf, pn);
+				V<T> cAb = vzero<T>();
+				mulv_rev(in.iwA, cA, wa1b, b.iwA, cAb);
+				cross_rev(rAf, pn, cAb, rAfb, pnb);
+				impb = sub(impb, pnb);
+			}
+			T Pb = -dot(impb, t);
+			V<T> tb = scale(-P, impb);
+			T pStopb = T(0);
+			if (takeStop)
+			{
+				pStopb = Pb;
+			}
+			else if (useMaxBranch)
+			{
+				b.mu += Pb * lN * invH;
+				lambdaNb[s] += Pb * c.mu * invH;
+			}
+			T vtLenb = pStopb / wt;
+			T wtb = -pStopb * vtLen / (wt * wt);
+			genInvMass_rev(in.iwA, rAf, t, wtb, b.imA, b.iwA, rAfb, tb);
+			genInvMass_rev(in.iwB, rBf, t, wtb, b.imB, b.iwB, rBfb, tb);
+			V<T> vtb = scale(T(1) / vtLen, tb);
+			vtLenb += -dot(tb, vt) / (vtLen * vtLen);
+			len_rev(vt, vtLen, vtLenb, vtb);
+			V<T> vrelb = sub(vtb, scale(dot(vtb, c.n), c.n));
+			vbb0 = add(vbb0, vrelb);
+			cross_rev(wb, rBf, vrelb, wbb0, rBfb);
+			vab0 = sub(vab0, vrelb);
+			cross_rev(wa, rAf, neg(vrelb), wab0, rAfb);
+		}
+		vab = vab0;
+		wab = wab0;
+		vbb = vbb0;
+		wbb = wbb0;
+		// arms
+		if (c.curved)
+		{
+			arm_rev(c.shapeA, in.qA, c.la[s], rAfb, b.qA);
+			arm_rev(c.shapeB, in.qB, c.lb[s], rBfb, b.qB);
+		}
+		else
+		{
+			pb.rA[s] = add(pb.rA[s], rAfb);
+			pb.rB[s] = add(pb.rB[s], rBfb);
+		}
+	}
+}
+
+// ---- one island through one recorded step ------------------------------------
+
+// tape record of one contact in one substep (float, as stored on the device)
+struct TapeContact
+{
+	int32_t a, b, pointCount, curved, shapeA, shapeB;
+	float radiusA, radiusB;
+	float n[3];
+	float mu, e, rolling;
+	float la[4][3], lb[4][3], off[4], fa[4][3], fb[4][3], slip[4][3];
+};
+
+template <typename T>
+M3D_DIFF_HD V<T> tv(const float* f)
+{
+	return v3<T>(T(f[0]), T(f[1]), T(f[2]));
+}
+
+template <typename T>
+M3D_DIFF_HD Contact<T> loadContact(const TapeContact& t)
+{
+	Contact<T> c;
+	c.a = t.a;
+	c.b = t.b;
+	c.pointCount = t.pointCount;
+	c.curved = t.curved;
+	c.shapeA = t.shapeA;
+	c.shapeB = t.shapeB;
+	c.radiusA = T(t.radiusA);
+	c.radiusB = T(t.radiusB);
+	c.n = tv<T>(t.n);
+	c.mu = T(t.mu);
+	c.e = T(t.e);
+	c.rolling = T(t.rolling);
+	for (int s = 0; s < 4; ++s)
+	{
+		c.la[s] = tv<T>(t.la[s]);
+		c.lb[s] = tv<T>(t.lb[s]);
+		c.off[s] = T(t.off[s]);
+		c.fa[s] = tv<T>(t.fa[s]);
+		c.fb[s] = tv<T>(t.fb[s]);
+		c.slip[s] = tv<T>(t.slip[s]);
+	}
+	return c;
+}
+
+// island of one step: its bodies (global indices) and its contacts, in solve
+// order, for each substep
+struct TapeIsland
+{
+	int32_t bodyStart, bodyCount, contactStart, contactCount;
+};
+
+// per-operation inputs saved by the recording replay of a substep
+template <typename T>
+struct PoseRec
+{
+	V<T> pA, pB;
+	Q<T> qA, qB;
+	T lam[4];
+	int gate;
+};
+template <typename T>
+struct VelRec
+{
+	V<T> va, wa, vb, wb;
+};
+
+// Everything the island driver reads and writes; body-indexed arrays are
+// global (the island owns its dynamic bodies), contact-indexed arrays are
+// indexed by the contact's position in the step's contact list.
+template <typename T>
+struct IslandCtx
+{
+	// constants
+	const BodyConst<T>* bc;
+	T h, invH, maxCorrection, gravityLen;
+	V<T> g;
+	int iterations, substeps;
+	// the step
+	const TapeIsland* island;
+	const int32_t* bodies;        // the step's body list
+	const TapeContact* contacts;  // [substep * contactsPerSubstep + position]
+	int32_t contactsPerSubstep;
+	// state: current (in/out), substep starts, integrated rotations and inverse
+	// inertias, poses before reconstruction
+	Body<T>* cur;
+	Body<T>* start; // [substep * bodyCount + body]
+	int32_t bodyCount;
+	M<T>* iw;
+	V<T>* x2;
+	Q<T>* q2;
+	// recording
+	Prepared<T>* prep; // per position
+	T* lamN;           // 4 per position
+	T* lamT;
+	PoseRec<T>* normRec; // [iteration * positions + position]
+	PoseRec<T>* fricRec;
+	VelRec<T>* velRec;
+	int32_t positions;
+	// adjoints
+	Body<T>* adj;    // per body
+	Body<T>* adj0;   // per body: adjoints of the substep start, accumulated
+	T* imBar;        // per body: inverse mass
+	T* ilBar;        // per body: isotropic inverse inertia
+	T* muBar;        // per body: friction coefficient
+	T* eBar;         // per body: restitution
+	M<T>* iwBar;     // per body
+	Prepared<T>* prepBar;
+	T* lamNBar;      // 4 per position
+	T* lamTBar;
+	const T* muBody; // per body friction and restitution (to split contact values)
+	const T* eBody;
+};
+
+template <typename T>
+M3D_DIFF_HD void substepForward(const IslandCtx<T>& x, const TapeIsland& r, int sub, bool record)
+{
+	const BodyConst<T>* bc = x.bc;
+	for (int k = 0; k < r.bodyCount; ++k)
+	{
+		int i = x.bodies[r.bodyStart + k];
+		if (!bc[i].dynamic)
+		{
+			continue;
+		}
+		Body<T> s1;
+		integrate(x.cur[i], bc[i], x.h, x.g, s1, x.iw[i]);
+		x.start[(size_t)sub * x.bodyCount + i] = x.cur[i];
+		x.cur[i] = s1;
+	}
+	const TapeContact* tc = x.contacts + (size_t)sub * x.contactsPerSubstep;
+	for (int j = 0; j < r.contactCount; ++j)
+	{
+		int pos = r.contactStart + j;
+		Contact<T> c = loadContact<T>(tc[pos]);
+		Prepared<T>& p = x.prep[pos];
+		preparedZero(p);
+		prepare(c, x.cur[c.a].q, x.cur[c.b].q, bc[c.a].invMass, bc[c.b].invMass, x.iw[c.a], x.iw[c.b], p);
+		for (int s = 0; s < 4; ++s)
+		{
+			x.lamN[4 * pos + s] = T(0);
+			x.lamT[4 * pos + s] = T(0);
+		}
+	}
+	for (int it = 0; it < x.iterations; ++it)
+	{
+		for (int j = 0; j < r.contactCount; ++j)
+		{
+			int pos = r.contactStart + j;
+			Contact<T> c = loadContact<T>(tc[pos]);
+			if (record)
+			{
+				PoseRec<T>& rec = x.normRec[(size_t)it * x.positions + pos];
+				rec.pA = x.cur[c.a].x;
+				rec.qA = x.cur[c.a].q;
+				rec.pB = x.cur[c.b].x;
+				rec.qB = x.cur[c.b].q;
+			}
+			if (c.pointCount == 0)
+			{
+				continue;
+			}
+			normals(c, x.prep[pos], bc[c.a].invMass, bc[c.b].invMass, x.maxCorrection, x.cur[c.a].x, x.cur[c.a].q,
+					x.cur[c.b].x, x.cur[c.b].q, x.lamN + 4 * pos);
+		}
+	}
+	for (int j = 0; j < r.contactCount; ++j)
+	{
+		int pos = r.contactStart + j;
+		Contact<T> c = loadContact<T>(tc[pos]);
+		bool gate = frictionGate(c, x.prep[pos], x.cur[c.a].v, x.cur[c.a].w, x.cur[c.b].v, x.cur[c.b].w);
+		if (record)
+		{
+			PoseRec<T>& rec = x.fricRec[pos];
+			rec.pA = x.cur[c.a].x;
+			rec.qA = x.cur[c.a].q;
+			rec.pB = x.cur[c.b].x;
+			rec.qB = x.cur[c.b].q;
+			for (int s = 0; s < 4; ++s)
+			{
+				rec.lam[s] = x.lamT[4 * pos + s];
+			}
+			rec.gate = gate ? 1 : 0;
+		}
+		if (gate)
+		{
+			friction(c, bc[c.a].invMass, bc[c.b].invMass, x.iw[c.a], x.iw[c.b], x.lamN + 4 * pos, x.cur[c.a].x,
+					 x.cur[c.a].q, x.cur[c.b].x, x.cur[c.b].q, x.lamT + 4 * pos);
+		}
+	}
+	for (int k = 0; k < r.bodyCount; ++k)
+	{
+		int i = x.bodies[r.bodyStart + k];
+		if (!bc[i].dynamic)
+		{
+			continue;
+		}
+		const Body<T>& s0 = x.start[(size_t)sub * x.bodyCount + i];
+		x.x2[i] = x.cur[i].x;
+		x.q2[i] = x.cur[i].q;
+		reconstruct(x.cur[i].x, x.cur[i].q, s0.x, s0.q, x.invH, x.cur[i].v, x.cur[i].w);
+	}
+	for (int j = 0; j < r.contactCount; ++j)
+	{
+		int pos = r.contactStart + j;
+		Contact<T> c = loadContact<T>(tc[pos]);
+		if (record)
+		{
+			VelRec<T>& rec = x.velRec[pos];
+			rec.va = x.cur[c.a].v;
+			rec.wa = x.cur[c.a].w;
+			rec.vb = x.cur[c.b].v;
+			rec.wb = x.cur[c.b].w;
+		}
+		VelocityIn<T> in;
+		in.imA = bc[c.a].invMass;
+		in.imB = bc[c.b].invMass;
+		in.iwA = x.iw[c.a];
+		in.iwB = x.iw[c.b];
+		in.qA = x.cur[c.a].q;
+		in.qB = x.cur[c.b].q;
+		const Body<T>& sa = x.start[(size_t)sub * x.bodyCount + c.a];
+		const Body<T>& sb = x.start[(size_t)sub * x.bodyCount + c.b];
+		in.pva = bc[c.a].dynamic ? sa.v : x.cur[c.a].v;
+		in.pwa = bc[c.a].dynamic ? sa.w : x.cur[c.a].w;
+		in.pvb = bc[c.b].dynamic ? sb.v : x.cur[c.b].v;
+		in.pwb = bc[c.b].dynamic ? sb.w : x.cur[c.b].w;
+		in.h = x.h;
+		in.gravityLen = x.gravityLen;
+		V<T> va = x.cur[c.a].v, wa = x.cur[c.a].w, vb = x.cur[c.b].v, wb = x.cur[c.b].w;
+		velocity(c, x.prep[pos], in, x.lamN + 4 * pos, va, wa, vb, wb);
+		if (bc[c.a].dynamic)
+		{
+			x.cur[c.a].v = va;
+			x.cur[c.a].w = wa;
+		}
+		if (bc[c.b].dynamic)
+		{
+			x.cur[c.b].v = vb;
+			x.cur[c.b].w = wb;
+		}
+	}
+}
+
+// friction coefficient of a contact: sqrt(mu_a mu_b); adjoint split
+template <typename T>
+M3D_DIFF_HD void scatterMaterials(const IslandCtx<T>& x, const Contact<T>& c, T muB, T eB)
+{
+	const T ma = x.muBody[c.a], mb = x.muBody[c.b];
+	if (x.bc[c.a].dynamic && ma > T(0))
+	{
+		x.muBar[c.a] += muB * T(0.5) * c.mu / ma;
+	}
+	if (x.bc[c.b].dynamic && mb > T(0))
+	{
+		x.muBar[c.b] += muB * T(0.5) * c.mu / mb;
+	}
+	// restitution: the larger of the two (A on ties, as the reference)
+	const int who = x.eBody[c.a] > x.eBody[c.b] ? c.a : (x.eBody[c.a] == x.eBody[c.b] ? c.a : c.b);
+	if (x.bc[who].dynamic)
+	{
+		x.eBar[who] += eB;
+	}
+}
+
+template <typename T>
+M3D_DIFF_HD void substepReverse(const IslandCtx<T>& x, const TapeIsland& r, int sub)
+{
+	const BodyConst<T>* bc = x.bc;
+	const TapeContact* tc = x.contacts + (size_t)sub * x.contactsPerSubstep;
+	for (int k = 0; k < r.bodyCount; ++k)
+	{
+		int i = x.bodies[r.bodyStart + k];
+		x.adj0[i] = bodyZero<T>();
+		M<T> z;
+		z.cx = z.cy = z.cz = vzero<T>();
+		x.iwBar[i] = z;
+	}
+	for (int j = 0; j < r.contactCount; ++j)
+	{
+		int pos = r.contactStart + j;
+		preparedZero(x.prepBar[pos]);
+		for (int s = 0; s < 4; ++s)
+		{
+			x.lamNBar[4 * pos + s] = T(0);
+			x.lamTBar[4 * pos + s] = T(0);
+		}
+	}
+	// velocity pass, in reverse contact order
+	for (int j = r.contactCount - 1; j >= 0; --j)
+	{
+		int pos = r.contactStart + j;
+		Contact<T> c = loadContact<T>(tc[pos]);
+		const VelRec<T>& rec = x.velRec[pos];
+		VelocityIn<T> in;
+		in.imA = bc[c.a].invMass;
+		in.imB = bc[c.b].invMass;
+		in.iwA = x.iw[c.a];
+		in.iwB = x.iw[c.b];
+		in.qA = x.x2 != nullptr && bc[c.a].dynamic ? x.q2[c.a] : x.cur[c.a].q;
+		in.qB = x.x2 != nullptr && bc[c.b].dynamic ? x.q2[c.b] : x.cur[c.b].q;
+		const Body<T>& sa = x.start[(size_t)sub * x.bodyCount + c.a];
+		const Body<T>& sb = x.start[(size_t)sub * x.bodyCount + c.b];
+		in.pva = bc[c.a].dynamic ? sa.v : x.cur[c.a].v;
+		in.pwa = bc[c.a].dynamic ? sa.w : x.cur[c.a].w;
+		in.pvb = bc[c.b].dynamic ? sb.v : x.cur[c.b].v;
+		in.pwb = bc[c.b].dynamic ? sb.w : x.cur[c.b].w;
+		in.h = x.h;
+		in.gravityLen = x.gravityLen;
+		VelocityBar<T> b;
+		b.imA = b.imB = b.mu = b.e = T(0);
+		b.iwA.cx = b.iwA.cy = b.iwA.cz = vzero<T>();
+		b.iwB = b.iwA;
+		b.qA = b.qB = qzero<T>();
+		b.pva = b.pwa = b.pvb = b.pwb = vzero<T>();
+		V<T> dummy0 = vzero<T>(), dummy1 = vzero<T>(), dummy2 = vzero<T>(), dummy3 = vzero<T>();
+		V<T>& vab = bc[c.a].dynamic ? x.adj[c.a].v : dummy0;
+		V<T>& wab = bc[c.a].dynamic ? x.adj[c.a].w : dummy1;
+		V<T>& vbb = bc[c.b].dynamic ? x.adj[c.b].v : dummy2;
+		V<T>& wbb = bc[c.b].dynamic ? x.adj[c.b].w : dummy3;
+		velocity_rev(c, x.prep[pos], in, x.lamN + 4 * pos, rec.va, rec.wa, rec.vb, rec.wb, vab, wab, vbb, wbb,
+					 x.prepBar[pos], x.lamNBar + 4 * pos, b);
+		if (bc[c.a].dynamic)
+		{
+			x.imBar[c.a] += b.imA;
+			x.iwBar[c.a].cx = add(x.iwBar[c.a].cx, b.iwA.cx);
+			x.iwBar[c.a].cy = add(x.iwBar[c.a].cy, b.iwA.cy);
+			x.iwBar[c.a].cz = add(x.iwBar[c.a].cz, b.iwA.cz);
+			x.adj[c.a].q = qadd(x.adj[c.a].q, b.qA);
+			x.adj0[c.a].v = add(x.adj0[c.a].v, b.pva);
+			x.adj0[c.a].w = add(x.adj0[c.a].w, b.pwa);
+		}
+		if (bc[c.b].dynamic)
+		{
+			x.imBar[c.b] += b.imB;
+			x.iwBar[c.b].cx = add(x.iwBar[c.b].cx, b.iwB.cx);
+			x.iwBar[c.b].cy = add(x.iwBar[c.b].cy, b.iwB.cy);
+			x.iwBar[c.b].cz = add(x.iwBar[c.b].cz, b.iwB.cz);
+			x.adj[c.b].q = qadd(x.adj[c.b].q, b.qB);
+			x.adj0[c.b].v = add(x.adj0[c.b].v, b.pvb);
+			x.adj0[c.b].w = add(x.adj0[c.b].w, b.pwb);
+		}
+		scatterMaterials(x, c, b.mu, b.e);
+	}
+	// reconstruction
+	for (int k = 0; k < r.bodyCount; ++k)
+	{
+		int i = x.bodies[r.bodyStart + k];
+		if (!bc[i].dynamic)
+		{
+			continue;
+		}
+		const Body<T>& s0 = x.start[(size_t)sub * x.bodyCount + i];
+		V<T> vb = x.adj[i].v, wb = x.adj[i].w;
+		x.adj[i].v = vzero<T>();
+		x.adj[i].w = vzero<T>();
+		reconstruct_rev(x.x2[i], x.q2[i], s0.x, s0.q, x.invH, vb, wb, x.adj[i].x, x.adj[i].q, x.adj0[i].x, x.adj0[i].q);
+	}
+	// friction, reverse contact order
+	for (int j = r.contactCount - 1; j >= 0; --j)
+	{
+		int pos = r.contactStart + j;
+		const PoseRec<T>& rec = x.fricRec[pos];
+		if (!rec.gate)
+		{
+			continue;
+		}
+		Contact<T> c = loadContact<T>(tc[pos]);
+		V<T> d0 = vzero<T>(), d1 = vzero<T>();
+		Q<T> e0 = qzero<T>(), e1 = qzero<T>();
+		V<T>& pAb = bc[c.a].dynamic ? x.adj[c.a].x : d0;
+		Q<T>& qAb = bc[c.a].dynamic ? x.adj[c.a].q : e0;
+		V<T>& pBb = bc[c.b].dynamic ? x.adj[c.b].x : d1;
+		Q<T>& qBb = bc[c.b].dynamic ? x.adj[c.b].q : e1;
+		T muB = T(0), imAb = T(0), imBb = T(0);
+		M<T> iwAb, iwBb;
+		iwAb.cx = iwAb.cy = iwAb.cz = vzero<T>();
+		iwBb = iwAb;
+		friction_rev(c, bc[c.a].invMass, bc[c.b].invMass, x.iw[c.a], x.iw[c.b], x.lamN + 4 * pos, rec.pA, rec.qA, rec.pB,
+					 rec.qB, rec.lam, pAb, qAb, pBb, qBb, x.lamNBar + 4 * pos, x.lamTBar + 4 * pos, muB, imAb, imBb, iwAb,
+					 iwBb);
+		if (bc[c.a].dynamic)
+		{
+			x.imBar[c.a] += imAb;
+			x.iwBar[c.a].cx = add(x.iwBar[c.a].cx, iwAb.cx);
+			x.iwBar[c.a].cy = add(x.iwBar[c.a].cy, iwAb.cy);
+			x.iwBar[c.a].cz = add(x.iwBar[c.a].cz, iwAb.cz);
+		}
+		if (bc[c.b].dynamic)
+		{
+			x.imBar[c.b] += imBb;
+			x.iwBar[c.b].cx = add(x.iwBar[c.b].cx, iwBb.cx);
+			x.iwBar[c.b].cy = add(x.iwBar[c.b].cy, iwBb.cy);
+			x.iwBar[c.b].cz = add(x.iwBar[c.b].cz, iwBb.cz);
+		}
+		scatterMaterials(x, c, muB, T(0));
+	}
+	// normal iterations, reverse
+	for (int it = x.iterations - 1; it >= 0; --it)
+	{
+		for (int j = r.contactCount - 1; j >= 0; --j)
+		{
+			int pos = r.contactStart + j;
+			Contact<T> c = loadContact<T>(tc[pos]);
+			if (c.pointCount == 0)
+			{
+				continue;
+			}
+			const PoseRec<T>& rec = x.normRec[(size_t)it * x.positions + pos];
+			V<T> d0 = vzero<T>(), d1 = vzero<T>();
+			Q<T> e0 = qzero<T>(), e1 = qzero<T>();
+			V<T>& pAb = bc[c.a].dynamic ? x.adj[c.a].x : d0;
+			Q<T>& qAb = bc[c.a].dynamic ? x.adj[c.a].q : e0;
+			V<T>& pBb = bc[c.b].dynamic ? x.adj[c.b].x : d1;
+			Q<T>& qBb = bc[c.b].dynamic ? x.adj[c.b].q : e1;
+			T imAb = T(0), imBb = T(0);
+			normals_rev(c, x.prep[pos], bc[c.a].invMass, bc[c.b].invMass, x.maxCorrection, rec.pA, rec.qA, rec.pB,
+						rec.qB, pAb, qAb, pBb, qBb, x.lamNBar + 4 * pos, x.prepBar[pos], imAb, imBb);
+			if (bc[c.a].dynamic)
+			{
+				x.imBar[c.a] += imAb;
+			}
+			if (bc[c.b].dynamic)
+			{
+				x.imBar[c.b] += imBb;
+			}
+		}
+	}
+	// contact preparation (poses at preparation = the integrated ones)
+	for (int j = 0; j < r.contactCount; ++j)
+	{
+		int pos = r.contactStart + j;
+		Contact<T> c = loadContact<T>(tc[pos]);
+		Q<T> qA1 = x.start[(size_t)sub * x.bodyCount + c.a].q, qB1 = x.start[(size_t)sub * x.bodyCount + c.b].q;
+		// the rotation at preparation is the integrated one, rebuilt here
+		if (bc[c.a].dynamic)
+		{
+			Body<T> s1;
+			M<T> iw;
+			integrate(x.start[(size_t)sub * x.bodyCount + c.a], bc[c.a], x.h, x.g, s1, iw);
+			qA1 = s1.q;
+		}
+		else
+		{
+			qA1 = x.cur[c.a].q;
+		}
+		if (bc[c.b].dynamic)
+		{
+			Body<T> s1;
+			M<T> iw;
+			integrate(x.start[(size_t)sub * x.bodyCount + c.b], bc[c.b], x.h, x.g, s1, iw);
+			qB1 = s1.q;
+		}
+		else
+		{
+			qB1 = x.cur[c.b].q;
+		}
+		Q<T> qAb = qzero<T>(), qBb = qzero<T>();
+		T imAb = T(0), imBb = T(0);
+		M<T> iwAb, iwBb;
+		iwAb.cx = iwAb.cy = iwAb.cz = vzero<T>();
+		iwBb = iwAb;
+		prepare_rev(c, qA1, qB1, x.iw[c.a], x.iw[c.b], x.prep[pos], x.prepBar[pos], qAb, qBb, imAb, imBb, iwAb, iwBb);
+		if (bc[c.a].dynamic)
+		{
+			x.adj[c.a].q = qadd(x.adj[c.a].q, qAb);
+			x.imBar[c.a] += imAb;
+			x.iwBar[c.a].cx = add(x.iwBar[c.a].cx, iwAb.cx);
+			x.iwBar[c.a].cy = add(x.iwBar[c.a].cy, iwAb.cy);
+			x.iwBar[c.a].cz = add(x.iwBar[c.a].cz, iwAb.cz);
+		}
+		if (bc[c.b].dynamic)
+		{
+			x.adj[c.b].q = qadd(x.adj[c.b].q, qBb);
+			x.imBar[c.b] += imBb;
+			x.iwBar[c.b].cx = add(x.iwBar[c.b].cx, iwBb.cx);
+			x.iwBar[c.b].cy = add(x.iwBar[c.b].cy, iwBb.cy);
+			x.iwBar[c.b].cz = add(x.iwBar[c.b].cz, iwBb.cz);
+		}
+	}
+	// integration
+	for (int k = 0; k < r.bodyCount; ++k)
+	{
+		int i = x.bodies[r.bodyStart + k];
+		if (!bc[i].dynamic)
+		{
+			continue;
+		}
+		Body<T> s1b = x.adj[i];
+		s1b.v = vzero<T>();
+		s1b.w = vzero<T>();
+		BodyConstBar<T> cb;
+		cb.invMass = T(0);
+		cb.il = T(0);
+		Body<T> s0b = x.adj0[i];
+		integrate_rev(x.start[(size_t)sub * x.bodyCount + i], bc[i], x.h, x.g, s1b, x.iwBar[i], s0b, cb);
+		x.ilBar[i] += cb.il;
+		x.adj[i] = s0b;
+	}
+}
+
+// One island through one step, backward: the state of its bodies at the
+// step's start is in cur; the adjoints of their state at the step's end in
+// adj.  On return adj holds the adjoints at the step's start and cur is
+// unchanged.
+template <typename T>
+M3D_DIFF_HD void islandStepBackward(const IslandCtx<T>& x)
+{
+	const TapeIsland& r = *x.island;
+	Body<T> keep[1];
+	(void)keep;
+	// forward through the first substeps to reach each substep's start
+	for (int sub = 0; sub < x.substeps; ++sub)
+	{
+		substepForward(x, r, sub, false);
+	}
+	for (int sub = x.substeps - 1; sub >= 0; --sub)
+	{
+		for (int k = 0; k < r.bodyCount; ++k)
+		{
+			int i = x.bodies[r.bodyStart + k];
+			if (x.bc[i].dynamic)
+			{
+				x.cur[i] = x.start[(size_t)sub * x.bodyCount + i];
+			}
+		}
+		substepForward(x, r, sub, true);
+		substepReverse(x, r, sub);
+	}
+	// cur: back to the step's start
+	for (int k = 0; k < r.bodyCount; ++k)
+	{
+		int i = x.bodies[r.bodyStart + k];
+		if (x.bc[i].dynamic)
+		{
+			x.cur[i] = x.start[i];
+		}
+	}
+}
+
+// One island through one step, forward only (the replay).
+template <typename T>
+M3D_DIFF_HD void islandStepForward(const IslandCtx<T>& x)
+{
+	const TapeIsland& r = *x.island;
+	for (int sub = 0; sub < x.substeps; ++sub)
+	{
+		substepForward(x, r, sub, false);
+	}
+}
+
+} // namespace m3d_diff
