@@ -9,12 +9,17 @@
 // operation's outputs and accumulates the adjoints of its inputs, recomputing
 // the forward temporaries it needs.
 //
-// What is held fixed (the "frozen tape"): the contact set, every manifold
-// (normal, anchors, separation offsets, point count) as the forward's contact
-// preparation left it in each substep, the stiction anchors and slip
-// directions, the solve order, and every branch the forward took (contact
-// gates, caps, stiction and coherence tests).  Derivatives flow through body
-// states, inverse masses and inertias, friction and restitution coefficients.
+// What is held fixed (the tape): the contact set, the solve order, which
+// contacts had their manifold regenerated when (narrowphase or contact
+// preparation), the feature ids of the points, which stiction anchors were
+// kept or re-seated, and every branch the forward took (contact gates, caps,
+// stiction, coherence and restitution tests, SAT axis and clipping choices).
+// Derivatives flow through body states, inverse masses and inertias, friction
+// and restitution coefficients, and through the manifold data as state: a
+// manifold's normal, local anchors and separation offsets are functions of
+// the poses it was generated at (m3d_diff_gen.h), stiction anchors start at
+// the local anchors or carry over, and all of them persist across substeps
+// and steps until the next generation (ContactBar carries their adjoint).
 //
 // Scope: spheres and boxes with isotropic inertia (cubes); no joints, no
 // external forces; serial islands.  For an isotropic body the world inverse
@@ -260,6 +265,13 @@ M3D_DIFF_HD void rotate_rev_q(Q<T> q, V<T> v, V<T> o, Q<T>& qb)
 	qb.y += ub.y;
 	qb.z += ub.z;
 }
+// adjoint of the rotated vector: rotate(q, v) is linear in v, M(q) v with
+// M = I + 2w[u]x + 2[u]x^2; its transpose is the rotation by conj(q)
+template <typename T>
+M3D_DIFF_HD V<T> rotate_rev_v(Q<T> q, V<T> o)
+{
+	return rotate(qconj(q), o);
+}
 // y = m v: adjoints of m (outer product) and v
 template <typename T>
 M3D_DIFF_HD void mulv_rev(const M<T>& m, V<T> v, V<T> o, M<T>& mb, V<T>& vb)
@@ -446,6 +458,26 @@ struct Contact
 	V<T> slip[4];      // slip directions of the last velocity pass
 };
 
+// adjoint of a contact's manifold data: normal, local anchors, separation
+// offsets, stiction anchors (the fields every substep reads)
+template <typename T>
+struct ContactBar
+{
+	V<T> n;
+	V<T> la[4], lb[4], fa[4], fb[4];
+	T off[4];
+};
+template <typename T>
+M3D_DIFF_HD void contactBarZero(ContactBar<T>& b)
+{
+	b.n = vzero<T>();
+	for (int s = 0; s < 4; ++s)
+	{
+		b.la[s] = b.lb[s] = b.fa[s] = b.fb[s] = vzero<T>();
+		b.off[s] = T(0);
+	}
+}
+
 // contact quantities frozen at preparation (reference src/xpbd.cpp:733-863)
 template <typename T>
 struct Prepared
@@ -470,11 +502,16 @@ M3D_DIFF_HD V<T> arm(int shape, T radius, Q<T> q, V<T> l, V<T> n, T sign)
 	return shape == kShapeSphere ? scale(sign * radius, n) : rotate(q, l);
 }
 template <typename T>
-M3D_DIFF_HD void arm_rev(int shape, Q<T> q, V<T> l, V<T> rb, Q<T>& qb)
+M3D_DIFF_HD void arm_rev(int shape, T radius, Q<T> q, V<T> l, T sign, V<T> rb, Q<T>& qb, V<T>& lb, V<T>& nb)
 {
 	if (shape != kShapeSphere)
 	{
 		rotate_rev_q(q, l, rb, qb);
+		lb = add(lb, rotate_rev_v(q, rb));
+	}
+	else
+	{
+		nb = madd(nb, sign * radius, rb);
 	}
 }
 
@@ -501,7 +538,7 @@ M3D_DIFF_HD void prepare(const Contact<T>& c, Q<T> qA, Q<T> qB, T imA, T imB, co
 template <typename T>
 M3D_DIFF_HD void prepare_rev(const Contact<T>& c, Q<T> qA, Q<T> qB, const M<T>& iwA, const M<T>& iwB,
 							 const Prepared<T>& p, const Prepared<T>& pb, Q<T>& qAb, Q<T>& qBb, T& imAb, T& imBb,
-							 M<T>& iwAb, M<T>& iwBb)
+							 M<T>& iwAb, M<T>& iwBb, ContactBar<T>& cb)
 {
 	for (int s = 0; s < c.pointCount; ++s)
 	{
@@ -516,11 +553,11 @@ M3D_DIFF_HD void prepare_rev(const Contact<T>& c, Q<T> qA, Q<T> qB, const M<T>& 
 		V<T> jBb = madd(pb.jB[s], wb, crossB);
 		mulv_rev(iwA, crossA, jAb, iwAb, cAb);
 		mulv_rev(iwB, crossB, jBb, iwBb, cBb);
-		V<T> rAb = pb.rA[s], rBb = pb.rB[s], nb = vzero<T>();
-		cross_rev(p.rA[s], c.n, cAb, rAb, nb);
-		cross_rev(p.rB[s], c.n, cBb, rBb, nb);
-		arm_rev(c.shapeA, qA, c.la[s], rAb, qAb);
-		arm_rev(c.shapeB, qB, c.lb[s], rBb, qBb);
+		V<T> rAb = pb.rA[s], rBb = pb.rB[s];
+		cross_rev(p.rA[s], c.n, cAb, rAb, cb.n);
+		cross_rev(p.rB[s], c.n, cBb, rBb, cb.n);
+		arm_rev(c.shapeA, c.radiusA, qA, c.la[s], T(1), rAb, qAb, cb.la[s], cb.n);
+		arm_rev(c.shapeB, c.radiusB, qB, c.lb[s], T(-1), rBb, qBb, cb.lb[s], cb.n);
 	}
 }
 
@@ -539,12 +576,14 @@ M3D_DIFF_HD void axisCorrection(V<T>& p, Q<T>& q, T im, T dl, V<T> n, V<T> j)
 }
 // inputs p, q (before); adjoints pb, qb of the outputs in, of the inputs out
 template <typename T>
-M3D_DIFF_HD void axisCorrection_rev(Q<T> q, T im, T dl, V<T> n, V<T> j, V<T>& pb, Q<T>& qb, T& dlb, T& imb, V<T>& jb)
+M3D_DIFF_HD void axisCorrection_rev(Q<T> q, T im, T dl, V<T> n, V<T> j, V<T>& pb, Q<T>& qb, T& dlb, T& imb, V<T>& jb,
+									V<T>& nb)
 {
 	if (im == T(0))
 	{
 		return;
 	}
+	nb = madd(nb, dl * im, pb);
 	T s1b = dot(pb, n);
 	dlb += s1b * im;
 	imb += s1b * dl;
@@ -599,7 +638,7 @@ M3D_DIFF_HD void normals(const Contact<T>& c, const Prepared<T>& p, T imA, T imB
 template <typename T>
 M3D_DIFF_HD void normals_rev(const Contact<T>& c, const Prepared<T>& p, T imA, T imB, T maxCorrection, V<T> pA0, Q<T> qA0,
 							 V<T> pB0, Q<T> qB0, V<T>& pAb, Q<T>& qAb, V<T>& pBb, Q<T>& qBb, const T* lambdaNb,
-							 Prepared<T>& pb, T& imAb, T& imBb)
+							 Prepared<T>& pb, T& imAb, T& imBb, ContactBar<T>& cb)
 {
 	// poses before each point
 	V<T> sA[4], sB[4];
@@ -658,8 +697,8 @@ M3D_DIFF_HD void normals_rev(const Contact<T>& c, const Prepared<T>& p, T imA, T
 		T dl = -sep / wN;
 		// B was corrected first, A second: reverse A, then B
 		T dlAb = T(0), dlBb = T(0);
-		axisCorrection_rev(qA, imA, -dl, c.n, p.jA[s], pAb, qAb, dlAb, imAb, pb.jA[s]);
-		axisCorrection_rev(qB, imB, dl, c.n, p.jB[s], pBb, qBb, dlBb, imBb, pb.jB[s]);
+		axisCorrection_rev(qA, imA, -dl, c.n, p.jA[s], pAb, qAb, dlAb, imAb, pb.jA[s], cb.n);
+		axisCorrection_rev(qB, imB, dl, c.n, p.jB[s], pBb, qBb, dlBb, imBb, pb.jB[s], cb.n);
 		T dlb = dlBb - dlAb + lambdaNb[s];
 		T sepb = T(0);
 		if (capped)
@@ -676,6 +715,10 @@ M3D_DIFF_HD void normals_rev(const Contact<T>& c, const Prepared<T>& p, T imA, T
 		pAb = sub(pAb, gb);
 		rotate_rev_q(qB, c.lb[s], gb, qBb);
 		rotate_rev_q(qA, c.la[s], neg(gb), qAb);
+		cb.off[s] += sepb;
+		cb.n = madd(cb.n, sepb, sub(add(pB, rB), add(pA, rA)));
+		cb.lb[s] = add(cb.lb[s], rotate_rev_v(qB, gb));
+		cb.la[s] = sub(cb.la[s], rotate_rev_v(qA, gb));
 	}
 }
 
@@ -821,9 +864,11 @@ M3D_DIFF_HD bool frictionGate(const Contact<T>& c, const Prepared<T>& p, V<T> va
 	return !(dot(vt, vt) > T(0.1) * T(0.1));
 }
 
+// resetMask (optional) receives the points whose anchors the engine re-seats
+// at the local anchors after this pass (needed > 2 allowed)
 template <typename T>
 M3D_DIFF_HD void friction(const Contact<T>& c, T imA, T imB, const M<T>& iwA, const M<T>& iwB, const T* lambdaN,
-						  V<T>& pA, Q<T>& qA, V<T>& pB, Q<T>& qB, T* lambdaT)
+						  V<T>& pA, Q<T>& qA, V<T>& pB, Q<T>& qB, T* lambdaT, int* resetMask = nullptr)
 {
 	for (int s = 0; s < c.pointCount; ++s)
 	{
@@ -858,6 +903,10 @@ M3D_DIFF_HD void friction(const Contact<T>& c, T imA, T imB, const M<T>& iwA, co
 		V<T> pt = scale(dL, t);
 		positionCorrection(pB, qB, imB, iwB, neg(pt), rB);
 		positionCorrection(pA, qA, imA, iwA, pt, rA);
+		if (resetMask != nullptr && needed > T(2) * allowed)
+		{
+			*resetMask |= 1 << s;
+		}
 	}
 }
 
@@ -865,7 +914,7 @@ template <typename T>
 M3D_DIFF_HD void friction_rev(const Contact<T>& c, T imA, T imB, const M<T>& iwA, const M<T>& iwB, const T* lambdaN,
 							  V<T> pA0, Q<T> qA0, V<T> pB0, Q<T> qB0, const T* lambdaT0, V<T>& pAb, Q<T>& qAb,
 							  V<T>& pBb, Q<T>& qBb, T* lambdaNb, T* lambdaTb, T& muB, T& imAb, T& imBb, M<T>& iwAb,
-							  M<T>& iwBb)
+							  M<T>& iwBb, ContactBar<T>& cb)
 {
 	V<T> sA[4], sB[4];
 	Q<T> tA[4], tB[4];
@@ -976,13 +1025,18 @@ M3D_DIFF_HD void friction_rev(const Contact<T>& c, T imA, T imB, const M<T>& iwA
 		V<T> dptb = scale(inv, tb);
 		ltb += -dot(tb, dpt) * inv * inv;
 		len_rev(dpt, lt, ltb, dptb);
-		V<T> gapb = sub(dptb, scale(dot(dptb, c.n), c.n));
+		// dpt = gap - (gap.n) n
+		T ndp = dot(dptb, c.n);
+		V<T> gapb = sub(dptb, scale(ndp, c.n));
+		cb.n = sub(cb.n, add(scale(gn, dptb), scale(ndp, gap)));
 		pBb = add(pBb, gapb);
 		pAb = sub(pAb, gapb);
 		rBb = add(rBb, gapb);
 		rAb = sub(rAb, gapb);
 		rotate_rev_q(qA, c.fa[s], rAb, qAb);
 		rotate_rev_q(qB, c.fb[s], rBb, qBb);
+		cb.fa[s] = add(cb.fa[s], rotate_rev_v(qA, rAb));
+		cb.fb[s] = add(cb.fb[s], rotate_rev_v(qB, rBb));
 	}
 }
 
@@ -1112,7 +1166,7 @@ struct VelocityBar
 template <typename T>
 M3D_DIFF_HD void velocity_rev(const Contact<T>& c, const Prepared<T>& p, const VelocityIn<T>& in, const T* lambdaN,
 							  V<T> va0, V<T> wa0, V<T> vb0, V<T> wb0, V<T>& vab, V<T>& wab, V<T>& vbb, V<T>& wbb,
-							  Prepared<T>& pb, T* lambdaNb, VelocityBar<T>& b)
+							  Prepared<T>& pb, T* lambdaNb, VelocityBar<T>& b, ContactBar<T>& cb)
 {
 	const T invH = in.h > T(0) ? T(1) / in.h : T(0);
 	// forward, keeping the velocities before each point
@@ -1235,7 +1289,9 @@ M3D_DIFF_HD void velocity_rev(const Contact<T>& c, const Prepared<T>& p, const V
 				V<T> wrollb = scale(inv, axisb);
 				wlb += -dot(axisb, wroll) * inv * inv;
 				len_rev(wroll, wl, wlb, wrollb);
-				V<T> wrelb = sub(wrollb, scale(dot(wrollb, c.n), c.n));
+				T nwr = dot(wrollb, c.n);
+				V<T> wrelb = sub(wrollb, scale(nwr, c.n));
+				cb.n = sub(cb.n, add(scale(wn, wrollb), scale(nwr, wrel)));
 				wbb = add(wbb, wrelb);
 				wab = sub(wab, wrelb);
 				for (int s = 0; s < c.pointCount; ++s)
@@ -1339,6 +1395,7 @@ M3D_DIFF_HD void velocity_rev(const Contact<T>& c, const Prepared<T>& p, const V
 				jb += in.imB * d + dot(wbb, p.jB[s]);
 				b.imB += j * d;
 				pb.jB[s] = madd(pb.jB[s], j, wbb);
+				cb.n = madd(cb.n, j * in.imB, vbb);
 			}
 			if (in.imA != T(0))
 			{
@@ -1347,6 +1404,7 @@ M3D_DIFF_HD void velocity_rev(const Contact<T>& c, const Prepared<T>& p, const V
 				T mjb = in.imA * d + dot(wab, p.jA[s]);
 				b.imA += mj * d;
 				pb.jA[s] = madd(pb.jA[s], mj, wab);
+				cb.n = madd(cb.n, mj * in.imA, vab);
 				jb -= mjb;
 			}
 			T targetb = jb / wN;
@@ -1361,12 +1419,14 @@ M3D_DIFF_HD void velocity_rev(const Contact<T>& c, const Prepared<T>& p, const V
 					b.e += eb;
 				}
 				V<T> vrelPrevb = scale(vnPrevb, c.n);
+				cb.n = madd(cb.n, vnPrevb, vrelPrev);
 				b.pvb = add(b.pvb, vrelPrevb);
 				cross_rev(in.pwb, rBf, vrelPrevb, b.pwb, rBfb);
 				b.pva = sub(b.pva, vrelPrevb);
 				cross_rev(in.pwa, rAf, neg(vrelPrevb), b.pwa, rAfb);
 			}
 			V<T> vrel2b = scale(vn2b, c.n);
+			cb.n = madd(cb.n, vn2b, vrel2);
 			vb1b = add(vb1b, vrel2b);
 			cross_rev(wb1, rBf, vrel2b, wb1b, rBfb);
 			va1b = sub(va1b, vrel2b);
@@ -1416,7 +1476,9 @@ M3D_DIFF_HD void velocity_rev(const Contact<T>& c, const Prepared<T>& p, const V
 			V<T> vtb = scale(T(1) / vtLen, tb);
 			vtLenb += -dot(tb, vt) / (vtLen * vtLen);
 			len_rev(vt, vtLen, vtLenb, vtb);
-			V<T> vrelb = sub(vtb, scale(dot(vtb, c.n), c.n));
+			T nvt = dot(vtb, c.n);
+			V<T> vrelb = sub(vtb, scale(nvt, c.n));
+			cb.n = sub(cb.n, add(scale(vn, vtb), scale(nvt, vrel)));
 			vbb0 = add(vbb0, vrelb);
 			cross_rev(wb, rBf, vrelb, wbb0, rBfb);
 			vab0 = sub(vab0, vrelb);
@@ -1429,8 +1491,8 @@ M3D_DIFF_HD void velocity_rev(const Contact<T>& c, const Prepared<T>& p, const V
 		// arms
 		if (c.curved)
 		{
-			arm_rev(c.shapeA, in.qA, c.la[s], rAfb, b.qA);
-			arm_rev(c.shapeB, in.qB, c.lb[s], rBfb, b.qB);
+			arm_rev(c.shapeA, c.radiusA, in.qA, c.la[s], T(1), rAfb, b.qA, cb.la[s], cb.n);
+			arm_rev(c.shapeB, c.radiusB, in.qB, c.lb[s], T(-1), rBfb, b.qB, cb.lb[s], cb.n);
 		}
 		else
 		{
@@ -1439,6 +1501,13 @@ M3D_DIFF_HD void velocity_rev(const Contact<T>& c, const Prepared<T>& p, const V
 		}
 	}
 }
+
+} // namespace m3d_diff
+
+#include "m3d_diff_gen.h"
+
+namespace m3d_diff
+{
 
 // ---- one island through one recorded step ------------------------------------
 
@@ -1450,6 +1519,21 @@ struct TapeContact
 	float n[3];
 	float mu, e, rolling;
 	float la[4][3], lb[4][3], off[4], fa[4][3], fb[4][3], slip[4][3];
+	uint32_t id[4]; // feature ids of the points
+	int32_t gen;    // kTapeGen* bits: how this substep's manifold came to be
+};
+
+// manifold generation events of a contact record
+constexpr int32_t kTapeGenNarrow = 1;  // regenerated by the step's narrowphase at the step-start poses (substep 0)
+constexpr int32_t kTapeGenPrepare = 2; // regenerated by this substep's contact preparation at the integrated poses
+constexpr int32_t kTapeGenHeld = 4;    // held by the tunnelling guard (no generation)
+
+// shape of a body, for manifold generation
+struct TapeShape
+{
+	int32_t type;
+	float radius;
+	float he[3];
 };
 
 template <typename T>
@@ -1501,6 +1585,7 @@ struct PoseRec
 	Q<T> qA, qB;
 	T lam[4];
 	int gate;
+	int reset; // points whose stiction anchors the pass re-seated at the local anchors
 };
 template <typename T>
 struct VelRec
@@ -1553,7 +1638,28 @@ struct IslandCtx
 	T* lamTBar;
 	const T* muBody; // per body friction and restitution (to split contact values)
 	const T* eBody;
+	// manifold data as state
+	ContactBar<T>* cbar;             // per position: adjoint of the contact's manifold data
+	const TapeShape* shapes;         // per body
+	const TapeContact* prevContacts; // the previous step's records (its last substep), or null
+	const int32_t* prevPos;          // per position: the contact's position in the previous step, or -1
+	T dt;                            // step length (narrowphase margin)
+	// regenerating replay (verification): when set, the manifolds are state
+	// carried here and regenerated at the recorded generation events instead
+	// of read from the tape
+	Contact<T>* live;
+	uint32_t* liveIds; // 4 per position
 };
+
+template <typename T>
+M3D_DIFF_HD Contact<T> contactOf(const IslandCtx<T>& x, const TapeContact* tc, int pos)
+{
+	return x.live != nullptr ? x.live[pos] : loadContact<T>(tc[pos]);
+}
+
+template <typename T>
+M3D_DIFF_HD void regenerateLive(const IslandCtx<T>& x, const TapeContact& rec, int pos, V<T> xA, Q<T> qA, V<T> xB,
+								Q<T> qB, T margin);
 
 template <typename T>
 M3D_DIFF_HD void substepForward(const IslandCtx<T>& x, const TapeIsland& r, int sub, bool record)
@@ -1572,10 +1678,29 @@ M3D_DIFF_HD void substepForward(const IslandCtx<T>& x, const TapeIsland& r, int 
 		x.cur[i] = s1;
 	}
 	const TapeContact* tc = x.contacts + (size_t)sub * x.contactsPerSubstep;
+	if (x.live != nullptr)
+	{
+		for (int j = 0; j < r.contactCount; ++j)
+		{
+			const int pos = r.contactStart + j;
+			if (tc[pos].gen & kTapeGenPrepare)
+			{
+				const Body<T>& A = x.cur[tc[pos].a];
+				const Body<T>& B = x.cur[tc[pos].b];
+				regenerateLive(x, tc[pos], pos, A.x, A.q, B.x, B.q,
+							   T(kGenSpeculativeBase) + x.h * len(m3d_diff::sub(A.v, B.v)));
+			}
+			// slip directions only steer branches: as the engine had them
+			for (int q = 0; q < 4; ++q)
+			{
+				x.live[pos].slip[q] = tv<T>(tc[pos].slip[q]);
+			}
+		}
+	}
 	for (int j = 0; j < r.contactCount; ++j)
 	{
 		int pos = r.contactStart + j;
-		Contact<T> c = loadContact<T>(tc[pos]);
+		Contact<T> c = contactOf(x, tc, pos);
 		Prepared<T>& p = x.prep[pos];
 		preparedZero(p);
 		prepare(c, x.cur[c.a].q, x.cur[c.b].q, bc[c.a].invMass, bc[c.b].invMass, x.iw[c.a], x.iw[c.b], p);
@@ -1590,7 +1715,7 @@ M3D_DIFF_HD void substepForward(const IslandCtx<T>& x, const TapeIsland& r, int 
 		for (int j = 0; j < r.contactCount; ++j)
 		{
 			int pos = r.contactStart + j;
-			Contact<T> c = loadContact<T>(tc[pos]);
+			Contact<T> c = contactOf(x, tc, pos);
 			if (record)
 			{
 				PoseRec<T>& rec = x.normRec[(size_t)it * x.positions + pos];
@@ -1610,7 +1735,7 @@ M3D_DIFF_HD void substepForward(const IslandCtx<T>& x, const TapeIsland& r, int 
 	for (int j = 0; j < r.contactCount; ++j)
 	{
 		int pos = r.contactStart + j;
-		Contact<T> c = loadContact<T>(tc[pos]);
+		Contact<T> c = contactOf(x, tc, pos);
 		bool gate = frictionGate(c, x.prep[pos], x.cur[c.a].v, x.cur[c.a].w, x.cur[c.b].v, x.cur[c.b].w);
 		if (record)
 		{
@@ -1625,10 +1750,29 @@ M3D_DIFF_HD void substepForward(const IslandCtx<T>& x, const TapeIsland& r, int 
 			}
 			rec.gate = gate ? 1 : 0;
 		}
+		// a sliding box-box contact re-seats all its anchors instead
+		int reset = c.shapeA == kShapeBox && c.shapeB == kShapeBox && c.pointCount > 0 && !gate
+						? (1 << c.pointCount) - 1
+						: 0;
 		if (gate)
 		{
 			friction(c, bc[c.a].invMass, bc[c.b].invMass, x.iw[c.a], x.iw[c.b], x.lamN + 4 * pos, x.cur[c.a].x,
-					 x.cur[c.a].q, x.cur[c.b].x, x.cur[c.b].q, x.lamT + 4 * pos);
+					 x.cur[c.a].q, x.cur[c.b].x, x.cur[c.b].q, x.lamT + 4 * pos, &reset);
+		}
+		if (record)
+		{
+			x.fricRec[pos].reset = reset;
+		}
+		if (x.live != nullptr)
+		{
+			for (int q = 0; q < 4; ++q)
+			{
+				if ((reset >> q) & 1)
+				{
+					x.live[pos].fa[q] = x.live[pos].la[q];
+					x.live[pos].fb[q] = x.live[pos].lb[q];
+				}
+			}
 		}
 	}
 	for (int k = 0; k < r.bodyCount; ++k)
@@ -1646,7 +1790,7 @@ M3D_DIFF_HD void substepForward(const IslandCtx<T>& x, const TapeIsland& r, int 
 	for (int j = 0; j < r.contactCount; ++j)
 	{
 		int pos = r.contactStart + j;
-		Contact<T> c = loadContact<T>(tc[pos]);
+		Contact<T> c = contactOf(x, tc, pos);
 		if (record)
 		{
 			VelRec<T>& rec = x.velRec[pos];
@@ -1698,12 +1842,225 @@ M3D_DIFF_HD void scatterMaterials(const IslandCtx<T>& x, const Contact<T>& c, T 
 	{
 		x.muBar[c.b] += muB * T(0.5) * c.mu / mb;
 	}
-	// restitution: the larger of the two (A on ties, as the reference)
-	const int who = x.eBody[c.a] > x.eBody[c.b] ? c.a : (x.eBody[c.a] == x.eBody[c.b] ? c.a : c.b);
+	// restitution: the larger of the two, B's on ties, as contact creation
+	// picks it (reference src/world.cpp:1540-1568)
+	const int who = x.eBody[c.a] > x.eBody[c.b] ? c.a : c.b;
 	if (x.bc[who].dynamic)
 	{
 		x.eBar[who] += eB;
 	}
+}
+
+// ---- manifold generation events ---------------------------------------------------
+
+template <typename T, int N>
+M3D_DIFF_HD Dual<T, N> seeded(T v, int k)
+{
+	Dual<T, N> r(v);
+	r.d[k] = T(1);
+	return r;
+}
+
+// Adds to the pose adjoints of the contact's bodies the adjoint that the
+// manifold data carries (cb: normal, local anchors, separation offsets),
+// through the generation at poses (xA, qA), (xB, qB) with the given margin.
+// Points are matched to the recorded ones by feature id.
+template <typename T>
+M3D_DIFF_HD void generationAdjoint(const IslandCtx<T>& x, const TapeContact& rec, V<T> xA, Q<T> qA, V<T> xB, Q<T> qB,
+								   T margin, const ContactBar<T>& cb)
+{
+	typedef Dual<T, 14> S;
+	const int a = rec.a, b = rec.b;
+	const bool dynA = x.bc[a].dynamic != 0, dynB = x.bc[b].dynamic != 0;
+	if ((!dynA && !dynB) || rec.pointCount == 0)
+	{
+		return;
+	}
+	GenShape<S> sa, sb;
+	sa.type = x.shapes[a].type;
+	sa.radius = S(T(x.shapes[a].radius));
+	sa.he = v3<S>(S(T(x.shapes[a].he[0])), S(T(x.shapes[a].he[1])), S(T(x.shapes[a].he[2])));
+	sb.type = x.shapes[b].type;
+	sb.radius = S(T(x.shapes[b].radius));
+	sb.he = v3<S>(S(T(x.shapes[b].he[0])), S(T(x.shapes[b].he[1])), S(T(x.shapes[b].he[2])));
+	V<S> gxA = v3<S>(seeded<T, 14>(xA.x, 0), seeded<T, 14>(xA.y, 1), seeded<T, 14>(xA.z, 2));
+	Q<S> gqA = q4<S>(seeded<T, 14>(qA.x, 3), seeded<T, 14>(qA.y, 4), seeded<T, 14>(qA.z, 5), seeded<T, 14>(qA.w, 6));
+	V<S> gxB = v3<S>(seeded<T, 14>(xB.x, 7), seeded<T, 14>(xB.y, 8), seeded<T, 14>(xB.z, 9));
+	Q<S> gqB =
+		q4<S>(seeded<T, 14>(qB.x, 10), seeded<T, 14>(qB.y, 11), seeded<T, 14>(qB.z, 12), seeded<T, 14>(qB.w, 13));
+	GenManifold<S> g;
+	genManifold(sa, gxA, gqA, sb, gxB, gqB, S(margin), g);
+	T acc[14];
+	for (int k = 0; k < 14; ++k)
+	{
+		acc[k] = T(0);
+	}
+	const bool sameNormal =
+		g.count > 0 && g.n.x.v * T(rec.n[0]) + g.n.y.v * T(rec.n[1]) + g.n.z.v * T(rec.n[2]) > T(0.999);
+	if (!sameNormal)
+	{
+		return;
+	}
+	for (int k = 0; k < 14; ++k)
+	{
+		acc[k] += cb.n.x * g.n.x.d[k] + cb.n.y * g.n.y.d[k] + cb.n.z * g.n.z.d[k];
+	}
+	for (int i = 0; i < rec.pointCount; ++i)
+	{
+		int j = -1;
+		for (int q = 0; q < g.count; ++q)
+		{
+			if (g.p[q].id == rec.id[i])
+			{
+				j = q;
+				break;
+			}
+		}
+		if (j < 0)
+		{
+			continue;
+		}
+		const GenPoint<S>& gp = g.p[j];
+		for (int k = 0; k < 14; ++k)
+		{
+			acc[k] += cb.la[i].x * gp.la.x.d[k] + cb.la[i].y * gp.la.y.d[k] + cb.la[i].z * gp.la.z.d[k] +
+					  cb.lb[i].x * gp.lb.x.d[k] + cb.lb[i].y * gp.lb.y.d[k] + cb.lb[i].z * gp.lb.z.d[k] +
+					  cb.off[i] * gp.off.d[k];
+		}
+	}
+	if (dynA)
+	{
+		x.adj[a].x = add(x.adj[a].x, v3<T>(acc[0], acc[1], acc[2]));
+		x.adj[a].q = qadd(x.adj[a].q, q4<T>(acc[3], acc[4], acc[5], acc[6]));
+	}
+	if (dynB)
+	{
+		x.adj[b].x = add(x.adj[b].x, v3<T>(acc[7], acc[8], acc[9]));
+		x.adj[b].q = qadd(x.adj[b].q, q4<T>(acc[10], acc[11], acc[12], acc[13]));
+	}
+}
+
+// The stiction anchors a generated manifold starts with are fresh (equal to
+// its local anchors) or kept from the old point with the same feature id.
+// Moves the anchor adjoints of cb accordingly: fresh ones onto the local
+// anchors, kept ones into cbOld (the adjoint of the old manifold, whose point
+// order oldIds gives; null: the old manifold is not on the tape and kept
+// anchors count as constants).  cb's anchor adjoints end at zero.
+template <typename T>
+M3D_DIFF_HD void generationAnchors(const TapeContact& rec, const uint32_t* oldIds, int oldCount, ContactBar<T>& cb,
+								   ContactBar<T>& cbOld)
+{
+	contactBarZero(cbOld);
+	for (int i = 0; i < rec.pointCount; ++i)
+	{
+		bool fresh = true;
+		for (int k = 0; k < 3; ++k)
+		{
+			fresh = fresh && rec.fa[i][k] == rec.la[i][k] && rec.fb[i][k] == rec.lb[i][k];
+		}
+		if (fresh)
+		{
+			cb.la[i] = add(cb.la[i], cb.fa[i]);
+			cb.lb[i] = add(cb.lb[i], cb.fb[i]);
+		}
+		else if (oldIds != nullptr)
+		{
+			for (int j = 0; j < oldCount; ++j)
+			{
+				if (oldIds[j] == rec.id[i])
+				{
+					cbOld.fa[j] = add(cbOld.fa[j], cb.fa[i]);
+					cbOld.fb[j] = add(cbOld.fb[j], cb.fb[i]);
+					break;
+				}
+			}
+		}
+		cb.fa[i] = vzero<T>();
+		cb.fb[i] = vzero<T>();
+	}
+}
+
+// A generation event of a contact: anchors, then the Jacobian at the
+// generation poses; cb becomes the old manifold's adjoint.
+template <typename T>
+M3D_DIFF_HD void reverseGeneration(const IslandCtx<T>& x, const TapeContact& rec, const TapeContact* old, V<T> xA,
+								   Q<T> qA, V<T> xB, Q<T> qB, T margin, ContactBar<T>& cb)
+{
+	ContactBar<T> cbOld;
+	generationAnchors(rec, old != nullptr ? old->id : nullptr, old != nullptr ? old->pointCount : 0, cb, cbOld);
+	generationAdjoint(x, rec, xA, qA, xB, qB, margin, cb);
+	cb = cbOld;
+}
+
+// Regeneration of a live manifold (regenerating replay): the engine's
+// collision at the given poses, then the inheritance of slip directions and,
+// box-box only, of stiction anchors that have neither slipped nor drifted
+// from the old manifold (reference src/collide.cpp:865-913).
+template <typename T>
+M3D_DIFF_HD void regenerateLive(const IslandCtx<T>& x, const TapeContact& rec, int pos, V<T> xA, Q<T> qA, V<T> xB,
+								Q<T> qB, T margin)
+{
+	Contact<T>& c = x.live[pos];
+	uint32_t* ids = x.liveIds + 4 * pos;
+	const Contact<T> old = c;
+	const uint32_t oldIds[4] = { ids[0], ids[1], ids[2], ids[3] };
+	GenShape<T> sa, sb;
+	sa.type = x.shapes[rec.a].type;
+	sa.radius = T(x.shapes[rec.a].radius);
+	sa.he = v3<T>(T(x.shapes[rec.a].he[0]), T(x.shapes[rec.a].he[1]), T(x.shapes[rec.a].he[2]));
+	sb.type = x.shapes[rec.b].type;
+	sb.radius = T(x.shapes[rec.b].radius);
+	sb.he = v3<T>(T(x.shapes[rec.b].he[0]), T(x.shapes[rec.b].he[1]), T(x.shapes[rec.b].he[2]));
+	GenManifold<T> g;
+	genManifold(sa, xA, qA, sb, xB, qB, margin, g);
+	const bool boxBox = sa.type == kShapeBox && sb.type == kShapeBox;
+	c.pointCount = g.count;
+	c.n = g.n;
+	for (int i = 0; i < g.count; ++i)
+	{
+		c.la[i] = g.p[i].la;
+		c.lb[i] = g.p[i].lb;
+		c.off[i] = g.p[i].off;
+		c.fa[i] = c.la[i];
+		c.fb[i] = c.lb[i];
+		c.slip[i] = vzero<T>();
+		ids[i] = g.p[i].id;
+		for (int j = 0; j < old.pointCount; ++j)
+		{
+			if (oldIds[j] != ids[i])
+			{
+				continue;
+			}
+			c.slip[i] = old.slip[j];
+			if (!boxBox)
+			{
+				break;
+			}
+			V<T> pAold = add(rotate(qA, old.fa[j]), xA);
+			V<T> pBold = add(rotate(qB, old.fb[j]), xB);
+			V<T> pAnew = add(rotate(qA, c.la[i]), xA);
+			V<T> gap = sub(pBold, pAold);
+			V<T> dpt = sub(gap, scale(dot(gap, c.n), c.n));
+			V<T> drift = sub(pAold, pAnew);
+			if (dot(dpt, dpt) < T(0.02f * 0.02f) && dot(drift, drift) < T(0.05f * 0.05f))
+			{
+				c.fa[i] = old.fa[j];
+				c.fb[i] = old.fb[j];
+			}
+			break;
+		}
+	}
+}
+
+// the record of a contact before the step (its previous step's last substep), or null
+template <typename T>
+M3D_DIFF_HD const TapeContact* previousRecord(const IslandCtx<T>& x, int pos)
+{
+	if (x.prevContacts == nullptr || x.prevPos == nullptr || x.prevPos[pos] < 0)
+	{
+		return nullptr;
+	}
+	return x.prevContacts + x.prevPos[pos];
 }
 
 template <typename T>
@@ -1762,7 +2119,7 @@ M3D_DIFF_HD void substepReverse(const IslandCtx<T>& x, const TapeIsland& r, int 
 		V<T>& vbb = bc[c.b].dynamic ? x.adj[c.b].v : dummy2;
 		V<T>& wbb = bc[c.b].dynamic ? x.adj[c.b].w : dummy3;
 		velocity_rev(c, x.prep[pos], in, x.lamN + 4 * pos, rec.va, rec.wa, rec.vb, rec.wb, vab, wab, vbb, wbb,
-					 x.prepBar[pos], x.lamNBar + 4 * pos, b);
+					 x.prepBar[pos], x.lamNBar + 4 * pos, b, x.cbar[pos]);
 		if (bc[c.a].dynamic)
 		{
 			x.imBar[c.a] += b.imA;
@@ -1804,6 +2161,18 @@ M3D_DIFF_HD void substepReverse(const IslandCtx<T>& x, const TapeIsland& r, int 
 	{
 		int pos = r.contactStart + j;
 		const PoseRec<T>& rec = x.fricRec[pos];
+		ContactBar<T>& cb = x.cbar[pos];
+		for (int s = 0; s < 4; ++s)
+		{
+			if ((rec.reset >> s) & 1)
+			{
+				// re-seated anchors: fa = la, fb = lb after the pass
+				cb.la[s] = add(cb.la[s], cb.fa[s]);
+				cb.lb[s] = add(cb.lb[s], cb.fb[s]);
+				cb.fa[s] = vzero<T>();
+				cb.fb[s] = vzero<T>();
+			}
+		}
 		if (!rec.gate)
 		{
 			continue;
@@ -1821,7 +2190,7 @@ M3D_DIFF_HD void substepReverse(const IslandCtx<T>& x, const TapeIsland& r, int 
 		iwBb = iwAb;
 		friction_rev(c, bc[c.a].invMass, bc[c.b].invMass, x.iw[c.a], x.iw[c.b], x.lamN + 4 * pos, rec.pA, rec.qA, rec.pB,
 					 rec.qB, rec.lam, pAb, qAb, pBb, qBb, x.lamNBar + 4 * pos, x.lamTBar + 4 * pos, muB, imAb, imBb, iwAb,
-					 iwBb);
+					 iwBb, cb);
 		if (bc[c.a].dynamic)
 		{
 			x.imBar[c.a] += imAb;
@@ -1858,7 +2227,7 @@ M3D_DIFF_HD void substepReverse(const IslandCtx<T>& x, const TapeIsland& r, int 
 			Q<T>& qBb = bc[c.b].dynamic ? x.adj[c.b].q : e1;
 			T imAb = T(0), imBb = T(0);
 			normals_rev(c, x.prep[pos], bc[c.a].invMass, bc[c.b].invMass, x.maxCorrection, rec.pA, rec.qA, rec.pB,
-						rec.qB, pAb, qAb, pBb, qBb, x.lamNBar + 4 * pos, x.prepBar[pos], imAb, imBb);
+						rec.qB, pAb, qAb, pBb, qBb, x.lamNBar + 4 * pos, x.prepBar[pos], imAb, imBb, x.cbar[pos]);
 			if (bc[c.a].dynamic)
 			{
 				x.imBar[c.a] += imAb;
@@ -1874,36 +2243,26 @@ M3D_DIFF_HD void substepReverse(const IslandCtx<T>& x, const TapeIsland& r, int 
 	{
 		int pos = r.contactStart + j;
 		Contact<T> c = loadContact<T>(tc[pos]);
-		Q<T> qA1 = x.start[(size_t)sub * x.bodyCount + c.a].q, qB1 = x.start[(size_t)sub * x.bodyCount + c.b].q;
-		// the rotation at preparation is the integrated one, rebuilt here
+		// the states at preparation are the integrated ones, rebuilt here
+		Body<T> sA = x.cur[c.a], sB = x.cur[c.b];
 		if (bc[c.a].dynamic)
 		{
-			Body<T> s1;
 			M<T> iw;
-			integrate(x.start[(size_t)sub * x.bodyCount + c.a], bc[c.a], x.h, x.g, s1, iw);
-			qA1 = s1.q;
-		}
-		else
-		{
-			qA1 = x.cur[c.a].q;
+			integrate(x.start[(size_t)sub * x.bodyCount + c.a], bc[c.a], x.h, x.g, sA, iw);
 		}
 		if (bc[c.b].dynamic)
 		{
-			Body<T> s1;
 			M<T> iw;
-			integrate(x.start[(size_t)sub * x.bodyCount + c.b], bc[c.b], x.h, x.g, s1, iw);
-			qB1 = s1.q;
+			integrate(x.start[(size_t)sub * x.bodyCount + c.b], bc[c.b], x.h, x.g, sB, iw);
 		}
-		else
-		{
-			qB1 = x.cur[c.b].q;
-		}
+		const Q<T> qA1 = sA.q, qB1 = sB.q;
 		Q<T> qAb = qzero<T>(), qBb = qzero<T>();
 		T imAb = T(0), imBb = T(0);
 		M<T> iwAb, iwBb;
 		iwAb.cx = iwAb.cy = iwAb.cz = vzero<T>();
 		iwBb = iwAb;
-		prepare_rev(c, qA1, qB1, x.iw[c.a], x.iw[c.b], x.prep[pos], x.prepBar[pos], qAb, qBb, imAb, imBb, iwAb, iwBb);
+		prepare_rev(c, qA1, qB1, x.iw[c.a], x.iw[c.b], x.prep[pos], x.prepBar[pos], qAb, qBb, imAb, imBb, iwAb, iwBb,
+					x.cbar[pos]);
 		if (bc[c.a].dynamic)
 		{
 			x.adj[c.a].q = qadd(x.adj[c.a].q, qAb);
@@ -1919,6 +2278,16 @@ M3D_DIFF_HD void substepReverse(const IslandCtx<T>& x, const TapeIsland& r, int 
 			x.iwBar[c.b].cx = add(x.iwBar[c.b].cx, iwBb.cx);
 			x.iwBar[c.b].cy = add(x.iwBar[c.b].cy, iwBb.cy);
 			x.iwBar[c.b].cz = add(x.iwBar[c.b].cz, iwBb.cz);
+		}
+		if (tc[pos].gen & kTapeGenPrepare)
+		{
+			// regenerated at the integrated poses; the manifold before it is
+			// the previous substep's, or for substep 0 the one the step began
+			// with (not on the tape when the narrowphase regenerated it too)
+			const TapeContact* old = sub > 0 ? &x.contacts[(size_t)(sub - 1) * x.contactsPerSubstep + pos]
+											 : ((tc[pos].gen & kTapeGenNarrow) ? nullptr : previousRecord(x, pos));
+			const T margin = T(kGenSpeculativeBase) + x.h * len(m3d_diff::sub(sA.v, sB.v));
+			reverseGeneration(x, tc[pos], old, sA.x, sA.q, sB.x, sB.q, margin, x.cbar[pos]);
 		}
 	}
 	// integration
@@ -1977,6 +2346,20 @@ M3D_DIFF_HD void islandStepBackward(const IslandCtx<T>& x)
 		if (x.bc[i].dynamic)
 		{
 			x.cur[i] = x.start[i];
+		}
+	}
+	// manifolds the step's narrowphase regenerated at the step-start poses
+	// (margin from the step-start velocities, as the narrowphase takes it)
+	for (int j = 0; j < r.contactCount; ++j)
+	{
+		const int pos = r.contactStart + j;
+		const TapeContact& rec = x.contacts[pos];
+		if ((rec.gen & kTapeGenNarrow) && !(rec.gen & kTapeGenPrepare))
+		{
+			const Body<T>& A = x.cur[rec.a];
+			const Body<T>& B = x.cur[rec.b];
+			const T margin = T(kGenSpeculativeBase) + x.dt * len(m3d_diff::sub(A.v, B.v));
+			reverseGeneration(x, rec, previousRecord(x, pos), A.x, A.q, B.x, B.q, margin, x.cbar[pos]);
 		}
 	}
 }

@@ -127,6 +127,112 @@ Contact<D> randomContact(Rng& g, int pc, int shapeA, int shapeB, int curved)
 	return c;
 }
 
+
+// contact manifold data as a flat vector: n, la[4], lb[4], off[4], fa[4], fb[4]
+void putContactData(std::vector<D>& v, const Contact<D>& c)
+{
+	put(v, c.n);
+	for (int s = 0; s < 4; ++s)
+		put(v, c.la[s]);
+	for (int s = 0; s < 4; ++s)
+		put(v, c.lb[s]);
+	for (int s = 0; s < 4; ++s)
+		v.push_back(c.off[s]);
+	for (int s = 0; s < 4; ++s)
+		put(v, c.fa[s]);
+	for (int s = 0; s < 4; ++s)
+		put(v, c.fb[s]);
+}
+void getContactData(const std::vector<D>& v, size_t& i, Contact<D>& c)
+{
+	c.n = getv(v, i);
+	for (int s = 0; s < 4; ++s)
+		c.la[s] = getv(v, i);
+	for (int s = 0; s < 4; ++s)
+		c.lb[s] = getv(v, i);
+	for (int s = 0; s < 4; ++s)
+		c.off[s] = v[i++];
+	for (int s = 0; s < 4; ++s)
+		c.fa[s] = getv(v, i);
+	for (int s = 0; s < 4; ++s)
+		c.fb[s] = getv(v, i);
+}
+void putBar(std::vector<D>& v, const ContactBar<D>& b)
+{
+	put(v, b.n);
+	for (int s = 0; s < 4; ++s)
+		put(v, b.la[s]);
+	for (int s = 0; s < 4; ++s)
+		put(v, b.lb[s]);
+	for (int s = 0; s < 4; ++s)
+		v.push_back(b.off[s]);
+	for (int s = 0; s < 4; ++s)
+		put(v, b.fa[s]);
+	for (int s = 0; s < 4; ++s)
+		put(v, b.fb[s]);
+}
+
+// poses of a touching pair: kind 0 box-box face (stacked, tilted), 1 box-box
+// edge (crossed, rotated 45 deg), 2 sphere-box, 3 box-sphere (flipped order),
+// 4 sphere-sphere
+void pairFor(int kind, Rng& g, GenShape<D>& a, GenShape<D>& b, V<D>& xA, Q<D>& qA, V<D>& xB, Q<D>& qB)
+{
+	auto smallRot = [&](double ang) {
+		V<D> ax = rv(g, 1);
+		ax = scale(1.0 / len(ax), ax);
+		double t = g.r(-ang, ang);
+		return q4<D>(sin(t) * ax.x, sin(t) * ax.y, sin(t) * ax.z, cos(t));
+	};
+	a.type = b.type = kShapeBox;
+	a.radius = b.radius = 0;
+	a.he = v3<D>(g.r(0.2, 0.4), g.r(0.2, 0.4), g.r(0.2, 0.4));
+	b.he = v3<D>(g.r(0.2, 0.4), g.r(0.2, 0.4), g.r(0.2, 0.4));
+	xA = rv(g, 0.1);
+	qA = smallRot(0.05);
+	qB = smallRot(0.05);
+	if (kind == 0)
+	{
+		xB = add(xA, v3<D>(g.r(-0.05, 0.05), a.he.y + b.he.y - 0.005, g.r(-0.05, 0.05)));
+	}
+	else if (kind == 1)
+	{
+		a.he = b.he = v3<D>(0.3, 0.3, 0.3);
+		Q<D> ra = q4<D>(sin(M_PI / 8), 0, 0, cos(M_PI / 8)); // 45 deg about x
+		Q<D> rb = q4<D>(0, 0, sin(M_PI / 8), cos(M_PI / 8)); // 45 deg about z
+		qA = qmul(smallRot(0.02), ra);
+		qB = qmul(smallRot(0.02), rb);
+		xB = add(xA, v3<D>(g.r(-0.02, 0.02), 2 * 0.3 * sqrt(2.0) - 0.01, g.r(-0.02, 0.02)));
+	}
+	else if (kind == 2 || kind == 3)
+	{
+		GenShape<D> sph;
+		sph.type = kShapeSphere;
+		sph.radius = g.r(0.1, 0.3);
+		sph.he = vzero<D>();
+		GenShape<D> box = b;
+		V<D> xs = add(xA, v3<D>(g.r(-0.1, 0.1), box.he.y + sph.radius - 0.005, g.r(-0.1, 0.1)));
+		if (kind == 2)
+		{
+			a = sph, b = box;
+			xB = xA;
+			xA = xs;
+		}
+		else
+		{
+			a = box, b = sph;
+			xB = xs;
+		}
+	}
+	else
+	{
+		a.type = b.type = kShapeSphere;
+		a.radius = g.r(0.1, 0.3);
+		b.radius = g.r(0.1, 0.3);
+		V<D> dir = rv(g, 1);
+		dir = scale(1.0 / len(dir), dir);
+		xB = madd(xA, a.radius + b.radius - 0.004, dir);
+	}
+}
 } // namespace
 
 extern "C"
@@ -271,7 +377,9 @@ double check_prepare(uint64_t seed)
 	M<D> iwAb, iwBb;
 	iwAb.cx = iwAb.cy = iwAb.cz = vzero<D>();
 	iwBb = iwAb;
-	prepare_rev(c, qA, qB, iwA, iwB, p, pb, qAb, qBb, imAb, imBb, iwAb, iwBb);
+	ContactBar<D> cbar;
+	contactBarZero(cbar);
+	prepare_rev(c, qA, qB, iwA, iwB, p, pb, qAb, qBb, imAb, imBb, iwAb, iwBb, cbar);
 	std::vector<D> grad;
 	put(grad, qAb), put(grad, qBb);
 	grad.push_back(imAb), grad.push_back(imBb);
@@ -353,7 +461,9 @@ double check_normals(uint64_t seed)
 	Prepared<D> pb;
 	preparedZero(pb);
 	D imAb = 0, imBb = 0;
-	normals_rev(c, pp, ia, ib, maxC, a, qa, b, qb, pAb, qAb, pBb, qBb, lamb, pb, imAb, imBb);
+	ContactBar<D> cbar;
+	contactBarZero(cbar);
+	normals_rev(c, pp, ia, ib, maxC, a, qa, b, qb, pAb, qAb, pBb, qBb, lamb, pb, imAb, imBb, cbar);
 	std::vector<D> grad;
 	put(grad, pAb), put(grad, qAb), put(grad, pBb), put(grad, qBb);
 	for (int s = 0; s < 4; ++s)
@@ -427,8 +537,10 @@ double check_friction(uint64_t seed)
 	M<D> iwAb, iwBb;
 	iwAb.cx = iwAb.cy = iwAb.cz = vzero<D>();
 	iwBb = iwAb;
+	ContactBar<D> cbar;
+	contactBarZero(cbar);
 	friction_rev(c, imA, imB, iwA, iwB, lamN, pA, qA, pB, qB, lamT, pAb, qAb, pBb, qBb, lNb, lTb, muB, imAb, imBb, iwAb,
-				 iwBb);
+				 iwBb, cbar);
 	std::vector<D> grad;
 	put(grad, pAb), put(grad, qAb), put(grad, pBb), put(grad, qBb);
 	for (int s = 0; s < 4; ++s)
@@ -578,7 +690,9 @@ double check_velocity(uint64_t seed)
 	b.iwB = b.iwA;
 	b.qA = b.qB = qzero<D>();
 	b.pva = b.pwa = b.pvb = b.pwb = vzero<D>();
-	velocity_rev(c, p, in, lamN, va, wa, vb, wb, vab, wab, vbb, wbb, pb, lNb, b);
+	ContactBar<D> cbar;
+	contactBarZero(cbar);
+	velocity_rev(c, p, in, lamN, va, wa, vb, wb, vab, wab, vbb, wbb, pb, lNb, b, cbar);
 	std::vector<D> grad;
 	put(grad, vab), put(grad, wab), put(grad, vbb), put(grad, wbb);
 	put(grad, b.pva), put(grad, b.pwa), put(grad, b.pvb), put(grad, b.pwb);
@@ -599,4 +713,322 @@ double check_velocity(uint64_t seed)
 	return fdCompare(x, grad, f, &skip);
 }
 
+
+// ---- adjoints of the manifold data (normal, anchors, offsets) ----------------------
+
+double check_prepare_contact(uint64_t seed)
+{
+	Rng g{ seed };
+	int curved = (int)(seed % 2);
+	Contact<D> c = randomContact(g, 1 + (int)(seed % 4), curved ? kShapeSphere : kShapeBox, kShapeBox, curved);
+	Q<D> qA = rq(g), qB = rq(g);
+	D imA = g.r(0.5, 2), imB = g.r(0.5, 2);
+	M<D> iwA = rm(g), iwB = rm(g);
+	std::vector<D> x;
+	putContactData(x, c);
+	std::vector<D> w(4 * 13);
+	for (auto& v : w)
+		v = g.r(-1, 1);
+	auto outv = [&](const Prepared<D>& p) {
+		std::vector<D> out;
+		for (int s = 0; s < 4; ++s)
+		{
+			put(out, p.rA[s]), put(out, p.rB[s]), put(out, p.jA[s]), put(out, p.jB[s]);
+			out.push_back(p.wN[s]);
+		}
+		return out;
+	};
+	auto f = [&](const std::vector<D>& in) {
+		Contact<D> cc = c;
+		size_t i = 0;
+		getContactData(in, i, cc);
+		Prepared<D> p;
+		preparedZero(p);
+		prepare(cc, qA, qB, imA, imB, iwA, iwB, p);
+		return lin(w, outv(p));
+	};
+	Prepared<D> p, pb;
+	preparedZero(p);
+	prepare(c, qA, qB, imA, imB, iwA, iwB, p);
+	size_t k = 0;
+	for (int s = 0; s < 4; ++s)
+	{
+		pb.rA[s] = getv(w, k), pb.rB[s] = getv(w, k), pb.jA[s] = getv(w, k), pb.jB[s] = getv(w, k);
+		pb.wN[s] = w[k++];
+	}
+	Q<D> qAb = qzero<D>(), qBb = qzero<D>();
+	D imAb = 0, imBb = 0;
+	M<D> iwAb, iwBb;
+	iwAb.cx = iwAb.cy = iwAb.cz = vzero<D>();
+	iwBb = iwAb;
+	ContactBar<D> cb;
+	contactBarZero(cb);
+	prepare_rev(c, qA, qB, iwA, iwB, p, pb, qAb, qBb, imAb, imBb, iwAb, iwBb, cb);
+	std::vector<D> grad;
+	putBar(grad, cb);
+	return fdCompare(x, grad, f);
+}
+
+double check_normals_contact(uint64_t seed)
+{
+	Rng g{ seed };
+	Contact<D> c = randomContact(g, 1 + (int)(seed % 4), kShapeBox, kShapeBox, 0);
+	Prepared<D> p;
+	preparedZero(p);
+	for (int s = 0; s < 4; ++s)
+	{
+		p.jA[s] = rv(g, 0.5);
+		p.jB[s] = rv(g, 0.5);
+		p.wN[s] = g.r(1, 3);
+	}
+	V<D> pA = rv(g, 0.01), pB = rv(g, 0.01);
+	Q<D> qA = rq(g), qB = rq(g);
+	D imA = g.r(0.5, 2), imB = (seed % 3 == 0) ? 0.0 : g.r(0.5, 2);
+	D maxC = 3.0 / 240.0;
+	for (int s = 0; s < c.pointCount; ++s)
+	{
+		V<D> rA = rotate(qA, c.la[s]), rB = rotate(qB, c.lb[s]);
+		D base = dot(sub(add(pB, rB), add(pA, rA)), c.n);
+		c.off[s] = -base - g.r(0.002, 0.006);
+	}
+	std::vector<D> x;
+	putContactData(x, c);
+	std::vector<D> w(14 + 4);
+	for (auto& v : w)
+		v = g.r(-1, 1);
+	auto f = [&](const std::vector<D>& in) {
+		Contact<D> cc = c;
+		size_t i = 0;
+		getContactData(in, i, cc);
+		V<D> a = pA, b = pB;
+		Q<D> qa = qA, qb = qB;
+		D lam[4] = { 0, 0, 0, 0 };
+		normals(cc, p, imA, imB, maxC, a, qa, b, qb, lam);
+		std::vector<D> out;
+		put(out, a), put(out, qa), put(out, b), put(out, qb);
+		for (int s = 0; s < 4; ++s)
+			out.push_back(lam[s]);
+		return lin(w, out);
+	};
+	size_t k = 0;
+	V<D> pAb = getv(w, k);
+	Q<D> qAb = getq(w, k);
+	V<D> pBb = getv(w, k);
+	Q<D> qBb = getq(w, k);
+	D lamb[4];
+	for (int s = 0; s < 4; ++s)
+		lamb[s] = w[k++];
+	Prepared<D> pb;
+	preparedZero(pb);
+	D imAb = 0, imBb = 0;
+	ContactBar<D> cb;
+	contactBarZero(cb);
+	normals_rev(c, p, imA, imB, maxC, pA, qA, pB, qB, pAb, qAb, pBb, qBb, lamb, pb, imAb, imBb, cb);
+	std::vector<D> grad;
+	putBar(grad, cb);
+	return fdCompare(x, grad, f);
+}
+
+double check_friction_contact(uint64_t seed)
+{
+	Rng g{ seed };
+	Contact<D> c = randomContact(g, 1 + (int)(seed % 4), kShapeBox, kShapeBox, 0);
+	V<D> pA = rv(g, 0.05), pB = rv(g, 0.05);
+	Q<D> qA = rq(g), qB = rq(g);
+	D imA = g.r(0.5, 2), imB = (seed % 3 == 0) ? 0.0 : g.r(0.5, 2);
+	M<D> iwA = rm(g), iwB = imB == 0.0 ? M<D>{ vzero<D>(), vzero<D>(), vzero<D>() } : rm(g);
+	D lamN[4], lamT[4];
+	for (int s = 0; s < 4; ++s)
+	{
+		lamN[s] = (s + seed) % 2 ? g.r(0.0005, 0.002) : g.r(0.5, 1.0);
+		lamT[s] = 0;
+	}
+	std::vector<D> x;
+	putContactData(x, c);
+	std::vector<D> w(14 + 4);
+	for (auto& v : w)
+		v = g.r(-1, 1);
+	auto f = [&](const std::vector<D>& in) {
+		Contact<D> cc = c;
+		size_t i = 0;
+		getContactData(in, i, cc);
+		V<D> a = pA, b = pB;
+		Q<D> qa = qA, qb = qB;
+		D lt[4] = { 0, 0, 0, 0 };
+		friction(cc, imA, imB, iwA, iwB, lamN, a, qa, b, qb, lt);
+		std::vector<D> out;
+		put(out, a), put(out, qa), put(out, b), put(out, qb);
+		for (int s = 0; s < 4; ++s)
+			out.push_back(lt[s]);
+		return lin(w, out);
+	};
+	size_t k = 0;
+	V<D> pAb = getv(w, k);
+	Q<D> qAb = getq(w, k);
+	V<D> pBb = getv(w, k);
+	Q<D> qBb = getq(w, k);
+	D lTb[4], lNb[4] = { 0, 0, 0, 0 };
+	for (int s = 0; s < 4; ++s)
+		lTb[s] = w[k++];
+	D muB = 0, imAb = 0, imBb = 0;
+	M<D> iwAb, iwBb;
+	iwAb.cx = iwAb.cy = iwAb.cz = vzero<D>();
+	iwBb = iwAb;
+	ContactBar<D> cb;
+	contactBarZero(cb);
+	friction_rev(c, imA, imB, iwA, iwB, lamN, pA, qA, pB, qB, lamT, pAb, qAb, pBb, qBb, lNb, lTb, muB, imAb, imBb, iwAb,
+				 iwBb, cb);
+	std::vector<D> grad;
+	putBar(grad, cb);
+	return fdCompare(x, grad, f);
+}
+
+double check_velocity_contact(uint64_t seed)
+{
+	Rng g{ seed };
+	int curved = (int)(seed % 2);
+	Contact<D> c = randomContact(g, 1 + (int)(seed % 4), curved ? kShapeSphere : kShapeBox, kShapeBox, curved);
+	Prepared<D> p;
+	preparedZero(p);
+	for (int s = 0; s < 4; ++s)
+	{
+		p.rA[s] = rv(g, 0.3);
+		p.rB[s] = rv(g, 0.3);
+		p.jA[s] = rv(g, 0.5);
+		p.jB[s] = rv(g, 0.5);
+		p.wN[s] = g.r(1, 3);
+		c.slip[s] = (s + seed) % 2 ? rv(g, 1) : v3<D>(0, 0, 0);
+	}
+	VelocityIn<D> in;
+	in.imA = g.r(0.5, 2);
+	in.imB = (seed % 3 == 0) ? 0.0 : g.r(0.5, 2);
+	in.iwA = rm(g);
+	in.iwB = in.imB == 0.0 ? M<D>{ vzero<D>(), vzero<D>(), vzero<D>() } : rm(g);
+	in.qA = rq(g);
+	in.qB = rq(g);
+	in.pva = rv(g, 2), in.pwa = rv(g, 2), in.pvb = rv(g, 2), in.pwb = rv(g, 2);
+	in.h = 1.0 / 240.0;
+	in.gravityLen = 9.81;
+	D lamN[4];
+	for (int s = 0; s < 4; ++s)
+		lamN[s] = (s + seed) % 3 ? g.r(0.001, 0.01) : g.r(0.00001, 0.0001);
+	V<D> va = rv(g, 1), wa = rv(g, 1), vb = rv(g, 1), wb = rv(g, 1);
+	std::vector<D> x;
+	putContactData(x, c);
+	std::vector<D> w(12);
+	for (auto& v : w)
+		v = g.r(-1, 1);
+	if (in.imB == 0.0)
+		w[6] = w[7] = w[8] = w[9] = w[10] = w[11] = 0;
+	auto f = [&](const std::vector<D>& v) {
+		Contact<D> cc = c;
+		size_t i = 0;
+		getContactData(v, i, cc);
+		V<D> a = va, aw = wa, b = vb, bw = wb;
+		velocity(cc, p, in, lamN, a, aw, b, bw);
+		std::vector<D> out;
+		put(out, a), put(out, aw), put(out, b), put(out, bw);
+		return lin(w, out);
+	};
+	V<D> vab = v3<D>(w[0], w[1], w[2]), wab = v3<D>(w[3], w[4], w[5]), vbb = v3<D>(w[6], w[7], w[8]),
+		 wbb = v3<D>(w[9], w[10], w[11]);
+	Prepared<D> pb;
+	preparedZero(pb);
+	D lNb[4] = { 0, 0, 0, 0 };
+	VelocityBar<D> b;
+	b.imA = b.imB = b.mu = b.e = 0;
+	b.iwA.cx = b.iwA.cy = b.iwA.cz = vzero<D>();
+	b.iwB = b.iwA;
+	b.qA = b.qB = qzero<D>();
+	b.pva = b.pwa = b.pvb = b.pwb = vzero<D>();
+	ContactBar<D> cb;
+	contactBarZero(cb);
+	velocity_rev(c, p, in, lamN, va, wa, vb, wb, vab, wab, vbb, wbb, pb, lNb, b, cb);
+	std::vector<D> grad;
+	putBar(grad, cb);
+	return fdCompare(x, grad, f);
+}
+
+// ---- manifold generation: dual-number Jacobian against central differences -------
+
+double check_generation(uint64_t seed)
+{
+	Rng g{ seed };
+	const int kind = (int)(seed % 5);
+	GenShape<D> a, b;
+	V<D> xA, xB;
+	Q<D> qA, qB;
+	pairFor(kind, g, a, b, xA, qA, xB, qB);
+	const D margin = 0.02;
+	GenManifold<D> m0;
+	genManifold(a, xA, qA, b, xB, qB, margin, m0);
+	if (m0.count == 0)
+	{
+		return 1e9; // the configuration must touch
+	}
+	typedef Dual<D, 14> S;
+	GenShape<S> sa, sb;
+	sa.type = a.type, sa.radius = S(a.radius), sa.he = v3<S>(S(a.he.x), S(a.he.y), S(a.he.z));
+	sb.type = b.type, sb.radius = S(b.radius), sb.he = v3<S>(S(b.he.x), S(b.he.y), S(b.he.z));
+	D in[14] = { xA.x, xA.y, xA.z, qA.x, qA.y, qA.z, qA.w, xB.x, xB.y, xB.z, qB.x, qB.y, qB.z, qB.w };
+	S d[14];
+	for (int k = 0; k < 14; ++k)
+	{
+		d[k] = S(in[k]);
+		d[k].d[k] = 1;
+	}
+	GenManifold<S> md;
+	genManifold(sa, v3<S>(d[0], d[1], d[2]), q4<S>(d[3], d[4], d[5], d[6]), sb, v3<S>(d[7], d[8], d[9]),
+				q4<S>(d[10], d[11], d[12], d[13]), S(margin), md);
+	if (md.count != m0.count)
+	{
+		return 1e9;
+	}
+	// outputs: n, then per point la, lb, off
+	auto outputs = [&](const D* v, std::vector<D>& out) {
+		GenManifold<D> m;
+		genManifold(a, v3<D>(v[0], v[1], v[2]), q4<D>(v[3], v[4], v[5], v[6]), b, v3<D>(v[7], v[8], v[9]),
+					q4<D>(v[10], v[11], v[12], v[13]), margin, m);
+		out.clear();
+		if (m.count != m0.count)
+		{
+			return false;
+		}
+		put(out, m.n);
+		for (int i = 0; i < m.count; ++i)
+		{
+			if (m.p[i].id != m0.p[i].id)
+				return false;
+			put(out, m.p[i].la), put(out, m.p[i].lb), out.push_back(m.p[i].off);
+		}
+		return true;
+	};
+	double worst = 0;
+	for (int k = 0; k < 14; ++k)
+	{
+		D vp[14], vm[14];
+		for (int j = 0; j < 14; ++j)
+			vp[j] = vm[j] = in[j];
+		const double h = 1e-7;
+		vp[k] += h;
+		vm[k] -= h;
+		std::vector<D> op, om;
+		if (!outputs(vp, op) || !outputs(vm, om))
+			continue; // a branch flipped within +-h
+		std::vector<D> jac;
+		jac.push_back(md.n.x.d[k]), jac.push_back(md.n.y.d[k]), jac.push_back(md.n.z.d[k]);
+		for (int i = 0; i < md.count; ++i)
+		{
+			jac.push_back(md.p[i].la.x.d[k]), jac.push_back(md.p[i].la.y.d[k]), jac.push_back(md.p[i].la.z.d[k]);
+			jac.push_back(md.p[i].lb.x.d[k]), jac.push_back(md.p[i].lb.y.d[k]), jac.push_back(md.p[i].lb.z.d[k]);
+			jac.push_back(md.p[i].off.d[k]);
+		}
+		for (size_t o = 0; o < jac.size(); ++o)
+		{
+			double fd = (op[o] - om[o]) / (2 * h);
+			worst = fmax(worst, fabs(jac[o] - fd) / fmax(fabs(fd), 1.0));
+		}
+	}
+	return worst;
+}
 } // extern "C"

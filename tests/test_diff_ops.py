@@ -26,7 +26,8 @@ def lib():
         subprocess.run(["g++", "-std=c++17", "-O1", "-fPIC", "-shared", "-I" + INC, SRC, "-o", so], check=True)
         _lib = C.CDLL(so)
         for name in ("check_integrate", "check_prepare", "check_normals", "check_friction", "check_reconstruct",
-                     "check_velocity"):
+                     "check_velocity", "check_prepare_contact", "check_normals_contact", "check_friction_contact",
+                     "check_velocity_contact", "check_generation"):
             f = getattr(_lib, name)
             f.restype = C.c_double
             f.argtypes = [C.c_uint64]
@@ -38,3 +39,20 @@ def test_reverse_matches_finite_differences(op):
     f = getattr(lib(), "check_" + op)
     worst = max(f(seed) for seed in range(1, 41))
     assert worst < 1e-5, "%s: worst relative error %.3g" % (op, worst)
+
+
+@pytest.mark.parametrize("op", ["prepare", "normals", "friction", "velocity"])
+def test_manifold_adjoints_match_finite_differences(op):
+    """Adjoints of the manifold data each operation reads (normal, local and
+    stiction anchors, separation offsets)."""
+    f = getattr(lib(), "check_%s_contact" % op)
+    worst = max(f(seed) for seed in range(1, 41))
+    assert worst < 1e-5, "%s: worst relative error %.3g" % (op, worst)
+
+
+def test_generation_jacobian_matches_finite_differences():
+    """Dual-number derivatives of a generated manifold (box-box face and edge
+    contacts, sphere-box both ways, sphere-sphere) with respect to the two
+    poses, against central differences of the same generation in double."""
+    worst = max(lib().check_generation(seed) for seed in range(1, 51))
+    assert worst < 1e-5, "worst relative error %.3g" % worst
