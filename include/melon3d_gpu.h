@@ -52,8 +52,8 @@ M3D_API float m3d_gpu_last_step_device_ms(m3d_world* world);
  * bodyCount, awakeBodyCount, hashFailures, colouredIslands, serialIslands,
  * freeIslands, waitErrors, contactCount, giantIslands, keptStable,
  * keptStableOversized, keptContacts, tinyIslands, warpIslands, islandPoints,
- * serialBodies, serialContacts.  Returns how many counters exist (writes at
- * most capacity). */
+ * serialBodies, serialContacts, sleptBodies (counted only while a tape
+ * records).  Returns how many counters exist (writes at most capacity). */
 M3D_API int32_t m3d_gpu_step_counters(m3d_world* world, uint32_t* out, int32_t capacity);
 
 /* Coloured islands (>= 300 contacts, solved with the reference's greedy
@@ -130,6 +130,67 @@ M3D_API void m3d_gpu_profiler_kernel(float* totalMs, int32_t* launches);
 M3D_API int32_t m3d_gpu_profiler_table(char* out, int32_t capacity);
 /* Host->device and device->host bytes the library copied since the reset. */
 M3D_API void m3d_gpu_profiler_bytes(long long* h2d, long long* d2h);
+
+/* ---- differentiation (no counterpart in the reference) ----------------------
+ * m3d_gpu_tape_begin opens a tape: every following m3d_world_step records
+ * what its adjoint needs (the contact set, solve order and manifolds of each
+ * substep with their point ids and generation events, the islands, the
+ * bodies put to sleep), and body states are checkpointed every
+ * `checkpointEvery` steps (<= 0: 10).  m3d_gpu_step_backward then runs the
+ * adjoint of all recorded steps on the device: given dL/d(final state) per
+ * body slot, it returns dL/d(state at the tape's start) and dL/d(mass,
+ * friction, restitution) per body slot.  The contact set, the solve order and
+ * every branch the forward took are held fixed: the gradient is that of the
+ * recorded branch.  Manifolds are differentiated as functions of the poses
+ * they were generated at, and stiction anchors as state.  Covered: spheres
+ * and boxes with isotropic inertia (cubes), free and contact-connected islands
+ * below 300 contacts, no joints, no kinematic bodies, no applied forces, no
+ * body edits between recorded steps.  Anything else marks the tape
+ * unsupported (m3d_gpu_tape_supported) and the backward returns
+ * M3D_GPU_ERR_UNSUPPORTED.
+ *
+ * Arrays are per body slot (m3d_gpu_body_capacity): positions and linear /
+ * angular velocities 3 floats, rotations 4 (xyzw), scalars 1.  Input adjoint
+ * arrays may be NULL (zero); output arrays may be NULL (not written). */
+#define M3D_GPU_ERR_UNSUPPORTED (-8) /* the recorded steps use a feature the adjoint does not cover */
+M3D_API int32_t m3d_gpu_tape_begin(m3d_world* world, int32_t checkpointEvery);
+/* Discards the tape (recording stops). */
+M3D_API void m3d_gpu_tape_end(m3d_world* world);
+/* Steps recorded so far (0 without a tape). */
+M3D_API int32_t m3d_gpu_tape_steps(m3d_world* world);
+/* 1 while the tape is differentiable; else 0 and the reason in why. */
+M3D_API int32_t m3d_gpu_tape_supported(m3d_world* world, char* why, int32_t capacity);
+/* Re-runs the recorded steps from the first checkpoint with the recorded
+ * manifolds (the forward half of the adjoint) and returns the final states;
+ * equal to the world's own states bit for bit. */
+M3D_API int32_t m3d_gpu_tape_replay(m3d_world* world, float* positions, float* rotations, float* velocities,
+								   float* angularVelocities, int32_t capacity);
+M3D_API int32_t m3d_gpu_step_backward(m3d_world* world, const float* dPositions, const float* dRotations,
+									  const float* dVelocities, const float* dAngularVelocities, float* gPositions,
+									  float* gRotations, float* gVelocities, float* gAngularVelocities, float* gMass,
+									  float* gFriction, float* gRestitution, int32_t capacity);
+/* The same adjoint evaluated in double precision on the host from the same
+ * tape: the FP64 reference gradient for checking m3d_gpu_step_backward. */
+M3D_API int32_t m3d_gpu_step_backward_fp64_host(m3d_world* world, const double* dPositions,
+												const double* dRotations, const double* dVelocities,
+												const double* dAngularVelocities, double* gPositions,
+												double* gRotations, double* gVelocities,
+												double* gAngularVelocities, double* gMass, double* gFriction,
+												double* gRestitution, int32_t capacity);
+/* Verification aid: re-runs the recorded steps on the host from the first
+ * checkpoint using only the tape's discrete record (islands, contact set,
+ * solve order, generation events, sleeps) and regenerating every manifold
+ * from the current poses at its recorded generation events.  In float
+ * (doublePrecision 0) the result equals the world's own states bit for bit;
+ * in double it is the function whose derivative m3d_gpu_step_backward
+ * computes, for finite differences.  Perturbations, each NULL for none:
+ * dVelocities (3 per body slot) is added to the initial linear velocities,
+ * dMass to the masses (inertia scaled along), dFriction and dRestitution to
+ * the bodies' coefficients (contacts mix them as at their creation). */
+M3D_API int32_t m3d_gpu_tape_regenerate_host(m3d_world* world, int32_t doublePrecision, const double* dVelocities,
+											 const double* dMass, const double* dFriction,
+											 const double* dRestitution, double* positions, double* rotations,
+											 double* velocities, double* angularVelocities, int32_t capacity);
 
 /* Snapshot records (melon3d_debug.h) — for tests and debugging. */
 M3D_API int32_t m3d_dbg_body_capacity(m3d_world* world);

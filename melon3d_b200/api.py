@@ -209,6 +209,14 @@ _GPU_PROTOS = {
     "m3d_gpu_profiler_bytes": (None, [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "m3d_gpu_profiler_table": (C.c_int32, [C.c_char_p, C.c_int32]),
     "m3d_gpu_sphere_cast_noalloc": (C.c_int32, [W, Vec3, C.c_float, Vec3, C.c_uint32, C.POINTER(RayResult)]),
+    "m3d_gpu_tape_begin": (C.c_int32, [W, C.c_int32]),
+    "m3d_gpu_tape_end": (None, [W]),
+    "m3d_gpu_tape_steps": (C.c_int32, [W]),
+    "m3d_gpu_tape_supported": (C.c_int32, [W, C.c_char_p, C.c_int32]),
+    "m3d_gpu_tape_replay": (C.c_int32, [W] + [C.POINTER(C.c_float)] * 4 + [C.c_int32]),
+    "m3d_gpu_step_backward": (C.c_int32, [W] + [C.POINTER(C.c_float)] * 11 + [C.c_int32]),
+    "m3d_gpu_step_backward_fp64_host": (C.c_int32, [W] + [C.POINTER(C.c_double)] * 11 + [C.c_int32]),
+    "m3d_gpu_tape_regenerate_host": (C.c_int32, [W, C.c_int32] + [C.POINTER(C.c_double)] * 8 + [C.c_int32]),
 }
 
 # status codes of melon3d_gpu.h
@@ -220,6 +228,7 @@ GPU_ERR_LIMIT = -4
 GPU_ERR_PENDING = -5
 GPU_ERR_ARGUMENT = -6
 GPU_ERR_WAIT = -7
+GPU_ERR_UNSUPPORTED = -8
 
 API_SYMBOLS = sorted(_PROTOS)
 GPU_SYMBOLS = sorted(_GPU_PROTOS)

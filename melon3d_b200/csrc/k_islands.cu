@@ -493,7 +493,7 @@ void launchIslands(DevWorld& w, int32_t n)
 			   &dc->islandContacts, w.jointKeys.as<uint64_t>(), J > 0 ? &dc->islandJoints : nullptr,
 			   w.islands.as<IslandRec>(), w.coloredList.as<int32_t>(), w.serialList.as<int32_t>(),
 			   w.tinyList.as<int32_t>(), w.giantList.as<int32_t>(), w.giantIslandContacts,
-			   w.lastSerialIslands > kTinyModeIslands ? kTinyIslandContacts : 0, dc);
+			   !w.recording && w.lastSerialIslands > kTinyModeIslands ? kTinyIslandContacts : 0, dc);
 	w.islandMax = n;
 }
 
@@ -566,7 +566,7 @@ __global__ void kSleepUpdate(BodySoA B, const uint32_t* vals, int32_t maxBodies,
 
 __global__ void kSleepApply(BodySoA B, const uint32_t* vals, int32_t maxBodies, const uint32_t* bodiesDev,
 							const int32_t* label, const int32_t* firstNo, const uint32_t* minBits,
-							uint32_t* stableDirty)
+							uint32_t* stableDirty, uint32_t* record, uint32_t* recordCount)
 {
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= maxBodies || k >= (int)*bodiesDev)
@@ -585,6 +585,10 @@ __global__ void kSleepApply(BodySoA B, const uint32_t* vals, int32_t maxBodies, 
 	B.angVel[i] = z;
 	B.bFlags[i] &= (uint8_t)~kBFAwake;
 	stableDirty[worldOfBody(B, i)] = 1;
+	if (record != nullptr)
+	{
+		record[atomicAdd(recordCount, 1u)] = (uint32_t)i;
+	}
 }
 
 void launchSleep(DevWorld& w, float dt)
@@ -608,7 +612,8 @@ void launchSleep(DevWorld& w, float dt)
 	M3G_LAUNCH(kSleepUpdate, blocksFor(nmax, 256), 256, s, w.B, vals, nmax, &dc->islandBodies, lab,
 			   w.sleepFirstNo.as<int32_t>(), w.sleepMin.as<uint32_t>(), dt);
 	M3G_LAUNCH(kSleepApply, blocksFor(nmax, 256), 256, s, w.B, vals, nmax, &dc->islandBodies, lab,
-			   w.sleepFirstNo.as<int32_t>(), w.sleepMin.as<uint32_t>(), stableDirtyWords(w));
+			   w.sleepFirstNo.as<int32_t>(), w.sleepMin.as<uint32_t>(), stableDirtyWords(w), w.sleepRecord,
+			   &dc->sleptBodies);
 }
 
 // kinematic integration, one-step force clear, profile counters

@@ -9,8 +9,11 @@
 namespace m3g
 {
 
+// genRecord (null unless a differentiation tape records): per contact,
+// kPrepRegenerated when the manifold was regenerated, kPrepHeld when the
+// tunnelling guard held it, 0 when it was kept
 __global__ void kNarrowphase(BodySoA B, ContactSoA C, int32_t maxCount, const uint32_t* countDev, float dt,
-							 int8_t* transition)
+							 int8_t* transition, uint8_t* genRecord)
 {
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c >= maxCount)
@@ -18,6 +21,10 @@ __global__ void kNarrowphase(BodySoA B, ContactSoA C, int32_t maxCount, const ui
 		return;
 	}
 	transition[c] = 0;
+	if (genRecord != nullptr)
+	{
+		genRecord[c] = 0;
+	}
 	if (c >= (int)*countDev)
 	{
 		return;
@@ -35,6 +42,10 @@ __global__ void kNarrowphase(BodySoA B, ContactSoA C, int32_t maxCount, const ui
 		loadManifold(C, c, held);
 		if (trackedMinSep(xa, xb, held) < -kLinearSlop)
 		{
+			if (genRecord != nullptr)
+			{
+				genRecord[c] = (uint8_t)kPrepHeld;
+			}
 			return; // keep the pre-crossing manifold, touching unchanged
 		}
 		fl &= (uint8_t)~kCFTunnelGuard;
@@ -60,6 +71,10 @@ __global__ void kNarrowphase(BodySoA B, ContactSoA C, int32_t maxCount, const ui
 		setSeparationOffsets(m, xa, xb);
 		storeManifold(C, c, m);
 		pc = m.pointCount;
+		if (genRecord != nullptr)
+		{
+			genRecord[c] = (uint8_t)kPrepRegenerated;
+		}
 	}
 	else
 	{
@@ -165,7 +180,13 @@ void launchNarrowphase(DevWorld& w, float dt)
 		return;
 	}
 	int8_t* tr = w.transition.as<int8_t>();
-	M3G_LAUNCH(kNarrowphase, blocksFor(M, 128), 128, s, w.B, w.C, M, &dc->contactCount, dt, tr);
+	uint8_t* gen = nullptr;
+	if (w.recording)
+	{
+		w.tapeGen.ensure((size_t)M + 1);
+		gen = w.tapeGen.as<uint8_t>();
+	}
+	M3G_LAUNCH(kNarrowphase, blocksFor(M, 128), 128, s, w.B, w.C, M, &dc->contactCount, dt, tr, gen);
 	M3G_LAUNCH(kTransitionFlags, blocksFor(M, 256), 256, s, tr, M, w.evBeginFlag.as<uint32_t>(),
 			   w.evEndFlag.as<uint32_t>());
 	uint32_t* beginScan = w.removeScan.as<uint32_t>();

@@ -13,6 +13,7 @@
 //    __syncthreads() where the reference joins its fork-join stages.
 // Islands are disjoint in their dynamic bodies, so all islands run at once.
 #include "m3d_dev.cuh"
+#include "m3d_diff.h"
 #include "m3d_solve.cuh"
 
 namespace m3g
@@ -58,6 +59,48 @@ __global__ void kSolveFree(BodySoA B, const IslandRec* islands, int32_t ni, cons
 // serial sweep leaves it.  Islands with joints, or larger than the shared
 // tables, sweep serially on lane 0.  __syncwarp() orders the global-memory
 // writes of one stage or level before the reads of the next.
+// Differentiation tape: the manifold of a contact right after its
+// preparation in one substep, with the point ids and how the manifold came to
+// be (what the adjoint holds as the record of the forward).
+static_assert(kPrepRegenerated == m3d_diff::kTapeGenPrepare && kPrepHeld == m3d_diff::kTapeGenHeld,
+			  "tape generation flags follow the preparation flags");
+
+__device__ void writeTapeContact(m3d_diff::TapeContact& t, const BodySoA& B, const ContactSoA& C, int c, int gen)
+{
+	const int2 ab = C.bodies[c];
+	const BodyCold& ca = B.cold[ab.x];
+	const BodyCold& cb = B.cold[ab.y];
+	t.gen = gen;
+	t.a = ab.x;
+	t.b = ab.y;
+	t.pointCount = C.pointCount[c];
+	t.curved = (C.flags[c] & kCFCurved) != 0 ? 1 : 0;
+	t.shapeA = (int32_t)ca.shape.type;
+	t.shapeB = (int32_t)cb.shape.type;
+	t.radiusA = ca.shape.radius;
+	t.radiusB = cb.shape.radius;
+	const float4 n = C.normal[c];
+	t.n[0] = n.x;
+	t.n[1] = n.y;
+	t.n[2] = n.z;
+	t.mu = n.w;
+	const float2 mat = C.mat[c];
+	t.e = mat.x;
+	t.rolling = mat.y;
+	for (int s = 0; s < 4; ++s)
+	{
+		const size_t k = pidx(C, c, s);
+		const float4 la = C.pAnchorA[k], lb = C.pAnchorB[k], fa = C.pFricA[k], fb = C.pFricB[k], sl = C.pSlip[k];
+		t.la[s][0] = la.x, t.la[s][1] = la.y, t.la[s][2] = la.z;
+		t.lb[s][0] = lb.x, t.lb[s][1] = lb.y, t.lb[s][2] = lb.z;
+		t.fa[s][0] = fa.x, t.fa[s][1] = fa.y, t.fa[s][2] = fa.z;
+		t.fb[s][0] = fb.x, t.fb[s][1] = fb.y, t.fb[s][2] = fb.z;
+		t.slip[s][0] = sl.x, t.slip[s][1] = sl.y, t.slip[s][2] = sl.z;
+		t.off[s] = sl.w;
+		t.id[s] = __float_as_uint(lb.w);
+	}
+}
+
 constexpr int kSerialWarpsPerBlock = 8;
 constexpr int kLevelTable = 320; // contacts and bodies per island for the level schedule
 constexpr uint32_t kNotIsland = 0xFFFFu;
@@ -129,7 +172,8 @@ __device__ __forceinline__ void sweepIsland(SweepOp op, const BodySoA& B, const 
 __global__ void __launch_bounds__(32 * kSerialWarpsPerBlock)
 	kSolveSerial(BodySoA B, ContactSoA C, JointRec* J, const IslandRec* islands, const int32_t* serialList,
 				 const uint32_t* serialDev, const uint32_t* bodyVals, const uint32_t* contactVals,
-				 const uint32_t* jointVals, uint32_t* localIndex, SolveParams P)
+				 const uint32_t* jointVals, uint32_t* localIndex, SolveParams P, m3d_diff::TapeContact* tape,
+				 const uint32_t* tapeStride, const uint8_t* narrowGen)
 {
 	__shared__ LevelTables tables[kSerialWarpsPerBlock];
 	const int lane = threadIdx.x & 31;
@@ -222,7 +266,16 @@ __global__ void __launch_bounds__(32 * kSerialWarpsPerBlock)
 			__syncwarp();
 			for (int c = lane; c < r.contactCount; c += 32)
 			{
-				prepareContact(B, C, (int)contacts[c], P.h);
+				const int what = prepareContact(B, C, (int)contacts[c], P.h);
+				if (tape != nullptr)
+				{
+					int gen = what;
+					if (sub == 0 && narrowGen[contacts[c]] == kPrepRegenerated)
+					{
+						gen |= m3d_diff::kTapeGenNarrow;
+					}
+					writeTapeContact(tape[(size_t)sub * *tapeStride + r.contactStart + c], B, C, (int)contacts[c], gen);
+				}
 			}
 			__syncwarp();
 			if (r.jointCount > 0)
@@ -583,14 +636,15 @@ void launchSolve(DevWorld& w, float dt, int substeps, V3 gravity, int positionIt
 	int serialBlocks = (ni + kSerialWarpsPerBlock - 1) / kSerialWarpsPerBlock;
 	serialBlocks = serialBlocks < 148 * 8 ? serialBlocks : 148 * 8;
 	w.colorMask.ensure((size_t)(w.bodyCap + 1) * sizeof(uint32_t)); // also the serial islands' local body index
-	if (w.lastSerialIslands > kTinyModeIslands) // the island table listed tiny islands this step
+	if (!w.recording && w.lastSerialIslands > kTinyModeIslands) // the island table listed tiny islands this step
 	{
 		M3G_LAUNCH(kSolveTiny, blocksFor(ni, 128), 128, s, w.B, w.C, isl, w.tinyList.as<int32_t>(), &dc->tinyIslands,
 				   w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(), P);
 	}
 	M3G_LAUNCH(kSolveSerial, serialBlocks, 32 * kSerialWarpsPerBlock, s, w.B, w.C, w.joints.as<JointRec>(), isl,
 			   w.serialList.as<int32_t>(), &dc->warpIslands, w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(),
-			   w.jointVals.as<uint32_t>(), w.colorMask.as<uint32_t>(), P);
+			   w.jointVals.as<uint32_t>(), w.colorMask.as<uint32_t>(), P, w.tapeContacts, &dc->islandContacts,
+			   w.tapeGen.as<uint8_t>());
 	size_t nc = (size_t)w.contactMax + 1;
 	w.colorOrder.ensure(nc * sizeof(int32_t));
 	w.packetMax.ensure(nc * sizeof(int32_t));

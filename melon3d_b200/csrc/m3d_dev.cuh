@@ -6,6 +6,11 @@
 #include "m3d_types.cuh"
 #include "prims.cuh"
 
+namespace m3d_diff
+{
+struct TapeContact;
+}
+
 namespace m3g
 {
 
@@ -50,6 +55,7 @@ struct StepCounters
 	uint32_t islandPoints;   // manifold points of the island contacts (before the solve)
 	uint32_t serialBodies;   // bodies of the serial islands
 	uint32_t serialContacts; // contacts of the serial islands
+	uint32_t sleptBodies;    // bodies put to sleep (counted only while a tape records)
 };
 
 // Host -> device body update record (one per body touched by the API
@@ -203,6 +209,12 @@ struct DevWorld
 	DevBuf vFlag, vScan, vSrc;   // per virtual contact (old then new, world-major)
 	DevBuf keptKeys, keptVals, keptOver; // stable-tier entries of worlds that keep their tier
 	ContactSoA C2 = {};          // second contact arena: target of the world-major re-layout
+
+	// differentiation tape (k_diff.cu): set for a step that records
+	bool recording = false;
+	m3d_diff::TapeContact* tapeContacts = nullptr; // this step's contact records
+	uint32_t* sleepRecord = nullptr;               // bodies put to sleep this step
+	DevBuf tapeGen;                                // per contact: what this step's narrowphase did to its manifold
 };
 
 // one stable-dirty word per world (StepCounters::stableDirty for one world)
@@ -272,5 +284,26 @@ constexpr size_t kCastRecBytes = 28;
 size_t sphereCastScratchBytes(int32_t n);
 void launchSphereCastInto(DevWorld& w, int32_t n, V3 origin, float radius, V3 translation, uint32_t maskBits,
 						  void* scratch, RayQueryOut* hostOut);
+
+// differentiation tape (k_diff.cu); status returns are M3D_GPU_* codes
+struct DiffTape;
+DiffTape* tapeCreate(DevWorld& w, int32_t nBodies, int checkpointEvery);
+void tapeDestroy(DiffTape* t);
+void tapeMarkUnsupported(DiffTape* t, const char* why);
+const char* tapeUnsupported(const DiffTape* t); // null while the tape is differentiable
+int32_t tapeSteps(const DiffTape* t);
+void tapeStepBegin(DiffTape* t, DevWorld& w, int32_t n, float dt, int substeps, V3 g, int iterations);
+void tapeBeforeIslands(DiffTape* t, DevWorld& w, int substeps);
+void tapeStepEnd(DiffTape* t, DevWorld& w, const StepCounters& hc);
+int32_t tapeReplay(DiffTape* t, DevWorld& w, float* pos, float* rot, float* vel, float* angVel, int32_t capacity);
+int32_t tapeBackward(DiffTape* t, DevWorld& w, const float* dPos, const float* dRot, const float* dVel,
+					 const float* dAngVel, float* gPos, float* gRot, float* gVel, float* gAngVel, float* gMass,
+					 float* gFriction, float* gRestitution, int32_t capacity);
+int32_t tapeBackwardHost(DiffTape* t, const double* dPos, const double* dRot, const double* dVel,
+						 const double* dAngVel, double* gPos, double* gRot, double* gVel, double* gAngVel,
+						 double* gMass, double* gFriction, double* gRestitution, int32_t capacity);
+int32_t tapeRegenerateHost(DiffTape* t, int doublePrecision, const double* dVel, const double* dMass,
+						   const double* dFriction, const double* dRestitution, double* pos, double* rot, double* vel,
+						   double* angVel, int32_t capacity);
 
 } // namespace m3g

@@ -289,8 +289,13 @@ M3G_HD void setSeparationOffsets(Manifold& m, Xf xa, Xf xb)
 // moved > 3 cm or ~5.7 deg since generation, the thin-feature tunnelling
 // rescue, then the freeze of arms, Jacobians and normal mass
 // (reference src/xpbd.cpp:718-863)
-M3G_D void prepareContact(const BodySoA& B, const ContactSoA& C, int c, float h)
+// what prepareContact did to the manifold (differentiation tape)
+constexpr int kPrepRegenerated = 2; // regenerated at the current poses
+constexpr int kPrepHeld = 4;        // stale, but held by the tunnelling guard
+
+M3G_D int prepareContact(const BodySoA& B, const ContactSoA& C, int c, float h)
 {
+	int what = 0;
 	int2 ab = C.bodies[c];
 	const BodyCold& ca = B.cold[ab.x];
 	const BodyCold& cb = B.cold[ab.y];
@@ -376,9 +381,11 @@ M3G_D void prepareContact(const BodySoA& B, const ContactSoA& C, int c, float h)
 		if (keepOld)
 		{
 			m = oldM; // cache pose intentionally not refreshed
+			what = kPrepHeld;
 		}
 		else
 		{
+			what = kPrepRegenerated;
 			inheritAnchors(oldM, m, ca.shape.type == kBox && cb.shape.type == kBox, xa, xb);
 			hasCache = true;
 			C.cachePosA[c] = st3(xa.p);
@@ -421,6 +428,7 @@ M3G_D void prepareContact(const BodySoA& B, const ContactSoA& C, int c, float h)
 		C.pJA[k] = st3(jA);
 		C.pJB[k] = st3(jB);
 	}
+	return what;
 }
 
 // Gauss-Seidel normal projection of one contact, serial-island form

@@ -112,6 +112,9 @@ struct m3d_world
 	std::vector<uint32_t> batchDirtyRead;
 	bool stepped = false;
 
+	// differentiation tape (m3d_gpu_tape_begin); null when not recording
+	DiffTape* tape = nullptr;
+
 	// pinned staging
 	std::vector<BodyUpload> uploadRecs;
 	float4* pinPos = nullptr;
@@ -772,6 +775,11 @@ void m3d_world_destroy(m3d_world* world)
 	}
 	DevWorld& d = world->dev;
 	cudaStreamSynchronize(d.stream);
+	if (world->tape != nullptr)
+	{
+		tapeDestroy(world->tape);
+		world->tape = nullptr;
+	}
 	BodySoA& B = d.B;
 	void* bp[] = { B.pos, B.rot, B.vel, B.angVel, B.prevPos, B.prevRot, B.prevVel, B.prevAngVel, B.massInv,
 				   B.iw0, B.iw1, B.iw2, B.force, B.torque, B.sleep, B.state, B.cold, B.fatLo, B.fatHi,
@@ -1581,9 +1589,24 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	world->endEvents.clear();
 	const int32_t n = (int32_t)world->bodies.size();
 
+	if (world->tape != nullptr)
+	{
+		if (tapeSteps(world->tape) > 0 && !world->dirtyList.empty())
+		{
+			tapeMarkUnsupported(world->tape, "bodies were edited between recorded steps");
+		}
+		if (world->anyForcesApplied)
+		{
+			tapeMarkUnsupported(world->tape, "applied forces are not differentiated");
+		}
+	}
 	flushHostChanges(world);
 	StepCounters* dc = devCounters(d);
 	cudaMemsetAsync(dc, 0, sizeof(StepCounters), d.stream);
+	if (world->tape != nullptr)
+	{
+		tapeStepBegin(world->tape, d, n, dt, substepCount, hv(world->def.gravity), world->def.positionIterations);
+	}
 	if (isBatch(world))
 	{
 		cudaMemsetAsync(d.worldStableDirty.ptr, 0, sizeof(uint32_t) * (size_t)d.worldCount, d.stream);
@@ -1625,6 +1648,10 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	auto tNarrow = Clock::now();
 	d.contactColor.ensure((size_t)(d.contactCap + 1) * sizeof(int32_t));
 	cudaMemsetAsync(d.contactColor.ptr, 0xFF, (size_t)(d.contactMax + 1) * sizeof(int32_t), d.stream);
+	if (world->tape != nullptr)
+	{
+		tapeBeforeIslands(world->tape, d, substepCount);
+	}
 	launchIslands(d, n);
 	launchSolve(d, dt, substepCount, hv(world->def.gravity), world->def.positionIterations);
 	launchSleep(d, dt);
@@ -1644,6 +1671,11 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	fetchEvents(world, evE, d.evEnd.as<int4>(), (int32_t)hc->endNP);
 	cudaStreamSynchronize(d.stream);
 	checkCuda(world, "step");
+	if (world->tape != nullptr)
+	{
+		tapeStepEnd(world->tape, d, *hc);
+		checkCuda(world, "tape");
+	}
 	if (isBatch(world))
 	{
 		world->batchDirtyRead.resize((size_t)d.worldCount);
@@ -2192,6 +2224,122 @@ void m3d_dbg_contact_colors(m3d_world* world, int32_t* out, int32_t capacity)
 	}
 	cudaMemcpyAsync(out, d.contactColor.ptr, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, d.stream);
 	cudaStreamSynchronize(d.stream);
+}
+
+// ---- differentiation --------------------------------------------------------------
+
+int32_t m3d_gpu_tape_begin(m3d_world* world, int32_t checkpointEvery)
+{
+	if (world == nullptr)
+	{
+		return M3D_GPU_ERR_ARGUMENT;
+	}
+	if (world->tape != nullptr)
+	{
+		tapeDestroy(world->tape);
+		world->tape = nullptr;
+	}
+	flushHostChanges(world);
+	world->tape = tapeCreate(world->dev, (int32_t)world->bodies.size(), checkpointEvery);
+	checkCuda(world, "tape begin");
+	return world->status;
+}
+
+void m3d_gpu_tape_end(m3d_world* world)
+{
+	if (world != nullptr && world->tape != nullptr)
+	{
+		cudaStreamSynchronize(world->dev.stream);
+		tapeDestroy(world->tape);
+		world->tape = nullptr;
+	}
+}
+
+int32_t m3d_gpu_tape_steps(m3d_world* world)
+{
+	return world != nullptr && world->tape != nullptr ? tapeSteps(world->tape) : 0;
+}
+
+int32_t m3d_gpu_tape_supported(m3d_world* world, char* why, int32_t capacity)
+{
+	const char* reason = world == nullptr || world->tape == nullptr ? "no tape is open" : tapeUnsupported(world->tape);
+	if (why != nullptr && capacity > 0)
+	{
+		snprintf(why, (size_t)capacity, "%s", reason != nullptr ? reason : "");
+	}
+	return reason == nullptr ? 1 : 0;
+}
+
+static int32_t tapeUsable(m3d_world* world)
+{
+	if (world == nullptr || world->tape == nullptr)
+	{
+		return M3D_GPU_ERR_ARGUMENT;
+	}
+	if (tapeUnsupported(world->tape) != nullptr)
+	{
+		fprintf(stderr, "melon3d_gpu: tape not differentiable: %s\n", tapeUnsupported(world->tape));
+		return M3D_GPU_ERR_UNSUPPORTED;
+	}
+	return tapeSteps(world->tape) > 0 ? M3D_GPU_OK : M3D_GPU_ERR_ARGUMENT;
+}
+
+int32_t m3d_gpu_tape_replay(m3d_world* world, float* positions, float* rotations, float* velocities,
+							float* angularVelocities, int32_t capacity)
+{
+	int32_t rc = tapeUsable(world);
+	if (rc != M3D_GPU_OK)
+	{
+		return rc;
+	}
+	rc = tapeReplay(world->tape, world->dev, positions, rotations, velocities, angularVelocities, capacity);
+	checkCuda(world, "tape replay");
+	return rc;
+}
+
+int32_t m3d_gpu_step_backward(m3d_world* world, const float* dPositions, const float* dRotations,
+							  const float* dVelocities, const float* dAngularVelocities, float* gPositions,
+							  float* gRotations, float* gVelocities, float* gAngularVelocities, float* gMass,
+							  float* gFriction, float* gRestitution, int32_t capacity)
+{
+	int32_t rc = tapeUsable(world);
+	if (rc != M3D_GPU_OK)
+	{
+		return rc;
+	}
+	rc = tapeBackward(world->tape, world->dev, dPositions, dRotations, dVelocities, dAngularVelocities, gPositions,
+					  gRotations, gVelocities, gAngularVelocities, gMass, gFriction, gRestitution, capacity);
+	checkCuda(world, "step backward");
+	return rc;
+}
+
+int32_t m3d_gpu_step_backward_fp64_host(m3d_world* world, const double* dPositions, const double* dRotations,
+										const double* dVelocities, const double* dAngularVelocities,
+										double* gPositions, double* gRotations, double* gVelocities,
+										double* gAngularVelocities, double* gMass, double* gFriction,
+										double* gRestitution, int32_t capacity)
+{
+	int32_t rc = tapeUsable(world);
+	if (rc != M3D_GPU_OK)
+	{
+		return rc;
+	}
+	return tapeBackwardHost(world->tape, dPositions, dRotations, dVelocities, dAngularVelocities, gPositions,
+							gRotations, gVelocities, gAngularVelocities, gMass, gFriction, gRestitution, capacity);
+}
+
+int32_t m3d_gpu_tape_regenerate_host(m3d_world* world, int32_t doublePrecision, const double* dVelocities,
+									 const double* dMass, const double* dFriction, const double* dRestitution,
+									 double* positions, double* rotations, double* velocities,
+									 double* angularVelocities, int32_t capacity)
+{
+	int32_t rc = tapeUsable(world);
+	if (rc != M3D_GPU_OK)
+	{
+		return rc;
+	}
+	return tapeRegenerateHost(world->tape, doublePrecision, dVelocities, dMass, dFriction, dRestitution, positions,
+							  rotations, velocities, angularVelocities, capacity);
 }
 
 } // extern "C"

@@ -11,7 +11,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 SRC = os.path.join(HERE, "scenes.cpp")
 LIB = os.path.join(os.path.dirname(HERE), "lib", "libm3d_scenes.so")
 
-PYRAMID, RAIN, PILE, RAFT, BATCH_WORLD = 0, 1, 2, 3, 4
+PYRAMID, RAIN, PILE, RAFT, BATCH_WORLD, INCLINE = 0, 1, 2, 3, 4, 5
 
 
 class M3dApi(C.Structure):

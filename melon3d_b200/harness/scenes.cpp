@@ -20,6 +20,12 @@
 //      the rain distributions inside a 10x10x10 m volume above it, and 0-4
 //      ball or hinge joints between random body pairs, anchored at the pair's
 //      midpoint (a > 0 fixes the body count, b > 0 leaves the joints out)
+//   5  one world of the differentiable batch: a static 16x0.5x10 m incline
+//      box tilted by theta~U[10,35] deg about z carrying an 8x8 grid of
+//      bodies (alternately cubes he~U[0.1,0.3] and spheres r~U[0.1,0.3]),
+//      each 0.01-0.3 m above the slope, v~N(0,1) per axis, mu~U[0.2,0.9],
+//      e~U[0,0.3]; the incline has mu 1, e 0.  Sleep is off (b > 0: on);
+//      0 < a < 64 sets the body count.
 #include "melon3d.h"
 
 #include <algorithm>
@@ -298,6 +304,10 @@ void* scn_create(const M3dApi* api, int kind, uint64_t seed, int a, int b, int c
 	{
 		wd.workerCount = workers; // the reference's thread pool; the GPU world ignores it
 	}
+	if (kind == 5)
+	{
+		wd.enableSleep = b > 0;
+	}
 	s->world = s->api.world_create(&wd);
 	if (s->world == nullptr)
 	{
@@ -365,6 +375,51 @@ void* scn_create(const M3dApi* api, int kind, uint64_t seed, int a, int b, int c
 		}
 		int joints = (int)(s->rng.next() % 5);
 		addBatchJoints(*s, b > 0 ? 0 : joints); // b > 0: no joints
+	}
+	else if (kind == 5)
+	{
+		Rng& r = s->rng;
+		const double theta = (10.0 + 25.0 * r.uniform()) * 3.141592653589793 / 180.0;
+		const m3d_quat q = { 0.0f, 0.0f, (float)sin(0.5 * theta), (float)cos(0.5 * theta) };
+		m3d_body_def gd = s->api.body_def_default();
+		gd.type = M3D_BODY_STATIC;
+		gd.orientation = q;
+		m3d_shape_def gs = s->api.shape_def_default();
+		gs.type = M3D_SHAPE_BOX;
+		gs.halfExtents = m3d_v3(8.0f, 0.25f, 5.0f);
+		gs.friction = 1.0f;
+		gs.restitution = 0.0f;
+		s->api.body_create(s->world, &gd, &gs);
+		const int count = a > 0 && a < 64 ? a : 64;
+		for (int i = 0; i < count; ++i)
+		{
+			const int gx = i % 8, gz = i / 8;
+			m3d_shape_def sd = s->api.shape_def_default();
+			float size = r.range(0.1, 0.3);
+			if (i % 2 == 0)
+			{
+				sd.type = M3D_SHAPE_BOX;
+				sd.halfExtents = m3d_v3(size, size, size);
+			}
+			else
+			{
+				sd.type = M3D_SHAPE_SPHERE;
+				sd.radius = size;
+			}
+			sd.friction = r.range(0.2, 0.9);
+			sd.restitution = r.range(0.0, 0.3);
+			const float gap = r.range(0.01, 0.3);
+			m3d_vec3 local = m3d_v3(-2.8f + 0.8f * (float)gx, 0.25f + size + gap, -2.8f + 0.8f * (float)gz);
+			m3d_body_def bd = s->api.body_def_default();
+			bd.type = M3D_BODY_DYNAMIC;
+			bd.position = m3d_rotate(q, local);
+			bd.orientation = q;
+			bd.linearVelocity = m3d_v3((float)r.normal(), (float)r.normal(), (float)r.normal());
+			m3d_body_id id = s->api.body_create(s->world, &bd, &sd);
+			s->dynamic.push_back(id);
+			s->positions.push_back(bd.position);
+			s->orientations.push_back(bd.orientation);
+		}
 	}
 	else if (kind == 3)
 	{
