@@ -184,13 +184,15 @@ M3D_API int32_t m3d_gpu_step_backward_fp64_host(m3d_world* world, const double* 
  * (doublePrecision 0) the result equals the world's own states bit for bit;
  * in double it is the function whose derivative m3d_gpu_step_backward
  * computes, for finite differences.  Perturbations, each NULL for none:
- * dVelocities (3 per body slot) is added to the initial linear velocities,
- * dMass to the masses (inertia scaled along), dFriction and dRestitution to
- * the bodies' coefficients (contacts mix them as at their creation). */
+ * dVelocities and dAngularVelocities (3 per body slot) are added to the
+ * initial velocities, dMass to the masses (inertia scaled along), dFriction
+ * and dRestitution to the bodies' coefficients (contacts mix them as at their
+ * creation). */
 M3D_API int32_t m3d_gpu_tape_regenerate_host(m3d_world* world, int32_t doublePrecision, const double* dVelocities,
-											 const double* dMass, const double* dFriction,
-											 const double* dRestitution, double* positions, double* rotations,
-											 double* velocities, double* angularVelocities, int32_t capacity);
+											 const double* dAngularVelocities, const double* dMass,
+											 const double* dFriction, const double* dRestitution, double* positions,
+											 double* rotations, double* velocities, double* angularVelocities,
+											 int32_t capacity);
 
 /* Snapshot records (melon3d_debug.h) — for tests and debugging. */
 M3D_API int32_t m3d_dbg_body_capacity(m3d_world* world);

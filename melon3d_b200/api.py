@@ -216,7 +216,7 @@ _GPU_PROTOS = {
     "m3d_gpu_tape_replay": (C.c_int32, [W] + [C.POINTER(C.c_float)] * 4 + [C.c_int32]),
     "m3d_gpu_step_backward": (C.c_int32, [W] + [C.POINTER(C.c_float)] * 11 + [C.c_int32]),
     "m3d_gpu_step_backward_fp64_host": (C.c_int32, [W] + [C.POINTER(C.c_double)] * 11 + [C.c_int32]),
-    "m3d_gpu_tape_regenerate_host": (C.c_int32, [W, C.c_int32] + [C.POINTER(C.c_double)] * 8 + [C.c_int32]),
+    "m3d_gpu_tape_regenerate_host": (C.c_int32, [W, C.c_int32] + [C.POINTER(C.c_double)] * 9 + [C.c_int32]),
 }
 
 # status codes of melon3d_gpu.h

@@ -1138,11 +1138,11 @@ int32_t tapeBackwardHost(DiffTape* t, const double* dPos, const double* dRot, co
 
 namespace
 {
-// perturbations (each may be null): initial linear velocities (3 per body),
-// masses, friction and restitution coefficients (1 per body)
+// perturbations (each may be null): initial linear and angular velocities
+// (3 per body), masses, friction and restitution coefficients (1 per body)
 struct Perturbation
 {
-	const double *dVel, *dMass, *dFriction, *dRestitution;
+	const double *dVel, *dAngVel, *dMass, *dFriction, *dRestitution;
 };
 
 template <typename T>
@@ -1207,6 +1207,12 @@ int32_t regenerateHost(DiffTape* t, const Perturbation& d, std::vector<Body<T>>&
 		{
 			k.cur[i].v = m3d_diff::v3<T>(T((double)ck[i].v.x + d.dVel[3 * i]), T((double)ck[i].v.y + d.dVel[3 * i + 1]),
 										 T((double)ck[i].v.z + d.dVel[3 * i + 2]));
+		}
+		if (d.dAngVel != nullptr)
+		{
+			k.cur[i].w =
+				m3d_diff::v3<T>(T((double)ck[i].w.x + d.dAngVel[3 * i]), T((double)ck[i].w.y + d.dAngVel[3 * i + 1]),
+								T((double)ck[i].w.z + d.dAngVel[3 * i + 2]));
 		}
 	}
 	std::vector<m3d_diff::Contact<T>> live[2];
@@ -1297,16 +1303,16 @@ int32_t regenerateHost(DiffTape* t, const Perturbation& d, std::vector<Body<T>>&
 }
 } // namespace
 
-int32_t tapeRegenerateHost(DiffTape* t, int doublePrecision, const double* dVel, const double* dMass,
-						   const double* dFriction, const double* dRestitution, double* pos, double* rot, double* vel,
-						   double* angVel, int32_t capacity)
+int32_t tapeRegenerateHost(DiffTape* t, int doublePrecision, const double* dVel, const double* dAngVel,
+						   const double* dMass, const double* dFriction, const double* dRestitution, double* pos,
+						   double* rot, double* vel, double* angVel, int32_t capacity)
 {
 	if (t->steps.empty() || t->checkpointStep.empty())
 	{
 		return M3D_GPU_ERR_ARGUMENT;
 	}
 	const int32_t m = t->nBodies < capacity ? t->nBodies : capacity;
-	const Perturbation d = { dVel, dMass, dFriction, dRestitution };
+	const Perturbation d = { dVel, dAngVel, dMass, dFriction, dRestitution };
 	if (doublePrecision)
 	{
 		std::vector<Body<double>> out;

@@ -302,8 +302,8 @@ int32_t tapeBackward(DiffTape* t, DevWorld& w, const float* dPos, const float* d
 int32_t tapeBackwardHost(DiffTape* t, const double* dPos, const double* dRot, const double* dVel,
 						 const double* dAngVel, double* gPos, double* gRot, double* gVel, double* gAngVel,
 						 double* gMass, double* gFriction, double* gRestitution, int32_t capacity);
-int32_t tapeRegenerateHost(DiffTape* t, int doublePrecision, const double* dVel, const double* dMass,
-						   const double* dFriction, const double* dRestitution, double* pos, double* rot, double* vel,
-						   double* angVel, int32_t capacity);
+int32_t tapeRegenerateHost(DiffTape* t, int doublePrecision, const double* dVel, const double* dAngVel,
+						   const double* dMass, const double* dFriction, const double* dRestitution, double* pos,
+						   double* rot, double* vel, double* angVel, int32_t capacity);
 
 } // namespace m3g

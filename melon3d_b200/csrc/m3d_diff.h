@@ -426,7 +426,14 @@ M3D_DIFF_HD void integrate_rev(const Body<T>& s0, const BodyConst<T>& c, T h, V<
 	}
 	else
 	{
+		// no spin: the engine leaves the rotation as it is.  The rotation is
+		// still a smooth function of the spin through zero (any spin takes
+		// the small-angle branch, q1 = q0 + h/2 (w, 0) q0 to first order), so
+		// the spin's adjoint is that branch's limit.
 		s0b.q = qadd(s0b.q, s1b.q);
+		Q<T> dqb = qzero<T>(), unused = qzero<T>();
+		qmul_rev(q4<T>(T(0), T(0), T(0), T(1)), s0.q, s1b.q, dqb, unused);
+		wb = madd(wb, T(0.5) * h, v3<T>(dqb.x, dqb.y, dqb.z));
 	}
 	s0b.w = madd(s0b.w, ca, wb);
 	cb.il += iw_rev_isotropic(iwb);

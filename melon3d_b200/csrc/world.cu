@@ -2329,17 +2329,17 @@ int32_t m3d_gpu_step_backward_fp64_host(m3d_world* world, const double* dPositio
 }
 
 int32_t m3d_gpu_tape_regenerate_host(m3d_world* world, int32_t doublePrecision, const double* dVelocities,
-									 const double* dMass, const double* dFriction, const double* dRestitution,
-									 double* positions, double* rotations, double* velocities,
-									 double* angularVelocities, int32_t capacity)
+									 const double* dAngularVelocities, const double* dMass, const double* dFriction,
+									 const double* dRestitution, double* positions, double* rotations,
+									 double* velocities, double* angularVelocities, int32_t capacity)
 {
 	int32_t rc = tapeUsable(world);
 	if (rc != M3D_GPU_OK)
 	{
 		return rc;
 	}
-	return tapeRegenerateHost(world->tape, doublePrecision, dVelocities, dMass, dFriction, dRestitution, positions,
-							  rotations, velocities, angularVelocities, capacity);
+	return tapeRegenerateHost(world->tape, doublePrecision, dVelocities, dAngularVelocities, dMass, dFriction,
+							  dRestitution, positions, rotations, velocities, angularVelocities, capacity);
 }
 
 } // extern "C"

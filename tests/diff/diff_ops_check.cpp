@@ -254,7 +254,9 @@ double check_integrate(uint64_t seed)
 	put(x, rv(g, 2));
 	put(x, rq(g));
 	put(x, rv(g, 2));
-	put(x, rv(g, seed % 2 ? 20.0 : 0.5)); // both rotation branches
+	// both rotation branches, and no spin at all (its adjoint is the
+	// small-angle branch's limit)
+	put(x, seed % 3 == 2 ? v3<D>(0, 0, 0) : rv(g, seed % 2 ? 20.0 : 0.5));
 	x.push_back(c.il);
 	std::vector<D> w(13 + 9);
 	for (auto& v : w)
