@@ -32,6 +32,8 @@ import time
 
 import ctypes as C
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -87,6 +89,8 @@ def parse():
     p.add_argument("--batch-worlds", type=int, default=4096)
     p.add_argument("--batch-steps", type=int, default=40)
     p.add_argument("--pile-steps", type=int, default=12)
+    p.add_argument("--adjoint-worlds", type=int, default=1024)
+    p.add_argument("--adjoint-steps", type=int, default=120)
     return p.parse_args()
 
 
@@ -302,6 +306,66 @@ def measure_batch(lib, args, ref_lib):
     return out
 
 
+def _incline_batch(lib, W):
+    scenes = [harness.Scene(lib, harness.INCLINE, k) for k in range(W)]
+    ids = [s.dynamic_ids() for s in scenes]
+    arr = (C.c_void_p * W)(*[s.world for s in scenes])
+    batch = lib.m3d_gpu_batch_create(arr, W)
+    slots = [[lib.m3d_gpu_batch_first_body(batch, k) + i.index for i in ids[k]] for k in range(W)]
+    for s in scenes:
+        s.close()
+    return batch, slots
+
+
+def measure_adjoint(lib, args):
+    """Differentiable batch: 1024 incline worlds x 64 bodies, 120 steps at
+    60 Hz x 4 substeps; loss = sum over worlds of |centroid - target|^2 with
+    seeded targets; gradients of v0, masses, friction, restitution from
+    m3d_gpu_step_backward with checkpoints every 10 steps.  Forward alone
+    against forward with the tape plus the backward, on the same worlds."""
+    W, steps = args.adjoint_worlds, args.adjoint_steps
+    batch, slots = _incline_batch(lib, W)
+    bodies = sum(len(s) for s in slots)
+    fwd_dev, fwd_wall = _device_steps(lib, batch, steps, args.substeps, bodies)
+    lib.m3d_world_destroy(batch)
+    batch, slots = _incline_batch(lib, W)
+    assert lib.m3d_gpu_tape_begin(batch, 10) == 0
+    rec_dev, rec_wall = _device_steps(lib, batch, steps, args.substeps, bodies)
+    why = C.create_string_buffer(200)
+    supported = lib.m3d_gpu_tape_supported(batch, why, 200) == 1
+    n = lib.m3d_gpu_body_capacity(batch)
+    pos = (C.c_float * (3 * n))()
+    lib.m3d_gpu_read_poses(batch, pos, None, n)
+    p = np.frombuffer(pos, dtype=np.float32).reshape(n, 3).astype(np.float64)
+    targets = np.random.default_rng(5).normal(size=(W, 3))
+    dpos = np.zeros((n, 3), np.float32)
+    loss = 0.0
+    for k, s in enumerate(slots):
+        r = p[s].mean(axis=0) - targets[k]
+        loss += float(r @ r)
+        dpos[s] = (2.0 * r / len(s)).astype(np.float32)
+    g = {k: np.zeros((n, 3) if k in ("pos", "vel", "ang") else ((n, 4) if k == "rot" else n), np.float32)
+         for k in ("pos", "rot", "vel", "ang", "mass", "mu", "e")}
+    fp = C.POINTER(C.c_float)
+    t = time.perf_counter()
+    rc = lib.m3d_gpu_step_backward(batch, dpos.ctypes.data_as(fp), None, None, None,
+                                   *[g[k].ctypes.data_as(fp) for k in ("pos", "rot", "vel", "ang", "mass", "mu", "e")], n)
+    bwd_wall = (time.perf_counter() - t) * 1000.0
+    lib.m3d_world_destroy(batch)
+    work = bodies * args.substeps * steps
+    total = rec_wall + bwd_wall
+    gv = np.concatenate([g["vel"][s] for s in slots])
+    return {"workload": "%d incline worlds x 64 bodies (cubes and spheres 0.1-0.3 m, v0~N(0,1), mu~U[0.2,0.9], "
+                        "e~U[0,0.3]), %d steps, checkpoints every 10" % (W, steps),
+            "bodies": bodies, "steps": steps, "status": rc, "tape_supported": supported,
+            "value": work / (total / 1000.0), "unit": "body-substeps/s",
+            "forward_ms": fwd_wall, "forward_device_ms": fwd_dev,
+            "recorded_forward_ms": rec_wall, "recorded_forward_device_ms": rec_dev, "backward_ms": bwd_wall,
+            "fwd_plus_adjoint_over_forward": total / fwd_wall,
+            "loss": loss, "grad_v0_norm": float(np.linalg.norm(gv)),
+            "grad_v0_median_abs": float(np.median(np.abs(gv)))}
+
+
 def main():
     args = parse()
     d = Dist(args.gpus)
@@ -401,7 +465,8 @@ def main():
     variants = None
     if d.rank == 0 and d.world == 1 and not args.no_variants:
         ref_lib = api.bind(C.CDLL(REF_RELEASE_LIB)) if os.path.exists(REF_RELEASE_LIB) else None
-        variants = {"batched": measure_batch(lib, args, ref_lib), "pile": measure_pile(lib, args, ref_lib)}
+        variants = {"batched": measure_batch(lib, args, ref_lib), "pile": measure_pile(lib, args, ref_lib),
+                    "fwd_adjoint": measure_adjoint(lib, args)}
     if d.rank == 0:
         line = {"metric": "body-substeps/s", "value": total_bs / (dev_ms_max / 1000.0), "unit": "body-substeps/s",
                 "n_gpus": d.world, "steps": args.steps, "warmup": args.warmup,

@@ -27,6 +27,7 @@
 #include <stdio.h>
 #include <string.h>
 #include <algorithm>
+#include <memory>
 #include <vector>
 
 namespace m3g
@@ -71,9 +72,36 @@ struct GrowBuf
 	char* at(size_t offsetBytes) const { return (char*)buf.ptr + offsetBytes; }
 };
 
+// Contact records: bump-allocated in large device chunks that never move
+// (a tape of a long trajectory holds gigabytes; growing one buffer by
+// doubling would copy them over and over).
+struct ChunkArena
+{
+	static constexpr size_t kChunkBytes = size_t(512) << 20;
+	std::vector<std::unique_ptr<DevBuf>> chunks;
+	size_t used = 0; // bytes used in the last chunk
+	// room for `bytes` at the end of the last chunk (a new chunk if needed)
+	char* reserve(size_t bytes)
+	{
+		if (chunks.empty() || used + bytes > chunks.back()->bytes)
+		{
+			std::unique_ptr<DevBuf> c(new DevBuf());
+			if (!c->ensure(bytes > kChunkBytes ? bytes : kChunkBytes))
+			{
+				return nullptr;
+			}
+			chunks.push_back(std::move(c));
+			used = 0;
+		}
+		return (char*)chunks.back()->ptr + used;
+	}
+	void commit(size_t bytes) { used += bytes; }
+};
+
 struct TapeStep
 {
-	size_t islandOff, bodyOff, contactOff, sleepOff, posOff; // element offsets into the tape buffers
+	size_t islandOff, bodyOff, sleepOff, posOff; // element offsets into the tape buffers
+	const TapeContact* recs;                     // [substep * contactsPerSubstep + position]
 	int32_t islands, bodies, contactsPerSubstep, sleeps;
 	float dt;
 	int substeps, iterations;
@@ -90,7 +118,8 @@ struct DiffTape
 	char why[160] = { 0 };
 	std::vector<TapeStep> steps;
 	std::vector<int> checkpointStep; // step index of each checkpoint
-	GrowBuf islands, bodies, contacts, sleeps, checkpoints;
+	GrowBuf islands, bodies, sleeps, checkpoints;
+	ChunkArena contacts;
 	GrowBuf prevPos; // per step and contact position: the contact's position in the previous step, or -1
 	DevBuf bodyConst, muBody, eBody, shapes, sleepScratch, flags;
 	DevBuf hashKeys, hashVals; // body-pair key -> position in the previous step
@@ -362,14 +391,15 @@ void tapeStepBegin(DiffTape* t, DevWorld& w, int32_t n, float dt, int substeps, 
 void tapeBeforeIslands(DiffTape* t, DevWorld& w, int substeps)
 {
 	const size_t bound = (size_t)substeps * (size_t)(w.contactMax + 1);
-	if (!t->supported || !t->contacts.reserve(t->contacts.used + bound * sizeof(TapeContact), w.stream))
+	char* room = t->supported ? t->contacts.reserve(bound * sizeof(TapeContact)) : nullptr;
+	if (room == nullptr)
 	{
 		tapeMarkUnsupported(t, "tape allocation failed");
 		w.tapeContacts = nullptr;
 		w.sleepRecord = nullptr;
 		return;
 	}
-	w.tapeContacts = (TapeContact*)t->contacts.at(t->contacts.used);
+	w.tapeContacts = (TapeContact*)room;
 	w.sleepRecord = t->sleepScratch.as<uint32_t>();
 }
 
@@ -387,7 +417,7 @@ void tapeStepEnd(DiffTape* t, DevWorld& w, const StepCounters& hc)
 	st.sleeps = (int32_t)hc.sleptBodies;
 	st.islandOff = t->islands.used / sizeof(TapeIsland);
 	st.bodyOff = t->bodies.used / sizeof(int32_t);
-	st.contactOff = t->contacts.used / sizeof(TapeContact);
+	st.recs = w.tapeContacts;
 	st.sleepOff = t->sleeps.used / sizeof(uint32_t);
 	st.posOff = t->prevPos.used / sizeof(int32_t);
 	if (hc.coloredIslands + hc.giantIslands > 0)
@@ -429,7 +459,7 @@ void tapeStepEnd(DiffTape* t, DevWorld& w, const StepCounters& hc)
 		{
 			// each contact's position in the previous recorded step
 			int32_t* out = (int32_t*)t->prevPos.at(t->prevPos.used);
-			const TapeContact* cur = (const TapeContact*)t->contacts.at(t->contacts.used);
+			const TapeContact* cur = st.recs;
 			const TapeStep* prev = t->steps.empty() ? nullptr : &t->steps.back();
 			if (prev == nullptr || prev->contactsPerSubstep == 0)
 			{
@@ -447,8 +477,7 @@ void tapeStepEnd(DiffTape* t, DevWorld& w, const StepCounters& hc)
 				{
 					t->hashMask = slots - 1;
 					cudaMemsetAsync(t->hashKeys.ptr, 0xFF, sizeof(unsigned long long) * slots, s);
-					const TapeContact* before =
-						(const TapeContact*)t->contacts.at(prev->contactOff * sizeof(TapeContact));
+					const TapeContact* before = prev->recs;
 					M3G_LAUNCH(kPairInsert, blocksFor(prev->contactsPerSubstep, 256), 256, s, before,
 							   prev->contactsPerSubstep, t->hashKeys.as<unsigned long long>(), t->hashVals.as<int32_t>(),
 							   t->hashMask);
@@ -469,7 +498,7 @@ void tapeStepEnd(DiffTape* t, DevWorld& w, const StepCounters& hc)
 		t->bodies.used += sizeof(int32_t) * (size_t)st.bodies;
 		t->sleeps.used += sizeof(uint32_t) * (size_t)st.sleeps;
 		t->prevPos.used += sizeof(int32_t) * (size_t)st.contactsPerSubstep;
-		t->contacts.used += sizeof(TapeContact) * (size_t)st.substeps * (size_t)st.contactsPerSubstep;
+		t->contacts.commit(sizeof(TapeContact) * (size_t)st.substeps * (size_t)st.contactsPerSubstep);
 		t->steps.push_back(st);
 	}
 	w.recording = false;
@@ -601,6 +630,7 @@ IslandCtx<T> makeCtx(const Work<T>& k, const BodyConst<T>* bc, const T* mu, cons
 					 const TapeContact* prevContacts = nullptr, const int32_t* prevPos = nullptr)
 {
 	IslandCtx<T> x;
+	x.genJ = nullptr;
 	x.live = nullptr;
 	x.liveIds = nullptr;
 	x.cbar = cbar;
@@ -686,6 +716,31 @@ __global__ void kTapeSleepCut(Body<float>* b, const uint32_t* list, int32_t n)
 	}
 }
 
+// The Jacobians of the step's narrowphase generations, one thread per
+// contact, at the step-start states (all the generations that happen at the
+// step's start; those in contact preparation are rare and are evaluated by
+// the island's own thread).
+__global__ void __launch_bounds__(128)
+	kTapeGenJacobian(const TapeContact* recs, int32_t n, const Body<float>* states, const BodyConst<float>* bc,
+					 const m3d_diff::TapeShape* shapes, float dt, double* J)
+{
+	const int p = blockIdx.x * blockDim.x + threadIdx.x;
+	if (p >= n)
+	{
+		return;
+	}
+	const TapeContact& rec = recs[p];
+	if (!(rec.gen & m3d_diff::kTapeGenNarrow) || (rec.gen & m3d_diff::kTapeGenPrepare))
+	{
+		return;
+	}
+	const Body<float>& A = states[rec.a];
+	const Body<float>& B = states[rec.b];
+	const float margin = m3d_diff::kGenSpeculativeBase + dt * m3d_diff::len(m3d_diff::sub(A.v, B.v));
+	m3d_diff::generationJacobian(bc, shapes, rec, A.x, A.q, B.x, B.q, margin,
+								 J + (size_t)p * (m3d_diff::kGenJRows * m3d_diff::kGenJCols));
+}
+
 // manifold adjoints carried to the previous step: contact p of this step is
 // contact prevPos[p] there (or new)
 __global__ void kTapeCarryBar(const m3d_diff::ContactBar<float>* cur, const int32_t* prevPos, int32_t n,
@@ -706,7 +761,7 @@ IslandCtx<float> deviceCtx(DiffTape* t, const Work<float>& k, const TapeStep& st
 	return makeCtx<float>(k, t->bodyConst.as<BodyConst<float>>(), t->muBody.as<float>(), t->eBody.as<float>(), st,
 						  (const TapeIsland*)t->islands.at(st.islandOff * sizeof(TapeIsland)),
 						  (const int32_t*)t->bodies.at(st.bodyOff * sizeof(int32_t)),
-						  (const TapeContact*)t->contacts.at(st.contactOff * sizeof(TapeContact)), t->nBodies);
+						  st.recs, t->nBodies);
 }
 
 // the records of step `step - 1` at its last substep (null when it has none)
@@ -717,8 +772,7 @@ const TapeContact* previousRecords(const DiffTape* t, int step)
 		return nullptr;
 	}
 	const TapeStep& p = t->steps[step - 1];
-	return (const TapeContact*)t->contacts.at(
-		(p.contactOff + (size_t)(p.substeps - 1) * (size_t)p.contactsPerSubstep) * sizeof(TapeContact));
+	return p.recs + (size_t)(p.substeps - 1) * (size_t)p.contactsPerSubstep;
 }
 
 // replay steps [s0, s1) from the state in k.cur; the start state of each step
@@ -849,6 +903,8 @@ int32_t tapeBackward(DiffTape* t, DevWorld& w, const float* dPos, const float* d
 	Body<float>* states = (Body<float>*)arena(sizeof(Body<float>) * (size_t)t->checkpointEvery * (size_t)(n + 1));
 	typedef m3d_diff::ContactBar<float> Bar;
 	Bar* bars[2] = { (Bar*)arena(sizeof(Bar) * (size_t)lim.positions), (Bar*)arena(sizeof(Bar) * (size_t)lim.positions) };
+	const size_t jPer = (size_t)m3d_diff::kGenJRows * m3d_diff::kGenJCols;
+	double* genJ = (double*)arena(sizeof(double) * jPer * (size_t)lim.positions);
 	int cur = 0;
 	if (!ok || !arena.ok)
 	{
@@ -883,7 +939,14 @@ int32_t tapeBackward(DiffTape* t, DevWorld& w, const float* dPos, const float* d
 			{
 				cudaMemcpyAsync(k.cur, states + (size_t)(step - s0) * n, sizeof(Body<float>) * (size_t)n,
 								cudaMemcpyDeviceToDevice, s);
+				if (st.contactsPerSubstep > 0)
+				{
+					M3G_LAUNCH(kTapeGenJacobian, blocksFor(st.contactsPerSubstep, 128), 128, s, st.recs,
+							   st.contactsPerSubstep, states + (size_t)(step - s0) * n,
+							   t->bodyConst.as<BodyConst<float>>(), t->shapes.as<m3d_diff::TapeShape>(), st.dt, genJ);
+				}
 				IslandCtx<float> x = deviceCtx(t, k, st);
+				x.genJ = genJ;
 				x.cbar = bars[cur];
 				x.shapes = t->shapes.as<m3d_diff::TapeShape>();
 				x.prevContacts = previousRecords(t, step);
@@ -973,8 +1036,12 @@ std::vector<HostStep> downloadSteps(const DiffTape* t)
 		const TapeStep& st = t->steps[q];
 		hs[q].islands = download<TapeIsland>(t->islands, st.islandOff * sizeof(TapeIsland), (size_t)st.islands);
 		hs[q].bodies = download<int32_t>(t->bodies, st.bodyOff * sizeof(int32_t), (size_t)st.bodies);
-		hs[q].contacts = download<TapeContact>(t->contacts, st.contactOff * sizeof(TapeContact),
-											   (size_t)st.substeps * (size_t)st.contactsPerSubstep);
+		hs[q].contacts.resize((size_t)st.substeps * (size_t)st.contactsPerSubstep);
+		if (!hs[q].contacts.empty())
+		{
+			cudaMemcpy(hs[q].contacts.data(), st.recs, sizeof(TapeContact) * hs[q].contacts.size(),
+					   cudaMemcpyDeviceToHost);
+		}
 		hs[q].sleeps = download<uint32_t>(t->sleeps, st.sleepOff * sizeof(uint32_t), (size_t)st.sleeps);
 		hs[q].prevPos = download<int32_t>(t->prevPos, st.posOff * sizeof(int32_t), (size_t)st.contactsPerSubstep);
 	}

@@ -331,7 +331,8 @@ __global__ void __launch_bounds__(32 * kSerialWarpsPerBlock)
 // loop in the reference's order (src/xpbd.cpp:898-974), 32 islands per warp.
 __global__ void __launch_bounds__(128)
 	kSolveTiny(BodySoA B, ContactSoA C, const IslandRec* islands, const int32_t* tinyList, const uint32_t* tinyDev,
-			   const uint32_t* bodyVals, const uint32_t* contactVals, SolveParams P)
+			   const uint32_t* bodyVals, const uint32_t* contactVals, SolveParams P, m3d_diff::TapeContact* tape,
+			   const uint32_t* tapeStride, const uint8_t* narrowGen)
 {
 	const int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= (int)*tinyDev)
@@ -349,7 +350,16 @@ __global__ void __launch_bounds__(128)
 		}
 		for (int c = 0; c < r.contactCount; ++c)
 		{
-			prepareContact(B, C, (int)contacts[c], P.h);
+			const int what = prepareContact(B, C, (int)contacts[c], P.h);
+			if (tape != nullptr)
+			{
+				int gen = what;
+				if (sub == 0 && narrowGen[contacts[c]] == kPrepRegenerated)
+				{
+					gen |= m3d_diff::kTapeGenNarrow;
+				}
+				writeTapeContact(tape[(size_t)sub * *tapeStride + r.contactStart + c], B, C, (int)contacts[c], gen);
+			}
 		}
 		for (int it = 0; it < P.iterations; ++it)
 		{
@@ -636,10 +646,11 @@ void launchSolve(DevWorld& w, float dt, int substeps, V3 gravity, int positionIt
 	int serialBlocks = (ni + kSerialWarpsPerBlock - 1) / kSerialWarpsPerBlock;
 	serialBlocks = serialBlocks < 148 * 8 ? serialBlocks : 148 * 8;
 	w.colorMask.ensure((size_t)(w.bodyCap + 1) * sizeof(uint32_t)); // also the serial islands' local body index
-	if (!w.recording && w.lastSerialIslands > kTinyModeIslands) // the island table listed tiny islands this step
+	if (w.lastSerialIslands > kTinyModeIslands) // the island table listed tiny islands this step
 	{
 		M3G_LAUNCH(kSolveTiny, blocksFor(ni, 128), 128, s, w.B, w.C, isl, w.tinyList.as<int32_t>(), &dc->tinyIslands,
-				   w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(), P);
+				   w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(), P, w.tapeContacts, &dc->islandContacts,
+				   w.tapeGen.as<uint8_t>());
 	}
 	M3G_LAUNCH(kSolveSerial, serialBlocks, 32 * kSerialWarpsPerBlock, s, w.B, w.C, w.joints.as<JointRec>(), isl,
 			   w.serialList.as<int32_t>(), &dc->warpIslands, w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(),

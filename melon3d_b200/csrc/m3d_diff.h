@@ -32,8 +32,13 @@
 
 #if defined(__CUDACC__)
 #define M3D_DIFF_HD __host__ __device__ __forceinline__
+// a real call on the device: for the few large functions (the dual-number
+// manifold generation) whose inlined copies would only cost registers and
+// compile time
+#define M3D_DIFF_HD_CALL __host__ __device__ __noinline__
 #else
 #define M3D_DIFF_HD inline
+#define M3D_DIFF_HD_CALL inline
 #endif
 
 namespace m3d_diff
@@ -1651,6 +1656,7 @@ struct IslandCtx
 	const TapeContact* prevContacts; // the previous step's records (its last substep), or null
 	const int32_t* prevPos;          // per position: the contact's position in the previous step, or -1
 	T dt;                            // step length (narrowphase margin)
+	const double* genJ;              // per position: the narrowphase generation's Jacobian, or null (computed here)
 	// regenerating replay (verification): when set, the manifolds are state
 	// carried here and regenerated at the recorded generation events instead
 	// of read from the tape
@@ -1669,7 +1675,7 @@ M3D_DIFF_HD void regenerateLive(const IslandCtx<T>& x, const TapeContact& rec, i
 								Q<T> qB, T margin);
 
 template <typename T>
-M3D_DIFF_HD void substepForward(const IslandCtx<T>& x, const TapeIsland& r, int sub, bool record)
+M3D_DIFF_HD_CALL void substepForward(const IslandCtx<T>& x, const TapeIsland& r, int sub, bool record)
 {
 	const BodyConst<T>* bc = x.bc;
 	for (int k = 0; k < r.bodyCount; ++k)
@@ -1860,57 +1866,69 @@ M3D_DIFF_HD void scatterMaterials(const IslandCtx<T>& x, const Contact<T>& c, T 
 
 // ---- manifold generation events ---------------------------------------------------
 
-template <typename T, int N>
-M3D_DIFF_HD Dual<T, N> seeded(T v, int k)
-{
-	Dual<T, N> r(v);
-	r.d[k] = T(1);
-	return r;
-}
+// Jacobian of a manifold generation (reference src/collide.cpp:813-859 with
+// the offsets of src/world.cpp:1738-1845) with respect to the generation
+// poses: J[o * kGenJCols + k], rows o = the normal (3), then per recorded
+// point i (up to 4, matched to the generated points by feature id) its local
+// anchors on A (3) and B (3) and its separation offset (1); columns k = A's
+// position and rotation (0..6), then B's (7..13).  Forward-mode dual numbers
+// carry only the seeded (dynamic) bodies' columns: N = 7 or 14.  Rows of an
+// unmatched point, and all rows when the generated normal is not the
+// recorded one, are zero.
+constexpr int kGenJRows = 31;
+constexpr int kGenJCols = 14;
 
-// Adds to the pose adjoints of the contact's bodies the adjoint that the
-// manifold data carries (cb: normal, local anchors, separation offsets),
-// through the generation at poses (xA, qA), (xB, qB) with the given margin.
-// Points are matched to the recorded ones by feature id.
-template <typename T>
-M3D_DIFF_HD void generationAdjoint(const IslandCtx<T>& x, const TapeContact& rec, V<T> xA, Q<T> qA, V<T> xB, Q<T> qB,
-								   T margin, const ContactBar<T>& cb)
+template <typename T, int N>
+M3D_DIFF_HD_CALL void generationJacobianN(const TapeShape& shA, const TapeShape& shB, const TapeContact& rec, V<T> xA,
+										  Q<T> qA, V<T> xB, Q<T> qB, T margin, bool seedA, bool seedB, double* J)
 {
-	typedef Dual<T, 14> S;
-	const int a = rec.a, b = rec.b;
-	const bool dynA = x.bc[a].dynamic != 0, dynB = x.bc[b].dynamic != 0;
-	if ((!dynA && !dynB) || rec.pointCount == 0)
+	typedef Dual<T, N> S;
+	for (int o = 0; o < kGenJRows * kGenJCols; ++o)
 	{
-		return;
+		J[o] = 0.0;
 	}
 	GenShape<S> sa, sb;
-	sa.type = x.shapes[a].type;
-	sa.radius = S(T(x.shapes[a].radius));
-	sa.he = v3<S>(S(T(x.shapes[a].he[0])), S(T(x.shapes[a].he[1])), S(T(x.shapes[a].he[2])));
-	sb.type = x.shapes[b].type;
-	sb.radius = S(T(x.shapes[b].radius));
-	sb.he = v3<S>(S(T(x.shapes[b].he[0])), S(T(x.shapes[b].he[1])), S(T(x.shapes[b].he[2])));
-	V<S> gxA = v3<S>(seeded<T, 14>(xA.x, 0), seeded<T, 14>(xA.y, 1), seeded<T, 14>(xA.z, 2));
-	Q<S> gqA = q4<S>(seeded<T, 14>(qA.x, 3), seeded<T, 14>(qA.y, 4), seeded<T, 14>(qA.z, 5), seeded<T, 14>(qA.w, 6));
-	V<S> gxB = v3<S>(seeded<T, 14>(xB.x, 7), seeded<T, 14>(xB.y, 8), seeded<T, 14>(xB.z, 9));
-	Q<S> gqB =
-		q4<S>(seeded<T, 14>(qB.x, 10), seeded<T, 14>(qB.y, 11), seeded<T, 14>(qB.z, 12), seeded<T, 14>(qB.w, 13));
+	sa.type = shA.type;
+	sa.radius = S(T(shA.radius));
+	sa.he = v3<S>(S(T(shA.he[0])), S(T(shA.he[1])), S(T(shA.he[2])));
+	sb.type = shB.type;
+	sb.radius = S(T(shB.radius));
+	sb.he = v3<S>(S(T(shB.he[0])), S(T(shB.he[1])), S(T(shB.he[2])));
+	// dual slots: A's pose first when A is seeded, then B's
+	const int oA = 0, oB = seedA ? 7 : 0;
+	V<S> gxA = v3<S>(S(xA.x), S(xA.y), S(xA.z));
+	Q<S> gqA = q4<S>(S(qA.x), S(qA.y), S(qA.z), S(qA.w));
+	V<S> gxB = v3<S>(S(xB.x), S(xB.y), S(xB.z));
+	Q<S> gqB = q4<S>(S(qB.x), S(qB.y), S(qB.z), S(qB.w));
+	if (seedA)
+	{
+		gxA.x.d[oA + 0] = gxA.y.d[oA + 1] = gxA.z.d[oA + 2] = 1.0;
+		gqA.x.d[oA + 3] = gqA.y.d[oA + 4] = gqA.z.d[oA + 5] = gqA.w.d[oA + 6] = 1.0;
+	}
+	if (seedB)
+	{
+		gxB.x.d[oB + 0] = gxB.y.d[oB + 1] = gxB.z.d[oB + 2] = 1.0;
+		gqB.x.d[oB + 3] = gqB.y.d[oB + 4] = gqB.z.d[oB + 5] = gqB.w.d[oB + 6] = 1.0;
+	}
 	GenManifold<S> g;
 	genManifold(sa, gxA, gqA, sb, gxB, gqB, S(margin), g);
-	T acc[14];
-	for (int k = 0; k < 14; ++k)
-	{
-		acc[k] = T(0);
-	}
 	const bool sameNormal =
 		g.count > 0 && g.n.x.v * T(rec.n[0]) + g.n.y.v * T(rec.n[1]) + g.n.z.v * T(rec.n[2]) > T(0.999);
 	if (!sameNormal)
 	{
 		return;
 	}
-	for (int k = 0; k < 14; ++k)
+	// dual slot k -> Jacobian column
+	int col[N];
+	for (int k = 0; k < N; ++k)
 	{
-		acc[k] += cb.n.x * g.n.x.d[k] + cb.n.y * g.n.y.d[k] + cb.n.z * g.n.z.d[k];
+		col[k] = (seedA && k < 7) ? k : 7 + (k - oB);
+	}
+	for (int k = 0; k < N; ++k)
+	{
+		J[0 * kGenJCols + col[k]] = g.n.x.d[k];
+		J[1 * kGenJCols + col[k]] = g.n.y.d[k];
+		J[2 * kGenJCols + col[k]] = g.n.z.d[k];
 	}
 	for (int i = 0; i < rec.pointCount; ++i)
 	{
@@ -1928,23 +1946,107 @@ M3D_DIFF_HD void generationAdjoint(const IslandCtx<T>& x, const TapeContact& rec
 			continue;
 		}
 		const GenPoint<S>& gp = g.p[j];
-		for (int k = 0; k < 14; ++k)
+		double* r = J + (3 + 7 * i) * kGenJCols;
+		for (int k = 0; k < N; ++k)
 		{
-			acc[k] += cb.la[i].x * gp.la.x.d[k] + cb.la[i].y * gp.la.y.d[k] + cb.la[i].z * gp.la.z.d[k] +
-					  cb.lb[i].x * gp.lb.x.d[k] + cb.lb[i].y * gp.lb.y.d[k] + cb.lb[i].z * gp.lb.z.d[k] +
-					  cb.off[i] * gp.off.d[k];
+			r[0 * kGenJCols + col[k]] = gp.la.x.d[k];
+			r[1 * kGenJCols + col[k]] = gp.la.y.d[k];
+			r[2 * kGenJCols + col[k]] = gp.la.z.d[k];
+			r[3 * kGenJCols + col[k]] = gp.lb.x.d[k];
+			r[4 * kGenJCols + col[k]] = gp.lb.y.d[k];
+			r[5 * kGenJCols + col[k]] = gp.lb.z.d[k];
+			r[6 * kGenJCols + col[k]] = gp.off.d[k];
 		}
 	}
-	if (dynA)
+}
+
+// the Jacobian of the contact's generation, for its dynamic bodies
+template <typename T>
+M3D_DIFF_HD void generationJacobian(const BodyConst<T>* bc, const TapeShape* shapes, const TapeContact& rec, V<T> xA,
+									Q<T> qA, V<T> xB, Q<T> qB, T margin, double* J)
+{
+	const bool dynA = bc[rec.a].dynamic != 0, dynB = bc[rec.b].dynamic != 0;
+	if ((!dynA && !dynB) || rec.pointCount == 0)
 	{
-		x.adj[a].x = add(x.adj[a].x, v3<T>(acc[0], acc[1], acc[2]));
-		x.adj[a].q = qadd(x.adj[a].q, q4<T>(acc[3], acc[4], acc[5], acc[6]));
+		for (int o = 0; o < kGenJRows * kGenJCols; ++o)
+		{
+			J[o] = 0.0;
+		}
+		return;
 	}
-	if (dynB)
+	if (dynA && dynB)
 	{
-		x.adj[b].x = add(x.adj[b].x, v3<T>(acc[7], acc[8], acc[9]));
-		x.adj[b].q = qadd(x.adj[b].q, q4<T>(acc[10], acc[11], acc[12], acc[13]));
+		generationJacobianN<T, 14>(shapes[rec.a], shapes[rec.b], rec, xA, qA, xB, qB, margin, true, true, J);
 	}
+	else
+	{
+		generationJacobianN<T, 7>(shapes[rec.a], shapes[rec.b], rec, xA, qA, xB, qB, margin, dynA, dynB, J);
+	}
+}
+
+// Adds J^T (adjoint of the manifold data) to the pose adjoints of the
+// contact's dynamic bodies, summed in double.
+template <typename T>
+M3D_DIFF_HD void applyGenerationJacobian(const IslandCtx<T>& x, const TapeContact& rec, const double* J,
+										 const ContactBar<T>& cb)
+{
+	T bar[kGenJRows];
+	bar[0] = cb.n.x;
+	bar[1] = cb.n.y;
+	bar[2] = cb.n.z;
+	for (int i = 0; i < 4; ++i)
+	{
+		const bool on = i < rec.pointCount;
+		T* r = bar + 3 + 7 * i;
+		r[0] = on ? cb.la[i].x : T(0);
+		r[1] = on ? cb.la[i].y : T(0);
+		r[2] = on ? cb.la[i].z : T(0);
+		r[3] = on ? cb.lb[i].x : T(0);
+		r[4] = on ? cb.lb[i].y : T(0);
+		r[5] = on ? cb.lb[i].z : T(0);
+		r[6] = on ? cb.off[i] : T(0);
+	}
+	double acc[kGenJCols];
+	for (int k = 0; k < kGenJCols; ++k)
+	{
+		acc[k] = 0.0;
+	}
+	for (int o = 0; o < kGenJRows; ++o)
+	{
+		if (bar[o] == T(0))
+		{
+			continue;
+		}
+		for (int k = 0; k < kGenJCols; ++k)
+		{
+			// a zero entry carries nothing (not even an infinite adjoint's NaN)
+			const double j = J[o * kGenJCols + k];
+			if (j != 0.0)
+			{
+				acc[k] += (double)bar[o] * j;
+			}
+		}
+	}
+	if (x.bc[rec.a].dynamic)
+	{
+		x.adj[rec.a].x = add(x.adj[rec.a].x, v3<T>(T(acc[0]), T(acc[1]), T(acc[2])));
+		x.adj[rec.a].q = qadd(x.adj[rec.a].q, q4<T>(T(acc[3]), T(acc[4]), T(acc[5]), T(acc[6])));
+	}
+	if (x.bc[rec.b].dynamic)
+	{
+		x.adj[rec.b].x = add(x.adj[rec.b].x, v3<T>(T(acc[7]), T(acc[8]), T(acc[9])));
+		x.adj[rec.b].q = qadd(x.adj[rec.b].q, q4<T>(T(acc[10]), T(acc[11]), T(acc[12]), T(acc[13])));
+	}
+}
+
+// the adjoint of a generation computed on the spot
+template <typename T>
+M3D_DIFF_HD_CALL void generationAdjoint(const IslandCtx<T>& x, const TapeContact& rec, V<T> xA, Q<T> qA, V<T> xB,
+										Q<T> qB, T margin, const ContactBar<T>& cb)
+{
+	double J[kGenJRows * kGenJCols];
+	generationJacobian(x.bc, x.shapes, rec, xA, qA, xB, qB, margin, J);
+	applyGenerationJacobian(x, rec, J, cb);
 }
 
 // The stiction anchors a generated manifold starts with are fresh (equal to
@@ -1991,11 +2093,18 @@ M3D_DIFF_HD void generationAnchors(const TapeContact& rec, const uint32_t* oldId
 // generation poses; cb becomes the old manifold's adjoint.
 template <typename T>
 M3D_DIFF_HD void reverseGeneration(const IslandCtx<T>& x, const TapeContact& rec, const TapeContact* old, V<T> xA,
-								   Q<T> qA, V<T> xB, Q<T> qB, T margin, ContactBar<T>& cb)
+								   Q<T> qA, V<T> xB, Q<T> qB, T margin, ContactBar<T>& cb, const double* J = nullptr)
 {
 	ContactBar<T> cbOld;
 	generationAnchors(rec, old != nullptr ? old->id : nullptr, old != nullptr ? old->pointCount : 0, cb, cbOld);
-	generationAdjoint(x, rec, xA, qA, xB, qB, margin, cb);
+	if (J != nullptr)
+	{
+		applyGenerationJacobian(x, rec, J, cb);
+	}
+	else
+	{
+		generationAdjoint(x, rec, xA, qA, xB, qB, margin, cb);
+	}
 	cb = cbOld;
 }
 
@@ -2071,7 +2180,7 @@ M3D_DIFF_HD const TapeContact* previousRecord(const IslandCtx<T>& x, int pos)
 }
 
 template <typename T>
-M3D_DIFF_HD void substepReverse(const IslandCtx<T>& x, const TapeIsland& r, int sub)
+M3D_DIFF_HD_CALL void substepReverse(const IslandCtx<T>& x, const TapeIsland& r, int sub)
 {
 	const BodyConst<T>* bc = x.bc;
 	const TapeContact* tc = x.contacts + (size_t)sub * x.contactsPerSubstep;
@@ -2366,7 +2475,8 @@ M3D_DIFF_HD void islandStepBackward(const IslandCtx<T>& x)
 			const Body<T>& A = x.cur[rec.a];
 			const Body<T>& B = x.cur[rec.b];
 			const T margin = T(kGenSpeculativeBase) + x.dt * len(m3d_diff::sub(A.v, B.v));
-			reverseGeneration(x, rec, previousRecord(x, pos), A.x, A.q, B.x, B.q, margin, x.cbar[pos]);
+			reverseGeneration(x, rec, previousRecord(x, pos), A.x, A.q, B.x, B.q, margin, x.cbar[pos],
+							  x.genJ != nullptr ? x.genJ + (size_t)pos * (kGenJRows * kGenJCols) : nullptr);
 		}
 	}
 }

@@ -24,20 +24,22 @@ namespace m3d_diff
 
 // ---- dual numbers -------------------------------------------------------------
 
+// value in T (float: the engine's own rounding, so its branches), derivatives
+// in double (a generation's derivative terms cancel strongly)
 template <typename T, int N>
 struct Dual
 {
 	T v;
-	T d[N];
+	double d[N];
 	M3D_DIFF_HD Dual() : v(T(0))
 	{
 		for (int i = 0; i < N; ++i)
-			d[i] = T(0);
+			d[i] = 0.0;
 	}
 	M3D_DIFF_HD Dual(T x) : v(x)
 	{
 		for (int i = 0; i < N; ++i)
-			d[i] = T(0);
+			d[i] = 0.0;
 	}
 };
 
@@ -74,7 +76,7 @@ M3D_DIFF_HD Dual<T, N> operator*(const Dual<T, N>& a, const Dual<T, N>& b)
 	Dual<T, N> r;
 	r.v = a.v * b.v;
 	for (int i = 0; i < N; ++i)
-		r.d[i] = a.d[i] * b.v + a.v * b.d[i];
+		r.d[i] = a.d[i] * (double)b.v + (double)a.v * b.d[i];
 	return r;
 }
 template <typename T, int N>
@@ -82,8 +84,9 @@ M3D_DIFF_HD Dual<T, N> operator/(const Dual<T, N>& a, const Dual<T, N>& b)
 {
 	Dual<T, N> r;
 	r.v = a.v / b.v;
+	const double q = (double)a.v / (double)b.v, ib = 1.0 / (double)b.v;
 	for (int i = 0; i < N; ++i)
-		r.d[i] = (a.d[i] - r.v * b.d[i]) / b.v;
+		r.d[i] = (a.d[i] - q * b.d[i]) * ib;
 	return r;
 }
 template <typename T, int N>
@@ -111,7 +114,7 @@ M3D_DIFF_HD Dual<T, N> dsqrt(const Dual<T, N>& a)
 {
 	Dual<T, N> r;
 	r.v = dsqrt(a.v);
-	const T k = r.v > T(0) ? T(0.5) / r.v : T(0);
+	const double k = r.v > T(0) ? 0.5 / dsqrt((double)a.v) : 0.0;
 	for (int i = 0; i < N; ++i)
 		r.d[i] = k * a.d[i];
 	return r;
@@ -229,7 +232,7 @@ M3D_DIFF_HD V<S> gClampBox(V<S> p, V<S> e)
 }
 
 template <typename S>
-M3D_DIFF_HD void gSphereBox(S ra, V<S> xA, Q<S> qA, V<S> e, V<S> xB, Q<S> qB, S margin, GenManifold<S>& m)
+M3D_DIFF_HD_CALL void gSphereBox(S ra, V<S> xA, Q<S> qA, V<S> e, V<S> xB, Q<S> qB, S margin, GenManifold<S>& m)
 {
 	V<S> c = gXfInvPoint(xB, qB, xA);
 	V<S> q = gClampBox(c, e);
@@ -286,7 +289,7 @@ struct GClip
 };
 
 template <typename S>
-M3D_DIFF_HD int gClipPoly(const GClip<S>* in, int inCount, V<S> n, S offset, uint32_t planeId, GClip<S>* out)
+M3D_DIFF_HD_CALL int gClipPoly(const GClip<S>* in, int inCount, V<S> n, S offset, uint32_t planeId, GClip<S>* out)
 {
 	int outCount = 0;
 	for (int i = 0; i < inCount; ++i)
@@ -315,7 +318,7 @@ M3D_DIFF_HD int gClipPoly(const GClip<S>* in, int inCount, V<S> n, S offset, uin
 }
 
 template <typename S>
-M3D_DIFF_HD void gSupportEdge(V<S> x, Q<S> qq, const M<S>& rot, V<S> e, V<S> dirWorld, V<S>* pOut, V<S>* qOut)
+M3D_DIFF_HD_CALL void gSupportEdge(V<S> x, Q<S> qq, const M<S>& rot, V<S> e, V<S> dirWorld, V<S>* pOut, V<S>* qOut)
 {
 	V<S> d = gMulvT(rot, dirWorld);
 	V<S> ad = v3<S>(dabs(d.x), dabs(d.y), dabs(d.z));
@@ -363,7 +366,7 @@ M3D_DIFF_HD S gProjRadius(const V<S>* axes, const S* ext, V<S> n)
 }
 
 template <typename S>
-M3D_DIFF_HD void gClosestSegSeg(V<S> p1, V<S> q1, V<S> p2, V<S> q2, V<S>* c1, V<S>* c2)
+M3D_DIFF_HD_CALL void gClosestSegSeg(V<S> p1, V<S> q1, V<S> p2, V<S> q2, V<S>* c1, V<S>* c2)
 {
 	V<S> d1 = sub(q1, p1);
 	V<S> d2 = sub(q2, p2);
@@ -416,7 +419,7 @@ M3D_DIFF_HD void gClosestSegSeg(V<S> p1, V<S> q1, V<S> p2, V<S> q2, V<S>* c1, V<
 }
 
 template <typename S>
-M3D_DIFF_HD void gBoxes(V<S> eA, V<S> xA, Q<S> qA, V<S> eB, V<S> xB, Q<S> qB, S margin, GenManifold<S>& m)
+M3D_DIFF_HD_CALL void gBoxes(V<S> eA, V<S> xA, Q<S> qA, V<S> eB, V<S> xB, Q<S> qB, S margin, GenManifold<S>& m)
 {
 	M<S> rotA = gQuatToMat(qA);
 	M<S> rotB = gQuatToMat(qB);
