@@ -565,15 +565,17 @@ bool carveWork(Work<T>& k, int32_t n, const Limits& l, Alloc alloc)
 	k.positions = l.positions;
 	k.cur = (Body<T>*)alloc(sizeof(Body<T>) * nb);
 	k.start = (Body<T>*)alloc(sizeof(Body<T>) * nb * (size_t)l.maxSub);
-	k.iw = (m3d_diff::M<T>*)alloc(sizeof(m3d_diff::M<T>) * nb);
-	k.x2 = (m3d_diff::V<T>*)alloc(sizeof(m3d_diff::V<T>) * nb);
-	k.q2 = (m3d_diff::Q<T>*)alloc(sizeof(m3d_diff::Q<T>) * nb);
-	k.prep = (m3d_diff::Prepared<T>*)alloc(sizeof(m3d_diff::Prepared<T>) * np);
-	k.lamN = (T*)alloc(sizeof(T) * 4 * np);
-	k.lamT = (T*)alloc(sizeof(T) * 4 * np);
-	k.normRec = (m3d_diff::PoseRec<T>*)alloc(sizeof(m3d_diff::PoseRec<T>) * np * (size_t)l.maxIt);
-	k.fricRec = (m3d_diff::PoseRec<T>*)alloc(sizeof(m3d_diff::PoseRec<T>) * np);
-	k.velRec = (m3d_diff::VelRec<T>*)alloc(sizeof(m3d_diff::VelRec<T>) * np);
+	// per-substep records: one slice per substep (see substepView)
+	const size_t S = (size_t)l.maxSub;
+	k.iw = (m3d_diff::M<T>*)alloc(sizeof(m3d_diff::M<T>) * nb * S);
+	k.x2 = (m3d_diff::V<T>*)alloc(sizeof(m3d_diff::V<T>) * nb * S);
+	k.q2 = (m3d_diff::Q<T>*)alloc(sizeof(m3d_diff::Q<T>) * nb * S);
+	k.prep = (m3d_diff::Prepared<T>*)alloc(sizeof(m3d_diff::Prepared<T>) * np * S);
+	k.lamN = (T*)alloc(sizeof(T) * 4 * np * S);
+	k.lamT = (T*)alloc(sizeof(T) * 4 * np * S);
+	k.normRec = (m3d_diff::PoseRec<T>*)alloc(sizeof(m3d_diff::PoseRec<T>) * np * (size_t)l.maxIt * S);
+	k.fricRec = (m3d_diff::PoseRec<T>*)alloc(sizeof(m3d_diff::PoseRec<T>) * np * S);
+	k.velRec = (m3d_diff::VelRec<T>*)alloc(sizeof(m3d_diff::VelRec<T>) * np * S);
 	k.adj = (Body<T>*)alloc(sizeof(Body<T>) * nb);
 	k.adj0 = (Body<T>*)alloc(sizeof(Body<T>) * nb);
 	k.imBar = (T*)alloc(sizeof(T) * nb);

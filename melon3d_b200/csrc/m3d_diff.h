@@ -2427,6 +2427,27 @@ M3D_DIFF_HD_CALL void substepReverse(const IslandCtx<T>& x, const TapeIsland& r,
 	}
 }
 
+// The slice of the per-substep records for substep `sub`: world inverse
+// inertias, poses before reconstruction, prepared contacts, impulses, pose
+// and velocity records (the work arrays hold one slice per substep; the
+// adjoint scratch is shared).
+template <typename T>
+M3D_DIFF_HD IslandCtx<T> substepView(const IslandCtx<T>& x, int sub)
+{
+	IslandCtx<T> y = x;
+	const size_t b = (size_t)sub * (size_t)x.bodyCount, p = (size_t)sub * (size_t)x.positions;
+	y.iw = x.iw + b;
+	y.x2 = x.x2 + b;
+	y.q2 = x.q2 + b;
+	y.prep = x.prep + p;
+	y.lamN = x.lamN + 4 * p;
+	y.lamT = x.lamT + 4 * p;
+	y.normRec = x.normRec + p * (size_t)x.iterations;
+	y.fricRec = x.fricRec + p;
+	y.velRec = x.velRec + p;
+	return y;
+}
+
 // One island through one step, backward: the state of its bodies at the
 // step's start is in cur; the adjoints of their state at the step's end in
 // adj.  On return adj holds the adjoints at the step's start and cur is
@@ -2435,25 +2456,15 @@ template <typename T>
 M3D_DIFF_HD void islandStepBackward(const IslandCtx<T>& x)
 {
 	const TapeIsland& r = *x.island;
-	Body<T> keep[1];
-	(void)keep;
-	// forward through the first substeps to reach each substep's start
+	// one recording pass forward (each substep's records in its own slice),
+	// then the substeps in reverse
 	for (int sub = 0; sub < x.substeps; ++sub)
 	{
-		substepForward(x, r, sub, false);
+		substepForward(substepView(x, sub), r, sub, true);
 	}
 	for (int sub = x.substeps - 1; sub >= 0; --sub)
 	{
-		for (int k = 0; k < r.bodyCount; ++k)
-		{
-			int i = x.bodies[r.bodyStart + k];
-			if (x.bc[i].dynamic)
-			{
-				x.cur[i] = x.start[(size_t)sub * x.bodyCount + i];
-			}
-		}
-		substepForward(x, r, sub, true);
-		substepReverse(x, r, sub);
+		substepReverse(substepView(x, sub), r, sub);
 	}
 	// cur: back to the step's start
 	for (int k = 0; k < r.bodyCount; ++k)
