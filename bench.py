@@ -91,6 +91,8 @@ def parse():
     p.add_argument("--pile-steps", type=int, default=12)
     p.add_argument("--adjoint-worlds", type=int, default=1024)
     p.add_argument("--adjoint-steps", type=int, default=120)
+    p.add_argument("--only-adjoint", action="store_true",
+                   help="run only the forward+adjoint measurement and print its JSON object")
     return p.parse_args()
 
 
@@ -391,6 +393,12 @@ def main():
     import torch
     torch.cuda.set_device(d.local)
     lib = api.load_gpu()
+    if args.only_adjoint:
+        if d.rank == 0:
+            print(json.dumps(measure_adjoint(lib, args)))
+        d.barrier()
+        d.close()
+        return
     scene = harness.Scene(lib, harness.RAIN, 2, args.bodies, args.churn, 0)
     world = scene.world
     scene.run(max(args.warmup, 3), args.substeps)
