@@ -14,8 +14,12 @@
 //
 // Backward, segment by segment from the last checkpoint down: the segment's
 // step-start states are recomputed by replaying the tape from its checkpoint
-// (the replay reproduces the engine bit for bit), then each step is reversed,
-// one thread per island, through islandStepBackward.  The adjoint of every
+// (the replay reproduces the engine bit for bit), then each step is reversed
+// in two launches, a recording forward (islandStepRecord) and the reverse
+// (islandStepReverse).  Islands with many contacts get a warp each, whose
+// lanes take the contacts of one dependency level at a time; the rest are
+// packed one per thread (the island table is ordered by contact count when it
+// is recorded).  The adjoint of every
 // contact's manifold data travels with it from step to step (ContactBar,
 // carried by the previous-position map) until the generation event that made
 // it, where it turns into adjoints of the generation poses.  Sleeping at a
@@ -25,6 +29,7 @@
 #include "melon3d_gpu.h"
 
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 #include <algorithm>
 #include <memory>
@@ -103,6 +108,7 @@ struct TapeStep
 	size_t islandOff, bodyOff, sleepOff, posOff; // element offsets into the tape buffers
 	const TapeContact* recs;                     // [substep * contactsPerSubstep + position]
 	int32_t islands, bodies, contactsPerSubstep, sleeps;
+	int32_t warpIslands; // islands [0, warpIslands) of the table are worked by a warp each
 	float dt;
 	int substeps, iterations;
 	float g[3];
@@ -114,6 +120,7 @@ struct DiffTape
 {
 	int checkpointEvery = 10;
 	int32_t nBodies = 0;
+	int32_t warpContacts = 8; // islands with at least this many contacts get a warp in the replay and backward
 	bool supported = true;
 	char why[160] = { 0 };
 	std::vector<TapeStep> steps;
@@ -124,6 +131,7 @@ struct DiffTape
 	DevBuf bodyConst, muBody, eBody, shapes, sleepScratch, flags;
 	DevBuf hashKeys, hashVals; // body-pair key -> position in the previous step
 	uint32_t hashMask = 0;
+	DevBuf islandRaw, orderKeys, orderVals; // island table before it is ordered
 	TapeStep pending;
 };
 
@@ -229,6 +237,37 @@ __global__ void kTapeIslands(const IslandRec* isl, const uint32_t* countDev, Tap
 	}
 }
 
+// Islands are independent (disjoint bodies and contacts, no sums across
+// them), so the replay and the backward may take them in any order.  The
+// table is ordered by falling contact count (then body count): the islands
+// with at least `warpContacts` contacts form its head, each worked by a warp
+// (its contacts level by level), and the rest are packed one per thread.
+__global__ void kIslandWorkKeys(const TapeIsland* isl, int32_t n, int32_t warpContacts, uint64_t* keys,
+								uint32_t* vals, uint32_t* warpCount)
+{
+	int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k < n)
+	{
+		const uint32_t c = (uint32_t)isl[k].contactCount, b = (uint32_t)isl[k].bodyCount;
+		const uint64_t work = ((uint64_t)(c < 0xFFFFFu ? c : 0xFFFFFu) << 12) | (b < 0xFFFu ? b : 0xFFFu);
+		keys[k] = 0xFFFFFFFFull - work;
+		vals[k] = (uint32_t)k;
+		if ((int32_t)c >= warpContacts)
+		{
+			atomicAdd(warpCount, 1u);
+		}
+	}
+}
+
+__global__ void kIslandGather(const TapeIsland* src, const uint32_t* order, int32_t n, TapeIsland* dst)
+{
+	int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k < n)
+	{
+		dst[k] = src[order[k]];
+	}
+}
+
 // contact identity across steps: a contact is its body pair (the engine keeps
 // one contact per pair, with a fixed body order)
 constexpr unsigned long long kNoPairKey = ~0ull;
@@ -325,6 +364,10 @@ DiffTape* tapeCreate(DevWorld& w, int32_t nBodies, int checkpointEvery)
 	DiffTape* t = new DiffTape();
 	t->checkpointEvery = checkpointEvery > 0 ? checkpointEvery : 10;
 	t->nBodies = nBodies;
+	if (const char* v = getenv("M3D_TAPE_WARP_CONTACTS"))
+	{
+		t->warpContacts = atoi(v) > 0 ? atoi(v) : 1 << 30;
+	}
 	const size_t n1 = (size_t)nBodies + 1;
 	bool ok = t->bodyConst.ensure(sizeof(BodyConst<float>) * n1) && t->muBody.ensure(sizeof(float) * n1) &&
 			  t->eBody.ensure(sizeof(float) * n1) && t->shapes.ensure(sizeof(m3d_diff::TapeShape) * n1) &&
@@ -445,8 +488,26 @@ void tapeStepEnd(DiffTape* t, DevWorld& w, const StepCounters& hc)
 	{
 		if (st.islands > 0)
 		{
-			M3G_LAUNCH(kTapeIslands, blocksFor(st.islands, 256), 256, s, w.islands.as<IslandRec>(),
-					   &dc->awakeIslands, (TapeIsland*)t->islands.at(t->islands.used), t->flags.as<uint32_t>());
+			TapeIsland* out = (TapeIsland*)t->islands.at(t->islands.used);
+			if (t->islandRaw.ensure(sizeof(TapeIsland) * (size_t)st.islands) &&
+				t->orderKeys.ensure(sizeof(uint64_t) * (size_t)st.islands) &&
+				t->orderVals.ensure(sizeof(uint32_t) * (size_t)st.islands))
+			{
+				TapeIsland* raw = t->islandRaw.as<TapeIsland>();
+				M3G_LAUNCH(kTapeIslands, blocksFor(st.islands, 256), 256, s, w.islands.as<IslandRec>(),
+						   &dc->awakeIslands, raw, t->flags.as<uint32_t>());
+				cudaMemsetAsync(t->flags.as<uint32_t>() + 1, 0, sizeof(uint32_t), s);
+				M3G_LAUNCH(kIslandWorkKeys, blocksFor(st.islands, 256), 256, s, raw, st.islands, t->warpContacts,
+						   t->orderKeys.as<uint64_t>(), t->orderVals.as<uint32_t>(), t->flags.as<uint32_t>() + 1);
+				radixSortPairs(t->orderKeys.as<uint64_t>(), t->orderVals.as<uint32_t>(), st.islands, 0xFFFFFFFFull,
+							   w.prim, s);
+				M3G_LAUNCH(kIslandGather, blocksFor(st.islands, 256), 256, s, raw, t->orderVals.as<uint32_t>(),
+						   st.islands, out);
+			}
+			else
+			{
+				tapeMarkUnsupported(t, "tape allocation failed");
+			}
 			cudaMemcpyAsync(t->bodies.at(t->bodies.used), w.bodyVals.ptr, sizeof(int32_t) * (size_t)st.bodies,
 							cudaMemcpyDeviceToDevice, s);
 		}
@@ -490,10 +551,11 @@ void tapeStepEnd(DiffTape* t, DevWorld& w, const StepCounters& hc)
 				}
 			}
 		}
-		uint32_t flags = 0;
-		cudaMemcpyAsync(&flags, t->flags.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+		uint32_t flags[2] = { 0, 0 };
+		cudaMemcpyAsync(flags, t->flags.ptr, sizeof(flags), cudaMemcpyDeviceToHost, s);
 		cudaStreamSynchronize(s);
-		applyFlags(t, flags);
+		applyFlags(t, flags[0]);
+		st.warpIslands = st.islands > 0 ? (int32_t)flags[1] : 0;
 		t->islands.used += sizeof(TapeIsland) * (size_t)st.islands;
 		t->bodies.used += sizeof(int32_t) * (size_t)st.bodies;
 		t->sleeps.used += sizeof(uint32_t) * (size_t)st.sleeps;
@@ -536,6 +598,13 @@ struct Work
 	m3d_diff::Prepared<T>* prepBar = nullptr;
 	T* lamNBar = nullptr;
 	T* lamTBar = nullptr;
+	// dependency levels of a warp's island: per body the latest level, per
+	// position the level, a level's count, and the positions by level
+	int32_t* bodyLevel = nullptr;
+	int32_t* levelOf = nullptr;
+	int32_t* levelCount = nullptr;
+	int32_t* order = nullptr;
+	int32_t* orderLevel = nullptr;
 	int32_t positions = 0;
 };
 
@@ -586,7 +655,12 @@ bool carveWork(Work<T>& k, int32_t n, const Limits& l, Alloc alloc)
 	k.prepBar = (m3d_diff::Prepared<T>*)alloc(sizeof(m3d_diff::Prepared<T>) * np);
 	k.lamNBar = (T*)alloc(sizeof(T) * 4 * np);
 	k.lamTBar = (T*)alloc(sizeof(T) * 4 * np);
-	return k.lamTBar != nullptr && k.cur != nullptr && k.start != nullptr && k.normRec != nullptr;
+	k.bodyLevel = (int32_t*)alloc(sizeof(int32_t) * nb);
+	k.levelOf = (int32_t*)alloc(sizeof(int32_t) * np);
+	k.levelCount = (int32_t*)alloc(sizeof(int32_t) * np);
+	k.order = (int32_t*)alloc(sizeof(int32_t) * np);
+	k.orderLevel = (int32_t*)alloc(sizeof(int32_t) * np);
+	return k.orderLevel != nullptr && k.lamTBar != nullptr && k.cur != nullptr && k.start != nullptr && k.normRec != nullptr;
 }
 
 // device allocations of one replay / backward call, freed together
@@ -632,6 +706,10 @@ IslandCtx<T> makeCtx(const Work<T>& k, const BodyConst<T>* bc, const T* mu, cons
 					 const TapeContact* prevContacts = nullptr, const int32_t* prevPos = nullptr)
 {
 	IslandCtx<T> x;
+	x.lane = 0;
+	x.width = 1;
+	x.order = nullptr;
+	x.orderLevel = nullptr;
 	x.genJ = nullptr;
 	x.live = nullptr;
 	x.liveIds = nullptr;
@@ -682,29 +760,130 @@ IslandCtx<T> makeCtx(const Work<T>& k, const BodyConst<T>* bc, const T* mu, cons
 
 } // namespace
 
-// one thread per island of the step
-__global__ void __launch_bounds__(64) kTapeReplayStep(IslandCtx<float> base, int32_t islands)
+// Dependency levels of the island's contacts (lane 0, then the warp
+// synchronises): each contact one level above the latest earlier contact that
+// shares a dynamic body with it; then the positions stably sorted by level.
+// The body pair of a position is the same in every substep of the step.
+__device__ void islandLevels(IslandCtx<float>& x, const Work<float>& k)
 {
-	int k = blockIdx.x * blockDim.x + threadIdx.x;
-	if (k >= islands)
+	const TapeIsland& r = *x.island;
+	if (x.lane == 0)
 	{
-		return;
+		for (int b = 0; b < r.bodyCount; ++b)
+		{
+			k.bodyLevel[x.bodies[r.bodyStart + b]] = -1;
+		}
+		int top = -1;
+		for (int j = 0; j < r.contactCount; ++j)
+		{
+			const int pos = r.contactStart + j;
+			const int a = x.contacts[pos].a, b = x.contacts[pos].b;
+			const bool da = x.bc[a].dynamic != 0, db = x.bc[b].dynamic != 0;
+			const int la = da ? k.bodyLevel[a] : -1, lb = db ? k.bodyLevel[b] : -1;
+			const int level = (la > lb ? la : lb) + 1;
+			k.levelOf[pos] = level;
+			if (da)
+			{
+				k.bodyLevel[a] = level;
+			}
+			if (db)
+			{
+				k.bodyLevel[b] = level;
+			}
+			top = level > top ? level : top;
+		}
+		for (int l = 0; l <= top; ++l)
+		{
+			k.levelCount[r.contactStart + l] = 0;
+		}
+		for (int j = 0; j < r.contactCount; ++j)
+		{
+			k.levelCount[r.contactStart + k.levelOf[r.contactStart + j]] += 1;
+		}
+		int sum = 0;
+		for (int l = 0; l <= top; ++l)
+		{
+			const int c = k.levelCount[r.contactStart + l];
+			k.levelCount[r.contactStart + l] = sum;
+			sum += c;
+		}
+		for (int j = 0; j < r.contactCount; ++j)
+		{
+			const int pos = r.contactStart + j;
+			const int level = k.levelOf[pos];
+			const int d = k.levelCount[r.contactStart + level]++;
+			k.order[r.contactStart + d] = pos;
+			k.orderLevel[r.contactStart + d] = level;
+		}
 	}
-	IslandCtx<float> x = base;
-	x.island = base.island + k;
-	m3d_diff::islandStepForward(x);
+	__syncwarp();
+	x.order = k.order;
+	x.orderLevel = k.orderLevel;
 }
 
-__global__ void __launch_bounds__(64) kTapeBackwardStep(IslandCtx<float> base, int32_t islands)
+// The island of this thread (one thread per island) or of this warp (the
+// head of the table, warpIslands islands, one warp each, two per block);
+// false when there is none.
+__device__ bool islandOfThread(IslandCtx<float>& x, const IslandCtx<float>& base, const Work<float>& k,
+							   int32_t islands, int32_t warpIslands)
 {
-	int k = blockIdx.x * blockDim.x + threadIdx.x;
-	if (k >= islands)
+	const int warpBlocks = (warpIslands + 1) / 2;
+	x = base;
+	if ((int)blockIdx.x < warpBlocks)
 	{
-		return;
+		const int i = (int)blockIdx.x * 2 + (int)(threadIdx.x >> 5);
+		if (i >= warpIslands)
+		{
+			return false; // the whole warp
+		}
+		x.island = base.island + i;
+		x.lane = (int)(threadIdx.x & 31);
+		x.width = 32;
+		islandLevels(x, k);
+		return true;
 	}
-	IslandCtx<float> x = base;
-	x.island = base.island + k;
-	m3d_diff::islandStepBackward(x);
+	const int i = warpIslands + ((int)blockIdx.x - warpBlocks) * (int)blockDim.x + (int)threadIdx.x;
+	if (i >= islands)
+	{
+		return false;
+	}
+	x.island = base.island + i;
+	return true;
+}
+
+int32_t islandBlocks(const TapeStep& st)
+{
+	return (st.warpIslands + 1) / 2 + (int32_t)blocksFor(st.islands - st.warpIslands, 64);
+}
+
+__global__ void __launch_bounds__(64) kTapeReplayStep(IslandCtx<float> base, Work<float> k, int32_t islands,
+													   int32_t warpIslands)
+{
+	IslandCtx<float> x;
+	if (islandOfThread(x, base, k, islands, warpIslands))
+	{
+		m3d_diff::islandStepForward(x);
+	}
+}
+
+__global__ void __launch_bounds__(64) kTapeRecordStep(IslandCtx<float> base, Work<float> k, int32_t islands,
+													  int32_t warpIslands)
+{
+	IslandCtx<float> x;
+	if (islandOfThread(x, base, k, islands, warpIslands))
+	{
+		m3d_diff::islandStepRecord(x);
+	}
+}
+
+__global__ void __launch_bounds__(64) kTapeReverseStep(IslandCtx<float> base, Work<float> k, int32_t islands,
+													   int32_t warpIslands)
+{
+	IslandCtx<float> x;
+	if (islandOfThread(x, base, k, islands, warpIslands))
+	{
+		m3d_diff::islandStepReverse(x);
+	}
 }
 
 // bodies put to sleep at a step's end: velocities (or their adjoints) zeroed
@@ -792,7 +971,7 @@ void replaySteps(DiffTape* t, cudaStream_t s, Work<float>& k, int s0, int s1, Bo
 		}
 		if (st.islands > 0)
 		{
-			M3G_LAUNCH(kTapeReplayStep, blocksFor(st.islands, 64), 64, s, deviceCtx(t, k, st), st.islands);
+			M3G_LAUNCH(kTapeReplayStep, islandBlocks(st), 64, s, deviceCtx(t, k, st), k, st.islands, st.warpIslands);
 		}
 		if (st.sleeps > 0)
 		{
@@ -953,7 +1132,8 @@ int32_t tapeBackward(DiffTape* t, DevWorld& w, const float* dPos, const float* d
 				x.shapes = t->shapes.as<m3d_diff::TapeShape>();
 				x.prevContacts = previousRecords(t, step);
 				x.prevPos = prevPos;
-				M3G_LAUNCH(kTapeBackwardStep, blocksFor(st.islands, 64), 64, s, x, st.islands);
+				M3G_LAUNCH(kTapeRecordStep, islandBlocks(st), 64, s, x, k, st.islands, st.warpIslands);
+				M3G_LAUNCH(kTapeReverseStep, islandBlocks(st), 64, s, x, k, st.islands, st.warpIslands);
 			}
 			if (step > 0)
 			{

@@ -1662,7 +1662,79 @@ struct IslandCtx
 	// of read from the tape
 	Contact<T>* live;
 	uint32_t* liveIds; // 4 per position
+	// the team working the island: one thread (lane 0 of width 1, order null),
+	// or a warp whose lanes take the contacts of one dependency level at a
+	// time (see ContactRun)
+	int lane, width;
+	const int32_t* order;      // per position of the island: its positions by level, or null
+	const int32_t* orderLevel; // the level of each entry of order
 };
+
+// ---- island teams -----------------------------------------------------------------
+// A contact's dependency level is one above the latest earlier contact of its
+// island that shares a dynamic body with it (static bodies are only read).
+// The contacts of one level touch disjoint dynamic bodies, and every body
+// meets its contacts in the recorded order when the levels are walked upwards
+// (forward passes) or downwards (reverse passes): lanes may take one level's
+// contacts at once and the result is bitwise that of one thread walking the
+// recorded order.  A run is up to `width` contacts of one level; after each
+// run the team synchronises.
+struct ContactRun
+{
+	int j, pos, count;
+	bool mine, more, rev;
+};
+
+template <typename T>
+M3D_DIFF_HD void teamSync(const IslandCtx<T>& x)
+{
+#ifdef __CUDA_ARCH__
+	if (x.width > 1)
+	{
+		__syncwarp();
+	}
+#endif
+}
+
+template <typename T>
+M3D_DIFF_HD void contactRunSetup(const IslandCtx<T>& x, const TapeIsland& r, ContactRun& u)
+{
+	const int n = r.contactCount;
+	u.more = u.rev ? u.j > 0 : u.j < n;
+	u.count = 1;
+	u.mine = u.more;
+	u.pos = r.contactStart + (u.rev ? u.j - 1 : u.j);
+#ifdef __CUDA_ARCH__
+	if (x.order != nullptr && u.more)
+	{
+		const int head = u.rev ? u.j - 1 : u.j;
+		const int level = x.orderLevel[r.contactStart + head];
+		const int idx = u.rev ? u.j - 1 - x.lane : u.j + x.lane;
+		u.mine = idx >= 0 && idx < n && x.orderLevel[r.contactStart + idx] == level;
+		u.pos = u.mine ? x.order[r.contactStart + idx] : -1;
+		u.count = __popc(__ballot_sync(0xffffffffu, u.mine));
+	}
+#endif
+}
+
+// the first run of the island's contacts, upwards (rev false) or downwards
+template <typename T>
+M3D_DIFF_HD ContactRun contactRunBegin(const IslandCtx<T>& x, const TapeIsland& r, bool rev)
+{
+	ContactRun u;
+	u.rev = rev;
+	u.j = rev ? r.contactCount : 0;
+	contactRunSetup(x, r, u);
+	return u;
+}
+
+template <typename T>
+M3D_DIFF_HD void contactRunNext(const IslandCtx<T>& x, const TapeIsland& r, ContactRun& u)
+{
+	teamSync(x);
+	u.j += u.rev ? -u.count : u.count;
+	contactRunSetup(x, r, u);
+}
 
 template <typename T>
 M3D_DIFF_HD Contact<T> contactOf(const IslandCtx<T>& x, const TapeContact* tc, int pos)
@@ -1678,7 +1750,7 @@ template <typename T>
 M3D_DIFF_HD_CALL void substepForward(const IslandCtx<T>& x, const TapeIsland& r, int sub, bool record)
 {
 	const BodyConst<T>* bc = x.bc;
-	for (int k = 0; k < r.bodyCount; ++k)
+	for (int k = x.lane; k < r.bodyCount; k += x.width)
 	{
 		int i = x.bodies[r.bodyStart + k];
 		if (!bc[i].dynamic)
@@ -1690,6 +1762,7 @@ M3D_DIFF_HD_CALL void substepForward(const IslandCtx<T>& x, const TapeIsland& r,
 		x.start[(size_t)sub * x.bodyCount + i] = x.cur[i];
 		x.cur[i] = s1;
 	}
+	teamSync(x);
 	const TapeContact* tc = x.contacts + (size_t)sub * x.contactsPerSubstep;
 	if (x.live != nullptr)
 	{
@@ -1710,7 +1783,7 @@ M3D_DIFF_HD_CALL void substepForward(const IslandCtx<T>& x, const TapeIsland& r,
 			}
 		}
 	}
-	for (int j = 0; j < r.contactCount; ++j)
+	for (int j = x.lane; j < r.contactCount; j += x.width)
 	{
 		int pos = r.contactStart + j;
 		Contact<T> c = contactOf(x, tc, pos);
@@ -1723,11 +1796,16 @@ M3D_DIFF_HD_CALL void substepForward(const IslandCtx<T>& x, const TapeIsland& r,
 			x.lamT[4 * pos + s] = T(0);
 		}
 	}
+	teamSync(x);
 	for (int it = 0; it < x.iterations; ++it)
 	{
-		for (int j = 0; j < r.contactCount; ++j)
+		for (ContactRun u = contactRunBegin(x, r, false); u.more; contactRunNext(x, r, u))
 		{
-			int pos = r.contactStart + j;
+			if (!u.mine)
+			{
+				continue;
+			}
+			const int pos = u.pos;
 			Contact<T> c = contactOf(x, tc, pos);
 			if (record)
 			{
@@ -1745,9 +1823,13 @@ M3D_DIFF_HD_CALL void substepForward(const IslandCtx<T>& x, const TapeIsland& r,
 					x.cur[c.b].x, x.cur[c.b].q, x.lamN + 4 * pos);
 		}
 	}
-	for (int j = 0; j < r.contactCount; ++j)
+	for (ContactRun u = contactRunBegin(x, r, false); u.more; contactRunNext(x, r, u))
 	{
-		int pos = r.contactStart + j;
+		if (!u.mine)
+		{
+			continue;
+		}
+		const int pos = u.pos;
 		Contact<T> c = contactOf(x, tc, pos);
 		bool gate = frictionGate(c, x.prep[pos], x.cur[c.a].v, x.cur[c.a].w, x.cur[c.b].v, x.cur[c.b].w);
 		if (record)
@@ -1788,7 +1870,7 @@ M3D_DIFF_HD_CALL void substepForward(const IslandCtx<T>& x, const TapeIsland& r,
 			}
 		}
 	}
-	for (int k = 0; k < r.bodyCount; ++k)
+	for (int k = x.lane; k < r.bodyCount; k += x.width)
 	{
 		int i = x.bodies[r.bodyStart + k];
 		if (!bc[i].dynamic)
@@ -1800,9 +1882,14 @@ M3D_DIFF_HD_CALL void substepForward(const IslandCtx<T>& x, const TapeIsland& r,
 		x.q2[i] = x.cur[i].q;
 		reconstruct(x.cur[i].x, x.cur[i].q, s0.x, s0.q, x.invH, x.cur[i].v, x.cur[i].w);
 	}
-	for (int j = 0; j < r.contactCount; ++j)
+	teamSync(x);
+	for (ContactRun u = contactRunBegin(x, r, false); u.more; contactRunNext(x, r, u))
 	{
-		int pos = r.contactStart + j;
+		if (!u.mine)
+		{
+			continue;
+		}
+		const int pos = u.pos;
 		Contact<T> c = contactOf(x, tc, pos);
 		if (record)
 		{
@@ -2184,7 +2271,7 @@ M3D_DIFF_HD_CALL void substepReverse(const IslandCtx<T>& x, const TapeIsland& r,
 {
 	const BodyConst<T>* bc = x.bc;
 	const TapeContact* tc = x.contacts + (size_t)sub * x.contactsPerSubstep;
-	for (int k = 0; k < r.bodyCount; ++k)
+	for (int k = x.lane; k < r.bodyCount; k += x.width)
 	{
 		int i = x.bodies[r.bodyStart + k];
 		x.adj0[i] = bodyZero<T>();
@@ -2192,7 +2279,8 @@ M3D_DIFF_HD_CALL void substepReverse(const IslandCtx<T>& x, const TapeIsland& r,
 		z.cx = z.cy = z.cz = vzero<T>();
 		x.iwBar[i] = z;
 	}
-	for (int j = 0; j < r.contactCount; ++j)
+	teamSync(x);
+	for (int j = x.lane; j < r.contactCount; j += x.width)
 	{
 		int pos = r.contactStart + j;
 		preparedZero(x.prepBar[pos]);
@@ -2202,10 +2290,15 @@ M3D_DIFF_HD_CALL void substepReverse(const IslandCtx<T>& x, const TapeIsland& r,
 			x.lamTBar[4 * pos + s] = T(0);
 		}
 	}
+	teamSync(x);
 	// velocity pass, in reverse contact order
-	for (int j = r.contactCount - 1; j >= 0; --j)
+	for (ContactRun u = contactRunBegin(x, r, true); u.more; contactRunNext(x, r, u))
 	{
-		int pos = r.contactStart + j;
+		if (!u.mine)
+		{
+			continue;
+		}
+		const int pos = u.pos;
 		Contact<T> c = loadContact<T>(tc[pos]);
 		const VelRec<T>& rec = x.velRec[pos];
 		VelocityIn<T> in;
@@ -2259,7 +2352,7 @@ M3D_DIFF_HD_CALL void substepReverse(const IslandCtx<T>& x, const TapeIsland& r,
 		scatterMaterials(x, c, b.mu, b.e);
 	}
 	// reconstruction
-	for (int k = 0; k < r.bodyCount; ++k)
+	for (int k = x.lane; k < r.bodyCount; k += x.width)
 	{
 		int i = x.bodies[r.bodyStart + k];
 		if (!bc[i].dynamic)
@@ -2272,10 +2365,15 @@ M3D_DIFF_HD_CALL void substepReverse(const IslandCtx<T>& x, const TapeIsland& r,
 		x.adj[i].w = vzero<T>();
 		reconstruct_rev(x.x2[i], x.q2[i], s0.x, s0.q, x.invH, vb, wb, x.adj[i].x, x.adj[i].q, x.adj0[i].x, x.adj0[i].q);
 	}
+	teamSync(x);
 	// friction, reverse contact order
-	for (int j = r.contactCount - 1; j >= 0; --j)
+	for (ContactRun u = contactRunBegin(x, r, true); u.more; contactRunNext(x, r, u))
 	{
-		int pos = r.contactStart + j;
+		if (!u.mine)
+		{
+			continue;
+		}
+		const int pos = u.pos;
 		const PoseRec<T>& rec = x.fricRec[pos];
 		ContactBar<T>& cb = x.cbar[pos];
 		for (int s = 0; s < 4; ++s)
@@ -2326,9 +2424,13 @@ M3D_DIFF_HD_CALL void substepReverse(const IslandCtx<T>& x, const TapeIsland& r,
 	// normal iterations, reverse
 	for (int it = x.iterations - 1; it >= 0; --it)
 	{
-		for (int j = r.contactCount - 1; j >= 0; --j)
+		for (ContactRun u = contactRunBegin(x, r, true); u.more; contactRunNext(x, r, u))
 		{
-			int pos = r.contactStart + j;
+			if (!u.mine)
+			{
+				continue;
+			}
+			const int pos = u.pos;
 			Contact<T> c = loadContact<T>(tc[pos]);
 			if (c.pointCount == 0)
 			{
@@ -2355,9 +2457,13 @@ M3D_DIFF_HD_CALL void substepReverse(const IslandCtx<T>& x, const TapeIsland& r,
 		}
 	}
 	// contact preparation (poses at preparation = the integrated ones)
-	for (int j = 0; j < r.contactCount; ++j)
+	for (ContactRun u = contactRunBegin(x, r, false); u.more; contactRunNext(x, r, u))
 	{
-		int pos = r.contactStart + j;
+		if (!u.mine)
+		{
+			continue;
+		}
+		const int pos = u.pos;
 		Contact<T> c = loadContact<T>(tc[pos]);
 		// the states at preparation are the integrated ones, rebuilt here
 		Body<T> sA = x.cur[c.a], sB = x.cur[c.b];
@@ -2407,7 +2513,7 @@ M3D_DIFF_HD_CALL void substepReverse(const IslandCtx<T>& x, const TapeIsland& r,
 		}
 	}
 	// integration
-	for (int k = 0; k < r.bodyCount; ++k)
+	for (int k = x.lane; k < r.bodyCount; k += x.width)
 	{
 		int i = x.bodies[r.bodyStart + k];
 		if (!bc[i].dynamic)
@@ -2425,6 +2531,7 @@ M3D_DIFF_HD_CALL void substepReverse(const IslandCtx<T>& x, const TapeIsland& r,
 		x.ilBar[i] += cb.il;
 		x.adj[i] = s0b;
 	}
+	teamSync(x);
 }
 
 // The slice of the per-substep records for substep `sub`: world inverse
@@ -2448,26 +2555,33 @@ M3D_DIFF_HD IslandCtx<T> substepView(const IslandCtx<T>& x, int sub)
 	return y;
 }
 
-// One island through one step, backward: the state of its bodies at the
-// step's start is in cur; the adjoints of their state at the step's end in
-// adj.  On return adj holds the adjoints at the step's start and cur is
-// unchanged.
+// One island through one step, recording: the forward pass with each
+// substep's records in its own slice.  cur goes from the step's start to its
+// end.
 template <typename T>
-M3D_DIFF_HD void islandStepBackward(const IslandCtx<T>& x)
+M3D_DIFF_HD void islandStepRecord(const IslandCtx<T>& x)
 {
 	const TapeIsland& r = *x.island;
-	// one recording pass forward (each substep's records in its own slice),
-	// then the substeps in reverse
 	for (int sub = 0; sub < x.substeps; ++sub)
 	{
 		substepForward(substepView(x, sub), r, sub, true);
 	}
+}
+
+// One island through one step, in reverse, from the records of
+// islandStepRecord: the adjoints of its bodies' state at the step's end in
+// adj; on return adj holds the adjoints at the step's start and cur the state
+// at the step's start.
+template <typename T>
+M3D_DIFF_HD void islandStepReverse(const IslandCtx<T>& x)
+{
+	const TapeIsland& r = *x.island;
 	for (int sub = x.substeps - 1; sub >= 0; --sub)
 	{
 		substepReverse(substepView(x, sub), r, sub);
 	}
 	// cur: back to the step's start
-	for (int k = 0; k < r.bodyCount; ++k)
+	for (int k = x.lane; k < r.bodyCount; k += x.width)
 	{
 		int i = x.bodies[r.bodyStart + k];
 		if (x.bc[i].dynamic)
@@ -2475,11 +2589,17 @@ M3D_DIFF_HD void islandStepBackward(const IslandCtx<T>& x)
 			x.cur[i] = x.start[i];
 		}
 	}
+	teamSync(x);
 	// manifolds the step's narrowphase regenerated at the step-start poses
-	// (margin from the step-start velocities, as the narrowphase takes it)
-	for (int j = 0; j < r.contactCount; ++j)
+	// (margin from the step-start velocities, as the narrowphase takes it);
+	// the generations add into the bodies' adjoints: walked by level
+	for (ContactRun u = contactRunBegin(x, r, false); u.more; contactRunNext(x, r, u))
 	{
-		const int pos = r.contactStart + j;
+		if (!u.mine)
+		{
+			continue;
+		}
+		const int pos = u.pos;
 		const TapeContact& rec = x.contacts[pos];
 		if ((rec.gen & kTapeGenNarrow) && !(rec.gen & kTapeGenPrepare))
 		{
@@ -2490,6 +2610,17 @@ M3D_DIFF_HD void islandStepBackward(const IslandCtx<T>& x)
 							  x.genJ != nullptr ? x.genJ + (size_t)pos * (kGenJRows * kGenJCols) : nullptr);
 		}
 	}
+}
+
+// One island through one step, backward: the state of its bodies at the
+// step's start is in cur; the adjoints of their state at the step's end in
+// adj.  On return adj holds the adjoints at the step's start and cur is
+// unchanged.
+template <typename T>
+M3D_DIFF_HD void islandStepBackward(const IslandCtx<T>& x)
+{
+	islandStepRecord(x);
+	islandStepReverse(x);
 }
 
 // One island through one step, forward only (the replay).
