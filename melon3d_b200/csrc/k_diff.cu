@@ -663,9 +663,14 @@ bool carveWork(Work<T>& k, int32_t n, const Limits& l, Alloc alloc)
 	return k.orderLevel != nullptr && k.lamTBar != nullptr && k.cur != nullptr && k.start != nullptr && k.normRec != nullptr;
 }
 
-// device allocations of one replay / backward call, freed together
+// device allocations of one replay / backward call, freed together; each is
+// zeroed on the call's stream, so the zeroing is ordered before the call's
+// copies and kernels (the world's stream does not synchronise with the
+// legacy default stream, where a plain cudaMemset would run)
 struct DevArena
 {
+	cudaStream_t stream;
+	explicit DevArena(cudaStream_t s) : stream(s) {}
 	std::vector<void*> owned;
 	bool ok = true;
 	void* operator()(size_t bytes)
@@ -676,7 +681,10 @@ struct DevArena
 			ok = false;
 			return nullptr;
 		}
-		cudaMemset(p, 0, bytes);
+		if (cudaMemsetAsync(p, 0, bytes, stream) != cudaSuccess)
+		{
+			ok = false;
+		}
 		owned.push_back(p);
 		return p;
 	}
@@ -1048,7 +1056,7 @@ int32_t tapeReplay(DiffTape* t, DevWorld& w, float* pos, float* rot, float* vel,
 		return M3D_GPU_ERR_ARGUMENT;
 	}
 	const int32_t n = t->nBodies;
-	DevArena arena;
+	DevArena arena(w.stream);
 	Work<float> k;
 	if (!carveWork(k, n, tapeLimits(t), [&](size_t b) { return arena(b); }) || !arena.ok)
 	{
@@ -1077,7 +1085,7 @@ int32_t tapeBackward(DiffTape* t, DevWorld& w, const float* dPos, const float* d
 		return M3D_GPU_ERR_ARGUMENT;
 	}
 	const int32_t n = t->nBodies;
-	DevArena arena;
+	DevArena arena(w.stream);
 	Work<float> k;
 	const Limits lim = tapeLimits(t);
 	bool ok = carveWork(k, n, lim, [&](size_t b) { return arena(b); });
