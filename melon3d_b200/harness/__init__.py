@@ -11,14 +11,15 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 SRC = os.path.join(HERE, "scenes.cpp")
 LIB = os.path.join(os.path.dirname(HERE), "lib", "libm3d_scenes.so")
 
-PYRAMID, RAIN, PILE, RAFT, BATCH_WORLD, INCLINE = 0, 1, 2, 3, 4, 5
+PYRAMID, RAIN, PILE, RAFT, BATCH_WORLD, INCLINE, JOINTED_RAFT = 0, 1, 2, 3, 4, 5, 6
 
 
 class M3dApi(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in (
         "world_def_default", "body_def_default", "shape_def_default", "world_create", "world_destroy",
         "world_step", "body_create", "body_destroy", "body_position", "world_profile", "read_poses",
-        "joint_create_ball", "joint_create_hinge", "hinge_joint_def_default")]
+        "joint_create_ball", "joint_create_hinge", "hinge_joint_def_default", "joint_create_distance",
+        "joint_create_weld", "weld_joint_def_default")]
 
 
 def build(force=False):
@@ -70,7 +71,10 @@ def api_table(lib):
     if hasattr(lib, "m3d_gpu_read_poses"):
         t.read_poses = C.cast(lib.m3d_gpu_read_poses, C.c_void_p).value
     for field, sym in (("joint_create_ball", "m3d_joint_create_ball"), ("joint_create_hinge", "m3d_joint_create_hinge"),
-                       ("hinge_joint_def_default", "m3d_hinge_joint_def_default")):
+                       ("hinge_joint_def_default", "m3d_hinge_joint_def_default"),
+                       ("joint_create_distance", "m3d_joint_create_distance"),
+                       ("joint_create_weld", "m3d_joint_create_weld"),
+                       ("weld_joint_def_default", "m3d_weld_joint_def_default")):
         setattr(t, field, C.cast(getattr(lib, sym), C.c_void_p).value)
     return t
 

@@ -26,6 +26,14 @@
 //      each 0.01-0.3 m above the slope, v~N(0,1) per axis, mu~U[0.2,0.9],
 //      e~U[0,0.3]; the incline has mu 1, e 0.  Sleep is off (b > 0: on);
 //      0 < a < 64 sets the body count.
+//   6  jointed raft: the raft of scene 3 (one island of > 300 contacts, the
+//      coloured path) with every joint type inside it - rigid and soft
+//      distance joints, ball joints, weld joints, hinges with a limit, a
+//      motor, or both - plus a hinged chain with a limited link swinging from
+//      a static pivot onto the raft, a motor-driven wheel on a static axle,
+//      a soft distance pendulum and spheres, capsules and boxes dropped on
+//      the raft (seeded); its joints all meet the one raft island once the
+//      chain lands
 #include "melon3d.h"
 
 #include <algorithm>
@@ -56,6 +64,10 @@ struct M3dApi
 	m3d_joint_id (*joint_create_ball)(m3d_world*, const m3d_ball_joint_def*);
 	m3d_joint_id (*joint_create_hinge)(m3d_world*, const m3d_hinge_joint_def*);
 	m3d_hinge_joint_def (*hinge_joint_def_default)(void);
+	// joints (scene 6)
+	m3d_joint_id (*joint_create_distance)(m3d_world*, const m3d_distance_joint_def*);
+	m3d_joint_id (*joint_create_weld)(m3d_world*, const m3d_weld_joint_def*);
+	m3d_weld_joint_def (*weld_joint_def_default)(void);
 };
 
 } // extern "C"
@@ -286,6 +298,179 @@ void churnStep(Scene& s)
 	}
 }
 
+
+m3d_body_id addStatic(Scene& s, m3d_vec3 p, m3d_vec3 he)
+{
+	m3d_body_def bd = s.api.body_def_default();
+	bd.type = M3D_BODY_STATIC;
+	bd.position = p;
+	m3d_shape_def sd = s.api.shape_def_default();
+	sd.type = M3D_SHAPE_BOX;
+	sd.halfExtents = he;
+	return s.api.body_create(s.world, &bd, &sd);
+}
+
+m3d_body_id addDynamic(Scene& s, m3d_vec3 p, m3d_shape_def sd)
+{
+	m3d_body_def bd = s.api.body_def_default();
+	bd.type = M3D_BODY_DYNAMIC;
+	bd.position = p;
+	m3d_body_id id = s.api.body_create(s.world, &bd, &sd);
+	s.dynamic.push_back(id);
+	return id;
+}
+
+m3d_shape_def boxShape(Scene& s, m3d_vec3 he)
+{
+	m3d_shape_def sd = s.api.shape_def_default();
+	sd.type = M3D_SHAPE_BOX;
+	sd.halfExtents = he;
+	return sd;
+}
+
+// scene 6 (see the file header)
+void buildJointedRaft(Scene& s)
+{
+	Rng& r = s.rng;
+	addGround(s, m3d_v3(0.0f, -1.0f, 0.0f), m3d_v3(50.0f, 1.0f, 50.0f));
+	const int N = 15;
+	m3d_body_id raft[N][N];
+	for (int gx = 0; gx < N; ++gx)
+	{
+		for (int gz = 0; gz < N; ++gz)
+		{
+			raft[gx][gz] = addBox(s, m3d_v3(1.0f * (float)gx - 7.0f, 0.5f, 1.0f * (float)gz - 7.0f), m3d_quat_identity(),
+								  m3d_v3(0.501f, 0.5f, 0.501f), 0.6f);
+		}
+	}
+	// joints between raft neighbours (joined pairs stop colliding): anchors
+	// on the shared face, so every joint starts satisfied
+	for (int k = 0; k < 24; ++k)
+	{
+		int gx = (int)(r.next() % (N - 1)), gz = (int)(r.next() % N);
+		m3d_body_id a = raft[gx][gz], b = raft[gx + 1][gz];
+		m3d_vec3 la = m3d_v3(0.5f, 0.0f, 0.0f), lb = m3d_v3(-0.5f, 0.0f, 0.0f);
+		switch (k % 6)
+		{
+		case 0:
+		case 1:
+		{
+			m3d_distance_joint_def d;
+			memset(&d, 0, sizeof(d));
+			d.bodyA = a;
+			d.bodyB = b;
+			d.localAnchorA = la;
+			d.localAnchorB = lb;
+			d.length = k % 6 == 0 ? 0.0f : 0.05f;
+			d.hertz = k % 6 == 0 ? 0.0f : 3.0f;
+			d.dampingRatio = k % 6 == 0 ? 0.0f : 0.7f;
+			s.api.joint_create_distance(s.world, &d);
+			break;
+		}
+		case 2:
+		{
+			m3d_ball_joint_def d;
+			memset(&d, 0, sizeof(d));
+			d.bodyA = a;
+			d.bodyB = b;
+			d.localAnchorA = la;
+			d.localAnchorB = lb;
+			s.api.joint_create_ball(s.world, &d);
+			break;
+		}
+		case 3:
+		{
+			m3d_weld_joint_def d = s.api.weld_joint_def_default();
+			d.bodyA = a;
+			d.bodyB = b;
+			d.localAnchorA = la;
+			d.localAnchorB = lb;
+			s.api.joint_create_weld(s.world, &d);
+			break;
+		}
+		default:
+		{
+			m3d_hinge_joint_def d = s.api.hinge_joint_def_default();
+			d.bodyA = a;
+			d.bodyB = b;
+			d.localAnchorA = la;
+			d.localAnchorB = lb;
+			d.localAxisA = m3d_v3(0.0f, 0.0f, 1.0f);
+			d.enableLimit = k % 6 == 4 || k % 12 == 5;
+			d.lowerAngle = -0.1f;
+			d.upperAngle = 0.15f;
+			d.enableMotor = k % 6 == 5;
+			d.motorSpeed = 1.5f;
+			d.maxMotorTorque = 40.0f;
+			s.api.joint_create_hinge(s.world, &d);
+			break;
+		}
+		}
+	}
+	// hinged chain from a static pivot above the raft's edge; the third link
+	// has a limit, the last one a motor
+	m3d_body_id prev = addStatic(s, m3d_v3(-7.0f, 6.0f, 0.0f), m3d_v3(0.1f, 0.1f, 0.1f));
+	for (int i = 0; i < 6; ++i)
+	{
+		m3d_body_id link = addDynamic(s, m3d_v3(-7.0f + 0.9f * (float)(i + 1), 6.0f, 0.0f),
+									  boxShape(s, m3d_v3(0.4f, 0.15f, 0.15f)));
+		m3d_hinge_joint_def d = s.api.hinge_joint_def_default();
+		d.bodyA = prev;
+		d.bodyB = link;
+		d.localAnchorA = i == 0 ? m3d_v3(0.0f, 0.0f, 0.0f) : m3d_v3(0.45f, 0.0f, 0.0f);
+		d.localAnchorB = m3d_v3(-0.45f, 0.0f, 0.0f);
+		d.localAxisA = m3d_v3(0.0f, 0.0f, 1.0f);
+		d.enableLimit = i == 2;
+		d.lowerAngle = -0.3f;
+		d.upperAngle = 0.3f;
+		d.enableMotor = i == 5;
+		d.motorSpeed = -2.0f;
+		d.maxMotorTorque = 5.0f;
+		s.api.joint_create_hinge(s.world, &d);
+		prev = link;
+	}
+	// motor-driven wheel on a static axle, limited to +-1 rad
+	{
+		m3d_body_id axle = addStatic(s, m3d_v3(12.0f, 3.0f, 0.0f), m3d_v3(0.1f, 0.1f, 0.1f));
+		m3d_shape_def ws = s.api.shape_def_default();
+		ws.type = M3D_SHAPE_CAPSULE;
+		ws.radius = 0.2f;
+		ws.halfHeight = 0.8f;
+		m3d_body_id wheel = addDynamic(s, m3d_v3(12.0f, 3.0f, 0.0f), ws);
+		m3d_hinge_joint_def d = s.api.hinge_joint_def_default();
+		d.bodyA = axle;
+		d.bodyB = wheel;
+		d.localAxisA = m3d_v3(0.0f, 0.0f, 1.0f);
+		d.enableMotor = true;
+		d.motorSpeed = 4.0f;
+		d.maxMotorTorque = 60.0f;
+		d.enableLimit = true;
+		d.lowerAngle = -1.0f;
+		d.upperAngle = 1.0f;
+		s.api.joint_create_hinge(s.world, &d);
+	}
+	// soft distance pendulum from a static hook
+	{
+		m3d_body_id hook = addStatic(s, m3d_v3(-12.0f, 5.0f, 0.0f), m3d_v3(0.1f, 0.1f, 0.1f));
+		m3d_shape_def bs = s.api.shape_def_default();
+		bs.type = M3D_SHAPE_SPHERE;
+		bs.radius = 0.3f;
+		m3d_body_id bob = addDynamic(s, m3d_v3(-10.5f, 5.0f, 0.5f), bs);
+		m3d_distance_joint_def d;
+		memset(&d, 0, sizeof(d));
+		d.bodyA = hook;
+		d.bodyB = bob;
+		d.hertz = 2.0f;
+		d.dampingRatio = 0.3f;
+		s.api.joint_create_distance(s.world, &d);
+	}
+	// droppers on the raft
+	for (int i = 0; i < 24; ++i)
+	{
+		spawnShape(s, i % 3, m3d_v3(-6.0f, 2.0f, -6.0f), m3d_v3(6.0f, 6.0f, 6.0f));
+	}
+}
+
 } // namespace
 
 extern "C"
@@ -437,6 +622,10 @@ void* scn_create(const M3dApi* api, int kind, uint64_t seed, int a, int b, int c
 			addBox(*s, m3d_v3(2.0f * (float)i - 4.0f, 3.0f + 0.7f * (float)i, 0.5f * (float)i - 1.0f),
 				   m3d_quat_identity(), m3d_v3(0.45f, 0.45f, 0.45f), 0.6f);
 		}
+	}
+	else if (kind == 6)
+	{
+		buildJointedRaft(*s);
 	}
 	return s;
 }

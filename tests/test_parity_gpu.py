@@ -14,6 +14,9 @@ state; the contact array (order, pairs, touch flags, manifold normals and
 points); island partitions; the greedy colouring of coloured islands; the
 profile counters.
 """
+import gc
+import os
+
 import numpy as np
 import pytest
 
@@ -24,9 +27,14 @@ from . import _util as U
 pytestmark = pytest.mark.gpu
 
 
-def lockstep(ref, kind, steps, seed=1, a=0, b=0, c=0, substeps=4, check_colors=True, giant=None):
+def lockstep(ref, kind, steps, seed=1, a=0, b=0, c=0, substeps=4, check_colors=True, giant=None, compare=None,
+             workers=0):
+    """Step the oracle and the GPU world side by side; after every step that
+    `compare(step)` selects (all by default) compare them bit for bit.
+    `workers` sets the reference's thread count (its result does not depend
+    on it: determinism across worker counts is one of its contracts)."""
     g = U.gpu()
-    sr = harness.Scene(ref, kind, seed, a, b, c)
+    sr = harness.Scene(ref, kind, seed, a, b, c, workers=workers)
     sg = harness.Scene(g, kind, seed, a, b, c)
     if giant is not None:
         g.m3d_gpu_set_giant_island_contacts(sg.world, giant)
@@ -36,6 +44,8 @@ def lockstep(ref, kind, steps, seed=1, a=0, b=0, c=0, substeps=4, check_colors=T
             sr.run(1, substeps)
             sg.run(1, substeps)
             assert g.m3d_gpu_status(sg.world) == 0, g.m3d_gpu_last_error_string(sg.world)
+            if compare is not None and not compare(step):
+                continue
             cr, cg = U.contacts(ref, sr.world), U.contacts(g, sg.world)
             d = U.diff_contacts(cr, cg)
             assert d is None, "step %d: %s" % (step, d)
@@ -61,9 +71,10 @@ def lockstep(ref, kind, steps, seed=1, a=0, b=0, c=0, substeps=4, check_colors=T
     return coloured_steps
 
 
-def test_pyramid_bit_exact_until_asleep():
-    # 210-box pyramid (one island, > 300 contacts: the coloured path)
-    assert lockstep(U.oracle(), harness.PYRAMID, 80) > 0
+def test_pyramid_bit_exact_all_300_steps():
+    # the pyramid workload as stated: 210 boxes (one island, > 300 contacts:
+    # the coloured path), 300 steps at 60 Hz x 4 substeps, through sleep
+    assert lockstep(U.oracle(), harness.PYRAMID, 300) > 0
 
 
 def test_raft_coloured_path_bit_exact():
@@ -85,6 +96,20 @@ def test_large_pile_whole_gpu_coloured_path_bit_exact():
     assert lockstep(U.oracle_cr(), harness.PILE, 5, seed=3, a=20, b=40, c=20) > 0
 
 
+def test_rain_20k_churn_200_first_60_steps_bit_exact():
+    # the streaming rain workload at its stated size: 20,000 bodies, 200
+    # destroyed and spawned per step, steps 0-59 compared after every step
+    lockstep(U.oracle_cr(), harness.RAIN, 60, seed=2, a=20000, b=200, workers=os.cpu_count() or 1)
+
+
+def test_rain_20k_churn_200_settled_phase_bit_exact():
+    # the same workload pre-rolled to its settled phase (piles on the ground,
+    # churn removing the lowest bodies): every 25th step of the first 300
+    # compared, then steps 300-359 after every step
+    lockstep(U.oracle_cr(), harness.RAIN, 360, seed=2, a=20000, b=200, workers=os.cpu_count() or 1,
+             compare=lambda k: k >= 300 or k % 25 == 24)
+
+
 def test_rain_with_churn_bit_exact():
     lockstep(U.oracle_cr(), harness.RAIN, 60, seed=2, a=1500, b=30)
 
@@ -98,6 +123,60 @@ def test_large_rain_bit_exact():
     # look-back walks several 32-tile windows; cell keys straddle the key
     # offset in every field, which the bias-subtracted sort digits cover
     lockstep(U.oracle_cr(), harness.RAIN, 4, seed=9, a=150000, b=500)
+
+
+def _pile_contacts_equal(ref, g, wr, wg, step):
+    cr = U.contacts(ref, wr)
+    cg = U.contacts(g, wg)
+    d = U.diff_contacts(cr, cg)
+    n = len(cr)
+    del cr, cg
+    gc.collect()
+    assert d is None, "step %d: %s" % (step, d)
+    return n
+
+
+def test_pile_250k_first_5_steps_bit_exact():
+    """The settled-pile workload at its stated size: 250,000 boxes in a
+    50x100x50 lattice (jitter), one giant island through the whole-GPU
+    coloured solve; steps 0-4 compared bit for bit (bodies, every contact and
+    manifold point, islands, colours, profile counters)."""
+    ref, g = U.oracle_cr(), U.gpu()
+    sr = harness.Scene(ref, harness.PILE, 3, 50, 100, 50, workers=os.cpu_count() or 1)
+    sg = harness.Scene(g, harness.PILE, 3, 50, 100, 50)
+    try:
+        for step in range(5):
+            sr.run(1)
+            sg.run(1)
+            assert g.m3d_gpu_status(sg.world) == 0, g.m3d_gpu_last_error_string(sg.world)
+            br, bg = U.bodies(ref, sr.world), U.bodies(g, sg.world)
+            d = U.diff_bodies(br, bg)
+            assert d is None, "step %d: %s (pose error %s)" % (step, d, U.pose_error(br, bg))
+            live = br["inUse"] != 0
+            del bg
+            lr, lg = U.island_labels(ref, sr.world), U.island_labels(g, sg.world)
+            assert np.array_equal(lr[live], lg[live]), "step %d: island partition differs" % step
+            n = _pile_contacts_equal(ref, g, sr.world, sg.world, step)
+            pr, pg = ref.m3d_world_profile(sr.world), g.m3d_world_profile(sg.world)
+            for f in ("bodyCount", "awakeBodyCount", "contactCount", "touchingContactCount", "islandCount"):
+                assert getattr(pr, f) == getattr(pg, f), "step %d: profile %s" % (step, f)
+            kr, kg = U.contact_colors(ref, sr.world), U.contact_colors(g, sg.world)
+            m = kr >= 0
+            assert np.array_equal(kr[m], kg[m]), "step %d: colouring differs" % step
+            print("step %d: %d contacts, %d touching, %d coloured" % (step, n, pr.touchingContactCount, int(m.sum())))
+        assert pr.touchingContactCount > 300000
+    finally:
+        sr.close()
+        sg.close()
+
+
+def test_jointed_raft_every_joint_type_bit_exact():
+    """Every joint type (rigid and soft distance, ball, weld, hinge with a
+    limit, a motor, or both) inside one coloured island of > 300 contacts,
+    plus a hinged chain, a motor-driven wheel and a soft pendulum: 120 steps
+    compared bit for bit.  Hinge limits evaluate atan2, so the oracle is the
+    one with correctly rounded float transcendentals."""
+    assert lockstep(U.oracle_cr(), harness.JOINTED_RAFT, 120, seed=11) > 0
 
 
 def test_small_pile_bit_exact():
