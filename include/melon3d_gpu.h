@@ -62,6 +62,18 @@ M3D_API int32_t m3d_gpu_step_counters(m3d_world* world, uint32_t* out, int32_t c
  * mean 300).  Results are identical either way; only the speed differs. */
 M3D_API void m3d_gpu_set_giant_island_contacts(m3d_world* world, int32_t contacts);
 
+/* Stage profile of the last giant-island solve (profiling aid, no
+ * counterpart in the reference): out[0..4] = device ns spent building the
+ * incidence lists, colouring, bucketing by colour, levelling the overflow
+ * bucket (and preparing joints), and running the substeps; out[5] = colours
+ * used, out[6] = contacts in the serial overflow bucket, out[7] = its levels;
+ * out[8..14] = device ns of the substep stages summed over the substeps:
+ * integration + preparation, coloured normal sweeps, overflow normal sweeps
+ * (and joints), friction, reconstruction, coloured velocity sweeps, overflow
+ * velocity sweep (and joints).  Returns the count written (at most 15; 0 if
+ * the world never solved a giant island). */
+M3D_API int32_t m3d_gpu_giant_profile(m3d_world* world, double* out, int32_t capacity);
+
 /* Batch of worlds (no counterpart in the reference).  Packs `count` worlds
  * built with melon3d.h and not stepped yet (same gravity, iterations, cell
  * size and sleep setting) into one new world whose step advances all of them

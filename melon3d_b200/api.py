@@ -198,6 +198,7 @@ _GPU_PROTOS = {
     "m3d_gpu_last_step_device_ms": (C.c_float, [W]),
     "m3d_gpu_status": (C.c_int32, [W]),
     "m3d_gpu_set_giant_island_contacts": (None, [W, C.c_int32]),
+    "m3d_gpu_giant_profile": (C.c_int32, [W, C.POINTER(C.c_double), C.c_int32]),
     "m3d_gpu_batch_create": (W, [C.POINTER(W), C.c_int32]),
     "m3d_gpu_batch_world_count": (C.c_int32, [W]),
     "m3d_gpu_batch_first_body": (C.c_int32, [W, C.c_int32]),

@@ -22,7 +22,12 @@
 //  - the overflow bucket (colour 8), solved serially by the reference, runs
 //    on CTA 0 level by level: overflow contacts that share no dynamic body
 //    commute, so each level's contacts run at once and every contact sees its
-//    bodies exactly as the serial order leaves them.
+//    bodies exactly as the serial order leaves them.  A contact's level is one
+//    above the levels of the previous overflow contact on each of its bodies
+//    (found by walking back the body's incidence list); the levels are
+//    computed by a grid-wide dataflow like the colouring and the overflow is
+//    regrouped by level with a counting sort, so a level's contacts are
+//    contiguous.
 //  - joints stay serial on one thread, as in the reference.
 // Every wait (dataflow or barrier) is bounded; one that runs out raises the
 // error word and lets the kernel finish.
@@ -32,8 +37,10 @@
 namespace m3g
 {
 
-constexpr int kGiantThreads = 256;
-constexpr int kGiantChunk = 256; // positions per colour-histogram chunk
+// one CTA of 512 threads per SM (128 registers each): the serial overflow
+// levels run on CTA 0, and a level of a few hundred contacts takes one pass
+constexpr int kGiantThreads = 512;
+constexpr int kGiantChunk = kGiantThreads; // positions per colour-histogram chunk
 constexpr uint32_t kGiantSpinLimit = 1u << 22;
 constexpr uint32_t kNoEnd = 0xFFFFFFFFu;
 
@@ -53,7 +60,10 @@ struct GiantArgs
 	uint32_t* bodyOffs;   // per island body + 1: incidence counts, then CSR offsets
 	uint32_t* bodyCursor; // per island body: fill cursor, then overflow levels
 	uint32_t* incidence;  // 2 per island contact: positions, ascending per body
-	int32_t* pred;        // 2 per island contact position: previous position on end A / B; then overflow levels
+	int32_t* pred;        // 2 per island contact position: previous position on end A / B; then, per
+	                      // position, its overflow index and, per overflow index, its level
+	int32_t* ovOrder;     // overflow contacts grouped by level
+	uint32_t* levelStart; // per level + 2: offsets into ovOrder
 	uint32_t* done;       // per island contact position: == epoch once coloured
 	int32_t* order;       // per island contact position: contact of the bucket order
 	int32_t* pmax;        // per position: colour during colouring, then the packet's point count
@@ -61,12 +71,41 @@ struct GiantArgs
 	uint32_t* chunkHist;  // colour-major chunk histograms, then their offsets
 	uint32_t* misc;       // [0..9] bucket starts, [10] colour count, [11] overflow levels
 	uint32_t* barrier;    // [0] arrivals, [1] generation
+	unsigned long long* phaseNs; // [0..5] globaltimer at the ends of the stages of the last island, [8..15]
+	                             // time per substep stage summed over the substeps (profiling)
 	uint32_t* error;
 	uint32_t epoch;
 	SolveParams P;
 };
 
 __device__ __forceinline__ uint32_t ldAcquire(const uint32_t* p) { return *(const volatile uint32_t*)p; }
+
+// stage timestamps of the giant solve, read by m3d_gpu_giant_profile
+__device__ __forceinline__ unsigned long long globalNs()
+{
+	unsigned long long t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+__device__ __forceinline__ void stamp(const GiantArgs& a, int k)
+{
+	if (blockIdx.x == 0 && threadIdx.x == 0)
+	{
+		a.phaseNs[k] = globalNs();
+	}
+}
+// substep stages: 0 integrate + prepare + packets, 1 coloured normals,
+// 2 overflow normals and joints, 3 friction, 4 reconstruct, 5 coloured
+// velocity pass, 6 overflow velocity pass and joints
+__device__ __forceinline__ void lap(const GiantArgs& a, unsigned long long& t0, int k)
+{
+	if (blockIdx.x == 0 && threadIdx.x == 0)
+	{
+		const unsigned long long t = globalNs();
+		a.phaseNs[8 + k] += t - t0;
+		t0 = t;
+	}
+}
 
 // island-local index of a contact end that the solve writes (non-zero inverse
 // mass) and that belongs to the island's body list; kNoEnd otherwise
@@ -171,7 +210,7 @@ __device__ __forceinline__ void giantContactOp(GiantOp op, const GiantArgs& a, i
 {
 	if (op == kGiantNormals)
 	{
-		solveContactNormals(a.B, a.C, c, a.P.maxCorrection);
+		solveContactNormalsPrefetched(a.B, a.C, c, a.P.maxCorrection);
 	}
 	else if (op == kGiantFriction)
 	{
@@ -184,8 +223,7 @@ __device__ __forceinline__ void giantContactOp(GiantOp op, const GiantArgs& a, i
 }
 
 // the overflow bucket in reference order, level by level on CTA 0
-__device__ void overflowSweep(GiantOp op, const GiantArgs& a, const int32_t* order, const int32_t* level, int o0,
-							  int o1, int levels)
+__device__ void overflowSweep(GiantOp op, const GiantArgs& a, int levels)
 {
 	if (blockIdx.x != 0)
 	{
@@ -193,18 +231,44 @@ __device__ void overflowSweep(GiantOp op, const GiantArgs& a, const int32_t* ord
 	}
 	for (int L = 1; L <= levels; ++L)
 	{
-		for (int q = o0 + threadIdx.x; q < o1; q += kGiantThreads)
+		const int e = (int)a.levelStart[L + 1];
+		for (int q = (int)a.levelStart[L] + threadIdx.x; q < e; q += kGiantThreads)
 		{
-			if (level[q] == L)
-			{
-				giantContactOp(op, a, order[q]);
-			}
+			giantContactOp(op, a, a.ovOrder[q]);
 		}
 		__syncthreads();
 	}
 }
 
-__global__ void __launch_bounds__(kGiantThreads) kSolveGiant(GiantArgs a)
+// Overflow index of the previous overflow contact on island body `l` before
+// island position p, or -1.  `ovIdx` maps island positions to overflow
+// indices (-1 for positions with a colour).
+__device__ __forceinline__ int32_t overflowPred(const GiantArgs& a, const uint32_t* incidence, const int32_t* ovIdx,
+												uint32_t l, uint32_t p)
+{
+	if (l == kNoEnd)
+	{
+		return -1;
+	}
+	const uint32_t s0 = a.bodyOffs[l], s1 = a.bodyOffs[l + 1];
+	uint32_t k = s0;
+	while (k < s1 && incidence[k] != p)
+	{
+		++k;
+	}
+	while (k > s0)
+	{
+		--k;
+		const int32_t i = ovIdx[incidence[k]];
+		if (i >= 0)
+		{
+			return i;
+		}
+	}
+	return -1;
+}
+
+__global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) kSolveGiant(GiantArgs a)
 {
 	__shared__ uint32_t gen;
 	__shared__ uint32_t warpSums[kGiantThreads / 32 + 1];
@@ -235,6 +299,9 @@ __global__ void __launch_bounds__(kGiantThreads) kSolveGiant(GiantArgs a)
 		uint32_t* done = a.done + r.contactStart;
 		uint32_t* incidence = a.incidence + 2 * (int64_t)r.contactStart;
 		const int nb = r.bodyCount, nc = r.contactCount;
+		int32_t* ovIdx = pred;       // per position, once the colouring is done
+		int32_t* ovLevel = pred + nc; // per overflow index
+		stamp(a, 0);
 
 		// ---- incidence lists: island contacts per dynamic body, ascending position
 		for (int b = gtid; b < nb; b += gthreads)
@@ -312,6 +379,7 @@ __global__ void __launch_bounds__(kGiantThreads) kSolveGiant(GiantArgs a)
 			}
 		}
 		gridSync(a, &gen);
+		stamp(a, 1);
 
 		// ---- greedy first-fit colouring as a dataflow (src/xpbd.cpp:1179-1235)
 		for (int p = gtid; p < nc; p += gthreads)
@@ -358,6 +426,7 @@ __global__ void __launch_bounds__(kGiantThreads) kSolveGiant(GiantArgs a)
 			*(volatile uint32_t*)&done[p] = a.epoch;
 		}
 		gridSync(a, &gen);
+		stamp(a, 2);
 
 		// ---- buckets: stable counting sort of positions by colour
 		const int chunks = (nc + kGiantChunk - 1) / kGiantChunk;
@@ -435,57 +504,102 @@ __global__ void __launch_bounds__(kGiantThreads) kSolveGiant(GiantArgs a)
 			__syncthreads();
 			if (valid)
 			{
-				order[a.chunkHist[color * chunks + k] + warpColor[warp][color] + rank] = (int32_t)contacts[p];
+				const int q = (int)(a.chunkHist[color * chunks + k] + warpColor[warp][color] + rank);
+				order[q] = (int32_t)contacts[p];
+				ovIdx[p] = color == kMaxGraphColors ? q - bucket[kMaxGraphColors] : -1;
 			}
 			__syncthreads();
 		}
 		gridSync(a, &gen);
+		stamp(a, 3);
 
 		// ---- overflow levels (serial order of the overflow bucket)
 		const int o0 = bucket[kMaxGraphColors], o1 = bucket[kMaxGraphColors + 1];
-		int32_t* level = pred; // the predecessor table is free again
-		if (gtid == 0 && o1 > o0)
+		const int nov = o1 - o0;
+		if (nov > 0)
 		{
-			for (int q = o0; q < o1; ++q)
+			for (int i = gtid; i < nov + 2; i += gthreads)
 			{
-				const int2 ab = C.bodies[order[q]];
-				const uint32_t la = islandEnd(a, bodies, nb, ab.x), lb = islandEnd(a, bodies, nb, ab.y);
-				if (la != kNoEnd)
+				a.levelStart[i] = 0u;
+				if (i < nov)
 				{
-					a.bodyCursor[la] = 0u;
-				}
-				if (lb != kNoEnd)
-				{
-					a.bodyCursor[lb] = 0u;
+					ovLevel[i] = 0;
 				}
 			}
-			uint32_t maxLevel = 0;
-			for (int q = o0; q < o1; ++q)
+			if (gtid == 0)
 			{
-				const int2 ab = C.bodies[order[q]];
-				const uint32_t la = islandEnd(a, bodies, nb, ab.x), lb = islandEnd(a, bodies, nb, ab.y);
-				uint32_t l = 0;
-				if (la != kNoEnd)
-				{
-					l = a.bodyCursor[la];
-				}
-				if (lb != kNoEnd && a.bodyCursor[lb] > l)
-				{
-					l = a.bodyCursor[lb];
-				}
-				++l;
-				level[q] = (int32_t)l;
-				if (la != kNoEnd)
-				{
-					a.bodyCursor[la] = l;
-				}
-				if (lb != kNoEnd)
-				{
-					a.bodyCursor[lb] = l;
-				}
-				maxLevel = l > maxLevel ? l : maxLevel;
+				a.misc[kMaxGraphColors + 3] = 0u;
 			}
-			a.misc[kMaxGraphColors + 3] = maxLevel;
+			gridSync(a, &gen);
+			// dataflow: an overflow contact waits for the levels of its
+			// predecessors; every thread takes its indices in ascending order,
+			// so the lowest unlevelled index can always proceed
+			for (int i = gtid; i < nov; i += gthreads)
+			{
+				const int c = order[o0 + i];
+				const int2 ab = C.bodies[c];
+				// island position of overflow index i: the position on the
+				// contact's first island body whose overflow index is i
+				const uint32_t la = islandEnd(a, bodies, nb, ab.x), lb = islandEnd(a, bodies, nb, ab.y);
+				uint32_t p = kNoEnd;
+				const uint32_t l0 = la != kNoEnd ? la : lb;
+				for (uint32_t k = l0 != kNoEnd ? a.bodyOffs[l0] : 0u; l0 != kNoEnd && k < a.bodyOffs[l0 + 1]; ++k)
+				{
+					const uint32_t pk = incidence[k];
+					if (ovIdx[pk] == i)
+					{
+						p = pk;
+						break;
+					}
+				}
+				const int32_t ia = overflowPred(a, incidence, ovIdx, la, p);
+				const int32_t ib = overflowPred(a, incidence, ovIdx, lb, p);
+				int32_t lvA = 0, lvB = 0;
+				for (uint32_t it = 0;; ++it)
+				{
+					lvA = ia >= 0 ? *(volatile int32_t*)&ovLevel[ia] : 1;
+					lvB = ib >= 0 ? *(volatile int32_t*)&ovLevel[ib] : 1;
+					if (lvA != 0 && lvB != 0)
+					{
+						break;
+					}
+					if (it > kGiantSpinLimit)
+					{
+						atomicOr(a.error, 1u);
+						lvA = lvA != 0 ? lvA : 1;
+						lvB = lvB != 0 ? lvB : 1;
+						break;
+					}
+					__nanosleep(20);
+				}
+				const int32_t lv = 1 + ((ia >= 0 ? lvA : 0) > (ib >= 0 ? lvB : 0) ? (ia >= 0 ? lvA : 0) : (ib >= 0 ? lvB : 0));
+				atomicAdd(&a.levelStart[lv + 1], 1u);
+				atomicMax(&a.misc[kMaxGraphColors + 3], (uint32_t)lv);
+				__threadfence();
+				*(volatile int32_t*)&ovLevel[i] = lv;
+			}
+			gridSync(a, &gen);
+			if (blockIdx.x == 0)
+			{
+				const int levels = (int)a.misc[kMaxGraphColors + 3];
+				ctaScan(a.levelStart, levels + 2, warpSums);
+			}
+			gridSync(a, &gen);
+			// placement; the order inside a level does not matter (its
+			// contacts share no dynamic body).  Level L's count sat at
+			// levelStart[L + 1]; after the exclusive scan that entry holds the
+			// level's start and the placement advances it to the level's end,
+			// so afterwards level L spans [levelStart[L], levelStart[L + 1]).
+			for (int i = gtid; i < nov; i += gthreads)
+			{
+				const int32_t lv = ovLevel[i];
+				a.ovOrder[atomicAdd(&a.levelStart[lv + 1], 1u)] = order[o0 + i];
+			}
+			gridSync(a, &gen);
+		}
+		if (gtid == 0)
+		{
+			a.misc[kMaxGraphColors + 4] = (uint32_t)nov;
 		}
 		if (r.jointCount > 0)
 		{
@@ -495,7 +609,7 @@ __global__ void __launch_bounds__(kGiantThreads) kSolveGiant(GiantArgs a)
 			}
 		}
 		gridSync(a, &gen);
-		const int overLevels = o1 > o0 ? (int)a.misc[kMaxGraphColors + 3] : 0;
+		const int overLevels = nov > 0 ? (int)a.misc[kMaxGraphColors + 3] : 0;
 		if (r.jointCount > 0)
 		{
 			if (gtid == 0)
@@ -508,8 +622,19 @@ __global__ void __launch_bounds__(kGiantThreads) kSolveGiant(GiantArgs a)
 			gridSync(a, &gen);
 		}
 
+		stamp(a, 4);
+
 		// ---- substeps (src/xpbd.cpp:1237-1369)
 		const int colored = bucket[kMaxGraphColors];
+		unsigned long long t0 = 0;
+		if (blockIdx.x == 0 && threadIdx.x == 0)
+		{
+			for (int k = 8; k < 15; ++k)
+			{
+				a.phaseNs[k] = 0ull;
+			}
+			t0 = globalNs();
+		}
 		for (int sub = 0; sub < P.substeps; ++sub)
 		{
 			for (int b = gtid; b < nb; b += gthreads)
@@ -549,6 +674,7 @@ __global__ void __launch_bounds__(kGiantThreads) kSolveGiant(GiantArgs a)
 				pmax[q] = m;
 			}
 			gridSync(a, &gen);
+			lap(a, t0, 0);
 			for (int it = 0; it < P.iterations; ++it)
 			{
 				if (r.jointCount > 0)
@@ -570,11 +696,13 @@ __global__ void __launch_bounds__(kGiantThreads) kSolveGiant(GiantArgs a)
 					}
 					gridSync(a, &gen);
 				}
+				lap(a, t0, 1);
 				if (overLevels > 0)
 				{
-					overflowSweep(kGiantNormals, a, order, level, o0, o1, overLevels);
+					overflowSweep(kGiantNormals, a, overLevels);
 					gridSync(a, &gen);
 				}
+				lap(a, t0, 2);
 			}
 			for (int color = 0; color < ncol; ++color)
 			{
@@ -586,14 +714,16 @@ __global__ void __launch_bounds__(kGiantThreads) kSolveGiant(GiantArgs a)
 			}
 			if (overLevels > 0)
 			{
-				overflowSweep(kGiantFriction, a, order, level, o0, o1, overLevels);
+				overflowSweep(kGiantFriction, a, overLevels);
 				gridSync(a, &gen);
 			}
+			lap(a, t0, 3);
 			for (int b = gtid; b < nb; b += gthreads)
 			{
 				reconstructBody(B, (int)bodies[b], P.invH);
 			}
 			gridSync(a, &gen);
+			lap(a, t0, 4);
 			for (int color = 0; color < ncol; ++color)
 			{
 				for (int q = bucket[color] + gtid; q < bucket[color + 1]; q += gthreads)
@@ -602,9 +732,10 @@ __global__ void __launch_bounds__(kGiantThreads) kSolveGiant(GiantArgs a)
 				}
 				gridSync(a, &gen);
 			}
+			lap(a, t0, 5);
 			if (overLevels > 0 || r.jointCount > 0)
 			{
-				overflowSweep(kGiantVelocity, a, order, level, o0, o1, overLevels);
+				overflowSweep(kGiantVelocity, a, overLevels);
 				if (gtid == 0)
 				{
 					for (int j = 0; j < r.jointCount; ++j)
@@ -614,7 +745,9 @@ __global__ void __launch_bounds__(kGiantThreads) kSolveGiant(GiantArgs a)
 				}
 				gridSync(a, &gen);
 			}
+			lap(a, t0, 6);
 		}
+		stamp(a, 5);
 	}
 }
 
@@ -636,7 +769,9 @@ void launchSolveGiant(DevWorld& w, const SolveParams& P)
 	void* doneBefore = w.giantDone.ptr;
 	w.giantDone.ensureZeroed(nc * sizeof(uint32_t), w.stream);
 	w.giantChunkHist.ensure((kMaxGraphColors + 1) * chunks * sizeof(uint32_t));
-	w.giantMisc.ensure(16 * sizeof(uint32_t));
+	w.giantMisc.ensure(16 * sizeof(uint32_t) + 16 * sizeof(unsigned long long));
+	w.giantOvOrder.ensure(nc * sizeof(int32_t));
+	w.giantLevelStart.ensure((nc + 2) * sizeof(uint32_t));
 	w.giantBarrier.ensureZeroed(4 * sizeof(uint32_t), w.stream);
 	if (w.giantDone.ptr != doneBefore || ++w.giantEpoch == 0u)
 	{
@@ -671,6 +806,8 @@ void launchSolveGiant(DevWorld& w, const SolveParams& P)
 	a.bodyCursor = w.giantBodyCursor.as<uint32_t>();
 	a.incidence = w.giantIncidence.as<uint32_t>();
 	a.pred = w.giantPred.as<int32_t>();
+	a.ovOrder = w.giantOvOrder.as<int32_t>();
+	a.levelStart = w.giantLevelStart.as<uint32_t>();
 	a.done = w.giantDone.as<uint32_t>();
 	a.order = w.colorOrder.as<int32_t>();
 	a.pmax = w.packetMax.as<int32_t>();
@@ -678,6 +815,7 @@ void launchSolveGiant(DevWorld& w, const SolveParams& P)
 	a.chunkHist = w.giantChunkHist.as<uint32_t>();
 	a.misc = w.giantMisc.as<uint32_t>();
 	a.barrier = w.giantBarrier.as<uint32_t>();
+	a.phaseNs = (unsigned long long*)(w.giantMisc.as<uint32_t>() + 16);
 	a.error = &dc->waitErrors;
 	a.epoch = w.giantEpoch;
 	a.P = P;

@@ -377,6 +377,8 @@ __global__ void kIslandTable(const int32_t* islandLabels, int32_t maxIslands, co
 		if (r.contactCount <= tinyContacts && r.jointCount == 0)
 		{
 			tinyList[atomicAdd(&dc->tinyIslands, 1u)] = k;
+			atomicAdd(&dc->tinyBodies, (uint32_t)r.bodyCount);
+			atomicAdd(&dc->tinyContacts, (uint32_t)r.contactCount);
 		}
 		else
 		{

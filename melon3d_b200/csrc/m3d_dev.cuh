@@ -56,6 +56,8 @@ struct StepCounters
 	uint32_t serialBodies;   // bodies of the serial islands
 	uint32_t serialContacts; // contacts of the serial islands
 	uint32_t sleptBodies;    // bodies put to sleep (counted only while a tape records)
+	uint32_t tinyBodies;     // bodies of the tiny serial islands (one thread each)
+	uint32_t tinyContacts;   // contacts of the tiny serial islands
 };
 
 // Host -> device body update record (one per body touched by the API
@@ -180,6 +182,7 @@ struct DevWorld
 	int32_t giantIslandContacts = 32768; // islands with at least this many contacts
 	DevBuf giantLocal, giantBodyOffs, giantBodyCursor, giantIncidence, giantPred, giantDone, giantChunkHist;
 	DevBuf giantMisc, giantBarrier;
+	DevBuf giantOvOrder, giantLevelStart; // overflow bucket regrouped by level, level offsets
 	uint32_t giantEpoch = 0;
 	int giantGrid = 0;
 

@@ -473,6 +473,70 @@ M3G_D void solveContactNormals(const BodySoA& B, const ContactSoA& C, int c, flo
 	storePose(B, ab.y, b);
 }
 
+// solveContactNormals with the data of every point loaded before the first
+// correction: none of it depends on the corrections, and issuing the loads
+// together costs the contact a few memory round trips instead of two per
+// point.  Same arithmetic, point by point.  It needs ~100 more registers, so
+// only the kernel whose sweeps are one level of contacts at a time on one CTA
+// (the overflow bucket of giant islands) uses it.
+M3G_D void solveContactNormalsPrefetched(const BodySoA& B, const ContactSoA& C, int c, float maxCorrection)
+{
+	int2 ab = C.bodies[c];
+	int pc = C.pointCount[c];
+	if (pc == 0)
+	{
+		return;
+	}
+	float wN[4], sepOff[4], lamN[4];
+	V3 anA[4], anB[4], jA[4], jB[4];
+#pragma unroll
+	for (int s = 0; s < 4; ++s)
+	{
+		if (s < pc)
+		{
+			size_t k = pidx(C, c, s);
+			wN[s] = C.pRA[k].w;
+			anA[s] = ld3(C.pAnchorA[k]);
+			anB[s] = ld3(C.pAnchorB[k]);
+			sepOff[s] = C.pSlip[k].w;
+			lamN[s] = C.pFricA[k].w;
+			jA[s] = ld3(C.pJA[k]);
+			jB[s] = ld3(C.pJB[k]);
+		}
+	}
+	BodyDyn a = loadDyn(B, ab.x), b = loadDyn(B, ab.y);
+	V3 n = ld3(C.normal[c]);
+#pragma unroll
+	for (int s = 0; s < 4; ++s)
+	{
+		if (s >= pc)
+		{
+			break;
+		}
+		if (wN[s] <= 0.0f)
+		{
+			continue;
+		}
+		V3 rA = rotate(a.q, anA[s]);
+		V3 rB = rotate(b.q, anB[s]);
+		float sep = sepOff[s] + dot(sub(add(b.p, rB), add(a.p, rA)), n);
+		if (sep >= 0.0f)
+		{
+			continue;
+		}
+		if (sep < -maxCorrection)
+		{
+			sep = -maxCorrection;
+		}
+		float dl = -sep / wN[s];
+		C.pFricA[pidx(C, c, s)].w = lamN[s] + dl;
+		applyAxisCorrection(b, dl, n, jB[s]);
+		applyAxisCorrection(a, -dl, n, jA[s]);
+	}
+	storePose(B, ab.x, a);
+	storePose(B, ab.y, b);
+}
+
 // Normal projection of one contact as one lane of a colour packet
 // (reference src/xpbd.cpp:1047-1141).  The lane sweeps `maxPoints` slots -
 // the largest point count among the 8 contacts of its packet - and slots past

@@ -1947,6 +1947,43 @@ int32_t m3d_gpu_batch_first_body(m3d_world* batch, int32_t worldIndex)
 	return batch->batchFirstBody[worldIndex];
 }
 
+int32_t m3d_gpu_giant_profile(m3d_world* world, double* out, int32_t capacity)
+{
+	DevWorld& d = world->dev;
+	if (d.giantMisc.ptr == nullptr || out == nullptr || capacity <= 0)
+	{
+		return 0;
+	}
+	uint32_t misc[16];
+	unsigned long long ns[16];
+	cudaMemcpyAsync(misc, d.giantMisc.ptr, sizeof(misc), cudaMemcpyDeviceToHost, d.stream);
+	cudaMemcpyAsync(ns, (const char*)d.giantMisc.ptr + sizeof(misc), sizeof(ns), cudaMemcpyDeviceToHost, d.stream);
+	cudaStreamSynchronize(d.stream);
+	int32_t ncol = 0;
+	for (int c = 0; c < kMaxGraphColors; ++c)
+	{
+		ncol = misc[c + 1] > misc[c] ? c + 1 : ncol;
+	}
+	double v[15];
+	for (int k = 0; k < 5; ++k)
+	{
+		v[k] = ns[k + 1] >= ns[k] ? (double)(ns[k + 1] - ns[k]) : 0.0;
+	}
+	v[5] = (double)ncol;
+	v[6] = (double)misc[kMaxGraphColors + 4];
+	v[7] = (double)misc[kMaxGraphColors + 3];
+	for (int k = 0; k < 7; ++k)
+	{
+		v[8 + k] = (double)ns[8 + k];
+	}
+	int32_t n = capacity < 15 ? capacity : 15;
+	for (int32_t k = 0; k < n; ++k)
+	{
+		out[k] = v[k];
+	}
+	return n;
+}
+
 void m3d_gpu_set_giant_island_contacts(m3d_world* world, int32_t contacts)
 {
 	world->dev.giantIslandContacts = contacts < kBigIslandContacts ? kBigIslandContacts : contacts;
