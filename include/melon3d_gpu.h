@@ -170,6 +170,9 @@ M3D_API int32_t m3d_gpu_tape_begin(m3d_world* world, int32_t checkpointEvery);
 M3D_API void m3d_gpu_tape_end(m3d_world* world);
 /* Steps recorded so far (0 without a tape). */
 M3D_API int32_t m3d_gpu_tape_steps(m3d_world* world);
+/* Device bytes the tape holds (contact records, island and body tables,
+ * checkpoints); the backward reads all of them at least once. */
+M3D_API int64_t m3d_gpu_tape_bytes(m3d_world* world);
 /* 1 while the tape is differentiable; else 0 and the reason in why. */
 M3D_API int32_t m3d_gpu_tape_supported(m3d_world* world, char* why, int32_t capacity);
 /* Re-runs the recorded steps from the first checkpoint with the recorded

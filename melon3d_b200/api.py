@@ -213,6 +213,7 @@ _GPU_PROTOS = {
     "m3d_gpu_tape_begin": (C.c_int32, [W, C.c_int32]),
     "m3d_gpu_tape_end": (None, [W]),
     "m3d_gpu_tape_steps": (C.c_int32, [W]),
+    "m3d_gpu_tape_bytes": (C.c_int64, [W]),
     "m3d_gpu_tape_supported": (C.c_int32, [W, C.c_char_p, C.c_int32]),
     "m3d_gpu_tape_replay": (C.c_int32, [W] + [C.POINTER(C.c_float)] * 4 + [C.c_int32]),
     "m3d_gpu_step_backward": (C.c_int32, [W] + [C.POINTER(C.c_float)] * 11 + [C.c_int32]),

@@ -148,6 +148,16 @@ const char* tapeUnsupported(const DiffTape* t) { return t->supported ? nullptr :
 
 int32_t tapeSteps(const DiffTape* t) { return (int32_t)t->steps.size(); }
 
+int64_t tapeBytes(const DiffTape* t)
+{
+	int64_t b = (int64_t)(t->islands.used + t->bodies.used + t->sleeps.used + t->checkpoints.used + t->prevPos.used);
+	for (const TapeStep& st : t->steps)
+	{
+		b += (int64_t)st.contactsPerSubstep * st.substeps * (int64_t)sizeof(TapeContact);
+	}
+	return b;
+}
+
 void tapeDestroy(DiffTape* t) { delete t; }
 
 // ---- recording -------------------------------------------------------------------

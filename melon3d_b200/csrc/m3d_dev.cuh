@@ -295,6 +295,7 @@ void tapeDestroy(DiffTape* t);
 void tapeMarkUnsupported(DiffTape* t, const char* why);
 const char* tapeUnsupported(const DiffTape* t); // null while the tape is differentiable
 int32_t tapeSteps(const DiffTape* t);
+int64_t tapeBytes(const DiffTape* t); // device bytes of the recorded steps (records, tables, checkpoints)
 void tapeStepBegin(DiffTape* t, DevWorld& w, int32_t n, float dt, int substeps, V3 g, int iterations);
 void tapeBeforeIslands(DiffTape* t, DevWorld& w, int substeps);
 void tapeStepEnd(DiffTape* t, DevWorld& w, const StepCounters& hc);

@@ -2292,6 +2292,11 @@ void m3d_gpu_tape_end(m3d_world* world)
 	}
 }
 
+int64_t m3d_gpu_tape_bytes(m3d_world* world)
+{
+	return world != nullptr && world->tape != nullptr ? tapeBytes(world->tape) : 0;
+}
+
 int32_t m3d_gpu_tape_steps(m3d_world* world)
 {
 	return world != nullptr && world->tape != nullptr ? tapeSteps(world->tape) : 0;

@@ -53,6 +53,8 @@ def _load():
         _lib.scn_churn.argtypes = [C.c_void_p]
         _lib.scn_step_only.restype = None
         _lib.scn_step_only.argtypes = [C.c_void_p, C.c_int]
+        _lib.scn_batch_world_bodies.restype = C.c_int32
+        _lib.scn_batch_world_bodies.argtypes = [C.c_uint64]
         _lib.scn_destroy.restype = None
         _lib.scn_destroy.argtypes = [C.c_void_p]
     return _lib
@@ -77,6 +79,12 @@ def api_table(lib):
                        ("weld_joint_def_default", "m3d_weld_joint_def_default")):
         setattr(t, field, C.cast(getattr(lib, sym), C.c_void_p).value)
     return t
+
+
+def batch_world_bodies(seed):
+    """Dynamic bodies of world `seed` of the batched-worlds scene, without
+    building it (same generator as the scene)."""
+    return int(_load().scn_batch_world_bodies(seed))
 
 
 class Scene:

@@ -670,6 +670,15 @@ void scn_step_only(void* scene, int substeps)
 	s.api.world_step(s.world, 1.0f / 60.0f, substeps);
 }
 
+// dynamic bodies of world `seed` of the batched-worlds scene (scene 4 with
+// a = 0), without building it
+int32_t scn_batch_world_bodies(uint64_t seed)
+{
+	Rng r{ seed };
+	double u = r.uniform();
+	return (int32_t)floor(exp(log(16.0) + u * (log(512.0) - log(16.0))));
+}
+
 // ids of the live dynamic bodies (creation order)
 int32_t scn_dynamic_ids(void* scene, m3d_body_id* out, int32_t cap)
 {
