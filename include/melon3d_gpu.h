@@ -93,6 +93,27 @@ M3D_API int32_t m3d_gpu_batch_world_count(m3d_world* batch);
 /* first body slot of world k; k == count gives the total slot count */
 M3D_API int32_t m3d_gpu_batch_first_body(m3d_world* batch, int32_t k);
 
+/* Steps this world took through the sleeping-world fast path: when the
+ * previous step changed nothing, every body was asleep before and after it
+ * and no API call has edited the world since, m3d_world_step does on the
+ * host what the reference's step does to such a world (advance the
+ * stable-tier schedule, report the profile) and launches nothing. */
+M3D_API int64_t m3d_gpu_fast_path_steps(m3d_world* world);
+
+/* Failure handling (no counterpart in the reference).  Every device-side
+ * wait of a step (the look-back of the scans, the grid barriers and the
+ * colouring / overflow-level dataflow of the whole-GPU island solve) gives up
+ * after a bounded number of unsuccessful polls and raises M3D_GPU_ERR_WAIT
+ * instead of hanging.  A scan that gives up computes its prefix directly, so
+ * the step's results stay exact; a giant-island solve that gives up stops at
+ * its next grid barrier, leaving that island's substeps unfinished (the
+ * world can be stepped on).  m3d_gpu_set_wait_limit sets the number of polls
+ * (< 0: the defaults, about a second; 0: no scan waits at all and a barrier
+ * gives up at its first unsuccessful poll) - a test aid for these paths.
+ * m3d_gpu_clear_status resets the sticky status to M3D_GPU_OK. */
+M3D_API void m3d_gpu_set_wait_limit(m3d_world* world, int64_t polls);
+M3D_API void m3d_gpu_clear_status(m3d_world* world);
+
 /* 0 when healthy, else the first M3D_GPU_ERR_* seen since creation. */
 M3D_API int32_t m3d_gpu_status(m3d_world* world);
 M3D_API const char* m3d_gpu_last_error_string(m3d_world* world);
@@ -119,7 +140,11 @@ M3D_API const char* m3d_gpu_last_error_string(m3d_world* world);
  *    stepped or queried through m3d_world_* once;
  *  - the first call on a device looks up the block's device address
  *    (cudaGetSymbolAddress, with the world's device made current) and caches
- *    it; make that first call before any stream capture on that device;
+ *    it with the device's current CUDA context; make that first call before
+ *    any stream capture on that device.  If the context is later destroyed
+ *    and recreated (cudaDeviceReset, or a framework resetting the primary
+ *    context), the next call sees a different context and looks the address
+ *    up again (again: not inside a stream capture);
  *  - the block is shared by every world and every call on the device and
  *    keeps the last call's contents (each call resets the parts it reads
  *    before use); each call waits for its own work, but calls whose work
@@ -142,6 +167,9 @@ M3D_API void m3d_gpu_profiler_kernel(float* totalMs, int32_t* launches);
 M3D_API int32_t m3d_gpu_profiler_table(char* out, int32_t capacity);
 /* Host->device and device->host bytes the library copied since the reset. */
 M3D_API void m3d_gpu_profiler_bytes(long long* h2d, long long* d2h);
+/* Device allocations (cudaMalloc calls) the library has made since it was
+ * loaded (not reset by m3d_gpu_profiler_reset). */
+M3D_API long long m3d_gpu_profiler_allocations(void);
 
 /* ---- differentiation (no counterpart in the reference) ----------------------
  * m3d_gpu_tape_begin opens a tape: every following m3d_world_step records
@@ -173,6 +201,11 @@ M3D_API int32_t m3d_gpu_tape_steps(m3d_world* world);
 /* Device bytes the tape holds (contact records, island and body tables,
  * checkpoints); the backward reads all of them at least once. */
 M3D_API int64_t m3d_gpu_tape_bytes(m3d_world* world);
+/* Islands of the recorded steps that the replay and the backward work with a
+ * whole warp each (islands with at least M3D_TAPE_WARP_CONTACTS contacts,
+ * read from the environment when the tape opens; default 8, 0 = none); the
+ * others take one thread each.  The results are the same either way. */
+M3D_API int64_t m3d_gpu_tape_warp_islands(m3d_world* world);
 /* 1 while the tape is differentiable; else 0 and the reason in why. */
 M3D_API int32_t m3d_gpu_tape_supported(m3d_world* world, char* why, int32_t capacity);
 /* Re-runs the recorded steps from the first checkpoint with the recorded

@@ -198,6 +198,9 @@ _GPU_PROTOS = {
     "m3d_gpu_last_step_device_ms": (C.c_float, [W]),
     "m3d_gpu_status": (C.c_int32, [W]),
     "m3d_gpu_set_giant_island_contacts": (None, [W, C.c_int32]),
+    "m3d_gpu_set_wait_limit": (None, [W, C.c_int64]),
+    "m3d_gpu_fast_path_steps": (C.c_int64, [W]),
+    "m3d_gpu_clear_status": (None, [W]),
     "m3d_gpu_giant_profile": (C.c_int32, [W, C.POINTER(C.c_double), C.c_int32]),
     "m3d_gpu_batch_create": (W, [C.POINTER(W), C.c_int32]),
     "m3d_gpu_batch_world_count": (C.c_int32, [W]),
@@ -206,6 +209,7 @@ _GPU_PROTOS = {
     "m3d_gpu_step_counters": (C.c_int32, [W, C.POINTER(C.c_uint32), C.c_int32]),
     "m3d_gpu_profiler_reset": (None, [C.c_char_p]),
     "m3d_gpu_profiler_launches": (C.c_longlong, []),
+    "m3d_gpu_profiler_allocations": (C.c_longlong, []),
     "m3d_gpu_profiler_kernel": (None, [C.POINTER(C.c_float), C.POINTER(C.c_int32)]),
     "m3d_gpu_profiler_bytes": (None, [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "m3d_gpu_profiler_table": (C.c_int32, [C.c_char_p, C.c_int32]),
@@ -214,6 +218,7 @@ _GPU_PROTOS = {
     "m3d_gpu_tape_end": (None, [W]),
     "m3d_gpu_tape_steps": (C.c_int32, [W]),
     "m3d_gpu_tape_bytes": (C.c_int64, [W]),
+    "m3d_gpu_tape_warp_islands": (C.c_int64, [W]),
     "m3d_gpu_tape_supported": (C.c_int32, [W, C.c_char_p, C.c_int32]),
     "m3d_gpu_tape_replay": (C.c_int32, [W] + [C.POINTER(C.c_float)] * 4 + [C.c_int32]),
     "m3d_gpu_step_backward": (C.c_int32, [W] + [C.POINTER(C.c_float)] * 11 + [C.c_int32]),

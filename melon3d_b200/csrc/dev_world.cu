@@ -12,6 +12,7 @@ template <typename T>
 static bool growArray(T*& p, int64_t oldCount, int64_t newCount, cudaStream_t s)
 {
 	T* np = nullptr;
+	countAllocation();
 	if (cudaMalloc((void**)&np, sizeof(T) * (size_t)newCount) != cudaSuccess)
 	{
 		return false;
@@ -81,6 +82,7 @@ template <typename T>
 static bool growPointArray(T*& p, int64_t oldCap, int64_t newCap, cudaStream_t s)
 {
 	T* np = nullptr;
+	countAllocation();
 	if (cudaMalloc((void**)&np, sizeof(T) * (size_t)newCap * 4) != cudaSuccess)
 	{
 		return false;

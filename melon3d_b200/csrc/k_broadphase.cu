@@ -949,6 +949,7 @@ int64_t launchOverPairsBatch(DevWorld& w, const PairCtx& P)
 	const int64_t maxN = w.maxWorldBodies;
 	const int64_t maxTotal = (int64_t)nO * (maxN + (nO < maxN ? nO : maxN));
 	w.overBlockOffs.ensure((size_t)(nO + 2) * sizeof(uint32_t));
+	w.overBlockCount.ensure((size_t)(nO + 2) * sizeof(uint32_t));
 	w.overFlag.ensure((size_t)(maxTotal + 1) * sizeof(uint32_t));
 	w.overScan.ensure((size_t)(maxTotal + 1) * sizeof(uint32_t));
 	w.overKeys.ensure((size_t)(maxTotal + 1) * sizeof(uint64_t));
@@ -960,10 +961,10 @@ int64_t launchOverPairsBatch(DevWorld& w, const PairCtx& P)
 	O.first = w.worldFirstBody.as<uint32_t>();
 	O.inActiveCells = w.inActiveCells.as<uint8_t>();
 	O.blockOffs = w.overBlockOffs.as<uint32_t>();
-	uint32_t* blocks = w.overBlockOffs.as<uint32_t>();
+	uint32_t* blocks = w.overBlockCount.as<uint32_t>();
 	M3G_LAUNCH(kOverBlocks, blocksFor(nO, 256), 256, s, w.B, O, blocks);
-	uint32_t* total = blocks + nO;
-	scanExclusive(blocks, blocks, nO, total, w.prim, s);
+	uint32_t* total = w.overBlockOffs.as<uint32_t>() + nO;
+	scanExclusive(blocks, w.overBlockOffs.as<uint32_t>(), nO, total, w.prim, s);
 	M3G_LAUNCH(kOverPairsBatch, blocksFor(maxTotal, 256), 256, s, P, O, maxTotal, total, w.overFlag.as<uint32_t>(),
 			   w.overKeys.as<uint64_t>());
 	scanExclusive(w.overFlag.as<uint32_t>(), w.overScan.as<uint32_t>(), maxTotal, &dc->overPairs, w.prim, s);

@@ -60,6 +60,7 @@ struct GrowBuf
 		}
 		size_t nb = buf.bytes * 2 > bytes ? buf.bytes * 2 : bytes;
 		void* p = nullptr;
+		countAllocation();
 		if (cudaMalloc(&p, nb) != cudaSuccess)
 		{
 			return false;
@@ -147,6 +148,16 @@ void tapeMarkUnsupported(DiffTape* t, const char* why)
 const char* tapeUnsupported(const DiffTape* t) { return t->supported ? nullptr : t->why; }
 
 int32_t tapeSteps(const DiffTape* t) { return (int32_t)t->steps.size(); }
+
+int64_t tapeWarpIslands(const DiffTape* t)
+{
+	int64_t n = 0;
+	for (const TapeStep& st : t->steps)
+	{
+		n += st.warpIslands;
+	}
+	return n;
+}
 
 int64_t tapeBytes(const DiffTape* t)
 {
@@ -686,6 +697,7 @@ struct DevArena
 	void* operator()(size_t bytes)
 	{
 		void* p = nullptr;
+		countAllocation();
 		if (cudaMalloc(&p, bytes) != cudaSuccess)
 		{
 			ok = false;

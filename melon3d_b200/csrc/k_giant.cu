@@ -70,10 +70,11 @@ struct GiantArgs
 	int32_t* contactColor;
 	uint32_t* chunkHist;  // colour-major chunk histograms, then their offsets
 	uint32_t* misc;       // [0..9] bucket starts, [10] colour count, [11] overflow levels
-	uint32_t* barrier;    // [0] arrivals, [1] generation
+	uint32_t* barrier;    // [0] arrivals, [1] generation, [2] stop: a wait of this launch gave up
 	unsigned long long* phaseNs; // [0..5] globaltimer at the ends of the stages of the last island, [8..15]
 	                             // time per substep stage summed over the substeps (profiling)
 	uint32_t* error;
+	uint32_t spinLimit; // unsuccessful polls before a wait gives up
 	uint32_t epoch;
 	SolveParams P;
 };
@@ -119,8 +120,19 @@ __device__ __forceinline__ uint32_t islandEnd(const GiantArgs& a, const uint32_t
 	return l < (uint32_t)nb && bodies[l] == (uint32_t)body ? l : kNoEnd;
 }
 
+// a wait gave up: raise the step's error word and make every CTA stop at its
+// next barrier
+__device__ __forceinline__ void giveUp(const GiantArgs& a)
+{
+	atomicOr(&a.barrier[2], 1u);
+	atomicOr(a.error, 1u);
+}
+
 // All CTAs meet here; writes before it are visible to reads after it.
-__device__ void gridSync(const GiantArgs& a, uint32_t* gen)
+// Returns true (to every thread of the CTA) when a wait of this launch gave
+// up: the caller returns at once, so no stage runs on the partial results of
+// the stage before.
+__device__ bool gridSync(const GiantArgs& a, uint32_t* gen, uint32_t* stop)
 {
 	__syncthreads();
 	if (threadIdx.x == 0)
@@ -138,9 +150,9 @@ __device__ void gridSync(const GiantArgs& a, uint32_t* gen)
 			uint32_t it = 0;
 			while (ldAcquire(&a.barrier[1]) == g)
 			{
-				if (++it > kGiantSpinLimit)
+				if (it++ >= a.spinLimit)
 				{
-					atomicOr(a.error, 1u);
+					giveUp(a);
 					break;
 				}
 				__nanosleep(32);
@@ -148,8 +160,10 @@ __device__ void gridSync(const GiantArgs& a, uint32_t* gen)
 		}
 		__threadfence();
 		*gen = g + 1u;
+		*stop = ldAcquire(&a.barrier[2]);
 	}
 	__syncthreads();
+	return *stop != 0u;
 }
 
 // exclusive scan of v[0..n) in place by the calling CTA; returns the total
@@ -270,7 +284,7 @@ __device__ __forceinline__ int32_t overflowPred(const GiantArgs& a, const uint32
 
 __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) kSolveGiant(GiantArgs a)
 {
-	__shared__ uint32_t gen;
+	__shared__ uint32_t gen, stop;
 	__shared__ uint32_t warpSums[kGiantThreads / 32 + 1];
 	__shared__ int32_t bucket[kMaxGraphColors + 2];
 	__shared__ uint32_t chunkCount[kMaxGraphColors + 1];
@@ -316,7 +330,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 		{
 			a.bodyOffs[nb] = 0u;
 		}
-		gridSync(a, &gen);
+		if (gridSync(a, &gen, &stop))
+		{
+			return;
+		}
 		for (int p = gtid; p < nc; p += gthreads)
 		{
 			const int2 ab = C.bodies[contacts[p]];
@@ -332,7 +349,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 				atomicAdd(&a.bodyOffs[lb], 1u);
 			}
 		}
-		gridSync(a, &gen);
+		if (gridSync(a, &gen, &stop))
+		{
+			return;
+		}
 		if (blockIdx.x == 0)
 		{
 			uint32_t total = ctaScan(a.bodyOffs, nb, warpSums);
@@ -341,7 +361,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 				a.bodyOffs[nb] = total;
 			}
 		}
-		gridSync(a, &gen);
+		if (gridSync(a, &gen, &stop))
+		{
+			return;
+		}
 		for (int p = gtid; p < nc; p += gthreads)
 		{
 			const int2 ab = C.bodies[contacts[p]];
@@ -355,7 +378,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 				incidence[a.bodyOffs[lb] + atomicAdd(&a.bodyCursor[lb], 1u)] = (uint32_t)p;
 			}
 		}
-		gridSync(a, &gen);
+		if (gridSync(a, &gen, &stop))
+		{
+			return;
+		}
 		for (int b = gtid; b < nb; b += gthreads)
 		{
 			const uint32_t s0 = a.bodyOffs[b], s1 = a.bodyOffs[b + 1];
@@ -378,7 +404,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 				pred[2 * p + ((uint32_t)ab.x == body ? 0 : 1)] = (int32_t)incidence[i - 1];
 			}
 		}
-		gridSync(a, &gen);
+		if (gridSync(a, &gen, &stop))
+		{
+			return;
+		}
 		stamp(a, 1);
 
 		// ---- greedy first-fit colouring as a dataflow (src/xpbd.cpp:1179-1235)
@@ -388,9 +417,9 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 			for (uint32_t it = 0; (pa >= 0 && ldAcquire(&done[pa]) != a.epoch) || (pb >= 0 && ldAcquire(&done[pb]) != a.epoch);
 				 ++it)
 			{
-				if (it > kGiantSpinLimit)
+				if (it >= a.spinLimit)
 				{
-					atomicOr(a.error, 1u);
+					giveUp(a);
 					break;
 				}
 				__nanosleep(20);
@@ -425,7 +454,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 			__threadfence();
 			*(volatile uint32_t*)&done[p] = a.epoch;
 		}
-		gridSync(a, &gen);
+		if (gridSync(a, &gen, &stop))
+		{
+			return;
+		}
 		stamp(a, 2);
 
 		// ---- buckets: stable counting sort of positions by colour
@@ -449,7 +481,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 			}
 			__syncthreads();
 		}
-		gridSync(a, &gen);
+		if (gridSync(a, &gen, &stop))
+		{
+			return;
+		}
 		if (blockIdx.x == 0)
 		{
 			ctaScan(a.chunkHist, (kMaxGraphColors + 1) * chunks, warpSums);
@@ -462,7 +497,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 				a.misc[kMaxGraphColors + 1] = (uint32_t)nc;
 			}
 		}
-		gridSync(a, &gen);
+		if (gridSync(a, &gen, &stop))
+		{
+			return;
+		}
 		if (threadIdx.x <= kMaxGraphColors + 1)
 		{
 			bucket[threadIdx.x] = (int32_t)a.misc[threadIdx.x];
@@ -510,7 +548,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 			}
 			__syncthreads();
 		}
-		gridSync(a, &gen);
+		if (gridSync(a, &gen, &stop))
+		{
+			return;
+		}
 		stamp(a, 3);
 
 		// ---- overflow levels (serial order of the overflow bucket)
@@ -530,7 +571,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 			{
 				a.misc[kMaxGraphColors + 3] = 0u;
 			}
-			gridSync(a, &gen);
+			if (gridSync(a, &gen, &stop))
+			{
+				return;
+			}
 			// dataflow: an overflow contact waits for the levels of its
 			// predecessors; every thread takes its indices in ascending order,
 			// so the lowest unlevelled index can always proceed
@@ -563,9 +607,9 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 					{
 						break;
 					}
-					if (it > kGiantSpinLimit)
+					if (it >= a.spinLimit)
 					{
-						atomicOr(a.error, 1u);
+						giveUp(a);
 						lvA = lvA != 0 ? lvA : 1;
 						lvB = lvB != 0 ? lvB : 1;
 						break;
@@ -578,13 +622,19 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 				__threadfence();
 				*(volatile int32_t*)&ovLevel[i] = lv;
 			}
-			gridSync(a, &gen);
+			if (gridSync(a, &gen, &stop))
+			{
+				return;
+			}
 			if (blockIdx.x == 0)
 			{
 				const int levels = (int)a.misc[kMaxGraphColors + 3];
 				ctaScan(a.levelStart, levels + 2, warpSums);
 			}
-			gridSync(a, &gen);
+			if (gridSync(a, &gen, &stop))
+			{
+				return;
+			}
 			// placement; the order inside a level does not matter (its
 			// contacts share no dynamic body).  Level L's count sat at
 			// levelStart[L + 1]; after the exclusive scan that entry holds the
@@ -595,7 +645,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 				const int32_t lv = ovLevel[i];
 				a.ovOrder[atomicAdd(&a.levelStart[lv + 1], 1u)] = order[o0 + i];
 			}
-			gridSync(a, &gen);
+			if (gridSync(a, &gen, &stop))
+			{
+				return;
+			}
 		}
 		if (gtid == 0)
 		{
@@ -608,7 +661,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 				refreshInvInertia(B, (int)bodies[b]);
 			}
 		}
-		gridSync(a, &gen);
+		if (gridSync(a, &gen, &stop))
+		{
+			return;
+		}
 		const int overLevels = nov > 0 ? (int)a.misc[kMaxGraphColors + 3] : 0;
 		if (r.jointCount > 0)
 		{
@@ -619,7 +675,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 					jointPrepare(B, a.J, (int)joints[j]);
 				}
 			}
-			gridSync(a, &gen);
+			if (gridSync(a, &gen, &stop))
+			{
+				return;
+			}
 		}
 
 		stamp(a, 4);
@@ -641,7 +700,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 			{
 				integrateBody(B, (int)bodies[b], P.h, P.gravity);
 			}
-			gridSync(a, &gen);
+			if (gridSync(a, &gen, &stop))
+			{
+				return;
+			}
 			for (int p = gtid; p < nc; p += gthreads)
 			{
 				prepareContact(B, C, (int)contacts[p], P.h);
@@ -653,7 +715,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 					jointReset(a.J, (int)joints[j]);
 				}
 			}
-			gridSync(a, &gen);
+			if (gridSync(a, &gen, &stop))
+			{
+				return;
+			}
 			// packets of 8 consecutive bucket entries share the largest point count
 			for (int q = gtid; q < colored; q += gthreads)
 			{
@@ -673,7 +738,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 				}
 				pmax[q] = m;
 			}
-			gridSync(a, &gen);
+			if (gridSync(a, &gen, &stop))
+			{
+				return;
+			}
 			lap(a, t0, 0);
 			for (int it = 0; it < P.iterations; ++it)
 			{
@@ -686,7 +754,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 							jointPosition(B, a.J, (int)joints[j], P.h);
 						}
 					}
-					gridSync(a, &gen);
+					if (gridSync(a, &gen, &stop))
+					{
+						return;
+					}
 				}
 				for (int color = 0; color < ncol; ++color)
 				{
@@ -694,13 +765,19 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 					{
 						solvePacketLane(B, C, order[q], pmax[q], P.maxCorrection);
 					}
-					gridSync(a, &gen);
+					if (gridSync(a, &gen, &stop))
+					{
+						return;
+					}
 				}
 				lap(a, t0, 1);
 				if (overLevels > 0)
 				{
 					overflowSweep(kGiantNormals, a, overLevels);
-					gridSync(a, &gen);
+					if (gridSync(a, &gen, &stop))
+					{
+						return;
+					}
 				}
 				lap(a, t0, 2);
 			}
@@ -710,19 +787,28 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 				{
 					applyContactFriction(B, C, order[q]);
 				}
-				gridSync(a, &gen);
+				if (gridSync(a, &gen, &stop))
+				{
+					return;
+				}
 			}
 			if (overLevels > 0)
 			{
 				overflowSweep(kGiantFriction, a, overLevels);
-				gridSync(a, &gen);
+				if (gridSync(a, &gen, &stop))
+				{
+					return;
+				}
 			}
 			lap(a, t0, 3);
 			for (int b = gtid; b < nb; b += gthreads)
 			{
 				reconstructBody(B, (int)bodies[b], P.invH);
 			}
-			gridSync(a, &gen);
+			if (gridSync(a, &gen, &stop))
+			{
+				return;
+			}
 			lap(a, t0, 4);
 			for (int color = 0; color < ncol; ++color)
 			{
@@ -730,7 +816,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 				{
 					solveContactVelocity(B, C, order[q], P.h, P.gravityLen);
 				}
-				gridSync(a, &gen);
+				if (gridSync(a, &gen, &stop))
+				{
+					return;
+				}
 			}
 			lap(a, t0, 5);
 			if (overLevels > 0 || r.jointCount > 0)
@@ -743,7 +832,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 						jointVelocity(B, a.J, (int)joints[j], P.h);
 					}
 				}
-				gridSync(a, &gen);
+				if (gridSync(a, &gen, &stop))
+				{
+					return;
+				}
 			}
 			lap(a, t0, 6);
 		}
@@ -819,8 +911,12 @@ void launchSolveGiant(DevWorld& w, const SolveParams& P)
 	a.error = &dc->waitErrors;
 	a.epoch = w.giantEpoch;
 	a.P = P;
-	// arrivals start from zero even if an earlier launch gave up on a wait
+	a.spinLimit = w.prim.waitLimit >= 0 ? (uint32_t)(w.prim.waitLimit < 0xFFFFFFFFll ? w.prim.waitLimit : 0xFFFFFFFFll)
+										  : kGiantSpinLimit;
+	// arrivals and the stop word start from zero even if an earlier launch
+	// gave up on a wait (the generation word keeps counting)
 	cudaMemsetAsync(w.giantBarrier.ptr, 0, sizeof(uint32_t), w.stream);
+	cudaMemsetAsync(w.giantBarrier.as<uint32_t>() + 2, 0, sizeof(uint32_t), w.stream);
 	void* args[] = { &a };
 	launchBegin("kSolveGiant", w.stream);
 	cudaLaunchCooperativeKernel((const void*)kSolveGiant, dim3((unsigned)w.giantGrid), dim3(kGiantThreads), args, 0,

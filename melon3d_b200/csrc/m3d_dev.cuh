@@ -203,6 +203,7 @@ struct DevWorld
 	DevBuf worldFirstBody;       // u32 per world + 1: first body slot of each world
 	int32_t maxWorldBodies = 0;  // largest world (body slots)
 	DevBuf overBlockOffs;        // oversized candidate blocks, world by world
+	DevBuf overBlockCount;       // their sizes (scanned into overBlockOffs)
 	DevBuf worldRebuild;         // u8 per world: stable tier rebuilt this step
 	DevBuf worldStableDirty;     // u32 per world: stable tier made dirty on the device
 	DevBuf worldContactCount;    // u32 per world: contacts at the start of the step
@@ -296,6 +297,7 @@ void tapeMarkUnsupported(DiffTape* t, const char* why);
 const char* tapeUnsupported(const DiffTape* t); // null while the tape is differentiable
 int32_t tapeSteps(const DiffTape* t);
 int64_t tapeBytes(const DiffTape* t); // device bytes of the recorded steps (records, tables, checkpoints)
+int64_t tapeWarpIslands(const DiffTape* t); // islands of the recorded steps worked by a warp each
 void tapeStepBegin(DiffTape* t, DevWorld& w, int32_t n, float dt, int substeps, V3 g, int iterations);
 void tapeBeforeIslands(DiffTape* t, DevWorld& w, int substeps);
 void tapeStepEnd(DiffTape* t, DevWorld& w, const StepCounters& hc);

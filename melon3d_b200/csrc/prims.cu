@@ -92,7 +92,9 @@ void drainPairs()
 namespace
 {
 std::atomic<long long> gH2D{ 0 }, gD2H{ 0 };
+std::atomic<long long> gAllocations{ 0 };
 }
+void countAllocation() { gAllocations.fetch_add(1, std::memory_order_relaxed); }
 
 cudaError_t countedMemcpyAsync(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s)
 {
@@ -171,9 +173,13 @@ bool DevBuf::ensure(size_t need)
 	{
 		return false;
 	}
+	countAllocation();
 	if (poisonAllocations())
 	{
+		// the fill runs on the legacy stream, which the worlds' non-blocking
+		// streams do not wait for: finish it before anything uses the buffer
 		cudaMemset(p, 0xA5, nb);
+		cudaDeviceSynchronize();
 	}
 	if (ptr != nullptr)
 	{
@@ -216,6 +222,8 @@ void PrimScratch::release()
 	sortKeys.release();
 	sortVals.release();
 	sortCounts.release();
+	sortOffs.release();
+	scanIn.release();
 	reduce.release();
 	if (hostReduce != nullptr)
 	{
@@ -301,9 +309,14 @@ __device__ __forceinline__ uint64_t statusWord(uint32_t epoch, uint32_t flag, ui
 	return ((uint64_t)epoch << 34) | ((uint64_t)flag << 32) | value;
 }
 
+// Decoupled look-back scan.  A tile's wait for a predecessor's status is
+// bounded (spinLimit unsuccessful polls; 0: the tile does not wait at all).
+// A tile that gives up raises the error word and computes its prefix by
+// summing the inputs of all earlier tiles directly: slower, but the same
+// exact result, so no later kernel ever indexes with a partial prefix.
 __global__ void __launch_bounds__(kScanThreads)
 	kScanLookback(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total, uint64_t* status,
-				  uint32_t* ticket, uint32_t epoch, uint32_t* error)
+				  uint32_t* ticket, uint32_t epoch, uint32_t* error, int64_t spinLimit)
 {
 	__shared__ uint32_t warpSums[kScanThreads / 32 + 1];
 	__shared__ uint32_t sTile, sPrefix;
@@ -345,27 +358,35 @@ __global__ void __launch_bounds__(kScanThreads)
 				vs[t] = statusWord(epoch, 1u, agg);
 			}
 			int idx = t - 1;
+			bool fallback = false;
 			while (true)
 			{
 				const int j = idx - lane;
 				uint32_t flag = 2u, value = 0u; // lanes before tile 0 contribute nothing
+				bool gaveUp = false;
 				if (j >= 0)
 				{
 					flag = 0u;
-					for (uint32_t it = 0; flag == 0u; ++it)
+					for (int64_t it = 0; flag == 0u; ++it)
 					{
+						if (it >= spinLimit)
+						{
+							gaveUp = true;
+							flag = 2u;
+							break;
+						}
 						uint64_t w = vs[j];
 						if ((uint32_t)(w >> 34) == epoch)
 						{
 							flag = (uint32_t)(w >> 32) & 3u;
 							value = (uint32_t)w;
 						}
-						else if (it >= kLookbackSpinLimit)
-						{
-							atomicOr(error, 1u);
-							flag = 2u;
-						}
 					}
+				}
+				if (__any_sync(0xffffffffu, gaveUp))
+				{
+					fallback = true;
+					break;
 				}
 				const uint32_t inclusive = __ballot_sync(0xffffffffu, flag == 2u);
 				if (inclusive != 0u)
@@ -376,6 +397,20 @@ __global__ void __launch_bounds__(kScanThreads)
 				}
 				excl += warpSum(value);
 				idx -= 32;
+			}
+			if (fallback)
+			{
+				if (lane == 0)
+				{
+					atomicOr(error, 1u);
+				}
+				uint32_t s = 0;
+				const int64_t end = (int64_t)t * kScanTile;
+				for (int64_t i = lane; i < end; i += 32)
+				{
+					s += in[i];
+				}
+				excl = warpSum(s);
 			}
 			if (lane == 0)
 			{
@@ -426,6 +461,12 @@ void scanExclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total
 		return;
 	}
 	const int64_t tiles = (n + kScanTile - 1) / kScanTile;
+	if (in == out && tiles > 1)
+	{
+		s.scanIn.ensure((size_t)n * sizeof(uint32_t));
+		cudaMemcpyAsync(s.scanIn.ptr, in, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream);
+		in = s.scanIn.as<uint32_t>();
+	}
 	s.scanTicket.ensureZeroed(4 * sizeof(uint32_t), stream);
 	s.waitError.ensureZeroed(4 * sizeof(uint32_t), stream);
 	void* before = s.scanStatus.ptr;
@@ -441,7 +482,8 @@ void scanExclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total
 	}
 	uint32_t* err = s.errorWord != nullptr ? s.errorWord : s.waitError.as<uint32_t>();
 	M3G_LAUNCH(kScanLookback, (unsigned)tiles, kScanThreads, stream, in, out, n, total, s.scanStatus.as<uint64_t>(),
-			   s.scanTicket.as<uint32_t>(), s.scanEpoch, err);
+			   s.scanTicket.as<uint32_t>(), s.scanEpoch, err,
+			   s.waitLimit >= 0 ? s.waitLimit : (int64_t)kLookbackSpinLimit);
 }
 
 // ---------------------------------------------------------------------------
@@ -578,11 +620,13 @@ void radixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, uint64_t varyMask
 	s.sortKeys.ensure((size_t)n * sizeof(uint64_t));
 	s.sortVals.ensure((size_t)n * sizeof(uint32_t));
 	s.sortCounts.ensure((size_t)kRadix * tiles * sizeof(uint32_t));
+	s.sortOffs.ensure((size_t)kRadix * tiles * sizeof(uint32_t));
 	uint64_t* k0 = keys;
 	uint32_t* v0 = vals;
 	uint64_t* k1 = s.sortKeys.as<uint64_t>();
 	uint32_t* v1 = s.sortVals.as<uint32_t>();
 	uint32_t* counts = s.sortCounts.as<uint32_t>();
+	uint32_t* offs = s.sortOffs.as<uint32_t>();
 	// 8-bit digit windows placed greedily on the bits that vary among the keys
 	// (constant bits need no pass): each window starts at the lowest varying
 	// bit not yet covered, clamped so it stays inside the key.  Windows rise
@@ -595,8 +639,8 @@ void radixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, uint64_t varyMask
 		shift = shift > 56 ? 56 : shift;
 		remaining &= ~(0xFFull << shift);
 		M3G_LAUNCH(kSortHistogram, tiles, kSortThreads, stream, k0, n, nDev, shift, bias, counts, tiles);
-		scanExclusive(counts, counts, (int64_t)kRadix * tiles, nullptr, s, stream);
-		M3G_LAUNCH(kSortScatter, tiles, kSortThreads, stream, k0, v0, k1, v1, n, nDev, shift, bias, counts, tiles);
+		scanExclusive(counts, offs, (int64_t)kRadix * tiles, nullptr, s, stream);
+		M3G_LAUNCH(kSortScatter, tiles, kSortThreads, stream, k0, v0, k1, v1, n, nDev, shift, bias, offs, tiles);
 		uint64_t* tk = k0;
 		k0 = k1;
 		k1 = tk;
@@ -691,6 +735,9 @@ void m3d_gpu_profiler_bytes(long long* h2d, long long* d2h)
 
 // Kernel launches of the library since the last reset (all kernels).
 long long m3d_gpu_profiler_launches(void) { return m3g::gLaunches.load(); }
+
+// Device allocations (cudaMalloc) the library made since it was loaded.
+long long m3d_gpu_profiler_allocations(void) { return m3g::gAllocations.load(); }
 
 // Total device time (ms) and launch count of the selected kernel since the
 // last reset, from CUDA events recorded around each of its launches.

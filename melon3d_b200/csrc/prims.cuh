@@ -38,8 +38,11 @@ struct PrimScratch
 	uint32_t scanEpoch = 0;      // epoch of the last scan launched
 	DevBuf waitError;            // fallback error word when errorWord is not set
 	uint32_t* errorWord = nullptr; // device word raised when a bounded wait runs out
+	int64_t waitLimit = -1;        // polls before a wait gives up; < 0: the default
 	DevBuf sortKeys, sortVals;   // ping-pong partner of a radix sort
 	DevBuf sortCounts;           // per-tile digit histograms
+	DevBuf sortOffs;             // their exclusive scan (the scatter's offsets)
+	DevBuf scanIn;               // copy of the input of an in-place scan
 	DevBuf reduce;               // 2 x u64: OR and AND of the keys
 	DevBuf hostPinned;           // not device memory: see hostReduce
 	uint64_t* hostReduce = nullptr; // pinned host copy of the reduce words
@@ -47,6 +50,8 @@ struct PrimScratch
 };
 
 // out[i] = sum(in[0..i)) for i < n; *total = sum(in[0..n)) when total != null.
+// A tile whose look-back gives up re-reads the inputs of the earlier tiles, so
+// an in-place scan (out == in) first copies its input aside.
 // in and out may alias.
 void scanExclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total, PrimScratch& s,
 				   cudaStream_t stream);
@@ -125,6 +130,10 @@ inline int blocksFor(int64_t n, int threads)
 // with m3d_gpu_profiler_reset, brackets it with CUDA events on its stream.
 void launchBegin(const char* name, cudaStream_t s);
 void launchEnd(const char* name, cudaStream_t s);
+
+// Counts one device allocation (every cudaMalloc of the library calls it);
+// read by m3d_gpu_profiler_allocations.
+void countAllocation();
 
 // Every async copy of the library goes through this wrapper (see the macro
 // below), which adds host->device and device->host bytes to the counters

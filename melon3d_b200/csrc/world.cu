@@ -111,6 +111,11 @@ struct m3d_world
 	std::vector<int32_t> batchStepsSinceStableBuild;
 	std::vector<uint32_t> batchDirtyRead;
 	bool stepped = false;
+	// the last step was a no-op that ended with every body asleep (see
+	// m3d_world_step); any API edit clears it
+	bool quiescent = false;
+	int64_t quiescentSteps = 0; // steps taken by the sleeping-world fast path
+	bool lastRebuiltStable = false; // the last step rebuilt the stable tier
 
 	// differentiation tape (m3d_gpu_tape_begin); null when not recording
 	DiffTape* tape = nullptr;
@@ -168,6 +173,7 @@ m3d_body_id makeId(m3d_world* w, int32_t index) { return { index, w->bodies[inde
 
 void markDirty(m3d_world* w, int32_t index, uint32_t mask)
 {
+	w->quiescent = false;
 	if ((int32_t)w->dirtyMask.size() < (int32_t)w->bodies.size())
 	{
 		w->dirtyMask.resize(w->bodies.size(), 0);
@@ -185,6 +191,7 @@ bool isBatch(const m3d_world* w) { return !w->batchFirstBody.empty(); }
 // rebuilt at the next step whatever its schedule)
 void markStableDirty(m3d_world* w, int32_t index, bool force = false)
 {
+	w->quiescent = false;
 	if (isBatch(w))
 	{
 		const uint32_t k = w->bodyWorld[index];
@@ -592,6 +599,7 @@ void refreshBroadphase(m3d_world* w, float dt)
 		}
 		cudaMemcpyAsync(d.worldRebuild.ptr, w->batchRebuild.data(), worlds, cudaMemcpyHostToDevice, d.stream);
 	}
+	w->lastRebuiltStable = rebuildStable;
 	launchRefresh(d, n, dt, rebuildStable, w->def.gridCellSize);
 	launchEmitGrid(d, n, w->def.gridCellSize, rebuildStable);
 	readCounters(d); // sync: tier sizes and cell-key masks
@@ -632,10 +640,38 @@ static __device__ __align__(256) unsigned char g_noAllocCastScratch[kNoAllocCast
 
 constexpr int kNoAllocMaxDevices = 64;
 static void* g_noAllocCastPtr[kNoAllocMaxDevices] = {};
+static void* g_noAllocCastCtx[kNoAllocMaxDevices] = {};
 static std::mutex g_noAllocCastMutex;
 
+// The current CUDA context (driver handle), through the runtime's driver
+// entry point so the library needs no link against libcuda; null if the
+// driver cannot say.
+static void* currentContext()
+{
+	typedef int (*CtxGetCurrent)(void**);
+	static CtxGetCurrent fn = [] {
+		void* p = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+			q != cudaDriverEntryPointSuccess)
+		{
+			p = nullptr;
+		}
+		return (CtxGetCurrent)p;
+	}();
+	void* ctx = nullptr;
+	if (fn == nullptr || fn(&ctx) != 0)
+	{
+		return nullptr;
+	}
+	return ctx;
+}
+
 // Device address of the scratch block on `device`, which must be current.
-// Looked up on the first call per device and cached.
+// Looked up on the first call per device and cached together with the
+// context it belongs to; when the device's context has been torn down and
+// recreated since (cudaDeviceReset, or a host framework resetting the
+// primary context), the cached address is stale and is looked up again.
 static cudaError_t noAllocCastScratch(int device, void** out)
 {
 	if (device < 0 || device >= kNoAllocMaxDevices)
@@ -643,7 +679,8 @@ static cudaError_t noAllocCastScratch(int device, void** out)
 		return cudaErrorInvalidDevice;
 	}
 	std::lock_guard<std::mutex> lock(g_noAllocCastMutex);
-	if (g_noAllocCastPtr[device] == nullptr)
+	void* ctx = currentContext();
+	if (g_noAllocCastPtr[device] == nullptr || ctx == nullptr || ctx != g_noAllocCastCtx[device])
 	{
 		void* ptr = nullptr;
 		cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_noAllocCastScratch);
@@ -652,6 +689,7 @@ static cudaError_t noAllocCastScratch(int device, void** out)
 			return e;
 		}
 		g_noAllocCastPtr[device] = ptr;
+		g_noAllocCastCtx[device] = ctx;
 	}
 	*out = g_noAllocCastPtr[device];
 	return cudaSuccess;
@@ -1205,7 +1243,11 @@ void m3d_body_set_restitution(m3d_world* world, m3d_body_id id, float restitutio
 }
 
 m3d_vec3 m3d_world_gravity(m3d_world* world) { return world->def.gravity; }
-void m3d_world_set_gravity(m3d_world* world, m3d_vec3 gravity) { world->def.gravity = gravity; }
+void m3d_world_set_gravity(m3d_world* world, m3d_vec3 gravity)
+{
+	world->def.gravity = gravity;
+	world->quiescent = false;
+}
 
 // ---- joints (reference src/world.cpp:868-1075) ------------------------------
 
@@ -1224,6 +1266,7 @@ static m3d_joint_id allocateJoint(m3d_world* world, JointRec** out)
 		memset(&world->joints[index], 0, sizeof(JointRec));
 		world->joints[index].generation = 1;
 	}
+	world->quiescent = false;
 	JointRec& j = world->joints[index];
 	uint32_t gen = j.generation;
 	memset(&j, 0, sizeof(JointRec));
@@ -1584,10 +1627,41 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	}
 	DevWorld& d = world->dev;
 	auto tStart = Clock::now();
-	cudaEventRecord(world->evStart, d.stream);
 	world->beginEvents.clear();
 	world->endEvents.clear();
+	if (world->quiescent && world->tape == nullptr && !isBatch(world) && world->dirtyList.empty() &&
+		!world->anyForcesApplied && !world->anyMaterialChange && !world->jointsDirty && !world->jointedPairsDirty &&
+		!(world->contactMirrorValid && world->contactsEdited) && !world->gridDirty && !world->stableDirty &&
+		!world->stableForce && world->status == M3D_GPU_OK)
+	{
+		// Sleeping-world fast path.  The last step changed nothing: every body
+		// was asleep before and after it, it admitted, created and removed no
+		// pair, saw no touch transition, did not rebuild the stable tier and
+		// left it clean, and no API call has edited the world since.  The
+		// reference's step on such a world refreshes no fat box, enumerates
+		// nothing (the active tier is empty), skips every sleeping pair in the
+		// narrowphase and takes the no-awake-body early-out
+		// (src/world.cpp:1848-1862), so it changes nothing but its stable-tier
+		// step count and profile: this step does the same on the host, with
+		// no device work.
+		++world->stepsSinceStableBuild;
+		world->lastDeviceMs = 0.0f;
+		auto tEnd = Clock::now();
+		world->profile.broadphaseMs = toMs(tStart, tEnd);
+		world->profile.narrowphaseMs = 0.0f;
+		world->profile.solverMs = 0.0f;
+		world->profile.stepMs = toMs(tStart, tEnd);
+		world->profile.awakeBodyCount = 0;
+		world->profile.touchingContactCount = 0;
+		world->profile.islandCount = 0;
+		++world->quiescentSteps;
+		return;
+	}
+	cudaEventRecord(world->evStart, d.stream);
 	const int32_t n = (int32_t)world->bodies.size();
+	const bool editsAtStart = !world->dirtyList.empty() || world->anyForcesApplied || world->anyMaterialChange ||
+							  world->jointsDirty || world->jointedPairsDirty ||
+							  (world->contactMirrorValid && world->contactsEdited);
 
 	if (world->tape != nullptr)
 	{
@@ -1746,6 +1820,13 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	world->profile.contactCount = d.contactCount;
 	world->profile.touchingContactCount = (int32_t)hc->touchingCount;
 	world->profile.islandCount = (int32_t)hc->islandCount;
+	// a no-op step on a sleeping world: the next one (without edits) takes the
+	// fast path at the top of this function
+	world->quiescent = !editsAtStart && !isBatch(world) && world->tape == nullptr && world->status == M3D_GPU_OK &&
+					   hc->awakeBodyCount == 0 && hc->anyAwakeDynamic == 0 && hc->newContacts == 0 &&
+					   hc->removed == 0 && hc->endRemoval == 0 && hc->beginNP == 0 && hc->endNP == 0 &&
+					   hc->stableDirty == 0 && hc->gridPairs == 0 && hc->overPairs == 0 && !world->lastRebuiltStable &&
+					   !world->stableDirty && !world->stableForce;
 }
 
 // ---- GPU extensions ------------------------------------------------------------
@@ -1946,6 +2027,19 @@ int32_t m3d_gpu_batch_first_body(m3d_world* batch, int32_t worldIndex)
 	}
 	return batch->batchFirstBody[worldIndex];
 }
+
+void m3d_gpu_set_wait_limit(m3d_world* world, int64_t polls)
+{
+	world->dev.prim.waitLimit = polls < 0 ? -1 : polls;
+}
+
+void m3d_gpu_clear_status(m3d_world* world)
+{
+	world->status = M3D_GPU_OK;
+	world->errorText[0] = 0;
+}
+
+int64_t m3d_gpu_fast_path_steps(m3d_world* world) { return world->quiescentSteps; }
 
 int32_t m3d_gpu_giant_profile(m3d_world* world, double* out, int32_t capacity)
 {
@@ -2290,6 +2384,11 @@ void m3d_gpu_tape_end(m3d_world* world)
 		tapeDestroy(world->tape);
 		world->tape = nullptr;
 	}
+}
+
+int64_t m3d_gpu_tape_warp_islands(m3d_world* world)
+{
+	return world != nullptr && world->tape != nullptr ? tapeWarpIslands(world->tape) : 0;
 }
 
 int64_t m3d_gpu_tape_bytes(m3d_world* world)

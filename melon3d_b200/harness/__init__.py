@@ -11,7 +11,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 SRC = os.path.join(HERE, "scenes.cpp")
 LIB = os.path.join(os.path.dirname(HERE), "lib", "libm3d_scenes.so")
 
-PYRAMID, RAIN, PILE, RAFT, BATCH_WORLD, INCLINE, JOINTED_RAFT = 0, 1, 2, 3, 4, 5, 6
+PYRAMID, RAIN, PILE, RAFT, BATCH_WORLD, INCLINE, JOINTED_RAFT, SETTLED_STACKS = 0, 1, 2, 3, 4, 5, 6, 7
 
 
 class M3dApi(C.Structure):

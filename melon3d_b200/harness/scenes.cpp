@@ -34,6 +34,10 @@
 //      a soft distance pendulum and spheres, capsules and boxes dropped on
 //      the raft (seeded); its joints all meet the one raft island once the
 //      chain lands
+//   7  settled stacks: an a x b grid of c-box stacks (unit cubes, 1.5 m
+//      apart, mu 0.6) resting on a static ground box; they fall asleep after
+//      about a second and then stay asleep (the fixed cost of a sleeping
+//      scene)
 #include "melon3d.h"
 
 #include <algorithm>
@@ -626,6 +630,24 @@ void* scn_create(const M3dApi* api, int kind, uint64_t seed, int a, int b, int c
 	else if (kind == 6)
 	{
 		buildJointedRaft(*s);
+	}
+	else if (kind == 7)
+	{
+		int nx = a > 0 ? a : 40, nz = b > 0 ? b : 30, ny = c > 0 ? c : 2;
+		const float sp = 1.5f;
+		float hx = 0.5f * sp * (float)nx + 5.0f, hz = 0.5f * sp * (float)nz + 5.0f;
+		addGround(*s, m3d_v3(0.0f, -0.5f, 0.0f), m3d_v3(hx, 0.5f, hz));
+		for (int i = 0; i < nx; ++i)
+		{
+			for (int k = 0; k < nz; ++k)
+			{
+				for (int j = 0; j < ny; ++j)
+				{
+					addBox(*s, m3d_v3(((float)i - 0.5f * (float)(nx - 1)) * sp, 0.5f + (float)j, ((float)k - 0.5f * (float)(nz - 1)) * sp),
+						   m3d_quat_identity(), m3d_v3(0.5f, 0.5f, 0.5f), 0.6f);
+				}
+			}
+		}
 	}
 	return s;
 }

@@ -444,3 +444,54 @@ def test_joints_make_the_tape_unsupported():
     lib.m3d_gpu_tape_end(sc.world)
     assert lib.m3d_gpu_tape_steps(sc.world) == 0
     sc.close()
+
+
+def _recorded_incline_batch(lib, seeds, steps):
+    scenes = [_incline(lib, s) for s in seeds]
+    arr = (C.c_void_p * len(scenes))(*[s.world for s in scenes])
+    batch = lib.m3d_gpu_batch_create(arr, len(scenes))
+    for s in scenes:
+        s.close()
+    assert lib.m3d_gpu_tape_begin(batch, 10) == api.GPU_OK
+    for _ in range(steps):
+        lib.m3d_world_step(batch, 1.0 / 60.0, 4)
+    return batch
+
+
+def test_warp_islands_give_the_one_thread_result():
+    """Islands of 8+ contacts are replayed and reversed by a whole warp (lanes
+    over one dependency level of contacts at a time).  The same recording
+    with every island on one thread (M3D_TAPE_WARP_CONTACTS=0, read when the
+    tape opens) must give the same replay states and gradients bit for bit."""
+    import os
+    lib = gpu()
+    seeds = [300 + k for k in range(12)]
+    results = []
+    old = os.environ.get("M3D_TAPE_WARP_CONTACTS")
+    try:
+        for setting in (None, "0"):
+            if setting is None:
+                os.environ.pop("M3D_TAPE_WARP_CONTACTS", None)
+            else:
+                os.environ["M3D_TAPE_WARP_CONTACTS"] = setting
+            batch = _recorded_incline_batch(lib, seeds, 50)
+            warp = lib.m3d_gpu_tape_warp_islands(batch)
+            rep = replay(lib, batch)
+            n = lib.m3d_gpu_body_capacity(batch)
+            dpos = np.random.default_rng(3).normal(size=(n, 3)).astype(np.float32)
+            rc, g = backward(lib, batch, dpos)
+            assert rc == api.GPU_OK, rc
+            results.append((warp, rep, g))
+            lib.m3d_world_destroy(batch)
+    finally:
+        if old is None:
+            os.environ.pop("M3D_TAPE_WARP_CONTACTS", None)
+        else:
+            os.environ["M3D_TAPE_WARP_CONTACTS"] = old
+    (w_warp, rep_w, g_w), (w_one, rep_1, g_1) = results
+    assert w_warp > 0, "no island reached the warp threshold: the warp path was not exercised"
+    assert w_one == 0
+    for a, b in zip(rep_w, rep_1):
+        assert _same_bits(a, b)
+    for k in ("pos", "rot", "vel", "ang", "mass", "mu", "e"):
+        assert _same_bits(g_w[k], g_1[k]), k

@@ -242,3 +242,44 @@ def test_runs_are_bit_identical_rain():
 
 def test_runs_are_bit_identical_pile():
     _gpu_twins(harness.PILE, 6, 3, a=20, b=40, c=20)
+
+
+def test_sleeping_world_fast_path_bit_exact():
+    """2,400 boxes in 2-box stacks fall asleep after ~33 steps; once a step
+    changes nothing, later steps take the host-only fast path.  Compared with
+    the reference after every step (bodies, contacts, profile counters),
+    before and after a body is woken by an impulse, which must end the fast
+    path until the world is asleep again."""
+    from melon3d_b200 import api
+    ref, g = U.oracle(), U.gpu()
+    sr = harness.Scene(ref, harness.SETTLED_STACKS, 1, 40, 30, 2)
+    sg = harness.Scene(g, harness.SETTLED_STACKS, 1, 40, 30, 2)
+    try:
+        def compare(step):
+            d = U.diff_contacts(U.contacts(ref, sr.world), U.contacts(g, sg.world))
+            assert d is None, "step %d: %s" % (step, d)
+            d = U.diff_bodies(U.bodies(ref, sr.world), U.bodies(g, sg.world))
+            assert d is None, "step %d: %s" % (step, d)
+            pr, pg = ref.m3d_world_profile(sr.world), g.m3d_world_profile(sg.world)
+            for f in ("bodyCount", "awakeBodyCount", "contactCount", "touchingContactCount", "islandCount"):
+                assert getattr(pr, f) == getattr(pg, f), "step %d: profile %s" % (step, f)
+            assert len(U.contacts(g, sg.world)) == pg.contactCount
+        for step in range(100):
+            sr.run(1)
+            sg.run(1)
+            compare(step)
+        fast = g.m3d_gpu_fast_path_steps(sg.world)
+        assert fast >= 40, fast
+        assert g.m3d_world_profile(sg.world).awakeBodyCount == 0
+        # wake one box with an impulse on both worlds: normal steps resume
+        ids_r, ids_g = sr.dynamic_ids(), sg.dynamic_ids()
+        for lib, w, ids in ((ref, sr.world, ids_r), (g, sg.world, ids_g)):
+            lib.m3d_body_apply_impulse(w, ids[7], api.Vec3(0.0, 4000.0, 0.0), lib.m3d_body_position(w, ids[7]))
+        for step in range(100, 130):
+            sr.run(1)
+            sg.run(1)
+            compare(step)
+        assert g.m3d_gpu_fast_path_steps(sg.world) == fast  # the woken world stepped normally
+    finally:
+        sr.close()
+        sg.close()

@@ -123,3 +123,42 @@ def test_worlds_beyond_the_limit_are_rejected():
             api.GPU_ERR_ARGUMENT
     finally:
         scene.close()
+
+
+def test_calls_allocate_no_device_memory():
+    """The defining property: on a warm world, a run of fixed-scratch casts
+    makes no device allocation (the library's cudaMalloc counter and the
+    device's free memory are unchanged), while the results still match the
+    allocating cast, which is made after the run."""
+    import torch
+    lib, scene = _scene(3000, 10)
+    try:
+        world = scene.world
+        casts = _casts(23, 16)
+        _noalloc(lib, world, casts[0])  # the first call on the device sets up the scratch address
+        torch.cuda.synchronize()
+        allocs = lib.m3d_gpu_profiler_allocations()
+        free0, _ = torch.cuda.mem_get_info()
+        got = [_noalloc(lib, world, c) for c in casts]
+        torch.cuda.synchronize()
+        assert lib.m3d_gpu_profiler_allocations() == allocs
+        assert torch.cuda.mem_get_info()[0] == free0
+        for c, (rc, r) in zip(casts, got):
+            assert rc == api.GPU_OK
+            assert _fields(r) == _fields(lib.m3d_world_sphere_cast(world, *c))
+    finally:
+        scene.close()
+
+
+def test_largest_accepted_world():
+    # exactly 65536 body slots (the ground and 65535 rain bodies): accepted
+    lib, scene = _scene(65535, 2)
+    try:
+        world = scene.world
+        assert lib.m3d_gpu_body_capacity(world) == 65536
+        for c in _casts(31, 6):
+            rc, r = _noalloc(lib, world, c)
+            assert rc == api.GPU_OK
+            assert _fields(r) == _fields(lib.m3d_world_sphere_cast(world, *c))
+    finally:
+        scene.close()
