@@ -495,6 +495,35 @@ def measure_batch_sharded(lib, args, d):
             "gathered_worlds": int(full.shape[0]), "centroid_checksum": float(np.nansum(full))}
 
 
+def measure_asleep(lib, args, ref_lib):
+    """Fixed per-step cost of fully asleep scenes: 2,400 / 8,000 / 18,000
+    unit boxes in 2-box stacks on a grid, stepped until every body sleeps and
+    the sleeping-world fast path is on, then timed (host wall time per step
+    through the C API, 200 steps); the reference steps the same scenes."""
+    out = {"workload": "fully asleep 2-box stacks (2,400 / 8,000 / 18,000 unit boxes), 60 Hz x 4 substeps",
+           "unit": "ms/step", "scenes": []}
+    cores = os.cpu_count() or 1
+    for dims in ((40, 30, 2), (80, 50, 2), (150, 60, 2)):
+        row = {"boxes": dims[0] * dims[1] * dims[2]}
+        for name, l, workers in (("gpu", lib, 0), ("reference", ref_lib, cores)):
+            if l is None or (name == "reference" and args.no_cpu_baseline):
+                continue
+            sc = harness.Scene(l, harness.SETTLED_STACKS, 1, *dims, workers=workers)
+            for _ in range(120):
+                sc.run(1, args.substeps)
+                if l.m3d_world_profile(sc.world).awakeBodyCount == 0 and (
+                        name == "reference" or l.m3d_gpu_fast_path_steps(sc.world) > 0):
+                    break
+            _, wall_ms, _ = sc.run(200, args.substeps)
+            row[name + "_ms_per_step"] = wall_ms / 200
+            if name == "gpu":
+                row["gpu_fast_path_steps"] = int(l.m3d_gpu_fast_path_steps(sc.world))
+            sc.close()
+        out["scenes"].append(row)
+    out["reference_sample"] = "reference release build, workerCount=%d, 200 steps after the scene sleeps" % cores
+    return out
+
+
 def _incline_batch(lib, W):
     scenes = [harness.Scene(lib, harness.INCLINE, k) for k in range(W)]
     ids = [s.dynamic_ids() for s in scenes]
@@ -659,7 +688,7 @@ def main():
         if d.world == 1:
             ref_lib = api.bind(C.CDLL(REF_RELEASE_LIB)) if os.path.exists(REF_RELEASE_LIB) else None
             variants = {"batched": measure_batch(lib, args, ref_lib), "pile": measure_pile(lib, args, ref_lib),
-                        "fwd_adjoint": measure_adjoint(lib, args)}
+                        "fwd_adjoint": measure_adjoint(lib, args), "asleep": measure_asleep(lib, args, ref_lib)}
         else:
             variants = {"batched_sharded": measure_batch_sharded(lib, args, d)}
     if d.rank == 0:
