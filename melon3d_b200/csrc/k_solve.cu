@@ -105,13 +105,45 @@ constexpr int kSerialWarpsPerBlock = 8;
 constexpr int kLevelTable = 320; // contacts and bodies per island for the level schedule
 constexpr uint32_t kNotIsland = 0xFFFFu;
 
+// Level schedules of one island (see kSolveSerial).  Positions index the
+// island's contacts; for islands with joints, the position sweeps run over
+// the joints followed by the contacts (the reference projects the joints
+// first in each iteration) and the velocity pass over the contacts followed
+// by the joints (it runs the joint motors after the contacts).
 struct LevelTables
 {
-	uint32_t contact[kLevelTable]; // contact index per island position
-	uint32_t ends[kLevelTable];    // island-local body of each end (kNotIsland: static / kinematic / other)
-	uint16_t level[kLevelTable];   // 1-based sweep level per island position
-	uint16_t last[kLevelTable];    // per island body: level of its latest contact
+	uint32_t contact[kLevelTable];  // contact index per island position
+	uint32_t ends[kLevelTable];     // island-local body of each end (kNotIsland: static / kinematic / other)
+	uint16_t level[kLevelTable];    // 1-based level per contact (friction sweep; every sweep without joints)
+	uint16_t last[kLevelTable];     // per island body: level of its latest element
+	uint16_t levelPos[kLevelTable]; // joints then contacts: level in the position sweeps
+	uint16_t levelVel[kLevelTable]; // contacts then joints: level in the velocity pass
 };
+
+// lane 0: levels of a sequence of elements given by their two island-local
+// ends; each element one level above the latest earlier element on either end
+__device__ __forceinline__ uint16_t levelOf(LevelTables& T, uint32_t la, uint32_t lb)
+{
+	uint16_t l = 0;
+	if (la != kNotIsland)
+	{
+		l = T.last[la];
+	}
+	if (lb != kNotIsland && T.last[lb] > l)
+	{
+		l = T.last[lb];
+	}
+	++l;
+	if (la != kNotIsland)
+	{
+		T.last[la] = l;
+	}
+	if (lb != kNotIsland)
+	{
+		T.last[lb] = l;
+	}
+	return l;
+}
 
 enum SweepOp
 {
@@ -134,6 +166,52 @@ __device__ __forceinline__ void sweepContact(SweepOp op, const BodySoA& B, const
 	else
 	{
 		solveContactVelocity(B, C, c, P.h, P.gravityLen);
+	}
+}
+
+// one sweep over the joints and contacts of an island with joints, level by
+// level (position: joints then contacts; velocity: contacts then joints)
+__device__ __forceinline__ void sweepJointedIsland(bool position, const BodySoA& B, const ContactSoA& C, JointRec* J,
+												   const IslandRec& r, const uint32_t* joints, const LevelTables& T,
+												   int levels, int lane, const SolveParams& P)
+{
+	const int nj = r.jointCount, nc = r.contactCount;
+	const uint16_t* lev = position ? T.levelPos : T.levelVel;
+	for (int L = 1; L <= levels; ++L)
+	{
+		for (int q = lane; q < nj + nc; q += 32)
+		{
+			if (lev[q] != L)
+			{
+				continue;
+			}
+			const bool isJoint = position ? q < nj : q >= nc;
+			if (isJoint)
+			{
+				const int j = (int)joints[position ? q : q - nc];
+				if (position)
+				{
+					jointPosition(B, J, j, P.h);
+				}
+				else
+				{
+					jointVelocity(B, J, j, P.h);
+				}
+			}
+			else
+			{
+				const int c = (int)T.contact[position ? q - nj : q];
+				if (position)
+				{
+					solveContactNormals(B, C, c, P.maxCorrection);
+				}
+				else
+				{
+					solveContactVelocity(B, C, c, P.h, P.gravityLen);
+				}
+			}
+		}
+		__syncwarp();
 	}
 }
 
@@ -169,6 +247,9 @@ __device__ __forceinline__ void sweepIsland(SweepOp op, const BodySoA& B, const 
 	}
 }
 
+// kTape: the instance used while a differentiation tape records (the plain
+// instance carries none of the recording code)
+template <bool kTape>
 __global__ void __launch_bounds__(32 * kSerialWarpsPerBlock)
 	kSolveSerial(BodySoA B, ContactSoA C, JointRec* J, const IslandRec* islands, const int32_t* serialList,
 				 const uint32_t* serialDev, const uint32_t* bodyVals, const uint32_t* contactVals,
@@ -187,9 +268,11 @@ __global__ void __launch_bounds__(32 * kSerialWarpsPerBlock)
 		const uint32_t* contacts = contactVals + r.contactStart;
 		const uint32_t* joints = jointVals + r.jointStart;
 
-		// level schedule of the island's contacts (fixed for the whole step)
-		int levels = 0;
-		if (r.jointCount == 0 && r.contactCount <= kLevelTable && r.bodyCount <= kLevelTable)
+		// level schedules of the island's contacts and joints (fixed for the
+		// whole step)
+		int levels = 0, levelsPos = 0, levelsVel = 0;
+		const int nj = r.jointCount, nc = r.contactCount;
+		if (nc + nj <= kLevelTable && r.bodyCount <= kLevelTable)
 		{
 			for (int b = lane; b < r.bodyCount; b += 32)
 			{
@@ -197,7 +280,7 @@ __global__ void __launch_bounds__(32 * kSerialWarpsPerBlock)
 				T.last[b] = 0;
 			}
 			__syncwarp();
-			for (int p = lane; p < r.contactCount; p += 32)
+			for (int p = lane; p < nc; p += 32)
 			{
 				const uint32_t c = contacts[p];
 				const int2 ab = C.bodies[c];
@@ -210,35 +293,72 @@ __global__ void __launch_bounds__(32 * kSerialWarpsPerBlock)
 			__syncwarp();
 			if (lane == 0)
 			{
-				int maxLevel = 0;
-				for (int p = 0; p < r.contactCount; ++p)
+				for (int p = 0; p < nc; ++p)
 				{
-					const uint32_t la = T.ends[p] & 0xFFFFu, lb = T.ends[p] >> 16;
-					int l = 0;
-					if (la != kNotIsland)
-					{
-						l = T.last[la];
-					}
-					if (lb != kNotIsland && T.last[lb] > l)
-					{
-						l = T.last[lb];
-					}
-					++l;
-					T.level[p] = (uint16_t)l;
-					if (la != kNotIsland)
-					{
-						T.last[la] = (uint16_t)l;
-					}
-					if (lb != kNotIsland)
-					{
-						T.last[lb] = (uint16_t)l;
-					}
-					maxLevel = l > maxLevel ? l : maxLevel;
+					T.level[p] = levelOf(T, T.ends[p] & 0xFFFFu, T.ends[p] >> 16);
+					levels = T.level[p] > levels ? T.level[p] : levels;
 				}
-				levels = maxLevel;
+				if (nj > 0)
+				{
+					// a joint's island-local ends (its static or kinematic end,
+					// never written, does not order anything)
+					auto jointEnds = [&](int q, uint32_t& la, uint32_t& lb) {
+						const JointRec& jr = J[joints[q]];
+						la = localIndex[jr.bodyA];
+						lb = localIndex[jr.bodyB];
+						la = la < (uint32_t)r.bodyCount && bodies[la] == (uint32_t)jr.bodyA ? la : kNotIsland;
+						lb = lb < (uint32_t)r.bodyCount && bodies[lb] == (uint32_t)jr.bodyB ? lb : kNotIsland;
+					};
+					for (int b = 0; b < r.bodyCount; ++b)
+					{
+						T.last[b] = 0;
+					}
+					for (int q = 0; q < nj + nc; ++q)
+					{
+						uint32_t la, lb;
+						if (q < nj)
+						{
+							jointEnds(q, la, lb);
+						}
+						else
+						{
+							la = T.ends[q - nj] & 0xFFFFu;
+							lb = T.ends[q - nj] >> 16;
+						}
+						T.levelPos[q] = levelOf(T, la, lb);
+						levelsPos = T.levelPos[q] > levelsPos ? T.levelPos[q] : levelsPos;
+					}
+					for (int b = 0; b < r.bodyCount; ++b)
+					{
+						T.last[b] = 0;
+					}
+					for (int q = 0; q < nj + nc; ++q)
+					{
+						uint32_t la, lb;
+						if (q < nc)
+						{
+							la = T.ends[q] & 0xFFFFu;
+							lb = T.ends[q] >> 16;
+						}
+						else
+						{
+							jointEnds(q - nc, la, lb);
+						}
+						T.levelVel[q] = levelOf(T, la, lb);
+						levelsVel = T.levelVel[q] > levelsVel ? T.levelVel[q] : levelsVel;
+					}
+				}
 			}
 			levels = __shfl_sync(0xffffffffu, levels, 0);
+			levelsPos = __shfl_sync(0xffffffffu, levelsPos, 0);
+			levelsVel = __shfl_sync(0xffffffffu, levelsVel, 0);
 			__syncwarp();
+		}
+		// islands with joints but too large for the tables stay serial on lane 0
+		const bool jointsLevelled = nj > 0 && levelsPos > 0;
+		if (nj > 0 && !jointsLevelled)
+		{
+			levels = 0;
 		}
 
 		if (r.jointCount > 0)
@@ -248,12 +368,11 @@ __global__ void __launch_bounds__(32 * kSerialWarpsPerBlock)
 				refreshInvInertia(B, (int)bodies[b]);
 			}
 			__syncwarp();
-			if (lane == 0)
+			// each joint's preparation reads the bodies and writes only its own
+			// record: any order gives the same records
+			for (int j = lane; j < r.jointCount; j += 32)
 			{
-				for (int j = 0; j < r.jointCount; ++j)
-				{
-					jointPrepare(B, J, (int)joints[j]);
-				}
+				jointPrepare(B, J, (int)joints[j]);
 			}
 			__syncwarp();
 		}
@@ -267,7 +386,7 @@ __global__ void __launch_bounds__(32 * kSerialWarpsPerBlock)
 			for (int c = lane; c < r.contactCount; c += 32)
 			{
 				const int what = prepareContact(B, C, (int)contacts[c], P.h);
-				if (tape != nullptr)
+				if (kTape && tape != nullptr)
 				{
 					int gen = what;
 					if (sub == 0 && narrowGen[contacts[c]] == kPrepRegenerated)
@@ -278,7 +397,19 @@ __global__ void __launch_bounds__(32 * kSerialWarpsPerBlock)
 				}
 			}
 			__syncwarp();
-			if (r.jointCount > 0)
+			if (jointsLevelled)
+			{
+				for (int j = lane; j < r.jointCount; j += 32)
+				{
+					jointReset(J, (int)joints[j]);
+				}
+				__syncwarp();
+				for (int it = 0; it < P.iterations; ++it)
+				{
+					sweepJointedIsland(true, B, C, J, r, joints, T, levelsPos, lane, P);
+				}
+			}
+			else if (r.jointCount > 0)
 			{
 				// joints interleave with the contact sweeps: serial on lane 0
 				if (lane == 0)
@@ -314,21 +445,29 @@ __global__ void __launch_bounds__(32 * kSerialWarpsPerBlock)
 				reconstructBody(B, (int)bodies[b], P.invH);
 			}
 			__syncwarp();
-			sweepIsland(kSweepVelocity, B, C, r, contacts, T, levels, lane, P);
-			if (lane == 0)
+			if (jointsLevelled)
 			{
-				for (int j = 0; j < r.jointCount; ++j)
-				{
-					jointVelocity(B, J, (int)joints[j], P.h);
-				}
+				sweepJointedIsland(false, B, C, J, r, joints, T, levelsVel, lane, P);
 			}
-			__syncwarp();
+			else
+			{
+				sweepIsland(kSweepVelocity, B, C, r, contacts, T, levels, lane, P);
+				if (lane == 0)
+				{
+					for (int j = 0; j < r.jointCount; ++j)
+					{
+						jointVelocity(B, J, (int)joints[j], P.h);
+					}
+				}
+				__syncwarp();
+			}
 		}
 	}
 }
 
 // Small serial islands without joints, one thread each: the whole substep
 // loop in the reference's order (src/xpbd.cpp:898-974), 32 islands per warp.
+template <bool kTape>
 __global__ void __launch_bounds__(128)
 	kSolveTiny(BodySoA B, ContactSoA C, const IslandRec* islands, const int32_t* tinyList, const uint32_t* tinyDev,
 			   const uint32_t* bodyVals, const uint32_t* contactVals, SolveParams P, m3d_diff::TapeContact* tape,
@@ -351,7 +490,7 @@ __global__ void __launch_bounds__(128)
 		for (int c = 0; c < r.contactCount; ++c)
 		{
 			const int what = prepareContact(B, C, (int)contacts[c], P.h);
-			if (tape != nullptr)
+			if (kTape && tape != nullptr)
 			{
 				int gen = what;
 				if (sub == 0 && narrowGen[contacts[c]] == kPrepRegenerated)
@@ -648,14 +787,33 @@ void launchSolve(DevWorld& w, float dt, int substeps, V3 gravity, int positionIt
 	w.colorMask.ensure((size_t)(w.bodyCap + 1) * sizeof(uint32_t)); // also the serial islands' local body index
 	if (w.lastSerialIslands > kTinyModeIslands) // the island table listed tiny islands this step
 	{
-		M3G_LAUNCH(kSolveTiny, blocksFor(ni, 128), 128, s, w.B, w.C, isl, w.tinyList.as<int32_t>(), &dc->tinyIslands,
-				   w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(), P, w.tapeContacts, &dc->islandContacts,
-				   w.tapeGen.as<uint8_t>());
+		if (w.tapeContacts != nullptr)
+		{
+			M3G_LAUNCH_AS("kSolveTiny", kSolveTiny<true>, blocksFor(ni, 128), 128, s, w.B, w.C, isl,
+						  w.tinyList.as<int32_t>(), &dc->tinyIslands, w.bodyVals.as<uint32_t>(),
+						  w.contactVals.as<uint32_t>(), P, w.tapeContacts, &dc->islandContacts, w.tapeGen.as<uint8_t>());
+		}
+		else
+		{
+			M3G_LAUNCH_AS("kSolveTiny", kSolveTiny<false>, blocksFor(ni, 128), 128, s, w.B, w.C, isl,
+						  w.tinyList.as<int32_t>(), &dc->tinyIslands, w.bodyVals.as<uint32_t>(),
+						  w.contactVals.as<uint32_t>(), P, w.tapeContacts, &dc->islandContacts, w.tapeGen.as<uint8_t>());
+		}
 	}
-	M3G_LAUNCH(kSolveSerial, serialBlocks, 32 * kSerialWarpsPerBlock, s, w.B, w.C, w.joints.as<JointRec>(), isl,
-			   w.serialList.as<int32_t>(), &dc->warpIslands, w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(),
-			   w.jointVals.as<uint32_t>(), w.colorMask.as<uint32_t>(), P, w.tapeContacts, &dc->islandContacts,
-			   w.tapeGen.as<uint8_t>());
+	if (w.tapeContacts != nullptr)
+	{
+		M3G_LAUNCH_AS("kSolveSerial", kSolveSerial<true>, serialBlocks, 32 * kSerialWarpsPerBlock, s, w.B, w.C,
+					  w.joints.as<JointRec>(), isl, w.serialList.as<int32_t>(), &dc->warpIslands,
+					  w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(), w.jointVals.as<uint32_t>(),
+					  w.colorMask.as<uint32_t>(), P, w.tapeContacts, &dc->islandContacts, w.tapeGen.as<uint8_t>());
+	}
+	else
+	{
+		M3G_LAUNCH_AS("kSolveSerial", kSolveSerial<false>, serialBlocks, 32 * kSerialWarpsPerBlock, s, w.B, w.C,
+					  w.joints.as<JointRec>(), isl, w.serialList.as<int32_t>(), &dc->warpIslands,
+					  w.bodyVals.as<uint32_t>(), w.contactVals.as<uint32_t>(), w.jointVals.as<uint32_t>(),
+					  w.colorMask.as<uint32_t>(), P, w.tapeContacts, &dc->islandContacts, w.tapeGen.as<uint8_t>());
+	}
 	size_t nc = (size_t)w.contactMax + 1;
 	w.colorOrder.ensure(nc * sizeof(int32_t));
 	w.packetMax.ensure(nc * sizeof(int32_t));

@@ -293,6 +293,96 @@ M3G_HD void setSeparationOffsets(Manifold& m, Xf xa, Xf xb)
 constexpr int kPrepRegenerated = 2; // regenerated at the current poses
 constexpr int kPrepHeld = 4;        // stale, but held by the tunnelling guard
 
+// The stale-manifold half of prepareContact: safety re-collision, tunnelling
+// rescue and anchor inheritance (reference src/xpbd.cpp:740-800).  Kept out
+// of line: it runs only for contacts whose bodies moved or turned past the
+// re-collision thresholds since the manifold was made, and inlining its
+// collision code into every solve kernel bloats their hot loops (the serial
+// and tiny-island kernels stall on instruction fetch).  Writes the new
+// manifold and flags; returns kPrepRegenerated or kPrepHeld.
+static __device__ __noinline__ int prepareStaleContact(const BodySoA& B, const ContactSoA& C, int c, float h, Xf xa, Xf xb,
+												uint8_t flags, bool hasCache)
+{
+	int what = 0;
+	int2 ab = C.bodies[c];
+	const BodyCold& ca = B.cold[ab.x];
+	const BodyCold& cb = B.cold[ab.y];
+	Manifold oldM, m;
+	loadManifold(C, c, oldM);
+	m = oldM; // regeneration writes into the existing storage
+	V3 va = ld3(B.vel[ab.x]), vb = ld3(B.vel[ab.y]);
+	float relSpeed = len(sub(va, vb));
+	collideShapes(ca.shape, xa, cb.shape, xb, kSpeculativeBase + h * relSpeed, &m);
+
+	bool keepOld = false;
+	bool guard = (flags & kCFTunnelGuard) != 0;
+	if (hasCache && oldM.pointCount > 0)
+	{
+		if (guard)
+		{
+			keepOld = trackedMinSep(xa, xb, oldM) < -kLinearSlop;
+		}
+		else
+		{
+			bool flipOrGone = m.pointCount == 0 || dot(m.normal, oldM.normal) < -0.5f;
+			if (flipOrGone)
+			{
+				V3 dB = cb.type == kDynamic ? sub(xb.p, ld3(B.prevPos[ab.y])) : vzero();
+				V3 dA = ca.type == kDynamic ? sub(xa.p, ld3(B.prevPos[ab.x])) : vzero();
+				V3 travel = sub(dB, dA);
+				float travelLen = len(travel);
+				float coreB = cb.shape.type == kBox ? fminf(cb.shape.he.x, fminf(cb.shape.he.y, cb.shape.he.z))
+													: cb.shape.radius;
+				float minHalfA = ca.shape.type == kBox ? fminf(ca.shape.he.x, fminf(ca.shape.he.y, ca.shape.he.z))
+													   : ca.shape.radius;
+				float crossSpan = 2.0f * (minHalfA + coreB);
+				if (travelLen > 0.04f && travelLen > 0.8f * crossSpan)
+				{
+					Shape infl = ca.shape;
+					if (infl.type == kBox)
+					{
+						infl.he = add(infl.he, v3(coreB, coreB, coreB));
+					}
+					else
+					{
+						infl.radius += coreB;
+					}
+					float backup = 2.0f * coreB + 0.02f;
+					V3 dir = scale(1.0f / travelLen, travel);
+					V3 origin = sub(sub(xb.p, dB), scale(backup, dir));
+					V3 seg = add(travel, scale(backup, dir));
+					float fhit;
+					V3 nhit;
+					keepOld = rayCastShape(infl, xa, origin, seg, &fhit, &nhit);
+				}
+			}
+		}
+		guard = keepOld;
+	}
+	if (keepOld)
+	{
+		m = oldM; // cache pose intentionally not refreshed
+		what = kPrepHeld;
+	}
+	else
+	{
+		what = kPrepRegenerated;
+		inheritAnchors(oldM, m, ca.shape.type == kBox && cb.shape.type == kBox, xa, xb);
+		hasCache = true;
+		C.cachePosA[c] = st3(xa.p);
+		C.cacheRotA[c] = stq(xa.q);
+		C.cachePosB[c] = st3(xb.p);
+		C.cacheRotB[c] = stq(xb.q);
+		setSeparationOffsets(m, xa, xb);
+	}
+	storeManifold(C, c, m);
+	uint8_t nf = flags;
+	nf = guard ? (uint8_t)(nf | kCFTunnelGuard) : (uint8_t)(nf & ~kCFTunnelGuard);
+	nf = hasCache ? (uint8_t)(nf | kCFHasCache) : nf;
+	C.flags[c] = nf;
+	return what;
+}
+
 M3G_D int prepareContact(const BodySoA& B, const ContactSoA& C, int c, float h)
 {
 	int what = 0;
@@ -322,87 +412,12 @@ M3G_D int prepareContact(const BodySoA& B, const ContactSoA& C, int c, float h)
 		}
 	}
 
-	int pointCount = C.pointCount[c];
-	V3 n = ld3(C.normal[c]);
 	if (stale)
 	{
-		Manifold oldM, m;
-		loadManifold(C, c, oldM);
-		m = oldM; // regeneration writes into the existing storage
-		V3 va = ld3(B.vel[ab.x]), vb = ld3(B.vel[ab.y]);
-		float relSpeed = len(sub(va, vb));
-		collideShapes(ca.shape, xa, cb.shape, xb, kSpeculativeBase + h * relSpeed, &m);
-
-		bool keepOld = false;
-		bool guard = (flags & kCFTunnelGuard) != 0;
-		if (hasCache && oldM.pointCount > 0)
-		{
-			if (guard)
-			{
-				keepOld = trackedMinSep(xa, xb, oldM) < -kLinearSlop;
-			}
-			else
-			{
-				bool flipOrGone = m.pointCount == 0 || dot(m.normal, oldM.normal) < -0.5f;
-				if (flipOrGone)
-				{
-					V3 dB = cb.type == kDynamic ? sub(xb.p, ld3(B.prevPos[ab.y])) : vzero();
-					V3 dA = ca.type == kDynamic ? sub(xa.p, ld3(B.prevPos[ab.x])) : vzero();
-					V3 travel = sub(dB, dA);
-					float travelLen = len(travel);
-					float coreB = cb.shape.type == kBox ? fminf(cb.shape.he.x, fminf(cb.shape.he.y, cb.shape.he.z))
-														: cb.shape.radius;
-					float minHalfA = ca.shape.type == kBox ? fminf(ca.shape.he.x, fminf(ca.shape.he.y, ca.shape.he.z))
-														   : ca.shape.radius;
-					float crossSpan = 2.0f * (minHalfA + coreB);
-					if (travelLen > 0.04f && travelLen > 0.8f * crossSpan)
-					{
-						Shape infl = ca.shape;
-						if (infl.type == kBox)
-						{
-							infl.he = add(infl.he, v3(coreB, coreB, coreB));
-						}
-						else
-						{
-							infl.radius += coreB;
-						}
-						float backup = 2.0f * coreB + 0.02f;
-						V3 dir = scale(1.0f / travelLen, travel);
-						V3 origin = sub(sub(xb.p, dB), scale(backup, dir));
-						V3 seg = add(travel, scale(backup, dir));
-						float fhit;
-						V3 nhit;
-						keepOld = rayCastShape(infl, xa, origin, seg, &fhit, &nhit);
-					}
-				}
-			}
-			guard = keepOld;
-		}
-		if (keepOld)
-		{
-			m = oldM; // cache pose intentionally not refreshed
-			what = kPrepHeld;
-		}
-		else
-		{
-			what = kPrepRegenerated;
-			inheritAnchors(oldM, m, ca.shape.type == kBox && cb.shape.type == kBox, xa, xb);
-			hasCache = true;
-			C.cachePosA[c] = st3(xa.p);
-			C.cacheRotA[c] = stq(xa.q);
-			C.cachePosB[c] = st3(xb.p);
-			C.cacheRotB[c] = stq(xb.q);
-			setSeparationOffsets(m, xa, xb);
-		}
-		storeManifold(C, c, m);
-		uint8_t nf = flags;
-		nf = guard ? (uint8_t)(nf | kCFTunnelGuard) : (uint8_t)(nf & ~kCFTunnelGuard);
-		nf = hasCache ? (uint8_t)(nf | kCFHasCache) : nf;
-		C.flags[c] = nf;
-		pointCount = m.pointCount;
-		n = m.normal;
+		what = prepareStaleContact(B, C, c, h, xa, xb, flags, hasCache);
 	}
-
+	int pointCount = C.pointCount[c];
+	V3 n = ld3(C.normal[c]);
 	float invMassA = B.massInv[ab.x].x, invMassB = B.massInv[ab.y].x;
 	M3 iwA = loadIW(B, ab.x), iwB = loadIW(B, ab.y);
 	for (int s = 0; s < pointCount; ++s)

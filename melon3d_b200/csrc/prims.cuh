@@ -144,6 +144,15 @@ cudaError_t countedMemcpyAsync(void* dst, const void* src, size_t bytes, cudaMem
 
 #define cudaMemcpyAsync(...) ::m3g::countedMemcpyAsync(__VA_ARGS__)
 
+// the same, accounted under an explicit name (template instances of one kernel)
+#define M3G_LAUNCH_AS(name, kern, grid, block, stream, ...)                                                            \
+	do                                                                                                                 \
+	{                                                                                                                  \
+		::m3g::launchBegin(name, (stream));                                                                           \
+		kern<<<(grid), (block), 0, (stream)>>>(__VA_ARGS__);                                                           \
+		::m3g::launchEnd(name, (stream));                                                                             \
+	} while (0)
+
 #define M3G_LAUNCH(kern, grid, block, stream, ...)                                                                     \
 	do                                                                                                                 \
 	{                                                                                                                  \
