@@ -421,8 +421,8 @@ def measure_batch(lib, args, ref_lib):
     for s in scenes:
         s.close()
     lib.m3d_world_step(batch, 1.0 / 60.0, args.substeps)
+    tm = Timed(lib, batch, BATCH_KERNELS, args.substeps)  # resets the launch counter
     launches0 = lib.m3d_gpu_profiler_launches()
-    tm = Timed(lib, batch, BATCH_KERNELS, args.substeps)
     for _ in range(args.batch_steps):
         tm.step(lambda: lib.m3d_world_step(batch, 1.0 / 60.0, args.substeps))
     launches = lib.m3d_gpu_profiler_launches() - launches0
