@@ -129,6 +129,7 @@ def parse():
     p.add_argument("--batch-steps", type=int, default=40)
     p.add_argument("--batch-solo-worlds", type=int, default=128,
                    help="worlds of the batch stepped one at a time through the plain path for the comparison")
+    p.add_argument("--no-autotune", action="store_true", help="batch variant with the default kernel choice")
     p.add_argument("--pile-steps", type=int, default=12)
     p.add_argument("--pile-cpu-steps", type=int, default=20)
     p.add_argument("--adjoint-worlds", type=int, default=1024)
@@ -420,6 +421,25 @@ def measure_batch(lib, args, ref_lib):
             solo_bs += cnt * args.substeps
     for s in scenes:
         s.close()
+    tuning = None
+    if not args.no_autotune:
+        # trials on a twin batch (steps 1-24), then this batch takes the
+        # choice from the cache file at once; results do not depend on it
+        import tempfile
+        os.environ.setdefault("M3D_AUTOTUNE_CACHE", os.path.join(tempfile.gettempdir(), "m3d_autotune.txt"))
+        if lib.m3d_gpu_autotune(batch, 2) == 0:
+            twin_scenes, _, twin = _batch_from(lib, range(W))
+            for s in twin_scenes:
+                s.close()
+            lib.m3d_gpu_autotune(twin, 2)
+            while lib.m3d_gpu_autotune_state(twin, None, None) == 1:
+                lib.m3d_world_step(twin, 1.0 / 60.0, args.substeps)
+            lib.m3d_world_destroy(twin)
+            lib.m3d_gpu_autotune(batch, 2)
+        tc, tmi = C.c_int32(), C.c_int32()
+        lib.m3d_gpu_autotune_state(batch, C.byref(tc), C.byref(tmi))
+        tuning = {"tiny_island_contacts": tc.value, "tiny_mode_islands": tmi.value,
+                  "cache": os.environ["M3D_AUTOTUNE_CACHE"]}
     lib.m3d_world_step(batch, 1.0 / 60.0, args.substeps)
     tm = Timed(lib, batch, BATCH_KERNELS, args.substeps)  # resets the launch counter
     launches0 = lib.m3d_gpu_profiler_launches()
@@ -437,7 +457,7 @@ def measure_batch(lib, args, ref_lib):
            "timed_window": "steps 1-%d" % tm.steps, "value": value, "unit": "body-substeps/s",
            "ms_per_step": tm.dev / tm.steps, "e2e": {"value": e2e, "ms_per_step": tm.wall / tm.steps},
            "one_at_a_time": solo, "speedup_vs_one_at_a_time": {"device": value / solo["value"], "e2e": e2e / solo["e2e"]},
-           "gpu_launches_per_step": launches / tm.steps, "roofline": roofs[0] if roofs else None,
+           "gpu_launches_per_step": launches / tm.steps, "autotuned": tuning, "roofline": roofs[0] if roofs else None,
            "roofline_others": roofs[1:], "status": lib.m3d_gpu_status(batch)}
     lib.m3d_world_destroy(batch)
     if ref_lib is not None and not args.no_cpu_baseline:

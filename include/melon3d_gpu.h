@@ -93,6 +93,21 @@ M3D_API int32_t m3d_gpu_batch_world_count(m3d_world* batch);
 /* first body slot of world k; k == count gives the total slot count */
 M3D_API int32_t m3d_gpu_batch_first_body(m3d_world* batch, int32_t k);
 
+/* Online autotuning (no counterpart in the reference).  The kernel that
+ * solves a serial island - one warp per island, or one thread per island for
+ * islands of a few contacts without joints - is chosen by two thresholds;
+ * every choice gives the same results bit for bit, so m3d_gpu_autotune tries
+ * the candidates on the world's own next steps (each for stepsPerTrial steps,
+ * two interleaved rounds), keeps the one with the lowest median device time,
+ * and appends it to the file named by M3D_AUTOTUNE_CACHE (one line per GPU
+ * model, body-count and world-count magnitude), where a later call with the
+ * same key finds it and applies it at once (returns 1; else 0).
+ * stepsPerTrial <= 0 restores the defaults.  m3d_gpu_autotune_state returns
+ * 0 (not tuning), 1 (trials running) or 2 (a choice applied) and the current
+ * thresholds. */
+M3D_API int32_t m3d_gpu_autotune(m3d_world* world, int32_t stepsPerTrial);
+M3D_API int32_t m3d_gpu_autotune_state(m3d_world* world, int32_t* tinyContacts, int32_t* tinyModeIslands);
+
 /* Steps this world took through the sleeping-world fast path: when the
  * previous step changed nothing, every body was asleep before and after it
  * and no API call has edited the world since, m3d_world_step does on the

@@ -200,6 +200,8 @@ _GPU_PROTOS = {
     "m3d_gpu_set_giant_island_contacts": (None, [W, C.c_int32]),
     "m3d_gpu_set_wait_limit": (None, [W, C.c_int64]),
     "m3d_gpu_fast_path_steps": (C.c_int64, [W]),
+    "m3d_gpu_autotune": (C.c_int32, [W, C.c_int32]),
+    "m3d_gpu_autotune_state": (C.c_int32, [W, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "m3d_gpu_clear_status": (None, [W]),
     "m3d_gpu_giant_profile": (C.c_int32, [W, C.POINTER(C.c_double), C.c_int32]),
     "m3d_gpu_batch_create": (W, [C.POINTER(W), C.c_int32]),

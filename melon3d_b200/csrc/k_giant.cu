@@ -64,7 +64,8 @@ struct GiantArgs
 	                      // position, its overflow index and, per overflow index, its level
 	int32_t* ovOrder;     // overflow contacts grouped by level
 	uint32_t* levelStart; // per level + 2: offsets into ovOrder
-	uint32_t* done;       // per island contact position: == epoch once coloured
+	unsigned long long* done; // per island contact position: epoch << 32 | its bodies' colour masks after it
+	                          // (end A << 8 | end B) once coloured
 	int32_t* order;       // per island contact position: contact of the bucket order
 	int32_t* pmax;        // per position: colour during colouring, then the packet's point count
 	int32_t* contactColor;
@@ -228,11 +229,11 @@ __device__ __forceinline__ void giantContactOp(GiantOp op, const GiantArgs& a, i
 	}
 	else if (op == kGiantFriction)
 	{
-		applyContactFriction(a.B, a.C, c);
+		applyContactFrictionPrefetched(a.B, a.C, c);
 	}
 	else
 	{
-		solveContactVelocity(a.B, a.C, c, a.P.h, a.P.gravityLen);
+		solveContactVelocityPrefetched(a.B, a.C, c, a.P.h, a.P.gravityLen);
 	}
 }
 
@@ -310,7 +311,7 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 		int32_t* order = a.order + r.contactStart;
 		int32_t* pmax = a.pmax + r.contactStart;
 		int32_t* pred = a.pred + 2 * (int64_t)r.contactStart;
-		uint32_t* done = a.done + r.contactStart;
+		unsigned long long* done = a.done + r.contactStart;
 		uint32_t* incidence = a.incidence + 2 * (int64_t)r.contactStart;
 		const int nb = r.bodyCount, nc = r.contactCount;
 		int32_t* ovIdx = pred;       // per position, once the colouring is done
@@ -411,12 +412,38 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 		stamp(a, 1);
 
 		// ---- greedy first-fit colouring as a dataflow (src/xpbd.cpp:1179-1235)
+		// A contact's done word carries its bodies' colour masks after it, so
+		// the next contact on a body reads the mask with the flag it waits
+		// on (one memory round trip per link of the chain).
 		for (int p = gtid; p < nc; p += gthreads)
 		{
 			const int32_t pa = pred[2 * p], pb = pred[2 * p + 1];
-			for (uint32_t it = 0; (pa >= 0 && ldAcquire(&done[pa]) != a.epoch) || (pb >= 0 && ldAcquire(&done[pb]) != a.epoch);
-				 ++it)
+			const int c = (int)contacts[p];
+			const int2 ab = C.bodies[c];
+			const bool dynA = B.massInv[ab.x].x > 0.0f;
+			const bool dynB = B.massInv[ab.y].x > 0.0f;
+			// which end of each predecessor is the shared body (static data,
+			// read before waiting): 8 = its end A, 0 = its end B
+			const int shA = pa >= 0 && C.bodies[contacts[pa]].x == ab.x ? 8 : 0;
+			const int shB = pb >= 0 && C.bodies[contacts[pb]].x == ab.y ? 8 : 0;
+			unsigned long long wa = 0ull, wb = 0ull;
+			for (uint32_t it = 0;; ++it)
 			{
+				bool ready = true;
+				if (pa >= 0)
+				{
+					wa = *(const volatile unsigned long long*)&done[pa];
+					ready = ready && (uint32_t)(wa >> 32) == a.epoch;
+				}
+				if (pb >= 0)
+				{
+					wb = *(const volatile unsigned long long*)&done[pb];
+					ready = ready && (uint32_t)(wb >> 32) == a.epoch;
+				}
+				if (ready)
+				{
+					break;
+				}
 				if (it >= a.spinLimit)
 				{
 					giveUp(a);
@@ -424,15 +451,11 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 				}
 				__nanosleep(20);
 			}
-			__threadfence();
-			const int c = (int)contacts[p];
-			const int2 ab = C.bodies[c];
-			const bool dynA = B.massInv[ab.x].x > 0.0f;
-			const bool dynB = B.massInv[ab.y].x > 0.0f;
-			const uint32_t ma = dynA ? __ldcg(&a.colorMask[ab.x]) : 0u;
-			const uint32_t mb = dynB ? __ldcg(&a.colorMask[ab.y]) : 0u;
+			const uint32_t ma = dynA && pa >= 0 ? (uint32_t)(wa >> shA) & 0xFFu : 0u;
+			const uint32_t mb = dynB && pb >= 0 ? (uint32_t)(wb >> shB) & 0xFFu : 0u;
 			const uint32_t freeBits = ~(ma | mb);
 			int color = freeBits != 0 ? __ffs((int)freeBits) - 1 : kMaxGraphColors;
+			uint32_t na = ma, nb = mb;
 			if (color >= kMaxGraphColors)
 			{
 				color = kMaxGraphColors;
@@ -440,19 +463,13 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 			else
 			{
 				const uint32_t bit = 1u << color;
-				if (dynA)
-				{
-					__stcg(&a.colorMask[ab.x], ma | bit);
-				}
-				if (dynB)
-				{
-					__stcg(&a.colorMask[ab.y], mb | bit);
-				}
+				na = dynA ? ma | bit : 0u;
+				nb = dynB ? mb | bit : 0u;
 			}
 			a.contactColor[c] = color;
 			pmax[p] = color;
-			__threadfence();
-			*(volatile uint32_t*)&done[p] = a.epoch;
+			*(volatile unsigned long long*)&done[p] =
+				((unsigned long long)a.epoch << 32) | (unsigned long long)((na << 8) | nb);
 		}
 		if (gridSync(a, &gen, &stop))
 		{
@@ -859,7 +876,7 @@ void launchSolveGiant(DevWorld& w, const SolveParams& P)
 	w.giantIncidence.ensure(2 * nc * sizeof(uint32_t));
 	w.giantPred.ensure(2 * nc * sizeof(int32_t));
 	void* doneBefore = w.giantDone.ptr;
-	w.giantDone.ensureZeroed(nc * sizeof(uint32_t), w.stream);
+	w.giantDone.ensureZeroed(nc * sizeof(unsigned long long), w.stream);
 	w.giantChunkHist.ensure((kMaxGraphColors + 1) * chunks * sizeof(uint32_t));
 	w.giantMisc.ensure(16 * sizeof(uint32_t) + 16 * sizeof(unsigned long long));
 	w.giantOvOrder.ensure(nc * sizeof(int32_t));
@@ -900,7 +917,7 @@ void launchSolveGiant(DevWorld& w, const SolveParams& P)
 	a.pred = w.giantPred.as<int32_t>();
 	a.ovOrder = w.giantOvOrder.as<int32_t>();
 	a.levelStart = w.giantLevelStart.as<uint32_t>();
-	a.done = w.giantDone.as<uint32_t>();
+	a.done = (unsigned long long*)w.giantDone.ptr;
 	a.order = w.colorOrder.as<int32_t>();
 	a.pmax = w.packetMax.as<int32_t>();
 	a.contactColor = w.contactColor.as<int32_t>();

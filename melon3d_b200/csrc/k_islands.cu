@@ -495,7 +495,7 @@ void launchIslands(DevWorld& w, int32_t n)
 			   &dc->islandContacts, w.jointKeys.as<uint64_t>(), J > 0 ? &dc->islandJoints : nullptr,
 			   w.islands.as<IslandRec>(), w.coloredList.as<int32_t>(), w.serialList.as<int32_t>(),
 			   w.tinyList.as<int32_t>(), w.giantList.as<int32_t>(), w.giantIslandContacts,
-			   w.lastSerialIslands > kTinyModeIslands ? kTinyIslandContacts : 0, dc);
+			   w.lastSerialIslands > w.tinyModeIslands ? w.tinyContacts : 0, dc);
 	w.islandMax = n;
 }
 

@@ -785,7 +785,7 @@ void launchSolve(DevWorld& w, float dt, int substeps, V3 gravity, int positionIt
 	int serialBlocks = (ni + kSerialWarpsPerBlock - 1) / kSerialWarpsPerBlock;
 	serialBlocks = serialBlocks < 148 * 8 ? serialBlocks : 148 * 8;
 	w.colorMask.ensure((size_t)(w.bodyCap + 1) * sizeof(uint32_t)); // also the serial islands' local body index
-	if (w.lastSerialIslands > kTinyModeIslands) // the island table listed tiny islands this step
+	if (w.lastSerialIslands > w.tinyModeIslands) // the island table listed tiny islands this step
 	{
 		if (w.tapeContacts != nullptr)
 		{

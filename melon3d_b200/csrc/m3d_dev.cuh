@@ -170,6 +170,11 @@ struct DevWorld
 	DevBuf islandListFlag, islandListOffs, islandLabels, coloredList, serialList, tinyList, giantList, jointScan;
 	int32_t islandMax = 0; // upper bound of the awake islands of the step
 	uint32_t lastSerialIslands = 0; // serial islands of the previous step (kernel choice)
+	// serial islands of at most tinyContacts contacts (no joints) take one
+	// thread each when the previous step had more than tinyModeIslands serial
+	// islands (m3d_gpu_autotune may change both; results do not depend on them)
+	int32_t tinyContacts = kTinyIslandContacts;
+	uint32_t tinyModeIslands = kTinyModeIslands;
 	int32_t islandCount = 0;
 	int32_t islandsBuiltFor = 0; // body count of the last island build (0: never)
 	DevBuf colorOf;      // per island-contact position: colour 0..8

@@ -741,6 +741,121 @@ M3G_D void applyContactFriction(const BodySoA& B, const ContactSoA& C, int c)
 	storePose(B, ab.y, b);
 }
 
+// applyContactFriction with every point's records loaded up front (see
+// solveContactVelocityPrefetched): same arithmetic, for the overflow levels of
+// giant islands.
+M3G_D void applyContactFrictionPrefetched(const BodySoA& B, const ContactSoA& C, int c)
+{
+	int2 ab = C.bodies[c];
+	const BodyCold& ca = B.cold[ab.x];
+	const BodyCold& cb = B.cold[ab.y];
+	if (ca.shape.type != kBox || cb.shape.type != kBox)
+	{
+		return;
+	}
+	int pc = C.pointCount[c];
+	if (pc == 0)
+	{
+		return;
+	}
+	float4 nf = C.normal[c];
+	V3 n = ld3(nf);
+	float friction = nf.w;
+	// every point's friction and local anchors, loaded before the first
+	// update (each point writes only its own records)
+	float4 faP[4], fbP[4], laP[4], lbP[4];
+#pragma unroll
+	for (int s = 0; s < 4; ++s)
+	{
+		if (s < pc)
+		{
+			size_t k = pidx(C, c, s);
+			faP[s] = C.pFricA[k];
+			fbP[s] = C.pFricB[k];
+			laP[s] = C.pAnchorA[k];
+			lbP[s] = C.pAnchorB[k];
+		}
+	}
+	{
+		const float kStictionMaxSpeedSq = 0.1f * 0.1f;
+		size_t k0 = pidx(C, c, 0);
+		V3 rA0 = ld3(C.pRA[k0]), rB0 = ld3(C.pRB[k0]);
+		V3 va = ld3(B.vel[ab.x]), wa = ld3(B.angVel[ab.x]);
+		V3 vb = ld3(B.vel[ab.y]), wb = ld3(B.angVel[ab.y]);
+		V3 vrel = sub(add(vb, cross(wb, rB0)), add(va, cross(wa, rA0)));
+		V3 vt = sub(vrel, scale(dot(vrel, n), n));
+		if (len2(vt) > kStictionMaxSpeedSq)
+		{
+#pragma unroll
+			for (int s = 0; s < 4; ++s)
+			{
+				if (s >= pc)
+				{
+					break;
+				}
+				size_t k = pidx(C, c, s);
+				float4 fa = faP[s], fb = fbP[s];
+				float4 la = laP[s], lb = lbP[s];
+				C.pFricA[k] = make_float4(la.x, la.y, la.z, fa.w);
+				C.pFricB[k] = make_float4(lb.x, lb.y, lb.z, fb.w);
+			}
+			return;
+		}
+	}
+	BodyDyn a = loadDyn(B, ab.x), b = loadDyn(B, ab.y);
+#pragma unroll
+	for (int s = 0; s < 4; ++s)
+	{
+		if (s >= pc)
+		{
+			break;
+		}
+		size_t k = pidx(C, c, s);
+		float4 fa = faP[s], fb = fbP[s];
+		float lambdaN = fa.w;
+		if (lambdaN <= 0.0f)
+		{
+			continue;
+		}
+		V3 rA = rotate(a.q, ld3(fa));
+		V3 rB = rotate(b.q, ld3(fb));
+		V3 gap = sub(add(b.p, rB), add(a.p, rA));
+		V3 dpt = sub(gap, scale(dot(gap, n), n));
+		float lt = len(dpt);
+		if (lt <= 1e-9f)
+		{
+			continue;
+		}
+		V3 t = scale(1.0f / lt, dpt);
+		float wt = generalizedInvMass(a, rA, t) + generalizedInvMass(b, rB, t);
+		if (wt <= 0.0f)
+		{
+			continue;
+		}
+		float needed = kFrictionRelaxation * (lt / wt);
+		float allowed = friction * lambdaN - fb.w;
+		if (allowed <= 0.0f)
+		{
+			continue;
+		}
+		float dL = needed < allowed ? needed : allowed;
+		fb.w += dL;
+		V3 pt = scale(dL, t);
+		applyPositionCorrection(b, neg(pt), rB);
+		applyPositionCorrection(a, pt, rA);
+		if (needed > 2.0f * allowed)
+		{
+			float4 la = laP[s], lb = lbP[s];
+			fa = make_float4(la.x, la.y, la.z, fa.w);
+			fb = make_float4(lb.x, lb.y, lb.z, fb.w);
+			C.pFricA[k] = fa;
+		}
+		C.pFricB[k] = fb;
+	}
+	storePose(B, ab.x, a);
+	storePose(B, ab.y, b);
+}
+
 // Velocity pass: Coulomb-capped dynamic friction with the coherence test,
 // restitution against the pre-substep normal velocity, the unconditional
 // normal-velocity fix and rolling resistance (reference src/xpbd.cpp:275-407)
@@ -843,6 +958,173 @@ M3G_D void solveContactVelocity(const BodySoA& B, const ContactSoA& C, int c, fl
 				float mj = -j;
 				va = madd(va, mj * imA, n);
 				wa = madd(wa, mj, ld3(C.pJA[k]));
+			}
+		}
+		lambdaNTotal += lambdaN > 0.0f ? lambdaN : 0.0f;
+	}
+
+	float rolling = mat.y;
+	if (rolling > 0.0f && lambdaNTotal > 0.0f)
+	{
+		V3 wrel = sub(wb, wa);
+		V3 wroll = sub(wrel, scale(dot(wrel, n), n));
+		float wl = len(wroll);
+		if (wl > 1e-6f)
+		{
+			V3 axis = scale(1.0f / wl, wroll);
+			float kk = dot(axis, mulv(iwA, axis)) + dot(axis, mulv(iwB, axis));
+			if (kk > 1e-12f)
+			{
+				float maxDw = rolling * lambdaNTotal * invH * kk;
+				float dw = maxDw < wl ? maxDw : wl;
+				V3 angImp = scale(dw / kk, axis);
+				wb = sub(wb, mulv(iwB, angImp));
+				wa = add(wa, mulv(iwA, angImp));
+			}
+		}
+	}
+	// the reference writes rolling resistance into static bodies too, but their
+	// inverse inertia is zero, so the write is a no-op; skip it
+	if (imA != 0.0f || ca.type == kDynamic)
+	{
+		B.vel[ab.x] = st3(va);
+		B.angVel[ab.x] = st3(wa);
+	}
+	if (imB != 0.0f || cb.type == kDynamic)
+	{
+		B.vel[ab.y] = st3(vb);
+		B.angVel[ab.y] = st3(wb);
+	}
+}
+
+// solveContactVelocity with the data of every point loaded before the first
+// update: a contact costs a few memory round trips instead of two per point.
+// Same arithmetic, point by point; ~90 more registers, so only the overflow
+// levels of giant islands (one level of contacts at a time on one CTA) use it.
+M3G_D void solveContactVelocityPrefetched(const BodySoA& B, const ContactSoA& C, int c, float h, float gravityLen)
+{
+	int2 ab = C.bodies[c];
+	int pc = C.pointCount[c];
+	const BodyCold& ca = B.cold[ab.x];
+	const BodyCold& cb = B.cold[ab.y];
+	float4 nf = C.normal[c];
+	V3 n = ld3(nf);
+	float friction = nf.w;
+	float2 mat = C.mat[c];
+	bool curved = (C.flags[c] & kCFCurved) != 0;
+	float invH = h > 0.0f ? 1.0f / h : 0.0f;
+	float lambdaNTotal = 0.0f;
+
+	float imA = B.massInv[ab.x].x, imB = B.massInv[ab.y].x;
+	M3 iwA = loadIW(B, ab.x), iwB = loadIW(B, ab.y);
+	Q4 qa = ldq(B.rot[ab.x]), qb = ldq(B.rot[ab.y]);
+	V3 va = ld3(B.vel[ab.x]), wa = ld3(B.angVel[ab.x]);
+	V3 vb = ld3(B.vel[ab.y]), wb = ld3(B.angVel[ab.y]);
+	V3 pva = ld3(B.prevVel[ab.x]), pwa = ld3(B.prevAngVel[ab.x]);
+	V3 pvb = ld3(B.prevVel[ab.y]), pwb = ld3(B.prevAngVel[ab.y]);
+	BodyDyn ga, gb; // for generalised masses
+	ga.invMass = imA;
+	ga.iw = iwA;
+	gb.invMass = imB;
+	gb.iw = iwB;
+
+	// every point's data is loaded before the first update: none of it
+	// depends on the updates (each point writes only its own slip direction)
+	float lamP[4];
+	float4 raP[4], slP[4];
+	V3 rbP[4], aaP[4], jaP[4], jbP[4];
+#pragma unroll
+	for (int s = 0; s < 4; ++s)
+	{
+		if (s < pc)
+		{
+			size_t k = pidx(C, c, s);
+			lamP[s] = C.pFricA[k].w;
+			raP[s] = C.pRA[k];
+			rbP[s] = curved ? ld3(C.pAnchorB[k]) : ld3(C.pRB[k]);
+			aaP[s] = curved ? ld3(C.pAnchorA[k]) : vzero();
+			slP[s] = C.pSlip[k];
+			jaP[s] = ld3(C.pJA[k]);
+			jbP[s] = ld3(C.pJB[k]);
+		}
+	}
+#pragma unroll
+	for (int s = 0; s < 4; ++s)
+	{
+		if (s >= pc)
+		{
+			break;
+		}
+		size_t k = pidx(C, c, s);
+		float lambdaN = lamP[s];
+		if (lambdaN <= 0.0f)
+		{
+			continue;
+		}
+		float4 ra4 = raP[s];
+		V3 rAf, rBf;
+		if (curved)
+		{
+			rAf = contactArm(ca.shape, qa, aaP[s], n, 1.0f);
+			rBf = contactArm(cb.shape, qb, rbP[s], n, -1.0f);
+		}
+		else
+		{
+			rAf = ld3(ra4);
+			rBf = rbP[s];
+		}
+		V3 vrel = sub(add(vb, cross(wb, rBf)), add(va, cross(wa, rAf)));
+		float vn = dot(vrel, n);
+		V3 vt = sub(vrel, scale(vn, n));
+		float vtLen = len(vt);
+		if (vtLen > 1e-9f)
+		{
+			V3 t = scale(1.0f / vtLen, vt);
+			float wt = generalizedInvMass(ga, rAf, t) + generalizedInvMass(gb, rBf, t);
+			if (wt > 0.0f)
+			{
+				const float kStaticSlipSpeed = 0.08f;
+				float4 sl = slP[s];
+				bool coherent = dot(t, ld3(sl)) > 0.7f;
+				float pStop = vtLen / wt;
+				float pMax = friction * lambdaN * invH;
+				float P = !coherent && vtLen < kStaticSlipSpeed ? pStop : (pStop < pMax ? pStop : pMax);
+				C.pSlip[k] = st3(t, sl.w);
+				V3 p = scale(-P, t);
+				if (imB != 0.0f)
+				{
+					vb = madd(vb, imB, p);
+					wb = add(wb, mulv(iwB, cross(rBf, p)));
+				}
+				if (imA != 0.0f)
+				{
+					V3 pn = neg(p);
+					va = madd(va, imA, pn);
+					wa = add(wa, mulv(iwA, cross(rAf, pn)));
+				}
+			}
+		}
+		V3 vrelPrev = sub(add(pvb, cross(pwb, rBf)), add(pva, cross(pwa, rAf)));
+		float vnPrev = dot(vrelPrev, n);
+		float e = fabsf(vnPrev) > 2.0f * gravityLen * h ? mat.x : 0.0f;
+		vrel = sub(add(vb, cross(wb, rBf)), add(va, cross(wa, rAf)));
+		vn = dot(vrel, n);
+		float target = -e * vnPrev;
+		target = target > 0.0f ? target : 0.0f;
+		float wN = ra4.w;
+		if (wN > 0.0f)
+		{
+			float j = (target - vn) / wN;
+			if (imB != 0.0f)
+			{
+				vb = madd(vb, j * imB, n);
+				wb = madd(wb, j, jbP[s]);
+			}
+			if (imA != 0.0f)
+			{
+				float mj = -j;
+				va = madd(va, mj * imA, n);
+				wa = madd(wa, mj, jaP[s]);
 			}
 		}
 		lambdaNTotal += lambdaN > 0.0f ? lambdaN : 0.0f;

@@ -23,6 +23,7 @@
 #include <string.h>
 #include <algorithm>
 #include <mutex>
+#include <string>
 #include <vector>
 
 using namespace m3g;
@@ -116,6 +117,16 @@ struct m3d_world
 	bool quiescent = false;
 	int64_t quiescentSteps = 0; // steps taken by the sleeping-world fast path
 	bool lastRebuiltStable = false; // the last step rebuilt the stable tier
+	// online autotuning of the serial-island kernel choice (m3d_gpu_autotune)
+	struct Tune
+	{
+		std::vector<int2> candidates; // (tinyContacts, tinyModeIslands)
+		std::vector<std::vector<float>> samples;
+		int32_t stepsPerTrial = 0, rounds = 0, step = 0;
+		bool active = false, done = false;
+		int32_t chosen = -1;
+		std::string key;
+	} tune;
 
 	// differentiation tape (m3d_gpu_tape_begin); null when not recording
 	DiffTape* tape = nullptr;
@@ -628,6 +639,117 @@ void fetchEvents(m3d_world* w, std::vector<int4>& tmp, const int4* dev, int32_t 
 }
 
 } // namespace
+
+
+// ---- online autotuning (m3d_gpu_autotune) -------------------------------------
+// Candidates differ only in which kernel solves a serial island (one warp, or
+// one thread for islands of a few contacts); every candidate gives the same
+// results bit for bit, so trials run on the world's real steps.
+
+static std::string tuneKey(m3d_world* w)
+{
+	int dev = 0;
+	cudaGetDevice(&dev);
+	cudaDeviceProp prop;
+	std::string name = cudaGetDeviceProperties(&prop, dev) == cudaSuccess ? prop.name : "unknown";
+	for (char& c : name)
+	{
+		c = c == ' ' ? '_' : c;
+	}
+	int lb = 0, lw = 0;
+	for (size_t n = w->bodies.size(); n > 1; n >>= 1)
+	{
+		++lb;
+	}
+	for (size_t n = w->batchFirstBody.size(); n > 1; n >>= 1)
+	{
+		++lw;
+	}
+	char buf[160];
+	snprintf(buf, sizeof(buf), "%s|bodies2^%d|worlds2^%d", name.c_str(), lb, lw);
+	return buf;
+}
+
+static bool tuneCacheLookup(const std::string& key, int2* out)
+{
+	const char* path = getenv("M3D_AUTOTUNE_CACHE");
+	FILE* f = path != nullptr ? fopen(path, "r") : nullptr;
+	if (f == nullptr)
+	{
+		return false;
+	}
+	char k[200];
+	int a = 0, b = 0;
+	bool found = false;
+	while (fscanf(f, "%199s %d %d", k, &a, &b) == 3)
+	{
+		if (key == k)
+		{
+			*out = make_int2(a, b); // the last entry for a key wins
+			found = true;
+		}
+	}
+	fclose(f);
+	return found;
+}
+
+static void tuneCacheStore(const std::string& key, int2 v)
+{
+	const char* path = getenv("M3D_AUTOTUNE_CACHE");
+	FILE* f = path != nullptr ? fopen(path, "a") : nullptr;
+	if (f != nullptr)
+	{
+		fprintf(f, "%s %d %d\n", key.c_str(), v.x, v.y);
+		fclose(f);
+	}
+}
+
+static void tuneApply(m3d_world* w, int2 v)
+{
+	w->dev.tinyContacts = v.x;
+	w->dev.tinyModeIslands = (uint32_t)v.y;
+}
+
+static void tuneBeforeStep(m3d_world* w)
+{
+	auto& t = w->tune;
+	if (t.active)
+	{
+		tuneApply(w, t.candidates[(size_t)(t.step / t.stepsPerTrial) % t.candidates.size()]);
+	}
+}
+
+static void tuneAfterStep(m3d_world* w)
+{
+	auto& t = w->tune;
+	if (!t.active)
+	{
+		return;
+	}
+	const size_t idx = (size_t)(t.step / t.stepsPerTrial) % t.candidates.size();
+	t.samples[idx].push_back(w->lastDeviceMs);
+	++t.step;
+	if (t.step < t.stepsPerTrial * (int32_t)t.candidates.size() * t.rounds)
+	{
+		return;
+	}
+	float best = 0.0f;
+	for (size_t k = 0; k < t.candidates.size(); ++k)
+	{
+		std::vector<float> v = t.samples[k];
+		std::sort(v.begin(), v.end());
+		const float med = v[v.size() / 2];
+		if (t.chosen < 0 || med < best)
+		{
+			best = med;
+			t.chosen = (int32_t)k;
+		}
+	}
+	tuneApply(w, t.candidates[(size_t)t.chosen]);
+	t.active = false;
+	t.done = true;
+	tuneCacheStore(t.key, t.candidates[(size_t)t.chosen]);
+}
 
 // ---- fixed scratch of m3d_gpu_sphere_cast_noalloc --------------------------------
 // One block of device memory in the library image, sized for worlds of up to
@@ -1657,6 +1779,7 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 		++world->quiescentSteps;
 		return;
 	}
+	tuneBeforeStep(world);
 	cudaEventRecord(world->evStart, d.stream);
 	const int32_t n = (int32_t)world->bodies.size();
 	const bool editsAtStart = !world->dirtyList.empty() || world->anyForcesApplied || world->anyMaterialChange ||
@@ -1806,6 +1929,7 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 		world->anyForcesApplied = false;
 	}
 	cudaEventElapsedTime(&world->lastDeviceMs, world->evStart, world->evStop);
+	tuneAfterStep(world);
 	world->mirrorStale = true;
 	world->awakeStale = true;
 	world->contactMirrorValid = false;
@@ -2037,6 +2161,50 @@ void m3d_gpu_clear_status(m3d_world* world)
 {
 	world->status = M3D_GPU_OK;
 	world->errorText[0] = 0;
+}
+
+int32_t m3d_gpu_autotune(m3d_world* world, int32_t stepsPerTrial)
+{
+	auto& t = world->tune;
+	t = m3d_world::Tune();
+	if (stepsPerTrial <= 0)
+	{
+		tuneApply(world, make_int2(kTinyIslandContacts, (int)kTinyModeIslands));
+		return 0;
+	}
+	t.key = tuneKey(world);
+	int2 cached;
+	if (tuneCacheLookup(t.key, &cached))
+	{
+		tuneApply(world, cached);
+		t.candidates.push_back(cached);
+		t.chosen = 0;
+		t.done = true;
+		return 1;
+	}
+	// the default (tiny islands one thread each once a step has more than
+	// 16384 serial islands), every serial island on a warp, and one thread for
+	// islands of up to 2, 4, 8 or 16 contacts at any island count
+	t.candidates = { make_int2(kTinyIslandContacts, (int)kTinyModeIslands), make_int2(0, 0), make_int2(2, 0),
+					 make_int2(4, 0), make_int2(8, 0), make_int2(16, 0) };
+	t.samples.assign(t.candidates.size(), std::vector<float>());
+	t.stepsPerTrial = stepsPerTrial;
+	t.rounds = 2;
+	t.active = true;
+	return 0;
+}
+
+int32_t m3d_gpu_autotune_state(m3d_world* world, int32_t* tinyContacts, int32_t* tinyModeIslands)
+{
+	if (tinyContacts != nullptr)
+	{
+		*tinyContacts = world->dev.tinyContacts;
+	}
+	if (tinyModeIslands != nullptr)
+	{
+		*tinyModeIslands = (int32_t)world->dev.tinyModeIslands;
+	}
+	return world->tune.active ? 1 : (world->tune.done ? 2 : 0);
 }
 
 int64_t m3d_gpu_fast_path_steps(m3d_world* world) { return world->quiescentSteps; }
