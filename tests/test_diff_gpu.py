@@ -378,9 +378,11 @@ def test_adjoint_matches_engine_central_differences(name):
     h = 1e-3 per initial linear velocity component: on these motions no
     contact branch flips within +-h, so the engine's loss is smooth there (on
     a collision, the restitution and speculative-contact tests do flip within
-    +-1e-3, and the engine's loss is not differentiable at that scale).  The
-    tolerance covers float rounding of the loss (about 1e-7 of it, divided by
-    2h)."""
+    +-1e-3, and the engine's loss is not differentiable at that scale).
+    Measured: 0.7 % (rolling) and 1.0 % (sliding) of the largest derivative,
+    above the float rounding of the engine's loss (about 5e-5 after division by
+    2h): the engine's differences at h = 1e-3 are not yet the derivative, so
+    the tolerance is 1e-2 of it plus 2e-4."""
     lib = gpu()
     w, s, spec, steps = _recorded(lib, name)
     n = lib.m3d_gpu_body_capacity(w)
@@ -399,6 +401,7 @@ def test_adjoint_matches_engine_central_differences(name):
                             _engine_loss(lib, spec, steps, u, **{arg: (i, k, -h)})) / (2 * h)
         adj = g[key][s]
         err = np.abs(adj - fd).max()
+        print(name, key, "max |adjoint - central difference| = %.3g, max |derivative| = %.3g" % (err, np.abs(fd).max()))
         assert err <= 1e-2 * np.abs(fd).max() + 2e-4, (name, key, adj.tolist(), fd.tolist())
 
 
@@ -495,3 +498,68 @@ def test_warp_islands_give_the_one_thread_result():
         assert _same_bits(a, b)
     for k in ("pos", "rot", "vel", "ang", "mass", "mu", "e"):
         assert _same_bits(g_w[k], g_1[k]), k
+
+
+def _world_loss(pos, s, target):
+    c = pos[s].astype(np.float64).mean(axis=0)
+    r = c - target
+    return float(r @ r), 2.0 * r / len(s)
+
+
+def _incline_engine_loss(lib, seed, steps, s, target, dv):
+    sc = _incline(lib, seed)
+    for k, i in enumerate(sc.dynamic_ids()):
+        v = lib.m3d_body_linear_velocity(sc.world, i)
+        lib.m3d_body_set_linear_velocity(sc.world, i, api.Vec3(v.x + dv[k, 0], v.y + dv[k, 1], v.z + dv[k, 2]))
+    for _ in range(steps):
+        sc.step_only(4)
+    pos = state(lib, sc.world)[0]
+    sc.close()
+    return _world_loss(pos, s, target)[0]
+
+
+def test_adjoint_agreement_by_horizon_on_config5_worlds():
+    """Config-5 incline worlds (64 bodies), loss |centroid - target|^2,
+    horizons 10/20/40/120 steps: the adjoint's directional derivative along a
+    random initial-velocity direction against (a) central differences of the
+    double-precision regenerating replay (h = 1e-6, the exact derivative of
+    the recorded branch) and (b) central differences of the engine (h = 1e-3,
+    and 2e-3 for the engine against itself).  Printed as a table; asserted:
+    at 10 steps some world agrees with the exact branch derivative to 1e-3,
+    and the gradient grows with the horizon (the engine's loss is not smooth
+    at the 1e-3 scale on these worlds, see the table)."""
+    lib = gpu()
+    rel = lambda a, b: abs(a - b) / max(abs(a), abs(b), 1e-30)  # noqa: E731
+    rows = []
+    for steps in (10, 20, 40, 120):
+        for seed in (1, 2, 3):
+            sc = _incline(lib, seed)
+            s = np.array([i.index for i in sc.dynamic_ids()])
+            assert lib.m3d_gpu_tape_begin(sc.world, 10) == api.GPU_OK
+            for _ in range(steps):
+                sc.step_only(4)
+            target = np.random.default_rng(100 + seed).normal(size=3)
+            _, dc = _world_loss(state(lib, sc.world)[0], s, target)
+            n = lib.m3d_gpu_body_capacity(sc.world)
+            dpos = np.zeros((n, 3))
+            dpos[s] = dc
+            rc, g = backward(lib, sc.world, dpos)
+            assert rc == api.GPU_OK
+            u = np.random.default_rng(seed * 7 + steps).normal(size=(len(s), 3))
+            ad = float((g["vel"][s] * u).sum())
+            full = np.zeros((n, 3))
+            full[s] = u
+            h6 = 1e-6
+            lp = _world_loss(regenerate(lib, sc.world, True, dvel=h6 * full)[0], s, target)[0]
+            lm = _world_loss(regenerate(lib, sc.world, True, dvel=-h6 * full)[0], s, target)[0]
+            exact = (lp - lm) / (2 * h6)
+            sc.close()
+            eng = {h: (_incline_engine_loss(lib, seed, steps, s, target, h * u) -
+                       _incline_engine_loss(lib, seed, steps, s, target, -h * u)) / (2 * h) for h in (1e-3, 2e-3)}
+            rows.append((steps, seed, abs(ad), rel(ad, exact), rel(ad, eng[1e-3]), rel(eng[1e-3], eng[2e-3])))
+    print("horizon seed |g.u| adjoint-vs-exact-branch adjoint-vs-engine(h=1e-3) engine(1e-3)-vs-engine(2e-3)")
+    for r in rows:
+        print("%4d %3d %10.4g %10.3g %10.3g %10.3g" % r)
+    assert min(r[3] for r in rows if r[0] == 10) <= 1e-3
+    mags = {steps: np.median([r[2] for r in rows if r[0] == steps]) for steps in (10, 120)}
+    assert mags[120] > 100.0 * mags[10]
