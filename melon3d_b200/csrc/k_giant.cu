@@ -238,21 +238,56 @@ __device__ __forceinline__ void giantContactOp(GiantOp op, const GiantArgs& a, i
 }
 
 // the overflow bucket in reference order, level by level on CTA 0
-__device__ void overflowSweep(GiantOp op, const GiantArgs& a, int levels)
+// Levels of more than one CTA pass run on the whole grid (one pass and a grid
+// barrier instead of several passes of CTA 0); runs of smaller levels run on
+// CTA 0 with block barriers, and a grid barrier separates a run from a large
+// level after it.  The caller's barrier after the sweep covers the last run.
+// Returns true when a wait gave up (the caller returns).
+__device__ bool overflowSweep(GiantOp op, const GiantArgs& a, int levels, uint32_t* gen, uint32_t* stop)
 {
-	if (blockIdx.x != 0)
+	const int gtid = blockIdx.x * kGiantThreads + threadIdx.x;
+	const int gthreads = gridDim.x * kGiantThreads;
+	int L = 1;
+	while (L <= levels)
 	{
-		return;
-	}
-	for (int L = 1; L <= levels; ++L)
-	{
-		const int e = (int)a.levelStart[L + 1];
-		for (int q = (int)a.levelStart[L] + threadIdx.x; q < e; q += kGiantThreads)
+		const int s0 = (int)a.levelStart[L], e0 = (int)a.levelStart[L + 1];
+		if (e0 - s0 > kGiantThreads)
 		{
-			giantContactOp(op, a, a.ovOrder[q]);
+			for (int q = s0 + gtid; q < e0; q += gthreads)
+			{
+				giantContactOp(op, a, a.ovOrder[q]);
+			}
+			if (gridSync(a, gen, stop))
+			{
+				return true;
+			}
+			++L;
+			continue;
 		}
-		__syncthreads();
+		int Lend = L;
+		while (Lend <= levels && (int)(a.levelStart[Lend + 1] - a.levelStart[Lend]) <= kGiantThreads)
+		{
+			++Lend;
+		}
+		if (blockIdx.x == 0)
+		{
+			for (int l = L; l < Lend; ++l)
+			{
+				const int e = (int)a.levelStart[l + 1];
+				for (int q = (int)a.levelStart[l] + threadIdx.x; q < e; q += kGiantThreads)
+				{
+					giantContactOp(op, a, a.ovOrder[q]);
+				}
+				__syncthreads();
+			}
+		}
+		if (Lend <= levels && gridSync(a, gen, stop))
+		{
+			return true;
+		}
+		L = Lend;
 	}
+	return false;
 }
 
 // Overflow index of the previous overflow contact on island body `l` before
@@ -790,7 +825,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 				lap(a, t0, 1);
 				if (overLevels > 0)
 				{
-					overflowSweep(kGiantNormals, a, overLevels);
+					if (overflowSweep(kGiantNormals, a, overLevels, &gen, &stop))
+					{
+						return;
+					}
 					if (gridSync(a, &gen, &stop))
 					{
 						return;
@@ -811,7 +849,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 			}
 			if (overLevels > 0)
 			{
-				overflowSweep(kGiantFriction, a, overLevels);
+				if (overflowSweep(kGiantFriction, a, overLevels, &gen, &stop))
+				{
+					return;
+				}
 				if (gridSync(a, &gen, &stop))
 				{
 					return;
@@ -841,7 +882,10 @@ __global__ void __launch_bounds__(kGiantThreads, 65536 / (kGiantThreads * 128)) 
 			lap(a, t0, 5);
 			if (overLevels > 0 || r.jointCount > 0)
 			{
-				overflowSweep(kGiantVelocity, a, overLevels);
+				if (overflowSweep(kGiantVelocity, a, overLevels, &gen, &stop))
+				{
+					return;
+				}
 				if (gtid == 0)
 				{
 					for (int j = 0; j < r.jointCount; ++j)
