@@ -393,6 +393,23 @@ __global__ void kIslandTable(const int32_t* islandLabels, int32_t maxIslands, co
 	islands[k] = r;
 }
 
+// sort key of a tiny island: contact count (up to 15) above body count (up to
+// 15) above the shape of its first body (the collision code its thread runs)
+__global__ void kTinyKeys(const IslandRec* islands, const int32_t* tinyList, int32_t maxN, const uint32_t* countDev,
+						  const uint32_t* bodyVals, const BodyCold* cold, uint64_t* keys)
+{
+	const int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k >= maxN || k >= (int)*countDev)
+	{
+		return;
+	}
+	const IslandRec r = islands[tinyList[k]];
+	const uint32_t c = r.contactCount < 15 ? (uint32_t)r.contactCount : 15u;
+	const uint32_t b = r.bodyCount < 15 ? (uint32_t)r.bodyCount : 15u;
+	const uint32_t shape = (uint32_t)cold[bodyVals[r.bodyStart]].shape.type & 3u;
+	keys[k] = (uint64_t)((((c << 4) | b) << 2) | shape);
+}
+
 static int bitsFor(int64_t n)
 {
 	int b = 1;
@@ -496,6 +513,16 @@ void launchIslands(DevWorld& w, int32_t n)
 			   w.islands.as<IslandRec>(), w.coloredList.as<int32_t>(), w.serialList.as<int32_t>(),
 			   w.tinyList.as<int32_t>(), w.giantList.as<int32_t>(), w.giantIslandContacts,
 			   w.lastSerialIslands > w.tinyModeIslands ? w.tinyContacts : 0, dc);
+	if (w.lastSerialIslands > w.tinyModeIslands && w.tinyContacts > 0)
+	{
+		// one thread per tiny island: group islands of equal contact and body
+		// counts into the same warps (the list order, filled by atomics, is
+		// arbitrary anyway, and every island is solved on its own)
+		w.tinyKeys.ensure((size_t)(n + 1) * sizeof(uint64_t));
+		M3G_LAUNCH(kTinyKeys, blocksFor(n, 256), 256, s, w.islands.as<IslandRec>(), w.tinyList.as<int32_t>(), n,
+				   &dc->tinyIslands, w.bodyVals.as<uint32_t>(), w.B.cold, w.tinyKeys.as<uint64_t>());
+		radixSortPairs(w.tinyKeys.as<uint64_t>(), (uint32_t*)w.tinyList.ptr, n, 0x3FFull, w.prim, s, &dc->tinyIslands);
+	}
 	w.islandMax = n;
 }
 

@@ -168,6 +168,7 @@ struct DevWorld
 	DevBuf islandKinds;
 	DevBuf labelCount, labelStart, labelCursor; // per label: island bodies
 	DevBuf islandListFlag, islandListOffs, islandLabels, coloredList, serialList, tinyList, giantList, jointScan;
+	DevBuf tinyKeys; // sort keys of the tiny-island list
 	int32_t islandMax = 0; // upper bound of the awake islands of the step
 	uint32_t lastSerialIslands = 0; // serial islands of the previous step (kernel choice)
 	// serial islands of at most tinyContacts contacts (no joints) take one
