@@ -410,6 +410,21 @@ __global__ void kTinyKeys(const IslandRec* islands, const int32_t* tinyList, int
 	keys[k] = (uint64_t)((((c << 4) | b) << 2) | shape);
 }
 
+// sort key of a warp island, largest first: 1023 minus its contacts plus
+// twice its joints
+__global__ void kWarpIslandKeys(const IslandRec* islands, const int32_t* serialList, int32_t maxN,
+								const uint32_t* countDev, uint64_t* keys)
+{
+	const int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k >= maxN || k >= (int)*countDev)
+	{
+		return;
+	}
+	const IslandRec r = islands[serialList[k]];
+	const int32_t size = r.contactCount + 2 * r.jointCount;
+	keys[k] = (uint64_t)(1023 - (size < 1023 ? size : 1023));
+}
+
 static int bitsFor(int64_t n)
 {
 	int b = 1;
@@ -522,6 +537,12 @@ void launchIslands(DevWorld& w, int32_t n)
 		M3G_LAUNCH(kTinyKeys, blocksFor(n, 256), 256, s, w.islands.as<IslandRec>(), w.tinyList.as<int32_t>(), n,
 				   &dc->tinyIslands, w.bodyVals.as<uint32_t>(), w.B.cold, w.tinyKeys.as<uint64_t>());
 		radixSortPairs(w.tinyKeys.as<uint64_t>(), (uint32_t*)w.tinyList.ptr, n, 0x3FFull, w.prim, s, &dc->tinyIslands);
+		// the warp islands largest first, so the last wave of warps is not
+		// left waiting on a few large islands
+		M3G_LAUNCH(kWarpIslandKeys, blocksFor(n, 256), 256, s, w.islands.as<IslandRec>(), w.serialList.as<int32_t>(),
+				   n, &dc->warpIslands, w.tinyKeys.as<uint64_t>());
+		radixSortPairs(w.tinyKeys.as<uint64_t>(), (uint32_t*)w.serialList.ptr, n, 0x3FFull, w.prim, s,
+					   &dc->warpIslands);
 	}
 	w.islandMax = n;
 }
