@@ -393,8 +393,9 @@ __global__ void kIslandTable(const int32_t* islandLabels, int32_t maxIslands, co
 	islands[k] = r;
 }
 
-// sort key of a tiny island: contact count (up to 15) above body count (up to
-// 15) above the shape of its first body (the collision code its thread runs)
+// sort key of a tiny island: contact count (up to 15, descending) above body
+// count (up to 15, descending) above the shape of its first body (the
+// collision code its thread runs)
 __global__ void kTinyKeys(const IslandRec* islands, const int32_t* tinyList, int32_t maxN, const uint32_t* countDev,
 						  const uint32_t* bodyVals, const BodyCold* cold, uint64_t* keys)
 {
@@ -407,7 +408,7 @@ __global__ void kTinyKeys(const IslandRec* islands, const int32_t* tinyList, int
 	const uint32_t c = r.contactCount < 15 ? (uint32_t)r.contactCount : 15u;
 	const uint32_t b = r.bodyCount < 15 ? (uint32_t)r.bodyCount : 15u;
 	const uint32_t shape = (uint32_t)cold[bodyVals[r.bodyStart]].shape.type & 3u;
-	keys[k] = (uint64_t)((((c << 4) | b) << 2) | shape);
+	keys[k] = (uint64_t)(((((15u - c) << 4) | (15u - b)) << 2) | shape); // largest islands first
 }
 
 // sort key of a warp island, largest first: 1023 minus its contacts plus
