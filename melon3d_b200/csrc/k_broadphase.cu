@@ -1259,6 +1259,55 @@ void launchContactMoves(DevWorld& w, const int2* hostMoves, int32_t count)
 	cudaStreamSynchronize(w.stream); // the host vector backing hostMoves is freed on return
 }
 
+__global__ void kContactAdjCount(const int2* bodies, int32_t count, uint32_t* perBody)
+{
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < count)
+	{
+		int2 ab = bodies[i];
+		atomicAdd(&perBody[ab.x], 1u);
+		atomicAdd(&perBody[ab.y], 1u);
+	}
+}
+
+__global__ void kContactAdjFill(const int2* bodies, int32_t count, const uint32_t* start, uint32_t* cursor,
+								int32_t* list)
+{
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < count)
+	{
+		int2 ab = bodies[i];
+		list[start[ab.x] + atomicAdd(&cursor[ab.x], 1u)] = i;
+		list[start[ab.y] + atomicAdd(&cursor[ab.y], 1u)] = i;
+	}
+}
+
+// Per-body contact lists of the current contact array (CSR: adjStart has
+// bodies + 1 offsets, adjList 2 x contacts indices).  The order inside one
+// body's list is not fixed (atomic slots); its user sorts them.
+void launchContactAdjacency(DevWorld& w, int32_t bodies)
+{
+	cudaStream_t s = w.stream;
+	int32_t c = w.contactCount;
+	size_t n4 = (size_t)(bodies + 1) * sizeof(uint32_t);
+	w.adjCount.ensure(n4);
+	w.adjStart.ensure(n4);
+	w.adjList.ensure((size_t)(2 * (size_t)c + 1) * sizeof(int32_t));
+	cudaMemsetAsync(w.adjCount.ptr, 0, n4, s);
+	if (c > 0)
+	{
+		M3G_LAUNCH(kContactAdjCount, blocksFor(c, 256), 256, s, (const int2*)w.C.bodies, c,
+				   w.adjCount.as<uint32_t>());
+	}
+	scanExclusive(w.adjCount.as<uint32_t>(), w.adjStart.as<uint32_t>(), bodies + 1, nullptr, w.prim, s);
+	if (c > 0)
+	{
+		cudaMemsetAsync(w.adjCount.ptr, 0, n4, s);
+		M3G_LAUNCH(kContactAdjFill, blocksFor(c, 256), 256, s, (const int2*)w.C.bodies, c, w.adjStart.as<uint32_t>(),
+				   w.adjCount.as<uint32_t>(), w.adjList.as<int32_t>());
+	}
+}
+
 __global__ void kRemovalFinish(uint32_t* countDev, const uint32_t* removedDev)
 {
 	*countDev -= *removedDev;

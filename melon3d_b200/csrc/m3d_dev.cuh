@@ -156,6 +156,8 @@ struct DevWorld
 	// removal / narrowphase / events
 	DevBuf removeFlag, removeScan; // u32 per contact
 	DevBuf moveSrc;                // i32 per hole rank
+	DevBuf adjCount, adjStart;     // u32 per body + 1: contacts touching each body (CSR)
+	DevBuf adjList;                // i32, 2 per contact
 	DevBuf transition;             // i8 per contact
 	DevBuf evBeginFlag, evEndFlag; // u32 per contact
 	DevBuf evBegin, evEnd;         // int4 (bodyA, bodyB, sensor, 0)
@@ -253,6 +255,7 @@ void launchCreateContacts(DevWorld& w);
 void launchRemoval(DevWorld& w);
 // destroy-time swap-removes computed on the host: move (dst, src) pairs
 void launchContactMoves(DevWorld& w, const int2* hostMoves, int32_t count);
+void launchContactAdjacency(DevWorld& w, int32_t bodies);
 
 // batch of worlds (k_batch.cu)
 void launchKeepStable(DevWorld& w, uint32_t* ranges);

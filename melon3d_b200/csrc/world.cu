@@ -85,14 +85,24 @@ struct m3d_world
 	bool mirrorStale = false; // device bodies newer than the host records
 	bool awakeStale = false;  // device awake bits newer than the host records
 
-	// contact sidecar (valid between a step and the next flush)
+	// contact sidecar (valid between a step and the next flush): the device's
+	// contact bodies and flags and its per-body contact lists (CSR over the
+	// original contact indices), downloaded into pinned memory by the first
+	// destroy after a step
 	bool contactMirrorValid = false;
-	std::vector<int2> cBodies;
-	std::vector<uint8_t> cFlags;
-	std::vector<int32_t> cPerm;   // original device index of each host-side slot
-	std::vector<int32_t> cPos;    // current slot of each original contact (-1: removed)
-	std::vector<int32_t> adjStart; // per body: contacts touching it (original indices), CSR
-	std::vector<int32_t> adjList;
+	int2* cBodies = nullptr;      // cCount live slots
+	uint8_t* cFlags = nullptr;
+	uint32_t* adjStart = nullptr; // adjBodies + 1 offsets into adjList
+	int32_t* adjList = nullptr;
+	int32_t cCount = 0;
+	int32_t adjBodies = 0;
+	int64_t sideContactCap = 0, sideBodyCap = 0;
+	// cPerm: original device index of each slot; cPos: current slot of each
+	// original contact (-1: removed).  Both are the identity outside the
+	// indices listed in cTouched, which the flush restores.
+	std::vector<int32_t> cPerm;
+	std::vector<int32_t> cPos;
+	std::vector<int32_t> cTouched;
 	bool contactsEdited = false;
 
 	std::vector<m3d_contact_event> beginEvents;
@@ -303,84 +313,84 @@ void syncMirror(m3d_world* w)
 	w->awakeStale = false;
 }
 
-void ensureContactMirror(m3d_world* w)
-{
-	if (w->contactMirrorValid)
-	{
-		return;
-	}
-	DevWorld& d = w->dev;
-	int32_t c = d.contactCount;
-	w->cBodies.resize(c);
-	w->cFlags.resize(c);
-	w->cPerm.resize(c);
-	if (c > 0)
-	{
-		cudaMemcpyAsync(w->cBodies.data(), d.C.bodies, sizeof(int2) * c, cudaMemcpyDeviceToHost, d.stream);
-		cudaMemcpyAsync(w->cFlags.data(), d.C.flags, sizeof(uint8_t) * c, cudaMemcpyDeviceToHost, d.stream);
-		cudaStreamSynchronize(d.stream);
-		checkCuda(w, "contact sidecar download");
-	}
-	w->cPos.resize(c);
-	for (int32_t i = 0; i < c; ++i)
-	{
-		w->cPerm[i] = i;
-		w->cPos[i] = i;
-	}
-	// per-body adjacency (CSR over original contact indices)
-	int32_t n = (int32_t)w->bodies.size();
-	w->adjStart.assign((size_t)n + 1, 0);
-	for (int32_t i = 0; i < c; ++i)
-	{
-		++w->adjStart[w->cBodies[i].x + 1];
-		++w->adjStart[w->cBodies[i].y + 1];
-	}
-	for (int32_t b = 0; b < n; ++b)
-	{
-		w->adjStart[b + 1] += w->adjStart[b];
-	}
-	w->adjList.resize((size_t)2 * c);
-	std::vector<int32_t> fill(w->adjStart.begin(), w->adjStart.end() - 1);
-	for (int32_t i = 0; i < c; ++i)
-	{
-		w->adjList[fill[w->cBodies[i].x]++] = i;
-		w->adjList[fill[w->cBodies[i].y]++] = i;
-	}
-	w->contactMirrorValid = true;
-	w->contactsEdited = false;
-}
-
 // RemoveContactAt on the host sidecar (reference src/world.cpp:100-119)
 void removeContactAt(m3d_world* w, int32_t i)
 {
-	int32_t last = (int32_t)w->cBodies.size() - 1;
-	w->cPos[w->cPerm[i]] = -1;
+	int32_t last = w->cCount - 1;
+	int32_t gone = w->cPerm[i];
+	w->cPos[gone] = -1;
+	w->cTouched.push_back(gone);
+	w->cTouched.push_back(i);
 	if (i != last)
 	{
 		w->cBodies[i] = w->cBodies[last];
 		w->cFlags[i] = w->cFlags[last];
 		w->cPerm[i] = w->cPerm[last];
 		w->cPos[w->cPerm[i]] = i;
+		w->cTouched.push_back(w->cPerm[i]);
 	}
-	w->cBodies.pop_back();
-	w->cFlags.pop_back();
-	w->cPerm.pop_back();
+	--w->cCount;
 	w->contactsEdited = true;
 }
 
-// Refresh only the awake bits of the host records (what a destroy needs).
-void syncAwake(m3d_world* w)
+void ensureSidecar(m3d_world* w, int32_t n, int32_t c)
 {
-	if (!w->awakeStale)
+	if (c > w->sideContactCap)
+	{
+		int64_t cap = w->sideContactCap * 2 > c ? w->sideContactCap * 2 : c;
+		cap = cap < 4096 ? 4096 : cap;
+		cudaFreeHost(w->cBodies);
+		cudaFreeHost(w->cFlags);
+		cudaFreeHost(w->adjList);
+		cudaMallocHost((void**)&w->cBodies, sizeof(int2) * cap);
+		cudaMallocHost((void**)&w->cFlags, sizeof(uint8_t) * cap);
+		cudaMallocHost((void**)&w->adjList, sizeof(int32_t) * 2 * cap);
+		w->sideContactCap = cap;
+	}
+	if (n + 1 > w->sideBodyCap)
+	{
+		int64_t cap = w->sideBodyCap * 2 > n + 1 ? w->sideBodyCap * 2 : n + 1;
+		cap = cap < 4096 ? 4096 : cap;
+		cudaFreeHost(w->adjStart);
+		cudaMallocHost((void**)&w->adjStart, sizeof(uint32_t) * cap);
+		w->sideBodyCap = cap;
+	}
+}
+
+// Everything a destroy reads from the device, in one download and one wait:
+// the awake bits when the device's are newer than the host records, and once
+// per step the contact sidecar, whose per-body contact lists are built on the
+// device.
+void prepareDestroy(m3d_world* w)
+{
+	const bool awake = w->awakeStale;
+	const bool contacts = !w->contactMirrorValid;
+	if (!awake && !contacts)
 	{
 		return;
 	}
-	int32_t n = (int32_t)w->bodies.size();
-	if (n > 0)
+	DevWorld& d = w->dev;
+	cudaStream_t s = d.stream;
+	const int32_t n = (int32_t)w->bodies.size();
+	const int32_t c = d.contactCount;
+	if (awake && n > 0)
 	{
 		ensurePinned(w, n);
-		cudaMemcpyAsync(w->pinState, w->dev.B.state, sizeof(uint8_t) * n, cudaMemcpyDeviceToHost, w->dev.stream);
-		cudaStreamSynchronize(w->dev.stream);
+		cudaMemcpyAsync(w->pinState, d.B.state, sizeof(uint8_t) * n, cudaMemcpyDeviceToHost, s);
+	}
+	if (contacts && c > 0)
+	{
+		ensureSidecar(w, n, c);
+		launchContactAdjacency(d, n);
+		cudaMemcpyAsync(w->cBodies, d.C.bodies, sizeof(int2) * c, cudaMemcpyDeviceToHost, s);
+		cudaMemcpyAsync(w->cFlags, d.C.flags, sizeof(uint8_t) * c, cudaMemcpyDeviceToHost, s);
+		cudaMemcpyAsync(w->adjStart, d.adjStart.ptr, sizeof(uint32_t) * (n + 1), cudaMemcpyDeviceToHost, s);
+		cudaMemcpyAsync(w->adjList, d.adjList.ptr, sizeof(int32_t) * 2 * c, cudaMemcpyDeviceToHost, s);
+	}
+	cudaStreamSynchronize(s);
+	checkCuda(w, "destroy download");
+	if (awake)
+	{
 		bool anyDirty = !w->dirtyList.empty();
 		for (int32_t i = 0; i < n; ++i)
 		{
@@ -392,8 +402,26 @@ void syncAwake(m3d_world* w)
 			}
 			b.isAwake = (w->pinState[i] & kStAwake) != 0;
 		}
+		w->awakeStale = false;
 	}
-	w->awakeStale = false;
+	if (contacts)
+	{
+		w->cCount = c;
+		w->adjBodies = c > 0 ? n : 0;
+		int32_t had = (int32_t)w->cPerm.size();
+		if (had < c)
+		{
+			w->cPerm.resize(c);
+			w->cPos.resize(c);
+			for (int32_t i = had; i < c; ++i)
+			{
+				w->cPerm[i] = i;
+				w->cPos[i] = i;
+			}
+		}
+		w->contactMirrorValid = true;
+		w->contactsEdited = false;
+	}
 }
 
 void wakeBodyHost(m3d_world* w, int32_t index)
@@ -525,19 +553,28 @@ void flushHostChanges(m3d_world* w)
 	}
 	if (w->contactMirrorValid && w->contactsEdited)
 	{
-		// destroy-time swap-removes: move the survivors the host moved
+		// destroy-time swap-removes: move the survivors the host moved (only
+		// slots listed in cTouched can differ from the identity)
+		std::sort(w->cTouched.begin(), w->cTouched.end());
+		w->cTouched.erase(std::unique(w->cTouched.begin(), w->cTouched.end()), w->cTouched.end());
 		std::vector<int2> moves;
-		for (int32_t k = 0; k < (int32_t)w->cPerm.size(); ++k)
+		for (int32_t k : w->cTouched)
 		{
-			if (w->cPerm[k] != k)
+			if (k < w->cCount && w->cPerm[k] != k)
 			{
 				moves.push_back(make_int2(k, w->cPerm[k]));
 			}
 		}
 		launchContactMoves(d, moves.data(), (int32_t)moves.size());
-		d.contactCount = (int32_t)w->cPerm.size();
+		d.contactCount = w->cCount;
 		w->contactsEdited = false;
 	}
+	for (int32_t k : w->cTouched)
+	{
+		w->cPerm[k] = k;
+		w->cPos[k] = k;
+	}
+	w->cTouched.clear();
 	w->contactMirrorValid = false;
 	if (w->anyMaterialChange)
 	{
@@ -968,7 +1005,7 @@ void m3d_world_destroy(m3d_world* world)
 					   &d.sleepMin, &d.bodyKeys, &d.bodyVals, &d.activeKeys, &d.activeVals, &d.stableKeys,
 					   &d.stableVals, &d.activeOver, &d.stableOver, &d.runStarts, &d.runFlag, &d.runPairCount,
 					   &d.pairKeys, &d.overFlag, &d.overScan, &d.existingSet, &d.newSet, &d.newSetPos, &d.keepFlag,
-					   &d.newContactKeys, &d.removeFlag, &d.removeScan, &d.moveSrc, &d.transition, &d.evBeginFlag,
+					   &d.newContactKeys, &d.removeFlag, &d.removeScan, &d.moveSrc, &d.adjCount, &d.adjStart, &d.adjList, &d.transition, &d.evBeginFlag,
 					   &d.evEndFlag, &d.evBegin, &d.evEnd, &d.evRemoval, &d.contactKeys, &d.contactVals,
 					   &d.jointKeys, &d.jointVals, &d.islandStartFlag, &d.islands, &d.islandKinds, &d.colorOf,
 					   &d.colorOrder, &d.colorStart, &d.packetMax, &d.contactColor, &d.uploads, &d.counters,
@@ -988,6 +1025,10 @@ void m3d_world_destroy(m3d_world* world)
 	cudaFreeHost(world->pinAng);
 	cudaFreeHost(world->pinState);
 	cudaFreeHost(world->pinSleep);
+	cudaFreeHost(world->cBodies);
+	cudaFreeHost(world->cFlags);
+	cudaFreeHost(world->adjStart);
+	cudaFreeHost(world->adjList);
 	cudaEventDestroy(world->evStart);
 	cudaEventDestroy(world->evStop);
 	cudaStreamDestroy(d.stream);
@@ -1065,18 +1106,17 @@ void m3d_body_destroy(m3d_world* world, m3d_body_id id)
 	{
 		return;
 	}
-	syncAwake(world);
+	prepareDestroy(world);
 	int32_t index = id.index;
-	ensureContactMirror(world);
 	// The reference scans every contact in descending index order
 	// (src/world.cpp:578-594).  Its matches never move before they are
 	// reached (only non-matching survivors from the tail are swapped down),
 	// so visiting this body's live contacts in descending current slot order
 	// removes the same contacts in the same order.
 	std::vector<int32_t> slots;
-	if (index + 1 < (int32_t)world->adjStart.size())
+	if (index < world->adjBodies)
 	{
-		for (int32_t k = world->adjStart[index]; k < world->adjStart[index + 1]; ++k)
+		for (uint32_t k = world->adjStart[index]; k < world->adjStart[index + 1]; ++k)
 		{
 			int32_t p = world->cPos[world->adjList[k]];
 			if (p >= 0)
