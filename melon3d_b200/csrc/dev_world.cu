@@ -186,7 +186,7 @@ uint32_t* stableDirtyWords(DevWorld& w)
 	return &devCounters(w)->stableDirty;
 }
 
-__global__ void kSetU32(uint32_t* p, uint32_t v) { *p = v; }
+__global__ void kSetU32(uint32_t* p, uint32_t v) { M3G_KERNEL_BEGIN(); *p = v; }
 
 void setDeviceCount(DevWorld& w, uint32_t* p, uint32_t v) { M3G_LAUNCH(kSetU32, 1, 1, w.stream, p, v); }
 
@@ -201,6 +201,7 @@ void readCounters(DevWorld& w)
 
 __global__ void kApplyUploads(BodySoA B, const BodyUpload* recs, int32_t count, uint8_t* matDirty)
 {
+	M3G_KERNEL_BEGIN();
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= count)
 	{
@@ -274,6 +275,7 @@ void launchApplyUploads(DevWorld& w, const BodyUpload* hostRecs, int32_t count)
 // (reference src/world.cpp:804-818)
 __global__ void kMaterialRefresh(BodySoA B, ContactSoA C, int32_t count, uint8_t* matDirty)
 {
+	M3G_KERNEL_BEGIN();
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c >= count)
 	{

@@ -33,6 +33,7 @@ __device__ __forceinline__ uint32_t contactWorld(const BodySoA& B, const Contact
 
 __global__ void kKeepFlags(const BodySoA B, const uint32_t* vals, int64_t n, const uint8_t* rebuild, uint32_t* flag)
 {
+	M3G_KERNEL_BEGIN();
 	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n)
 	{
@@ -43,6 +44,7 @@ __global__ void kKeepFlags(const BodySoA B, const uint32_t* vals, int64_t n, con
 __global__ void kKeepScatter(const uint64_t* keys, const uint32_t* vals, int64_t n, const uint32_t* flag,
 							 const uint32_t* scan, uint64_t* outKeys, uint32_t* outVals, int bits, uint32_t* ranges)
 {
+	M3G_KERNEL_BEGIN();
 	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n || !flag[i])
 	{
@@ -63,6 +65,7 @@ __global__ void kKeepScatter(const uint64_t* keys, const uint32_t* vals, int64_t
 
 __global__ void kKeepOver(const BodySoA B, const int32_t* over, int32_t n, const uint8_t* rebuild, uint32_t* flag)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n)
 	{
@@ -72,6 +75,7 @@ __global__ void kKeepOver(const BodySoA B, const int32_t* over, int32_t n, const
 
 __global__ void kKeepOverScatter(const int32_t* over, int32_t n, const uint32_t* flag, const uint32_t* scan, int32_t* out)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n && flag[i])
 	{
@@ -122,6 +126,7 @@ void launchKeepStable(DevWorld& w, uint32_t* ranges)
 // merge of two ascending lists of distinct body indices
 __global__ void kMergeOver(const int32_t* a, int32_t na, const int32_t* b, int32_t nb, int32_t* out)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < na)
 	{
@@ -187,6 +192,7 @@ void launchAppendKeptStable(DevWorld& w, int64_t fresh, int32_t freshOver)
 __global__ void kRemovalTest(const BodySoA B, const ContactSoA C, int32_t maxCount, const uint32_t* countDev,
 							 uint32_t* removeFlag)
 {
+	M3G_KERNEL_BEGIN();
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c >= maxCount || c >= (int)*countDev)
 	{
@@ -209,6 +215,7 @@ __global__ void kRemovalTest(const BodySoA B, const ContactSoA C, int32_t maxCou
 __global__ void kNewByWorld(const BodySoA B, const ContactSoA C, int32_t maxNew, const uint32_t* newDev, int32_t base,
 							uint32_t* wNew, uint64_t* keys, uint32_t* vals)
 {
+	M3G_KERNEL_BEGIN();
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= maxNew || k >= (int)*newDev)
 	{
@@ -223,6 +230,7 @@ __global__ void kNewByWorld(const BodySoA B, const ContactSoA C, int32_t maxNew,
 
 __global__ void kWorldSizes(const uint32_t* wCount, const uint32_t* wNew, int32_t worlds, uint32_t* wA)
 {
+	M3G_KERNEL_BEGIN();
 	int w = blockIdx.x * blockDim.x + threadIdx.x;
 	if (w < worlds)
 	{
@@ -236,6 +244,7 @@ __global__ void kVirtualOrder(const BodySoA B, const ContactSoA C, int32_t oldCo
 							  const uint32_t* wCount, const uint32_t* wNewStart, const uint32_t* vStart,
 							  const uint32_t* removeFlag, uint32_t* vFlag, uint32_t* vSrc)
 {
+	M3G_KERNEL_BEGIN();
 	int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= oldCount + (int)*newDev)
 	{
@@ -263,6 +272,7 @@ __global__ void kVirtualOrder(const BodySoA B, const ContactSoA C, int32_t oldCo
 __global__ void kWorldKeep(const uint32_t* wA, const uint32_t* vStart, const uint32_t* vScan, int32_t worlds,
 						   uint32_t* wKeep)
 {
+	M3G_KERNEL_BEGIN();
 	int w = blockIdx.x * blockDim.x + threadIdx.x;
 	if (w < worlds)
 	{
@@ -304,6 +314,7 @@ __global__ void kRelayout(const ContactSoA D, const ContactSoA S, const BodySoA 
 						  const uint32_t* vStart, const uint32_t* wA, const uint32_t* wKeep,
 						  const uint32_t* wFinalStart)
 {
+	M3G_KERNEL_BEGIN();
 	int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= total || t >= (int)*totalDev)
 	{
@@ -333,6 +344,7 @@ __global__ void kRelayout(const ContactSoA D, const ContactSoA S, const BodySoA 
 __global__ void kRelayoutFinish(uint32_t* contactCountDev, const uint32_t* keptTotal, uint32_t* wCount,
 								const uint32_t* wKeep, uint32_t* wStart, const uint32_t* wFinalStart, int32_t worlds)
 {
+	M3G_KERNEL_BEGIN();
 	int w = blockIdx.x * blockDim.x + threadIdx.x;
 	if (w < worlds)
 	{

@@ -71,6 +71,7 @@ __device__ __forceinline__ int64_t cellSpan(const Box& b, float inv)
 __global__ void kRefresh(BodySoA B, int32_t n, float dt, int rebuildAny, const uint8_t* worldRebuild, float inv,
 						 uint32_t* cntA, uint32_t* overA, uint32_t* cntS, uint32_t* overS, uint8_t* inActiveCells)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
 	{
@@ -202,6 +203,7 @@ void launchRefresh(DevWorld& w, int32_t n, float dt, bool rebuildStable, float c
 __global__ void kEmitEntries(BodySoA B, int32_t n, float inv, int bits, const uint32_t* cnt, const uint32_t* offs,
 							 uint64_t* keys, uint32_t* vals, uint32_t* ranges)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	uint32_t lo[4] = { 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu }, hi[4] = { 0u, 0u, 0u, 0u };
 	const uint64_t mask = (1ull << bits) - 1ull;
@@ -256,6 +258,7 @@ __global__ void kEmitEntries(BodySoA B, int32_t n, float inv, int bits, const ui
 
 __global__ void kCompactIndices(const uint32_t* flags, const uint32_t* offs, int32_t n, int32_t* out)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n && flags[i])
 	{
@@ -266,6 +269,7 @@ __global__ void kCompactIndices(const uint32_t* flags, const uint32_t* offs, int
 // per tier: min of (world, x, y, z) fields, then their max
 __global__ void kInitRanges(uint32_t* ranges)
 {
+	M3G_KERNEL_BEGIN();
 	for (int t = 0; t < 2; ++t)
 	{
 		for (int a = 0; a < 4; ++a)
@@ -391,6 +395,7 @@ void launchSortGrid(DevWorld& w, bool rebuildStable)
 
 __global__ void kRunFlags(const uint64_t* keys, int64_t n, uint32_t* flag)
 {
+	M3G_KERNEL_BEGIN();
 	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n)
 	{
@@ -400,6 +405,7 @@ __global__ void kRunFlags(const uint64_t* keys, int64_t n, uint32_t* flag)
 
 __global__ void kRunStarts(const uint32_t* flag, const uint32_t* offs, int64_t n, int32_t* starts, const uint32_t* total)
 {
+	M3G_KERNEL_BEGIN();
 	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n && flag[i])
 	{
@@ -545,6 +551,7 @@ __global__ void kRunPairs(PairCtx P, const uint64_t* actKeys, const uint32_t* ac
 						  int32_t runMax, const uint32_t* runsDev, const uint64_t* stabKeys, const uint32_t* stabVals,
 						  int64_t stabCount, uint32_t* counts, const uint32_t* offsets, uint64_t* out)
 {
+	M3G_KERNEL_BEGIN();
 	int r = blockIdx.x * blockDim.x + threadIdx.x;
 	if (r >= runMax)
 	{
@@ -675,6 +682,7 @@ __device__ bool overCandidate(const OverCtx& O, int64_t idx, int32_t* aOut, int3
 
 __global__ void kOverPairs(PairCtx P, OverCtx O, int64_t total, uint32_t* flags, uint64_t* keys)
 {
+	M3G_KERNEL_BEGIN();
 	int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= total)
 	{
@@ -712,6 +720,7 @@ __global__ void kOverPairs(PairCtx P, OverCtx O, int64_t total, uint32_t* flags,
 
 __global__ void kScatterKeys(const uint32_t* flags, const uint32_t* offs, const uint64_t* keys, int64_t n, uint64_t* out)
 {
+	M3G_KERNEL_BEGIN();
 	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n && flags[i])
 	{
@@ -721,6 +730,7 @@ __global__ void kScatterKeys(const uint32_t* flags, const uint32_t* offs, const 
 
 __global__ void kInsertExisting(const int2* bodies, int32_t count, uint64_t* table, uint32_t mask, uint32_t* fail)
 {
+	M3G_KERNEL_BEGIN();
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c >= count)
 	{
@@ -737,6 +747,7 @@ __global__ void kInsertExisting(const int2* bodies, int32_t count, uint64_t* tab
 __global__ void kDedupeMark(const uint64_t* keys, int64_t n, uint64_t* table, uint32_t* pos, uint32_t mask,
 							uint32_t* fail)
 {
+	M3G_KERNEL_BEGIN();
 	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
 	{
@@ -773,6 +784,7 @@ __device__ __forceinline__ uint32_t hashFind(const uint64_t* table, uint32_t cap
 __global__ void kDedupeKeep(const uint64_t* keys, int64_t n, const uint64_t* table, const uint32_t* pos, uint32_t mask,
 							uint32_t* keep)
 {
+	M3G_KERNEL_BEGIN();
 	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
 	{
@@ -852,6 +864,7 @@ struct OverBatch
 
 __global__ void kOverBlocks(const BodySoA B, OverBatch O, uint32_t* blocks)
 {
+	M3G_KERNEL_BEGIN();
 	int o = blockIdx.x * blockDim.x + threadIdx.x;
 	if (o >= O.nAO + O.nSO)
 	{
@@ -873,6 +886,7 @@ __global__ void kOverBlocks(const BodySoA B, OverBatch O, uint32_t* blocks)
 __global__ void kOverPairsBatch(PairCtx P, OverBatch O, int64_t maxTotal, const uint32_t* totalDev, uint32_t* flags,
 								uint64_t* keys)
 {
+	M3G_KERNEL_BEGIN();
 	const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= maxTotal)
 	{
@@ -1081,6 +1095,7 @@ void launchPairEmit(DevWorld& w, int32_t n, float cellSize)
 __global__ void kCreateContacts(BodySoA B, ContactSoA C, const uint64_t* keys, int32_t maxCount,
 								const uint32_t* newCount, int32_t base, uint32_t* contactCountDev)
 {
+	M3G_KERNEL_BEGIN();
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	uint32_t count = *newCount;
 	if (k == 0)
@@ -1152,6 +1167,7 @@ void launchCreateContacts(DevWorld& w)
 __global__ void kRemovalFlags(BodySoA B, ContactSoA C, int32_t maxCount, const uint32_t* countDev, uint32_t* removeFlag,
 							  uint32_t* evFlag)
 {
+	M3G_KERNEL_BEGIN();
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c > maxCount)
 	{
@@ -1182,6 +1198,7 @@ __global__ void kRemovalFlags(BodySoA B, ContactSoA C, int32_t maxCount, const u
 __global__ void kRemovalEvents(const ContactSoA C, int32_t maxCount, const uint32_t* evFlag, const uint32_t* evScan,
 							   const uint32_t* evTotal, int4* events)
 {
+	M3G_KERNEL_BEGIN();
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c >= maxCount || !evFlag[c])
 	{
@@ -1221,6 +1238,7 @@ __device__ void copyContact(const ContactSoA& C, int dst, int src)
 __global__ void kRemovalMoves(ContactSoA C, int32_t maxCount, const uint32_t* countDev, const uint32_t* removedDev,
 							  const uint32_t* removeFlag, const uint32_t* removeScan)
 {
+	M3G_KERNEL_BEGIN();
 	int32_t count = (int32_t)*countDev;
 	int32_t S = count - (int32_t)*removedDev;
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1238,6 +1256,7 @@ __global__ void kRemovalMoves(ContactSoA C, int32_t maxCount, const uint32_t* co
 
 __global__ void kContactMoves(ContactSoA C, const int2* moves, int32_t count)
 {
+	M3G_KERNEL_BEGIN();
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k < count)
 	{
@@ -1261,6 +1280,7 @@ void launchContactMoves(DevWorld& w, const int2* hostMoves, int32_t count)
 
 __global__ void kContactAdjCount(const int2* bodies, int32_t count, uint32_t* perBody)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < count)
 	{
@@ -1273,6 +1293,7 @@ __global__ void kContactAdjCount(const int2* bodies, int32_t count, uint32_t* pe
 __global__ void kContactAdjFill(const int2* bodies, int32_t count, const uint32_t* start, uint32_t* cursor,
 								int32_t* list)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < count)
 	{
@@ -1310,6 +1331,7 @@ void launchContactAdjacency(DevWorld& w, int32_t bodies)
 
 __global__ void kRemovalFinish(uint32_t* countDev, const uint32_t* removedDev)
 {
+	M3G_KERNEL_BEGIN();
 	*countDev -= *removedDev;
 }
 

@@ -176,6 +176,7 @@ void tapeDestroy(DiffTape* t) { delete t; }
 __global__ void kTapeBodyConst(BodySoA B, int32_t n, BodyConst<float>* bc, float* mu, float* e,
 							   m3d_diff::TapeShape* shapes, uint32_t* bad)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
 	{
@@ -220,6 +221,7 @@ __global__ void kTapeBodyConst(BodySoA B, int32_t n, BodyConst<float>* bc, float
 
 __global__ void kTapeCheckpoint(BodySoA B, int32_t n, Body<float>* out)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
 	{
@@ -236,6 +238,7 @@ __global__ void kTapeCheckpoint(BodySoA B, int32_t n, Body<float>* out)
 
 __global__ void kTapeIslands(const IslandRec* isl, const uint32_t* countDev, TapeIsland* out, uint32_t* bad)
 {
+	M3G_KERNEL_BEGIN();
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= (int)*countDev)
 	{
@@ -266,6 +269,7 @@ __global__ void kTapeIslands(const IslandRec* isl, const uint32_t* countDev, Tap
 __global__ void kIslandWorkKeys(const TapeIsland* isl, int32_t n, int32_t warpContacts, uint64_t* keys,
 								uint32_t* vals, uint32_t* warpCount)
 {
+	M3G_KERNEL_BEGIN();
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k < n)
 	{
@@ -282,6 +286,7 @@ __global__ void kIslandWorkKeys(const TapeIsland* isl, int32_t n, int32_t warpCo
 
 __global__ void kIslandGather(const TapeIsland* src, const uint32_t* order, int32_t n, TapeIsland* dst)
 {
+	M3G_KERNEL_BEGIN();
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k < n)
 	{
@@ -309,6 +314,7 @@ __device__ __forceinline__ uint32_t pairHash(unsigned long long k)
 // slots as keys, so every probe sequence ends at an empty slot
 __global__ void kPairInsert(const TapeContact* recs, int32_t n, unsigned long long* keys, int32_t* vals, uint32_t mask)
 {
+	M3G_KERNEL_BEGIN();
 	int p = blockIdx.x * blockDim.x + threadIdx.x;
 	if (p >= n)
 	{
@@ -331,6 +337,7 @@ __global__ void kPairInsert(const TapeContact* recs, int32_t n, unsigned long lo
 __global__ void kPairLookup(const TapeContact* recs, int32_t n, const unsigned long long* keys, const int32_t* vals,
 							uint32_t mask, int32_t* out)
 {
+	M3G_KERNEL_BEGIN();
 	int p = blockIdx.x * blockDim.x + threadIdx.x;
 	if (p >= n)
 	{
@@ -889,6 +896,7 @@ int32_t islandBlocks(const TapeStep& st)
 __global__ void __launch_bounds__(64) kTapeReplayStep(IslandCtx<float> base, Work<float> k, int32_t islands,
 													   int32_t warpIslands)
 {
+	M3G_KERNEL_BEGIN();
 	IslandCtx<float> x;
 	if (islandOfThread(x, base, k, islands, warpIslands))
 	{
@@ -899,6 +907,7 @@ __global__ void __launch_bounds__(64) kTapeReplayStep(IslandCtx<float> base, Wor
 __global__ void __launch_bounds__(64) kTapeRecordStep(IslandCtx<float> base, Work<float> k, int32_t islands,
 													  int32_t warpIslands)
 {
+	M3G_KERNEL_BEGIN();
 	IslandCtx<float> x;
 	if (islandOfThread(x, base, k, islands, warpIslands))
 	{
@@ -909,6 +918,7 @@ __global__ void __launch_bounds__(64) kTapeRecordStep(IslandCtx<float> base, Wor
 __global__ void __launch_bounds__(64) kTapeReverseStep(IslandCtx<float> base, Work<float> k, int32_t islands,
 													   int32_t warpIslands)
 {
+	M3G_KERNEL_BEGIN();
 	IslandCtx<float> x;
 	if (islandOfThread(x, base, k, islands, warpIslands))
 	{
@@ -919,6 +929,7 @@ __global__ void __launch_bounds__(64) kTapeReverseStep(IslandCtx<float> base, Wo
 // bodies put to sleep at a step's end: velocities (or their adjoints) zeroed
 __global__ void kTapeSleepCut(Body<float>* b, const uint32_t* list, int32_t n)
 {
+	M3G_KERNEL_BEGIN();
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k < n)
 	{
@@ -935,6 +946,7 @@ __global__ void __launch_bounds__(128)
 	kTapeGenJacobian(const TapeContact* recs, int32_t n, const Body<float>* states, const BodyConst<float>* bc,
 					 const m3d_diff::TapeShape* shapes, float dt, double* J)
 {
+	M3G_KERNEL_BEGIN();
 	const int p = blockIdx.x * blockDim.x + threadIdx.x;
 	if (p >= n)
 	{
@@ -957,6 +969,7 @@ __global__ void __launch_bounds__(128)
 __global__ void kTapeCarryBar(const m3d_diff::ContactBar<float>* cur, const int32_t* prevPos, int32_t n,
 							  m3d_diff::ContactBar<float>* prev)
 {
+	M3G_KERNEL_BEGIN();
 	int p = blockIdx.x * blockDim.x + threadIdx.x;
 	if (p < n && prevPos[p] >= 0)
 	{

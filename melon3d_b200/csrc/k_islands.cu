@@ -24,6 +24,7 @@ namespace m3g
 
 __global__ void kAnyAwakeDynamic(const uint8_t* bFlags, int32_t n, uint32_t* flag)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n && (bFlags[i] & (kBFDynamic | kBFAwake)) == (kBFDynamic | kBFAwake))
 	{
@@ -44,6 +45,7 @@ void launchAnyAwakeDynamic(DevWorld& w, int32_t n)
 __global__ void kInitParent(int32_t* parent, int32_t n, const uint32_t* active, uint32_t* labelCount,
 							uint32_t* cursor)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n)
 	{
@@ -117,6 +119,7 @@ __device__ void ufUnite(int32_t* parent, int32_t a, int32_t b)
 __global__ void kUnionContacts(const ContactSoA C, int32_t maxCount, const uint32_t* countDev, const uint8_t* bFlags,
 							   int32_t* parent, const uint32_t* active)
 {
+	M3G_KERNEL_BEGIN();
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c >= maxCount || c >= (int)*countDev || !*active)
 	{
@@ -137,6 +140,7 @@ __global__ void kUnionContacts(const ContactSoA C, int32_t maxCount, const uint3
 __global__ void kUnionJoints(const JointRec* joints, int32_t count, const BodyCold* cold, int32_t* parent,
 							 const uint32_t* active)
 {
+	M3G_KERNEL_BEGIN();
 	int j = blockIdx.x * blockDim.x + threadIdx.x;
 	if (j >= count || !*active)
 	{
@@ -152,6 +156,7 @@ __global__ void kUnionJoints(const JointRec* joints, int32_t count, const BodyCo
 __global__ void kLabels(int32_t* parent, int32_t n, const uint8_t* bFlags, int32_t* label, uint32_t* islandFlag,
 						uint32_t* islandCount, const uint32_t* active)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n || !*active)
 	{
@@ -178,6 +183,7 @@ __global__ void kLabels(int32_t* parent, int32_t n, const uint8_t* bFlags, int32
 __global__ void kIslandAwake(const uint8_t* bFlags, int32_t n, const int32_t* label, uint32_t* islandFlag,
 							 const uint32_t* active)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n && *active && (bFlags[i] & kBFDynamic) && (bFlags[i] & kBFAwake))
 	{
@@ -189,6 +195,7 @@ __global__ void kIslandAwake(const uint8_t* bFlags, int32_t n, const int32_t* la
 __global__ void kIslandBodies(BodySoA B, int32_t n, const int32_t* label, const uint32_t* islandFlag,
 							  uint32_t* labelCount, uint32_t* stableDirty, const uint32_t* active)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n || !*active)
 	{
@@ -206,6 +213,7 @@ __global__ void kIslandBodies(BodySoA B, int32_t n, const int32_t* label, const 
 
 __global__ void kIslandListFlags(const uint32_t* labelCount, int32_t n, uint32_t* flag)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n)
 	{
@@ -215,6 +223,7 @@ __global__ void kIslandListFlags(const uint32_t* labelCount, int32_t n, uint32_t
 
 __global__ void kIslandListCompact(const uint32_t* flag, const uint32_t* offs, int32_t n, int32_t* islandLabels)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n && flag[i])
 	{
@@ -225,6 +234,7 @@ __global__ void kIslandListCompact(const uint32_t* flag, const uint32_t* offs, i
 __global__ void kPlaceBodies(const BodySoA B, int32_t n, const int32_t* label, const uint32_t* islandFlag,
 							 const uint32_t* labelStart, uint32_t* cursor, uint32_t* bodyVals, const uint32_t* active)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n || !*active)
 	{
@@ -242,6 +252,7 @@ __global__ void kContactIslandFlags(const ContactSoA C, int32_t maxCount, const 
 									const uint8_t* bFlags, const int32_t* label, const uint32_t* islandFlag,
 									uint32_t* flag, uint32_t* touchingCount, uint32_t* pointCount, const uint32_t* active)
 {
+	M3G_KERNEL_BEGIN();
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
 	uint32_t f = 0, points = 0;
 	if (c < maxCount && c < (int)*countDev && *active)
@@ -277,6 +288,7 @@ __global__ void kContactIslandFlags(const ContactSoA C, int32_t maxCount, const 
 __global__ void kJointIslandFlags(const JointRec* joints, int32_t count, const BodyCold* cold, const int32_t* label,
 								  const uint32_t* islandFlag, uint32_t* flag, const uint32_t* active)
 {
+	M3G_KERNEL_BEGIN();
 	int j = blockIdx.x * blockDim.x + threadIdx.x;
 	if (j >= count)
 	{
@@ -300,6 +312,7 @@ __global__ void kLabelPairs(const uint32_t* flag, const uint32_t* offs, int32_t 
 							const int2* contactBodies, const JointRec* joints, const uint8_t* bFlags, const BodyCold* cold,
 							int mode, uint64_t* keys, uint32_t* vals)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= count || !flag[i])
 	{
@@ -341,6 +354,7 @@ __global__ void kIslandTable(const int32_t* islandLabels, int32_t maxIslands, co
 							 IslandRec* islands, int32_t* coloredList, int32_t* serialList, int32_t* tinyList,
 							 int32_t* giantList, int32_t giantContacts, int32_t tinyContacts, StepCounters* dc)
 {
+	M3G_KERNEL_BEGIN();
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= maxIslands || k >= (int)*islandsDev)
 	{
@@ -399,6 +413,7 @@ __global__ void kIslandTable(const int32_t* islandLabels, int32_t maxIslands, co
 __global__ void kTinyKeys(const IslandRec* islands, const int32_t* tinyList, int32_t maxN, const uint32_t* countDev,
 						  const uint32_t* bodyVals, const BodyCold* cold, uint64_t* keys)
 {
+	M3G_KERNEL_BEGIN();
 	const int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= maxN || k >= (int)*countDev)
 	{
@@ -416,6 +431,7 @@ __global__ void kTinyKeys(const IslandRec* islands, const int32_t* tinyList, int
 __global__ void kWarpIslandKeys(const IslandRec* islands, const int32_t* serialList, int32_t maxN,
 								const uint32_t* countDev, uint64_t* keys)
 {
+	M3G_KERNEL_BEGIN();
 	const int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= maxN || k >= (int)*countDev)
 	{
@@ -558,6 +574,7 @@ void launchIslands(DevWorld& w, int32_t n)
 __global__ void kSleepInit(const int32_t* islandLabels, int32_t maxIslands, const uint32_t* islandsDev, int32_t* firstNo,
 						   uint32_t* minBits)
 {
+	M3G_KERNEL_BEGIN();
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k < maxIslands && k < (int)*islandsDev)
 	{
@@ -570,6 +587,7 @@ __global__ void kSleepInit(const int32_t* islandLabels, int32_t maxIslands, cons
 __global__ void kSleepNoFlags(const BodySoA B, const uint32_t* vals, int32_t maxBodies, const uint32_t* bodiesDev,
 							  const int32_t* label, int32_t* firstNo)
 {
+	M3G_KERNEL_BEGIN();
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= maxBodies || k >= (int)*bodiesDev)
 	{
@@ -585,6 +603,7 @@ __global__ void kSleepNoFlags(const BodySoA B, const uint32_t* vals, int32_t max
 __global__ void kSleepUpdate(BodySoA B, const uint32_t* vals, int32_t maxBodies, const uint32_t* bodiesDev,
 							 const int32_t* label, const int32_t* firstNo, uint32_t* minBits, float dt)
 {
+	M3G_KERNEL_BEGIN();
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= maxBodies || k >= (int)*bodiesDev)
 	{
@@ -619,6 +638,7 @@ __global__ void kSleepApply(BodySoA B, const uint32_t* vals, int32_t maxBodies, 
 							const int32_t* label, const int32_t* firstNo, const uint32_t* minBits,
 							uint32_t* stableDirty, uint32_t* record, uint32_t* recordCount)
 {
+	M3G_KERNEL_BEGIN();
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= maxBodies || k >= (int)*bodiesDev)
 	{
@@ -671,6 +691,7 @@ void launchSleep(DevWorld& w, float dt)
 // (reference src/world.cpp:2111-2155)
 __global__ void kFinish(BodySoA B, int32_t n, float dt, int clearForces, StepCounters* dc)
 {
+	M3G_KERNEL_BEGIN();
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
 	{

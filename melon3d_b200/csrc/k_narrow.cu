@@ -15,6 +15,7 @@ namespace m3g
 __global__ void kNarrowphase(BodySoA B, ContactSoA C, int32_t maxCount, const uint32_t* countDev, float dt,
 							 int8_t* transition, uint8_t* genRecord)
 {
+	M3G_KERNEL_BEGIN();
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c >= maxCount)
 	{
@@ -89,6 +90,7 @@ __global__ void kNarrowphase(BodySoA B, ContactSoA C, int32_t maxCount, const ui
 
 __global__ void kTransitionFlags(const int8_t* transition, int32_t count, uint32_t* beginFlag, uint32_t* endFlag)
 {
+	M3G_KERNEL_BEGIN();
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c < count)
 	{
@@ -101,6 +103,7 @@ __global__ void kTransitionFlags(const int8_t* transition, int32_t count, uint32
 __global__ void kTransitionEvents(const ContactSoA C, int32_t count, const int8_t* transition, const uint32_t* beginScan,
 								  const uint32_t* endScan, int4* beginEv, int4* endEv)
 {
+	M3G_KERNEL_BEGIN();
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c >= count)
 	{
@@ -130,6 +133,7 @@ __global__ void kTransitionEvents(const ContactSoA C, int32_t count, const int8_
 __global__ void kWakeDecide(const BodySoA B, const ContactSoA C, int32_t count, const int8_t* transition,
 							int32_t* target)
 {
+	M3G_KERNEL_BEGIN();
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c >= count)
 	{
@@ -154,6 +158,7 @@ __global__ void kWakeDecide(const BodySoA B, const ContactSoA C, int32_t count, 
 
 __global__ void kWakeApply(BodySoA B, int32_t count, const int32_t* target, uint32_t* stableDirty)
 {
+	M3G_KERNEL_BEGIN();
 	int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c < count && target[c] >= 0)
 	{

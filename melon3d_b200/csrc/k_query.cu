@@ -75,6 +75,7 @@ __global__ void kRayCast(BodySoA B, const uint64_t* actKeys, const uint32_t* act
 						 int32_t nAO, const int32_t* stabOver, int32_t nSO, uint32_t* stamps, uint32_t stamp,
 						 uint32_t mask, V3 origin, V3 translation, float cs, RayQueryOut* out)
 {
+	M3G_KERNEL_BEGIN();
 	RayState st;
 	st.out.body = -1;
 	V3 end = add(origin, translation);
@@ -251,6 +252,7 @@ struct CastRec
 __global__ void kSphereCast(BodySoA B, int32_t n, V3 origin, float radius, V3 translation, uint32_t mask, CastRec* recs,
 							unsigned long long* keys)
 {
+	M3G_KERNEL_BEGIN();
 	int bi = blockIdx.x * blockDim.x + threadIdx.x;
 	if (bi >= n)
 	{
@@ -351,6 +353,7 @@ __global__ void kSphereCast(BodySoA B, int32_t n, V3 origin, float radius, V3 tr
 __global__ void kSphereCastPick(const CastRec* recs, const unsigned long long* keys, V3 origin, V3 translation,
 								RayQueryOut* out)
 {
+	M3G_KERNEL_BEGIN();
 	RayQueryOut r;
 	V3 end = add(origin, translation);
 	r.body = -1;
@@ -436,6 +439,7 @@ void launchSphereCastInto(DevWorld& w, int32_t n, V3 origin, float radius, V3 tr
 
 __global__ void kOverlap(BodySoA B, int32_t n, Box box, uint8_t* flags)
 {
+	M3G_KERNEL_BEGIN();
 	int bi = blockIdx.x * blockDim.x + threadIdx.x;
 	if (bi >= n)
 	{

@@ -23,6 +23,7 @@ namespace m3g
 __global__ void kSolveFree(BodySoA B, const IslandRec* islands, int32_t ni, const uint32_t* islandsDev,
 						   const uint32_t* bodyVals, SolveParams P)
 {
+	M3G_KERNEL_BEGIN();
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= ni || k >= (int)*islandsDev)
 	{
@@ -256,6 +257,7 @@ __global__ void __launch_bounds__(32 * kSerialWarpsPerBlock)
 				 const uint32_t* jointVals, uint32_t* localIndex, SolveParams P, m3d_diff::TapeContact* tape,
 				 const uint32_t* tapeStride, const uint8_t* narrowGen)
 {
+	M3G_KERNEL_BEGIN();
 	__shared__ LevelTables tables[kSerialWarpsPerBlock];
 	const int lane = threadIdx.x & 31;
 	LevelTables& T = tables[threadIdx.x >> 5];
@@ -473,6 +475,7 @@ __global__ void __launch_bounds__(128)
 			   const uint32_t* bodyVals, const uint32_t* contactVals, SolveParams P, m3d_diff::TapeContact* tape,
 			   const uint32_t* tapeStride, const uint8_t* narrowGen)
 {
+	M3G_KERNEL_BEGIN();
 	const int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= (int)*tinyDev)
 	{
@@ -752,6 +755,7 @@ __global__ void __launch_bounds__(kColorThreads)
 				  const uint32_t* jointVals, uint32_t* colorMask, int32_t* colorOrder, int32_t* packetMax,
 				  int32_t* contactColor, SolveParams P)
 {
+	M3G_KERNEL_BEGIN();
 	__shared__ int32_t bucketStart[kMaxGraphColors + 2];
 	__shared__ int32_t colorCount;
 	for (int ci = blockIdx.x; ci < (int)*coloredDev; ci += gridDim.x)

@@ -318,6 +318,7 @@ __global__ void __launch_bounds__(kScanThreads)
 	kScanLookback(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total, uint64_t* status,
 				  uint32_t* ticket, uint32_t epoch, uint32_t* error, int64_t spinLimit)
 {
+	M3G_KERNEL_BEGIN();
 	__shared__ uint32_t warpSums[kScanThreads / 32 + 1];
 	__shared__ uint32_t sTile, sPrefix;
 	const int tiles = (int)((n + kScanTile - 1) / kScanTile);
@@ -510,6 +511,7 @@ __device__ __forceinline__ int64_t effectiveN(int64_t nMax, const uint32_t* nDev
 __global__ void kSortHistogram(const uint64_t* keys, int64_t nMax, const uint32_t* nDev, int shift, uint64_t bias,
 							   uint32_t* counts, int tiles)
 {
+	M3G_KERNEL_BEGIN();
 	__shared__ uint32_t hist[kRadix];
 	const int64_t n = effectiveN(nMax, nDev);
 	for (int d = threadIdx.x; d < kRadix; d += kSortThreads)
@@ -537,6 +539,7 @@ __global__ void kSortScatter(const uint64_t* keysIn, const uint32_t* valsIn, uin
 							 int64_t nMax, const uint32_t* nDev, int shift, uint64_t bias, const uint32_t* offsets,
 							 int tiles)
 {
+	M3G_KERNEL_BEGIN();
 	__shared__ uint32_t warpHist[kSortWarps][kRadix];
 	const int64_t n = effectiveN(nMax, nDev);
 	int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -600,6 +603,7 @@ __global__ void kSortScatter(const uint64_t* keysIn, const uint32_t* valsIn, uin
 __global__ void kCopyPairs(const uint64_t* ks, const uint32_t* vs, uint64_t* kd, uint32_t* vd, int64_t nMax,
 						   const uint32_t* nDev)
 {
+	M3G_KERNEL_BEGIN();
 	const int64_t n = effectiveN(nMax, nDev);
 	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n)
@@ -657,12 +661,14 @@ void radixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, uint64_t varyMask
 
 __global__ void kReduceInit(uint64_t* r)
 {
+	M3G_KERNEL_BEGIN();
 	r[0] = 0ull;
 	r[1] = ~0ull;
 }
 
 __global__ void kReduceKeys(const uint64_t* keys, int64_t n, uint64_t* r)
 {
+	M3G_KERNEL_BEGIN();
 	uint64_t o = 0ull, a = ~0ull;
 	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
 	{

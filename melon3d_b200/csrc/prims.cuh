@@ -144,12 +144,53 @@ cudaError_t countedMemcpyAsync(void* dst, const void* src, size_t bytes, cudaMem
 
 #define cudaMemcpyAsync(...) ::m3g::countedMemcpyAsync(__VA_ARGS__)
 
+namespace m3g
+{
+
+// Programmatic dependent launch.  Every kernel of the library is launched
+// with programmatic stream serialisation allowed, so the next kernel of the
+// stream is scheduled while this one's last blocks still run and its launch
+// latency hides behind them.  Every kernel therefore begins with
+// M3G_KERNEL_BEGIN: griddepcontrol.wait holds it until the previous grid of
+// the stream has completed and its writes are visible (a no-op when the
+// launch had no programmatic dependency), then launch_dependents lets the
+// next grid be scheduled.  Because every grid waits before touching memory,
+// each one also starts after every earlier grid of the stream has completed,
+// as without the attribute.
+__device__ __forceinline__ void gridDependencyWait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void gridLaunchDependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... Params, typename... Args>
+inline void launchProgrammatic(void (*kern)(Params...), dim3 grid, dim3 block, cudaStream_t stream, Args&&... args)
+{
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	attr[0].val.programmaticStreamSerializationAllowed = 1;
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = grid;
+	cfg.blockDim = block;
+	cfg.dynamicSmemBytes = 0;
+	cfg.stream = stream;
+	cfg.attrs = attr;
+	cfg.numAttrs = 1;
+	cudaLaunchKernelEx(&cfg, kern, static_cast<Args&&>(args)...);
+}
+
+} // namespace m3g
+
+#define M3G_KERNEL_BEGIN()                                                                                             \
+	do                                                                                                                 \
+	{                                                                                                                  \
+		::m3g::gridDependencyWait();                                                                                   \
+		::m3g::gridLaunchDependents();                                                                                 \
+	} while (0)
+
 // the same, accounted under an explicit name (template instances of one kernel)
 #define M3G_LAUNCH_AS(name, kern, grid, block, stream, ...)                                                            \
 	do                                                                                                                 \
 	{                                                                                                                  \
 		::m3g::launchBegin(name, (stream));                                                                           \
-		kern<<<(grid), (block), 0, (stream)>>>(__VA_ARGS__);                                                           \
+		::m3g::launchProgrammatic(kern, dim3(grid), dim3(block), (stream), __VA_ARGS__);                              \
 		::m3g::launchEnd(name, (stream));                                                                             \
 	} while (0)
 
@@ -157,6 +198,6 @@ cudaError_t countedMemcpyAsync(void* dst, const void* src, size_t bytes, cudaMem
 	do                                                                                                                 \
 	{                                                                                                                  \
 		::m3g::launchBegin(#kern, (stream));                                                                          \
-		kern<<<(grid), (block), 0, (stream)>>>(__VA_ARGS__);                                                           \
+		::m3g::launchProgrammatic(kern, dim3(grid), dim3(block), (stream), __VA_ARGS__);                              \
 		::m3g::launchEnd(#kern, (stream));                                                                            \
 	} while (0)
