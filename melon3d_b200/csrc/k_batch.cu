@@ -387,7 +387,7 @@ void launchBatchRelayout(DevWorld& w)
 	w.newByWorldVals.ensure((size_t)(maxNew + 1) * sizeof(uint32_t));
 	uint32_t* wNew = w.worldNewCount.as<uint32_t>();
 	uint32_t* wA = w.worldRemoved.as<uint32_t>(); // |A_w|: old + new contacts of each world
-	cudaMemsetAsync(wNew, 0, w4, s);
+	fillWords(wNew, 0u, w4, s);
 	if (maxNew > 0)
 	{
 		M3G_LAUNCH(kNewByWorld, blocksFor(maxNew, 256), 256, s, w.B, w.C, maxNew, &dc->newContacts, oldCount, wNew,

@@ -427,7 +427,7 @@ void launchFindRuns(DevWorld& w)
 	w.runCount = (int32_t)n; // upper bound; the exact count stays on the device
 	if (n <= 0)
 	{
-		cudaMemsetAsync(&dc->runs, 0, sizeof(uint32_t), w.stream);
+		fillWords(&dc->runs, 0u, sizeof(uint32_t), w.stream);
 		return;
 	}
 	M3G_LAUNCH(kRunFlags, blocksFor(n, 256), 256, w.stream, w.activeKeys.as<uint64_t>(), n, w.runFlag.as<uint32_t>());
@@ -996,7 +996,7 @@ void launchPairCount(DevWorld& w, int32_t n, float cellSize)
 	uint32_t ecap = tableCapacity(w.contactCount);
 	w.existingSet.ensure((size_t)ecap * sizeof(uint64_t));
 	w.existingMask = ecap - 1;
-	cudaMemsetAsync(w.existingSet.ptr, 0xFF, (size_t)ecap * sizeof(uint64_t), s);
+	fillWords(w.existingSet.ptr, 0xFFFFFFFFu, (size_t)ecap * sizeof(uint64_t), s);
 	if (w.contactCount > 0)
 	{
 		M3G_LAUNCH(kInsertExisting, blocksFor(w.contactCount, 256), 256, s, w.C.bodies, w.contactCount,
@@ -1073,8 +1073,8 @@ void launchPairEmit(DevWorld& w, int32_t n, float cellSize)
 	w.newContactKeys.ensure((size_t)(total + 1) * sizeof(uint64_t));
 	if (total > 0)
 	{
-		cudaMemsetAsync(w.newSet.ptr, 0xFF, (size_t)ncap * sizeof(uint64_t), s);
-		cudaMemsetAsync(w.newSetPos.ptr, 0xFF, (size_t)ncap * sizeof(uint32_t), s);
+		fillWords(w.newSet.ptr, 0xFFFFFFFFu, (size_t)ncap * sizeof(uint64_t), s);
+		fillWords(w.newSetPos.ptr, 0xFFFFFFFFu, (size_t)ncap * sizeof(uint32_t), s);
 		M3G_LAUNCH(kDedupeMark, blocksFor(total, 256), 256, s, pk, total, w.newSet.as<uint64_t>(),
 				   w.newSetPos.as<uint32_t>(), w.newMask, &dc->hashFail);
 		M3G_LAUNCH(kDedupeKeep, blocksFor(total, 256), 256, s, pk, total, w.newSet.as<uint64_t>(),

@@ -35,7 +35,7 @@ __global__ void kAnyAwakeDynamic(const uint8_t* bFlags, int32_t n, uint32_t* fla
 void launchAnyAwakeDynamic(DevWorld& w, int32_t n)
 {
 	StepCounters* dc = devCounters(w);
-	cudaMemsetAsync(&dc->anyAwakeDynamic, 0, sizeof(uint32_t), w.stream);
+	fillWords(&dc->anyAwakeDynamic, 0u, sizeof(uint32_t), w.stream);
 	if (n > 0)
 	{
 		M3G_LAUNCH(kAnyAwakeDynamic, blocksFor(n, 256), 256, w.stream, w.B.bFlags, n, &dc->anyAwakeDynamic);
@@ -724,7 +724,7 @@ __global__ void kFinish(BodySoA B, int32_t n, float dt, int clearForces, StepCou
 void launchFinish(DevWorld& w, int32_t n, float dt, bool clearForces)
 {
 	StepCounters* dc = devCounters(w);
-	cudaMemsetAsync(&dc->bodyCount, 0, 2 * sizeof(uint32_t), w.stream);
+	fillWords(&dc->bodyCount, 0u, 2 * sizeof(uint32_t), w.stream);
 	if (n > 0)
 	{
 		M3G_LAUNCH(kFinish, blocksFor(n, 256), 256, w.stream, w.B, n, dt, clearForces ? 1 : 0, dc);

@@ -181,7 +181,7 @@ void launchNarrowphase(DevWorld& w, float dt)
 	w.evEnd.ensure((size_t)(M + 1) * sizeof(int4));
 	if (M <= 0)
 	{
-		cudaMemsetAsync(&dc->beginNP, 0, 2 * sizeof(uint32_t), s);
+		fillWords(&dc->beginNP, 0u, 2 * sizeof(uint32_t), s);
 		return;
 	}
 	int8_t* tr = w.transition.as<int8_t>();

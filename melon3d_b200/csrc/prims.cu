@@ -688,6 +688,39 @@ __global__ void kReduceKeys(const uint64_t* keys, int64_t n, uint64_t* r)
 	}
 }
 
+__global__ void kFillWords(uint32_t* p, uint32_t v, int64_t words)
+{
+	M3G_KERNEL_BEGIN();
+	const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (((uintptr_t)p & 15u) == 0 && (words & 3) == 0)
+	{
+		uint4* q = (uint4*)p;
+		const uint4 v4 = make_uint4(v, v, v, v);
+		for (; i < words / 4; i += stride)
+		{
+			q[i] = v4;
+		}
+		return;
+	}
+	for (; i < words; i += stride)
+	{
+		p[i] = v;
+	}
+}
+
+void fillWords(void* p, uint32_t v, size_t bytes, cudaStream_t stream)
+{
+	const int64_t words = (int64_t)(bytes / sizeof(uint32_t));
+	if (words <= 0)
+	{
+		return;
+	}
+	int blocks = blocksFor(words, 256 * 4);
+	blocks = blocks > 4 * 148 ? 4 * 148 : blocks;
+	M3G_LAUNCH(kFillWords, blocks, 256, stream, (uint32_t*)p, v, words);
+}
+
 void reduceKeyRange(const uint64_t* keys, int64_t n, PrimScratch& s, cudaStream_t stream)
 {
 	s.reduce.ensure(2 * sizeof(uint64_t));

@@ -66,6 +66,10 @@ void scanExclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total
 void radixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, uint64_t varyMask, PrimScratch& s,
 					cudaStream_t stream, const uint32_t* nDev = nullptr, uint64_t bias = 0ull);
 
+// p[0 .. bytes/4) = v, as a kernel of the library (a memset node would break
+// the stream's programmatic launch chain); bytes must be a multiple of 4.
+void fillWords(void* p, uint32_t v, size_t bytes, cudaStream_t stream);
+
 // Device-side OR / AND of n keys into s.reduce (two u64 words), then copied
 // to the pinned host words s.hostReduce[0..1] (stream-ordered, no sync).
 void reduceKeyRange(const uint64_t* keys, int64_t n, PrimScratch& s, cudaStream_t stream);

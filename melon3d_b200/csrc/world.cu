@@ -120,7 +120,6 @@ struct m3d_world
 	std::vector<uint32_t> bodyWorld;     // world of each body slot
 	std::vector<uint8_t> batchStableDirty, batchStableForce, batchRebuild;
 	std::vector<int32_t> batchStepsSinceStableBuild;
-	std::vector<uint32_t> batchDirtyRead;
 	bool stepped = false;
 	// the last step was a no-op that ended with every body asleep (see
 	// m3d_world_step); any API edit clears it
@@ -150,6 +149,12 @@ struct m3d_world
 	uint8_t* pinState = nullptr;
 	float2* pinSleep = nullptr;
 	int32_t pinCap = 0;
+	// the step's three event lists (removal ends, begins, ends), pinCap each,
+	// and a batch's per-world stable-dirty words
+	int4* pinEvents = nullptr;
+	int32_t pinEventCap = 0;
+	uint32_t* pinWorldDirty = nullptr;
+	int32_t pinWorldDirtyCap = 0;
 };
 
 namespace
@@ -665,13 +670,79 @@ void refreshBroadphase(m3d_world* w, float dt)
 	w->gridDirty = false;
 }
 
-// copy `count` device events to the host list (stream-ordered; the caller syncs)
-void fetchEvents(m3d_world* w, std::vector<int4>& tmp, const int4* dev, int32_t count)
+// Events copied with the step's counters, before their counts are known: the
+// first kEventHead entries of each list travel in the same round trip.
+constexpr int32_t kEventHead = 1024;
+
+// Pinned room for `need` events per list (contents are lost when it grows).
+bool ensurePinnedEvents(m3d_world* w, int32_t need)
 {
-	tmp.resize((size_t)(count > 0 ? count : 0));
-	if (count > 0)
+	if (need <= w->pinEventCap)
 	{
-		cudaMemcpyAsync(tmp.data(), dev, sizeof(int4) * count, cudaMemcpyDeviceToHost, w->dev.stream);
+		return false;
+	}
+	int32_t cap = w->pinEventCap * 2 > need ? w->pinEventCap * 2 : need;
+	cap = cap < kEventHead ? kEventHead : cap;
+	cudaFreeHost(w->pinEvents);
+	cudaMallocHost((void**)&w->pinEvents, sizeof(int4) * 3 * (size_t)cap);
+	w->pinEventCap = cap;
+	return true;
+}
+
+// The step's last round trip: counters, the three event lists and (batch)
+// the per-world stable-dirty words.  One stream wait, a second only when a
+// list is longer than what travelled with the counters.  On return
+// w->pinEvents + k * w->pinEventCap holds list k (removal ends, begins, ends).
+void readStepResults(m3d_world* w)
+{
+	DevWorld& d = w->dev;
+	cudaStream_t s = d.stream;
+	ensurePinnedEvents(w, kEventHead);
+	const DevBuf* lists[3] = { &d.evRemoval, &d.evBegin, &d.evEnd };
+	int32_t copied[3];
+	cudaMemcpyAsync(d.hostCounters, d.counters.ptr, sizeof(StepCounters), cudaMemcpyDeviceToHost, s);
+	for (int k = 0; k < 3; ++k)
+	{
+		int64_t room = (int64_t)(lists[k]->bytes / sizeof(int4));
+		copied[k] = (int32_t)(room < kEventHead ? room : kEventHead);
+		if (copied[k] > 0)
+		{
+			cudaMemcpyAsync(w->pinEvents + (size_t)k * w->pinEventCap, lists[k]->ptr, sizeof(int4) * copied[k],
+							cudaMemcpyDeviceToHost, s);
+		}
+	}
+	if (isBatch(w))
+	{
+		if (d.worldCount > w->pinWorldDirtyCap)
+		{
+			cudaFreeHost(w->pinWorldDirty);
+			cudaMallocHost((void**)&w->pinWorldDirty, sizeof(uint32_t) * (size_t)d.worldCount);
+			w->pinWorldDirtyCap = d.worldCount;
+		}
+		cudaMemcpyAsync(w->pinWorldDirty, d.worldStableDirty.ptr, sizeof(uint32_t) * (size_t)d.worldCount,
+						cudaMemcpyDeviceToHost, s);
+	}
+	cudaStreamSynchronize(s);
+	const StepCounters* hc = d.hostCounters;
+	const int32_t counts[3] = { (int32_t)hc->endRemoval, (int32_t)hc->beginNP, (int32_t)hc->endNP };
+	if (counts[0] > copied[0] || counts[1] > copied[1] || counts[2] > copied[2])
+	{
+		int32_t need = counts[0] > counts[1] ? counts[0] : counts[1];
+		need = need > counts[2] ? need : counts[2];
+		if (ensurePinnedEvents(w, need))
+		{
+			copied[0] = copied[1] = copied[2] = 0;
+		}
+		for (int k = 0; k < 3; ++k)
+		{
+			if (counts[k] > copied[k])
+			{
+				cudaMemcpyAsync(w->pinEvents + (size_t)k * w->pinEventCap + copied[k],
+								lists[k]->as<int4>() + copied[k], sizeof(int4) * (size_t)(counts[k] - copied[k]),
+								cudaMemcpyDeviceToHost, s);
+			}
+		}
+		cudaStreamSynchronize(s);
 	}
 }
 
@@ -1029,6 +1100,8 @@ void m3d_world_destroy(m3d_world* world)
 	cudaFreeHost(world->cFlags);
 	cudaFreeHost(world->adjStart);
 	cudaFreeHost(world->adjList);
+	cudaFreeHost(world->pinEvents);
+	cudaFreeHost(world->pinWorldDirty);
 	cudaEventDestroy(world->evStart);
 	cudaEventDestroy(world->evStop);
 	cudaStreamDestroy(d.stream);
@@ -1839,14 +1912,14 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	}
 	flushHostChanges(world);
 	StepCounters* dc = devCounters(d);
-	cudaMemsetAsync(dc, 0, sizeof(StepCounters), d.stream);
+	fillWords(dc, 0u, sizeof(StepCounters), d.stream);
 	if (world->tape != nullptr)
 	{
 		tapeStepBegin(world->tape, d, n, dt, substepCount, hv(world->def.gravity), world->def.positionIterations);
 	}
 	if (isBatch(world))
 	{
-		cudaMemsetAsync(d.worldStableDirty.ptr, 0, sizeof(uint32_t) * (size_t)d.worldCount, d.stream);
+		fillWords(d.worldStableDirty.ptr, 0u, sizeof(uint32_t) * (size_t)d.worldCount, d.stream);
 	}
 	setDeviceCount(d, &dc->contactCount, (uint32_t)d.contactCount);
 
@@ -1884,7 +1957,7 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	launchAnyAwakeDynamic(d, n);
 	auto tNarrow = Clock::now();
 	d.contactColor.ensure((size_t)(d.contactCap + 1) * sizeof(int32_t));
-	cudaMemsetAsync(d.contactColor.ptr, 0xFF, (size_t)(d.contactMax + 1) * sizeof(int32_t), d.stream);
+	fillWords(d.contactColor.ptr, 0xFFFFFFFFu, (size_t)(d.contactMax + 1) * sizeof(int32_t), d.stream);
 	if (world->tape != nullptr)
 	{
 		tapeBeforeIslands(world->tape, d, substepCount);
@@ -1895,18 +1968,13 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	launchFinish(d, n, dt, world->anyForcesApplied);
 	cudaEventRecord(world->evStop, d.stream);
 
-	// sync 3: counters, then the step's events in one batch
-	readCounters(d);
+	// sync 3: counters with the step's events
+	readStepResults(world);
 	const StepCounters* hc = d.hostCounters;
 	if (hc->waitErrors != 0)
 	{
 		setError(world, M3D_GPU_ERR_WAIT, "a bounded device wait ran out during the step");
 	}
-	std::vector<int4> evR, evB, evE;
-	fetchEvents(world, evR, d.evRemoval.as<int4>(), (int32_t)hc->endRemoval);
-	fetchEvents(world, evB, d.evBegin.as<int4>(), (int32_t)hc->beginNP);
-	fetchEvents(world, evE, d.evEnd.as<int4>(), (int32_t)hc->endNP);
-	cudaStreamSynchronize(d.stream);
 	checkCuda(world, "step");
 	if (world->tape != nullptr)
 	{
@@ -1915,12 +1983,9 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	}
 	if (isBatch(world))
 	{
-		world->batchDirtyRead.resize((size_t)d.worldCount);
-		cudaMemcpy(world->batchDirtyRead.data(), d.worldStableDirty.ptr, sizeof(uint32_t) * (size_t)d.worldCount,
-				   cudaMemcpyDeviceToHost);
 		for (int32_t k = 0; k < d.worldCount; ++k)
 		{
-			if (world->batchDirtyRead[k] != 0)
+			if (world->pinWorldDirty[k] != 0)
 			{
 				world->batchStableDirty[k] = 1;
 			}
@@ -1934,17 +1999,20 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 		ev.isSensor = e.z != 0;
 		return ev;
 	};
-	for (const int4& e : evR)
+	const int4* evR = world->pinEvents;
+	const int4* evB = world->pinEvents + world->pinEventCap;
+	const int4* evE = world->pinEvents + 2 * (size_t)world->pinEventCap;
+	for (uint32_t k = 0; k < hc->endRemoval; ++k)
 	{
-		world->endEvents.push_back(toEvent(e));
+		world->endEvents.push_back(toEvent(evR[k]));
 	}
-	for (const int4& e : evB)
+	for (uint32_t k = 0; k < hc->beginNP; ++k)
 	{
-		world->beginEvents.push_back(toEvent(e));
+		world->beginEvents.push_back(toEvent(evB[k]));
 	}
-	for (const int4& e : evE)
+	for (uint32_t k = 0; k < hc->endNP; ++k)
 	{
-		world->endEvents.push_back(toEvent(e));
+		world->endEvents.push_back(toEvent(evE[k]));
 	}
 	d.contactCount = (int32_t)hc->contactCount;
 	d.lastSerialIslands = hc->serialIslands;

@@ -74,6 +74,33 @@ def contact_colors(lib, world):
     return np.array(out[:n], dtype=np.int32)
 
 
+def events(lib, world):
+    """The world's current contact events, in list order: (begin, end), each
+    an int64 array of rows (bodyA index, generation, bodyB index, generation,
+    isSensor)."""
+    ev = lib.m3d_world_contact_events(world)
+
+    def rows(ptr, n):
+        if n <= 0:
+            return np.zeros((0, 5), np.int64)
+        a = np.ctypeslib.as_array(ptr, shape=(n,))
+        return np.stack([a["bodyA"]["index"], a["bodyA"]["generation"], a["bodyB"]["index"],
+                         a["bodyB"]["generation"], a["isSensor"]], axis=1).astype(np.int64)
+    return rows(ev.beginEvents, ev.beginCount), rows(ev.endEvents, ev.endCount)
+
+
+def diff_events(er, eg):
+    """First difference between two worlds' event lists (order included)."""
+    for name, a, b in (("begin", er[0], eg[0]), ("end", er[1], eg[1])):
+        if len(a) != len(b):
+            return "%s events: %d vs %d" % (name, len(a), len(b))
+        bad = np.nonzero((a != b).any(axis=1))[0]
+        if len(bad):
+            k = int(bad[0])
+            return "%s event %d: %s vs %s" % (name, k, a[k].tolist(), b[k].tolist())
+    return None
+
+
 BODY_FIELDS = ("position", "rotation", "linearVelocity", "angularVelocity", "sleepTime", "smoothedEnergy",
                "isAwake", "inUse")
 CONTACT_FIELDS = ("bodyA", "bodyB", "pointCount", "touching", "isSensor", "tunnelGuard", "normal", "friction",

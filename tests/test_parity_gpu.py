@@ -11,8 +11,8 @@ Oracles (all built from the reference's own sources, oracle/Makefile):
 
 Bit-exact comparisons, per step: every body's pose, velocities and sleep
 state; the contact array (order, pairs, touch flags, manifold normals and
-points); island partitions; the greedy colouring of coloured islands; the
-profile counters.
+points); the step's begin and end contact events, in order; island
+partitions; the greedy colouring of coloured islands; the profile counters.
 """
 import gc
 import os
@@ -48,6 +48,8 @@ def lockstep(ref, kind, steps, seed=1, a=0, b=0, c=0, substeps=4, check_colors=T
                 continue
             cr, cg = U.contacts(ref, sr.world), U.contacts(g, sg.world)
             d = U.diff_contacts(cr, cg)
+            assert d is None, "step %d: %s" % (step, d)
+            d = U.diff_events(U.events(ref, sr.world), U.events(g, sg.world))
             assert d is None, "step %d: %s" % (step, d)
             br, bg = U.bodies(ref, sr.world), U.bodies(g, sg.world)
             d = U.diff_bodies(br, bg)
@@ -140,10 +142,11 @@ def test_pile_250k_first_5_steps_bit_exact():
     """The settled-pile workload at its stated size: 250,000 boxes in a
     50x100x50 lattice (jitter), one giant island through the whole-GPU
     coloured solve; steps 0-4 compared bit for bit (bodies, every contact and
-    manifold point, islands, colours, profile counters)."""
+    manifold point, contact events, islands, colours, profile counters)."""
     ref, g = U.oracle_cr(), U.gpu()
     sr = harness.Scene(ref, harness.PILE, 3, 50, 100, 50, workers=os.cpu_count() or 1)
     sg = harness.Scene(g, harness.PILE, 3, 50, 100, 50)
+    events_max = 0
     try:
         for step in range(5):
             sr.run(1)
@@ -157,6 +160,10 @@ def test_pile_250k_first_5_steps_bit_exact():
             lr, lg = U.island_labels(ref, sr.world), U.island_labels(g, sg.world)
             assert np.array_equal(lr[live], lg[live]), "step %d: island partition differs" % step
             n = _pile_contacts_equal(ref, g, sr.world, sg.world, step)
+            er, eg = U.events(ref, sr.world), U.events(g, sg.world)
+            d = U.diff_events(er, eg)
+            assert d is None, "step %d: %s" % (step, d)
+            events_max = max(events_max, len(er[0]), len(er[1]))
             pr, pg = ref.m3d_world_profile(sr.world), g.m3d_world_profile(sg.world)
             for f in ("bodyCount", "awakeBodyCount", "contactCount", "touchingContactCount", "islandCount"):
                 assert getattr(pr, f) == getattr(pg, f), "step %d: profile %s" % (step, f)
@@ -165,6 +172,7 @@ def test_pile_250k_first_5_steps_bit_exact():
             assert np.array_equal(kr[m], kg[m]), "step %d: colouring differs" % step
             print("step %d: %d contacts, %d touching, %d coloured" % (step, n, pr.touchingContactCount, int(m.sum())))
         assert pr.touchingContactCount > 300000
+        assert events_max > 1024  # longer than the event head copied with the step's counters
     finally:
         sr.close()
         sg.close()

@@ -124,6 +124,11 @@ def test_queries_match_the_reference(seed):
         # churn without a step: the queries refresh the stale broadphase
         sr.churn()
         sg.churn()
+        # the destroys' end events (touching contacts of each destroyed body)
+        er, eg = U.events(ref, sr.world), U.events(g, sg.world)
+        assert len(er[1]) > 0
+        d = U.diff_events(er, eg)
+        assert d is None, d
         _compare_queries(ref, g, sr.world, sg.world, rng, "after churn")
         for step in range(5):
             sr.step_only()
