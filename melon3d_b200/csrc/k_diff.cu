@@ -938,16 +938,17 @@ __global__ void kTapeSleepCut(Body<float>* b, const uint32_t* list, int32_t n)
 	}
 }
 
-// The Jacobians of the step's narrowphase generations, one thread per
-// contact, at the step-start states (all the generations that happen at the
-// step's start; those in contact preparation are rare and are evaluated by
-// the island's own thread).
+// The Jacobians of the step's narrowphase generations, seven threads per
+// contact (two columns each), at the step-start states (all the generations
+// that happen at the step's start; those in contact preparation are evaluated
+// by the island's own thread).
 __global__ void __launch_bounds__(128)
 	kTapeGenJacobian(const TapeContact* recs, int32_t n, const Body<float>* states, const BodyConst<float>* bc,
 					 const m3d_diff::TapeShape* shapes, float dt, double* J)
 {
 	M3G_KERNEL_BEGIN();
-	const int p = blockIdx.x * blockDim.x + threadIdx.x;
+	const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	const int64_t p = t / 7; // seven threads per contact, two Jacobian columns each
 	if (p >= n)
 	{
 		return;
@@ -960,8 +961,8 @@ __global__ void __launch_bounds__(128)
 	const Body<float>& A = states[rec.a];
 	const Body<float>& B = states[rec.b];
 	const float margin = m3d_diff::kGenSpeculativeBase + dt * m3d_diff::len(m3d_diff::sub(A.v, B.v));
-	m3d_diff::generationJacobian(bc, shapes, rec, A.x, A.q, B.x, B.q, margin,
-								 J + (size_t)p * (m3d_diff::kGenJRows * m3d_diff::kGenJCols));
+	m3d_diff::generationJacobianPair(bc, shapes, rec, A.x, A.q, B.x, B.q, margin, (int)(t % 7),
+									 J + (size_t)p * (m3d_diff::kGenJRows * m3d_diff::kGenJCols));
 }
 
 // manifold adjoints carried to the previous step: contact p of this step is
@@ -1165,7 +1166,7 @@ int32_t tapeBackward(DiffTape* t, DevWorld& w, const float* dPos, const float* d
 								cudaMemcpyDeviceToDevice, s);
 				if (st.contactsPerSubstep > 0)
 				{
-					M3G_LAUNCH(kTapeGenJacobian, blocksFor(st.contactsPerSubstep, 128), 128, s, st.recs,
+					M3G_LAUNCH(kTapeGenJacobian, blocksFor((int64_t)st.contactsPerSubstep * 7, 128), 128, s, st.recs,
 							   st.contactsPerSubstep, states + (size_t)(step - s0) * n,
 							   t->bodyConst.as<BodyConst<float>>(), t->shapes.as<m3d_diff::TapeShape>(), st.dt, genJ);
 				}

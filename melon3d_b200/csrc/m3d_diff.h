@@ -2047,6 +2047,103 @@ M3D_DIFF_HD_CALL void generationJacobianN(const TapeShape& shA, const TapeShape&
 	}
 }
 
+// Columns p and p + 7 of the same Jacobian (component p of A's and of B's
+// pose: x, y, z, qx, qy, qz, qw), two dual slots wide, so that seven threads
+// share one generation.  Forward-mode lanes do not mix, so each column equals
+// the one generationJacobian gives; a column of a non-dynamic body is zero.
+template <typename T>
+M3D_DIFF_HD_CALL void generationJacobianPair(const BodyConst<T>* bc, const TapeShape* shapes, const TapeContact& rec,
+											 V<T> xA, Q<T> qA, V<T> xB, Q<T> qB, T margin, int p, double* J)
+{
+	typedef Dual<T, 2> S;
+	const int cA = p, cB = 7 + p;
+	for (int o = 0; o < kGenJRows; ++o)
+	{
+		J[o * kGenJCols + cA] = 0.0;
+		J[o * kGenJCols + cB] = 0.0;
+	}
+	const bool dynA = bc[rec.a].dynamic != 0, dynB = bc[rec.b].dynamic != 0;
+	if ((!dynA && !dynB) || rec.pointCount == 0)
+	{
+		return;
+	}
+	const TapeShape& shA = shapes[rec.a];
+	const TapeShape& shB = shapes[rec.b];
+	GenShape<S> sa, sb;
+	sa.type = shA.type;
+	sa.radius = S(T(shA.radius));
+	sa.he = v3<S>(S(T(shA.he[0])), S(T(shA.he[1])), S(T(shA.he[2])));
+	sb.type = shB.type;
+	sb.radius = S(T(shB.radius));
+	sb.he = v3<S>(S(T(shB.he[0])), S(T(shB.he[1])), S(T(shB.he[2])));
+	V<S> gxA = v3<S>(S(xA.x), S(xA.y), S(xA.z));
+	Q<S> gqA = q4<S>(S(qA.x), S(qA.y), S(qA.z), S(qA.w));
+	V<S> gxB = v3<S>(S(xB.x), S(xB.y), S(xB.z));
+	Q<S> gqB = q4<S>(S(qB.x), S(qB.y), S(qB.z), S(qB.w));
+	S* inA[7] = { &gxA.x, &gxA.y, &gxA.z, &gqA.x, &gqA.y, &gqA.z, &gqA.w };
+	S* inB[7] = { &gxB.x, &gxB.y, &gxB.z, &gqB.x, &gqB.y, &gqB.z, &gqB.w };
+	if (dynA)
+	{
+		inA[p]->d[0] = 1.0;
+	}
+	if (dynB)
+	{
+		inB[p]->d[1] = 1.0;
+	}
+	GenManifold<S> g;
+	genManifold(sa, gxA, gqA, sb, gxB, gqB, S(margin), g);
+	const bool sameNormal =
+		g.count > 0 && g.n.x.v * T(rec.n[0]) + g.n.y.v * T(rec.n[1]) + g.n.z.v * T(rec.n[2]) > T(0.999);
+	if (!sameNormal)
+	{
+		return;
+	}
+	const int col[2] = { cA, cB };
+	const bool live[2] = { dynA, dynB };
+	for (int k = 0; k < 2; ++k)
+	{
+		if (!live[k])
+		{
+			continue;
+		}
+		J[0 * kGenJCols + col[k]] = g.n.x.d[k];
+		J[1 * kGenJCols + col[k]] = g.n.y.d[k];
+		J[2 * kGenJCols + col[k]] = g.n.z.d[k];
+	}
+	for (int i = 0; i < rec.pointCount; ++i)
+	{
+		int j = -1;
+		for (int q = 0; q < g.count; ++q)
+		{
+			if (g.p[q].id == rec.id[i])
+			{
+				j = q;
+				break;
+			}
+		}
+		if (j < 0)
+		{
+			continue;
+		}
+		const GenPoint<S>& gp = g.p[j];
+		double* r = J + (3 + 7 * i) * kGenJCols;
+		for (int k = 0; k < 2; ++k)
+		{
+			if (!live[k])
+			{
+				continue;
+			}
+			r[0 * kGenJCols + col[k]] = gp.la.x.d[k];
+			r[1 * kGenJCols + col[k]] = gp.la.y.d[k];
+			r[2 * kGenJCols + col[k]] = gp.la.z.d[k];
+			r[3 * kGenJCols + col[k]] = gp.lb.x.d[k];
+			r[4 * kGenJCols + col[k]] = gp.lb.y.d[k];
+			r[5 * kGenJCols + col[k]] = gp.lb.z.d[k];
+			r[6 * kGenJCols + col[k]] = gp.off.d[k];
+		}
+	}
+}
+
 // the Jacobian of the contact's generation, for its dynamic bodies
 template <typename T>
 M3D_DIFF_HD void generationJacobian(const BodyConst<T>* bc, const TapeShape* shapes, const TapeContact& rec, V<T> xA,
