@@ -1305,10 +1305,11 @@ __global__ void kContactAdjFill(const int2* bodies, int32_t count, const uint32_
 
 // Per-body contact lists of the current contact array (CSR: adjStart has
 // bodies + 1 offsets, adjList 2 x contacts indices).  The order inside one
-// body's list is not fixed (atomic slots); its user sorts them.
-void launchContactAdjacency(DevWorld& w, int32_t bodies)
+// body's list is not fixed (atomic slots); its user sorts them.  Runs on
+// stream s with the scan scratch prim (the world's own, or a second one when
+// s is not the world's stream).
+void launchContactAdjacency(DevWorld& w, int32_t bodies, cudaStream_t s, PrimScratch& prim)
 {
-	cudaStream_t s = w.stream;
 	int32_t c = w.contactCount;
 	size_t n4 = (size_t)(bodies + 1) * sizeof(uint32_t);
 	w.adjCount.ensure(n4);
@@ -1320,7 +1321,7 @@ void launchContactAdjacency(DevWorld& w, int32_t bodies)
 		M3G_LAUNCH(kContactAdjCount, blocksFor(c, 256), 256, s, (const int2*)w.C.bodies, c,
 				   w.adjCount.as<uint32_t>());
 	}
-	scanExclusive(w.adjCount.as<uint32_t>(), w.adjStart.as<uint32_t>(), bodies + 1, nullptr, w.prim, s);
+	scanExclusive(w.adjCount.as<uint32_t>(), w.adjStart.as<uint32_t>(), bodies + 1, nullptr, prim, s);
 	if (c > 0)
 	{
 		cudaMemsetAsync(w.adjCount.ptr, 0, n4, s);

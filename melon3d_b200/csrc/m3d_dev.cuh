@@ -255,7 +255,7 @@ void launchCreateContacts(DevWorld& w);
 void launchRemoval(DevWorld& w);
 // destroy-time swap-removes computed on the host: move (dst, src) pairs
 void launchContactMoves(DevWorld& w, const int2* hostMoves, int32_t count);
-void launchContactAdjacency(DevWorld& w, int32_t bodies);
+void launchContactAdjacency(DevWorld& w, int32_t bodies, cudaStream_t s, PrimScratch& prim);
 
 // batch of worlds (k_batch.cu)
 void launchKeepStable(DevWorld& w, uint32_t* ranges);

@@ -84,6 +84,10 @@ struct m3d_world
 	bool anyForcesApplied = false;
 	bool mirrorStale = false; // device bodies newer than the host records
 	bool awakeStale = false;  // device awake bits newer than the host records
+	// the device's awake bits as a destroy downloaded them (while awakeStale,
+	// until the device or the host records change); read per body on demand
+	std::vector<uint8_t> awakeBits;
+	bool awakeBitsValid = false;
 
 	// contact sidecar (valid between a step and the next flush): the device's
 	// contact bodies and flags and its per-body contact lists (CSR over the
@@ -155,6 +159,17 @@ struct m3d_world
 	int32_t pinEventCap = 0;
 	uint32_t* pinWorldDirty = nullptr;
 	int32_t pinWorldDirtyCap = 0;
+	// the destroy download issued right after a step that followed destroys
+	// (on its own stream, so it overlaps the host's work until the next
+	// destroy); sideN bodies, sideC contacts, the awake bits in pinSideState
+	cudaStream_t sideStream = nullptr;
+	cudaEvent_t sideDone = nullptr;
+	PrimScratch sidePrim;
+	uint8_t* pinSideState = nullptr;
+	int32_t pinSideCap = 0;
+	bool sidecarPending = false;
+	int32_t sideN = 0, sideC = 0;
+	int32_t destroysSinceStep = 0;
 };
 
 namespace
@@ -316,6 +331,7 @@ void syncMirror(m3d_world* w)
 	}
 	w->mirrorStale = false;
 	w->awakeStale = false;
+	w->awakeBitsValid = false;
 }
 
 // RemoveContactAt on the host sidecar (reference src/world.cpp:100-119)
@@ -366,48 +382,37 @@ void ensureSidecar(m3d_world* w, int32_t n, int32_t c)
 // the awake bits when the device's are newer than the host records, and once
 // per step the contact sidecar, whose per-body contact lists are built on the
 // device.
-void prepareDestroy(m3d_world* w)
+// Issue on stream s what a destroy reads from the device: the awake bits of n
+// bodies into `state`, and the contact sidecar of c contacts, whose per-body
+// contact lists are built on the device (scan scratch prim).
+void enqueueDestroyDownload(m3d_world* w, cudaStream_t s, PrimScratch& prim, bool awake, bool contacts, int32_t n,
+							int32_t c, uint8_t* state)
 {
-	const bool awake = w->awakeStale;
-	const bool contacts = !w->contactMirrorValid;
-	if (!awake && !contacts)
-	{
-		return;
-	}
 	DevWorld& d = w->dev;
-	cudaStream_t s = d.stream;
-	const int32_t n = (int32_t)w->bodies.size();
-	const int32_t c = d.contactCount;
 	if (awake && n > 0)
 	{
-		ensurePinned(w, n);
-		cudaMemcpyAsync(w->pinState, d.B.state, sizeof(uint8_t) * n, cudaMemcpyDeviceToHost, s);
+		cudaMemcpyAsync(state, d.B.state, sizeof(uint8_t) * n, cudaMemcpyDeviceToHost, s);
 	}
 	if (contacts && c > 0)
 	{
 		ensureSidecar(w, n, c);
-		launchContactAdjacency(d, n);
+		launchContactAdjacency(d, n, s, prim);
 		cudaMemcpyAsync(w->cBodies, d.C.bodies, sizeof(int2) * c, cudaMemcpyDeviceToHost, s);
 		cudaMemcpyAsync(w->cFlags, d.C.flags, sizeof(uint8_t) * c, cudaMemcpyDeviceToHost, s);
 		cudaMemcpyAsync(w->adjStart, d.adjStart.ptr, sizeof(uint32_t) * (n + 1), cudaMemcpyDeviceToHost, s);
 		cudaMemcpyAsync(w->adjList, d.adjList.ptr, sizeof(int32_t) * 2 * c, cudaMemcpyDeviceToHost, s);
 	}
-	cudaStreamSynchronize(s);
-	checkCuda(w, "destroy download");
+}
+
+// Take a completed destroy download: the awake bits of the first n bodies
+// (kept aside and read per body by hostAwake), the contact sidecar of c
+// contacts.
+void applyDestroyDownload(m3d_world* w, bool awake, bool contacts, int32_t n, int32_t c, const uint8_t* state)
+{
 	if (awake)
 	{
-		bool anyDirty = !w->dirtyList.empty();
-		for (int32_t i = 0; i < n; ++i)
-		{
-			HostBody& b = w->bodies[i];
-			uint32_t dm = (anyDirty && i < (int32_t)w->dirtyMask.size()) ? w->dirtyMask[i] : 0u;
-			if (!b.inUse || (dm & (kUpAll | kUpState)))
-			{
-				continue;
-			}
-			b.isAwake = (w->pinState[i] & kStAwake) != 0;
-		}
-		w->awakeStale = false;
+		w->awakeBits.assign(state, state + (n > 0 ? n : 0));
+		w->awakeBitsValid = true;
 	}
 	if (contacts)
 	{
@@ -429,6 +434,96 @@ void prepareDestroy(m3d_world* w)
 	}
 }
 
+// A streaming world destroys after most steps: right after a step that
+// followed destroys, the download the next destroy needs is issued on a
+// second stream and left running.  Nothing on the device changes until the
+// next step or flush, both of which first drop it (dropSidecar).
+void prefetchSidecar(m3d_world* w)
+{
+	DevWorld& d = w->dev;
+	if (w->sideStream == nullptr)
+	{
+		cudaStreamCreateWithFlags(&w->sideStream, cudaStreamNonBlocking);
+		cudaEventCreateWithFlags(&w->sideDone, cudaEventDisableTiming);
+		w->sidePrim.errorWord = d.prim.errorWord;
+	}
+	w->sidePrim.waitLimit = d.prim.waitLimit;
+	const int32_t n = (int32_t)w->bodies.size();
+	const int32_t c = d.contactCount;
+	if (n > w->pinSideCap)
+	{
+		cudaFreeHost(w->pinSideState);
+		int32_t cap = n * 2 > 1024 ? n * 2 : 1024;
+		cudaMallocHost((void**)&w->pinSideState, cap);
+		w->pinSideCap = cap;
+	}
+	enqueueDestroyDownload(w, w->sideStream, w->sidePrim, true, true, n, c, w->pinSideState);
+	cudaEventRecord(w->sideDone, w->sideStream);
+	w->sidecarPending = true;
+	w->sideN = n;
+	w->sideC = c;
+}
+
+// Forget a prefetched destroy download (the device is about to change), once
+// its copies have landed.
+void dropSidecar(m3d_world* w)
+{
+	if (w->sidecarPending)
+	{
+		cudaEventSynchronize(w->sideDone);
+		w->sidecarPending = false;
+	}
+}
+
+// Everything a destroy reads from the device, in one download and one wait:
+// the awake bits when the device's are newer than the host records, and once
+// per step the contact sidecar, whose per-body contact lists are built on the
+// device.  Taken from the prefetch when one is pending.
+void prepareDestroy(m3d_world* w)
+{
+	const bool awake = w->awakeStale && !w->awakeBitsValid;
+	const bool contacts = !w->contactMirrorValid;
+	if (!awake && !contacts)
+	{
+		return;
+	}
+	if (w->sidecarPending && contacts)
+	{
+		cudaEventSynchronize(w->sideDone);
+		w->sidecarPending = false;
+		checkCuda(w, "destroy download");
+		applyDestroyDownload(w, awake, contacts, w->sideN, w->sideC, w->pinSideState);
+		return;
+	}
+	dropSidecar(w);
+	DevWorld& d = w->dev;
+	const int32_t n = (int32_t)w->bodies.size();
+	const int32_t c = d.contactCount;
+	if (awake && n > 0)
+	{
+		ensurePinned(w, n);
+	}
+	enqueueDestroyDownload(w, d.stream, d.prim, awake, contacts, n, c, w->pinState);
+	cudaStreamSynchronize(d.stream);
+	checkCuda(w, "destroy download");
+	applyDestroyDownload(w, awake, contacts, n, c, w->pinState);
+}
+
+// Whether a body is awake: the host record when it is current (edited since
+// the step, or refreshed from the device), else the bits a destroy downloaded.
+bool hostAwake(m3d_world* w, int32_t i)
+{
+	if (w->awakeStale && w->awakeBitsValid && i < (int32_t)w->awakeBits.size())
+	{
+		uint32_t dm = i < (int32_t)w->dirtyMask.size() ? w->dirtyMask[i] : 0u;
+		if (!(dm & (kUpAll | kUpState)))
+		{
+			return (w->awakeBits[i] & kStAwake) != 0;
+		}
+	}
+	return w->bodies[i].isAwake;
+}
+
 void wakeBodyHost(m3d_world* w, int32_t index)
 {
 	HostBody& b = w->bodies[index];
@@ -436,7 +531,7 @@ void wakeBodyHost(m3d_world* w, int32_t index)
 	{
 		return;
 	}
-	if (!b.isAwake)
+	if (!hostAwake(w, index))
 	{
 		markStableDirty(w, index);
 	}
@@ -523,6 +618,15 @@ void flushHostChanges(m3d_world* w)
 {
 	DevWorld& d = w->dev;
 	int32_t n = (int32_t)w->bodies.size();
+	if (w->sidecarPending && (n + 1 > d.bodyCap || !w->dirtyList.empty() || (w->contactMirrorValid && w->contactsEdited) ||
+							  w->anyMaterialChange || w->jointsDirty || w->jointedPairsDirty))
+	{
+		dropSidecar(w); // the device is about to change under the prefetch
+	}
+	if (!w->dirtyList.empty())
+	{
+		w->awakeBitsValid = false; // uploads change the device, edit masks are cleared
+	}
 	if (!growBodies(d, n + 1))
 	{
 		setError(w, M3D_GPU_ERR_ALLOC, "body arena growth failed");
@@ -1102,6 +1206,14 @@ void m3d_world_destroy(m3d_world* world)
 	cudaFreeHost(world->adjList);
 	cudaFreeHost(world->pinEvents);
 	cudaFreeHost(world->pinWorldDirty);
+	dropSidecar(world);
+	if (world->sideStream != nullptr)
+	{
+		cudaStreamDestroy(world->sideStream);
+		cudaEventDestroy(world->sideDone);
+	}
+	world->sidePrim.release();
+	cudaFreeHost(world->pinSideState);
 	cudaEventDestroy(world->evStart);
 	cudaEventDestroy(world->evStop);
 	cudaStreamDestroy(d.stream);
@@ -1180,6 +1292,7 @@ void m3d_body_destroy(m3d_world* world, m3d_body_id id)
 		return;
 	}
 	prepareDestroy(world);
+	++world->destroysSinceStep;
 	int32_t index = id.index;
 	// The reference scans every contact in descending index order
 	// (src/world.cpp:578-594).  Its matches never move before they are
@@ -1231,6 +1344,7 @@ void m3d_body_destroy(m3d_world* world, m3d_body_id id)
 			world->jointsDirty = true;
 		}
 	}
+	b->isAwake = hostAwake(world, index); // the state uploaded for the freed slot keeps the device's awake bit
 	b->inUse = false;
 	b->generation++;
 	world->freeBodies.push_back(index);
@@ -1862,6 +1976,10 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	}
 	DevWorld& d = world->dev;
 	auto tStart = Clock::now();
+	dropSidecar(world);
+	world->awakeBitsValid = false;
+	const bool churned = world->destroysSinceStep > 0; // destroys since the last step
+	world->destroysSinceStep = 0;
 	world->beginEvents.clear();
 	world->endEvents.clear();
 	if (world->quiescent && world->tape == nullptr && !isBatch(world) && world->dirtyList.empty() &&
@@ -2059,6 +2177,10 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 					   hc->removed == 0 && hc->endRemoval == 0 && hc->beginNP == 0 && hc->endNP == 0 &&
 					   hc->stableDirty == 0 && hc->gridPairs == 0 && hc->overPairs == 0 && !world->lastRebuiltStable &&
 					   !world->stableDirty && !world->stableForce;
+	if (churned && !isBatch(world) && world->tape == nullptr && world->status == M3D_GPU_OK)
+	{
+		prefetchSidecar(world);
+	}
 }
 
 // ---- GPU extensions ------------------------------------------------------------
