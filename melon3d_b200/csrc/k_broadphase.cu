@@ -319,8 +319,8 @@ static void emitTier(DevWorld& w, int32_t n, float inv, DevBuf& cnt, DevBuf& ove
 	keys.ensure(bound * sizeof(uint64_t));
 	vals.ensure(bound * sizeof(uint32_t));
 	overList.ensure((size_t)(n + 1) * sizeof(int32_t));
-	scanExclusive(cnt.as<uint32_t>(), offs.as<uint32_t>(), n, entryTotal, w.prim, w.stream);
-	scanExclusive(over.as<uint32_t>(), ooffs.as<uint32_t>(), n, overTotal, w.prim, w.stream);
+	scanExclusive2(cnt.as<uint32_t>(), offs.as<uint32_t>(), n, entryTotal, over.as<uint32_t>(), ooffs.as<uint32_t>(), n,
+				   overTotal, w.prim, w.stream);
 	if (n > 0)
 	{
 		M3G_LAUNCH(kEmitEntries, blocksFor(n, 128), 128, w.stream, w.B, n, inv, w.keyBits, cnt.as<uint32_t>(),
@@ -1351,8 +1351,8 @@ void launchRemoval(DevWorld& w)
 	M3G_LAUNCH(kRemovalFlags, blocksFor(M + 1, 256), 256, s, w.B, w.C, M, &dc->contactCount, w.removeFlag.as<uint32_t>(),
 			   w.evEndFlag.as<uint32_t>());
 	// M + 1 entries so that removeScan[count] exists
-	scanExclusive(w.removeFlag.as<uint32_t>(), w.removeScan.as<uint32_t>(), M + 1, &dc->removed, w.prim, s);
-	scanExclusive(w.evEndFlag.as<uint32_t>(), w.evBeginFlag.as<uint32_t>(), M, &dc->endRemoval, w.prim, s);
+	scanExclusive2(w.removeFlag.as<uint32_t>(), w.removeScan.as<uint32_t>(), M + 1, &dc->removed,
+				   w.evEndFlag.as<uint32_t>(), w.evBeginFlag.as<uint32_t>(), M, &dc->endRemoval, w.prim, s);
 	if (M > 0)
 	{
 		M3G_LAUNCH(kRemovalEvents, blocksFor(M, 256), 256, s, w.C, M, w.evEndFlag.as<uint32_t>(),

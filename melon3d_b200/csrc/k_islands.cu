@@ -492,10 +492,10 @@ void launchIslands(DevWorld& w, int32_t n)
 	M3G_LAUNCH(kIslandBodies, blocksFor(n, 256), 256, s, w.B, n, w.label.as<int32_t>(), w.islandFlag.as<uint32_t>(),
 			   w.labelCount.as<uint32_t>(), stableDirtyWords(w), active);
 	// bodies per island: label counts -> starts -> placement
-	scanExclusive(w.labelCount.as<uint32_t>(), w.labelStart.as<uint32_t>(), n, &dc->islandBodies, w.prim, s);
 	M3G_LAUNCH(kIslandListFlags, blocksFor(n, 256), 256, s, w.labelCount.as<uint32_t>(), n,
 			   w.islandListFlag.as<uint32_t>());
-	scanExclusive(w.islandListFlag.as<uint32_t>(), w.islandListOffs.as<uint32_t>(), n, &dc->awakeIslands, w.prim, s);
+	scanExclusive2(w.labelCount.as<uint32_t>(), w.labelStart.as<uint32_t>(), n, &dc->islandBodies,
+				   w.islandListFlag.as<uint32_t>(), w.islandListOffs.as<uint32_t>(), n, &dc->awakeIslands, w.prim, s);
 	M3G_LAUNCH(kIslandListCompact, blocksFor(n, 256), 256, s, w.islandListFlag.as<uint32_t>(),
 			   w.islandListOffs.as<uint32_t>(), n, w.islandLabels.as<int32_t>());
 	M3G_LAUNCH(kPlaceBodies, blocksFor(n, 256), 256, s, w.B, n, w.label.as<int32_t>(), w.islandFlag.as<uint32_t>(),

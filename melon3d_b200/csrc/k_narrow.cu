@@ -196,8 +196,8 @@ void launchNarrowphase(DevWorld& w, float dt)
 			   w.evEndFlag.as<uint32_t>());
 	uint32_t* beginScan = w.removeScan.as<uint32_t>();
 	uint32_t* endScan = (uint32_t*)w.moveSrc.ptr;
-	scanExclusive(w.evBeginFlag.as<uint32_t>(), beginScan, M, &dc->beginNP, w.prim, s);
-	scanExclusive(w.evEndFlag.as<uint32_t>(), endScan, M, &dc->endNP, w.prim, s);
+	scanExclusive2(w.evBeginFlag.as<uint32_t>(), beginScan, M, &dc->beginNP, w.evEndFlag.as<uint32_t>(), endScan, M,
+				   &dc->endNP, w.prim, s);
 	M3G_LAUNCH(kTransitionEvents, blocksFor(M, 256), 256, s, w.C, M, tr, beginScan, endScan, w.evBegin.as<int4>(),
 			   w.evEnd.as<int4>());
 	int32_t* target = (int32_t*)w.evBeginFlag.ptr; // flags no longer needed

@@ -309,26 +309,50 @@ __device__ __forceinline__ uint64_t statusWord(uint32_t epoch, uint32_t flag, ui
 	return ((uint64_t)epoch << 34) | ((uint64_t)flag << 32) | value;
 }
 
+// One launch scans one or two independent arrays (segments): segment 1's
+// tiles follow segment 0's in the ticket order and look back only as far as
+// its own first tile.
+struct ScanSeg
+{
+	const uint32_t* in;
+	uint32_t* out;
+	int64_t n;
+	uint32_t* total;
+	int32_t tile0, tiles;
+};
+struct ScanSegs
+{
+	ScanSeg s[2];
+	int32_t count, allTiles;
+};
+
 // Decoupled look-back scan.  A tile's wait for a predecessor's status is
 // bounded (spinLimit unsuccessful polls; 0: the tile does not wait at all).
 // A tile that gives up raises the error word and computes its prefix by
 // summing the inputs of all earlier tiles directly: slower, but the same
 // exact result, so no later kernel ever indexes with a partial prefix.
 __global__ void __launch_bounds__(kScanThreads)
-	kScanLookback(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total, uint64_t* status,
-				  uint32_t* ticket, uint32_t epoch, uint32_t* error, int64_t spinLimit)
+	kScanLookback(ScanSegs segs, uint64_t* status, uint32_t* ticket, uint32_t epoch, uint32_t* error,
+				  int64_t spinLimit)
 {
 	M3G_KERNEL_BEGIN();
 	__shared__ uint32_t warpSums[kScanThreads / 32 + 1];
 	__shared__ uint32_t sTile, sPrefix;
-	const int tiles = (int)((n + kScanTile - 1) / kScanTile);
 	if (threadIdx.x == 0)
 	{
 		sTile = atomicAdd(&ticket[0], 1u);
 	}
 	__syncthreads();
-	const int t = (int)sTile;
-	const int64_t base = (int64_t)t * kScanTile + (int64_t)threadIdx.x * kScanItems;
+	const int t = (int)sTile; // global tile: status word index
+	const bool second = segs.count > 1 && t >= segs.s[1].tile0;
+	const uint32_t* in = second ? segs.s[1].in : segs.s[0].in;
+	uint32_t* out = second ? segs.s[1].out : segs.s[0].out;
+	const int64_t n = second ? segs.s[1].n : segs.s[0].n;
+	uint32_t* total = second ? segs.s[1].total : segs.s[0].total;
+	const int first = second ? segs.s[1].tile0 : 0; // the segment's first global tile
+	const int tiles = second ? segs.s[1].tiles : segs.s[0].tiles;
+	const int lt = t - first; // tile inside the segment
+	const int64_t base = (int64_t)lt * kScanTile + (int64_t)threadIdx.x * kScanItems;
 	uint32_t vals[kScanItems];
 	uint32_t sum = 0;
 #pragma unroll
@@ -345,11 +369,11 @@ __global__ void __launch_bounds__(kScanThreads)
 	{
 		const int lane = threadIdx.x;
 		uint32_t excl = 0;
-		if (t == 0)
+		if (lt == 0)
 		{
 			if (lane == 0)
 			{
-				vs[0] = statusWord(epoch, 2u, agg);
+				vs[t] = statusWord(epoch, 2u, agg);
 			}
 		}
 		else
@@ -363,9 +387,9 @@ __global__ void __launch_bounds__(kScanThreads)
 			while (true)
 			{
 				const int j = idx - lane;
-				uint32_t flag = 2u, value = 0u; // lanes before tile 0 contribute nothing
+				uint32_t flag = 2u, value = 0u; // lanes before the segment's first tile contribute nothing
 				bool gaveUp = false;
-				if (j >= 0)
+				if (j >= first)
 				{
 					flag = 0u;
 					for (int64_t it = 0; flag == 0u; ++it)
@@ -406,7 +430,7 @@ __global__ void __launch_bounds__(kScanThreads)
 					atomicOr(error, 1u);
 				}
 				uint32_t s = 0;
-				const int64_t end = (int64_t)t * kScanTile;
+				const int64_t end = (int64_t)lt * kScanTile;
 				for (int64_t i = lane; i < end; i += 32)
 				{
 					s += in[i];
@@ -437,12 +461,12 @@ __global__ void __launch_bounds__(kScanThreads)
 	}
 	if (threadIdx.x == 0)
 	{
-		if (t == tiles - 1 && total != nullptr)
+		if (lt == tiles - 1 && total != nullptr)
 		{
 			*total = sPrefix + agg;
 		}
 		// the last CTA to finish rewinds the ticket for the next call
-		if (atomicAdd(&ticket[1], 1u) == (uint32_t)tiles - 1u)
+		if (atomicAdd(&ticket[1], 1u) == (uint32_t)segs.allTiles - 1u)
 		{
 			ticket[0] = 0u;
 			ticket[1] = 0u;
@@ -450,28 +474,25 @@ __global__ void __launch_bounds__(kScanThreads)
 	}
 }
 
-void scanExclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total, PrimScratch& s,
-				   cudaStream_t stream)
+// Copy an in-place multi-tile scan's input aside (a tile that gives up
+// re-reads the inputs of the tiles before it).
+static const uint32_t* scanInput(const uint32_t* in, uint32_t* out, int64_t n, PrimScratch& s, cudaStream_t stream)
 {
-	if (n <= 0)
-	{
-		if (total != nullptr)
-		{
-			cudaMemsetAsync(total, 0, sizeof(uint32_t), stream);
-		}
-		return;
-	}
-	const int64_t tiles = (n + kScanTile - 1) / kScanTile;
-	if (in == out && tiles > 1)
+	if (in == out && n > kScanTile)
 	{
 		s.scanIn.ensure((size_t)n * sizeof(uint32_t));
 		cudaMemcpyAsync(s.scanIn.ptr, in, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream);
-		in = s.scanIn.as<uint32_t>();
+		return s.scanIn.as<uint32_t>();
 	}
+	return in;
+}
+
+static void launchScan(ScanSegs& g, PrimScratch& s, cudaStream_t stream)
+{
 	s.scanTicket.ensureZeroed(4 * sizeof(uint32_t), stream);
 	s.waitError.ensureZeroed(4 * sizeof(uint32_t), stream);
 	void* before = s.scanStatus.ptr;
-	s.scanStatus.ensureZeroed((size_t)(tiles + 1) * sizeof(uint64_t), stream);
+	s.scanStatus.ensureZeroed((size_t)(g.allTiles + 1) * sizeof(uint64_t), stream);
 	if (s.scanStatus.ptr != before || ++s.scanEpoch >= kEpochLimit)
 	{
 		// fresh (zeroed) status words, or the epoch wrapped: restart at 1
@@ -482,9 +503,46 @@ void scanExclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total
 		s.scanEpoch = 1;
 	}
 	uint32_t* err = s.errorWord != nullptr ? s.errorWord : s.waitError.as<uint32_t>();
-	M3G_LAUNCH(kScanLookback, (unsigned)tiles, kScanThreads, stream, in, out, n, total, s.scanStatus.as<uint64_t>(),
+	M3G_LAUNCH(kScanLookback, (unsigned)g.allTiles, kScanThreads, stream, g, s.scanStatus.as<uint64_t>(),
 			   s.scanTicket.as<uint32_t>(), s.scanEpoch, err,
 			   s.waitLimit >= 0 ? s.waitLimit : (int64_t)kLookbackSpinLimit);
+}
+
+void scanExclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total, PrimScratch& s,
+				   cudaStream_t stream)
+{
+	if (n <= 0)
+	{
+		if (total != nullptr)
+		{
+			fillWords(total, 0u, sizeof(uint32_t), stream);
+		}
+		return;
+	}
+	ScanSegs g = {};
+	g.s[0] = { scanInput(in, out, n, s, stream), out, n, total, 0, (int32_t)((n + kScanTile - 1) / kScanTile) };
+	g.count = 1;
+	g.allTiles = g.s[0].tiles;
+	launchScan(g, s, stream);
+}
+
+void scanExclusive2(const uint32_t* in0, uint32_t* out0, int64_t n0, uint32_t* total0, const uint32_t* in1,
+					uint32_t* out1, int64_t n1, uint32_t* total1, PrimScratch& s, cudaStream_t stream)
+{
+	if (n0 <= 0 || n1 <= 0 || in0 == out0 || in1 == out1)
+	{
+		scanExclusive(in0, out0, n0, total0, s, stream);
+		scanExclusive(in1, out1, n1, total1, s, stream);
+		return;
+	}
+	ScanSegs g = {};
+	const int32_t t0 = (int32_t)((n0 + kScanTile - 1) / kScanTile);
+	const int32_t t1 = (int32_t)((n1 + kScanTile - 1) / kScanTile);
+	g.s[0] = { in0, out0, n0, total0, 0, t0 };
+	g.s[1] = { in1, out1, n1, total1, t0, t1 };
+	g.count = 2;
+	g.allTiles = t0 + t1;
+	launchScan(g, s, stream);
 }
 
 // ---------------------------------------------------------------------------

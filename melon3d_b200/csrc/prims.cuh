@@ -55,6 +55,10 @@ struct PrimScratch
 // in and out may alias.
 void scanExclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total, PrimScratch& s,
 				   cudaStream_t stream);
+// Two independent scans (different arrays, neither in place) in one launch,
+// with the results of two scanExclusive calls.
+void scanExclusive2(const uint32_t* in0, uint32_t* out0, int64_t n0, uint32_t* total0, const uint32_t* in1,
+					uint32_t* out1, int64_t n1, uint32_t* total1, PrimScratch& s, cudaStream_t stream);
 
 // Stable sort of n (key, val) pairs by key.  Digits are taken from
 // (key - bias), which must preserve the key order over the keys sorted (every
