@@ -1014,10 +1014,9 @@ void launchPairCount(DevWorld& w, int32_t n, float cellSize)
 				   w.stableKeys.as<uint64_t>(), w.stableVals.as<uint32_t>(), w.stableEntries,
 				   w.runPairCount.as<uint32_t>(), nullptr, nullptr);
 	}
-	scanExclusive(w.runPairCount.as<uint32_t>(), w.runPairOffs.as<uint32_t>(), runMax, &dc->gridPairs, w.prim, s);
-
 	if (w.batched)
 	{
+		scanExclusive(w.runPairCount.as<uint32_t>(), w.runPairOffs.as<uint32_t>(), runMax, &dc->gridPairs, w.prim, s);
 		w.overTotal = launchOverPairsBatch(w, P);
 		return;
 	}
@@ -1032,7 +1031,10 @@ void launchPairCount(DevWorld& w, int32_t n, float cellSize)
 		M3G_LAUNCH(kOverPairs, blocksFor(overTotal, 256), 256, s, P, O, overTotal, w.overFlag.as<uint32_t>(),
 				   w.overKeys.as<uint64_t>());
 	}
-	scanExclusive(w.overFlag.as<uint32_t>(), w.overScan.as<uint32_t>(), overTotal, &dc->overPairs, w.prim, s);
+	// the run-pair offsets and the oversized-candidate offsets do not depend on
+	// one another: one launch
+	scanExclusive2(w.runPairCount.as<uint32_t>(), w.runPairOffs.as<uint32_t>(), runMax, &dc->gridPairs,
+				   w.overFlag.as<uint32_t>(), w.overScan.as<uint32_t>(), overTotal, &dc->overPairs, w.prim, s);
 }
 
 // After the second sync: write the admitted pairs in emission order, keep the
