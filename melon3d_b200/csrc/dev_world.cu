@@ -190,6 +190,26 @@ __global__ void kSetU32(uint32_t* p, uint32_t v) { M3G_KERNEL_BEGIN(); *p = v; }
 
 void setDeviceCount(DevWorld& w, uint32_t* p, uint32_t v) { M3G_LAUNCH(kSetU32, 1, 1, w.stream, p, v); }
 
+__global__ void kResetCounters(StepCounters* c, uint32_t contactCount)
+{
+	M3G_KERNEL_BEGIN();
+	uint32_t* words = (uint32_t*)c;
+	for (int i = threadIdx.x; i < (int)(sizeof(StepCounters) / sizeof(uint32_t)); i += blockDim.x)
+	{
+		words[i] = 0u;
+	}
+	__syncthreads();
+	if (threadIdx.x == 0)
+	{
+		c->contactCount = contactCount;
+	}
+}
+
+void resetStepCounters(DevWorld& w, uint32_t contactCount)
+{
+	M3G_LAUNCH(kResetCounters, 1, 128, w.stream, devCounters(w), contactCount);
+}
+
 void readCounters(DevWorld& w)
 {
 	devCounters(w);

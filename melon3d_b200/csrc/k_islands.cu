@@ -32,10 +32,10 @@ __global__ void kAnyAwakeDynamic(const uint8_t* bFlags, int32_t n, uint32_t* fla
 	}
 }
 
+// the flag starts at zero: the step's counters are reset at its start
 void launchAnyAwakeDynamic(DevWorld& w, int32_t n)
 {
 	StepCounters* dc = devCounters(w);
-	fillWords(&dc->anyAwakeDynamic, 0u, sizeof(uint32_t), w.stream);
 	if (n > 0)
 	{
 		M3G_LAUNCH(kAnyAwakeDynamic, blocksFor(n, 256), 256, w.stream, w.B.bFlags, n, &dc->anyAwakeDynamic);
@@ -721,10 +721,10 @@ __global__ void kFinish(BodySoA B, int32_t n, float dt, int clearForces, StepCou
 	}
 }
 
+// the body counts start at zero: the step's counters are reset at its start
 void launchFinish(DevWorld& w, int32_t n, float dt, bool clearForces)
 {
 	StepCounters* dc = devCounters(w);
-	fillWords(&dc->bodyCount, 0u, 2 * sizeof(uint32_t), w.stream);
 	if (n > 0)
 	{
 		M3G_LAUNCH(kFinish, blocksFor(n, 256), 256, w.stream, w.B, n, dt, clearForces ? 1 : 0, dc);

@@ -238,6 +238,7 @@ bool growBodies(DevWorld& w, int32_t capacity);
 bool growContacts(DevWorld& w, int32_t capacity);
 void readCounters(DevWorld& w); // stream sync + D2H of StepCounters
 void setDeviceCount(DevWorld& w, uint32_t* p, uint32_t v); // stream-ordered store
+void resetStepCounters(DevWorld& w, uint32_t contactCount); // StepCounters zero but contactCount, one launch
 StepCounters* devCounters(DevWorld& w);
 
 void launchApplyUploads(DevWorld& w, const BodyUpload* hostRecs, int32_t count);

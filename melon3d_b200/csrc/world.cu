@@ -2030,7 +2030,7 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	}
 	flushHostChanges(world);
 	StepCounters* dc = devCounters(d);
-	fillWords(dc, 0u, sizeof(StepCounters), d.stream);
+	resetStepCounters(d, (uint32_t)d.contactCount); // all zero but the contact count
 	if (world->tape != nullptr)
 	{
 		tapeStepBegin(world->tape, d, n, dt, substepCount, hv(world->def.gravity), world->def.positionIterations);
@@ -2039,7 +2039,6 @@ void m3d_world_step(m3d_world* world, float dt, int substepCount)
 	{
 		fillWords(d.worldStableDirty.ptr, 0u, sizeof(uint32_t) * (size_t)d.worldCount, d.stream);
 	}
-	setDeviceCount(d, &dc->contactCount, (uint32_t)d.contactCount);
 
 	// broadphase and pair bookkeeping: sync 1 inside (tier sizes), sync 2
 	// after counting the admitted pairs (buffer sizes)
