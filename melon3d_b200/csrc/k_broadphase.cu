@@ -1075,8 +1075,8 @@ void launchPairEmit(DevWorld& w, int32_t n, float cellSize)
 	w.newContactKeys.ensure((size_t)(total + 1) * sizeof(uint64_t));
 	if (total > 0)
 	{
-		fillWords(w.newSet.ptr, 0xFFFFFFFFu, (size_t)ncap * sizeof(uint64_t), s);
-		fillWords(w.newSetPos.ptr, 0xFFFFFFFFu, (size_t)ncap * sizeof(uint32_t), s);
+		fillWords2(w.newSet.ptr, 0xFFFFFFFFu, (size_t)ncap * sizeof(uint64_t), w.newSetPos.ptr, 0xFFFFFFFFu,
+				   (size_t)ncap * sizeof(uint32_t), s);
 		M3G_LAUNCH(kDedupeMark, blocksFor(total, 256), 256, s, pk, total, w.newSet.as<uint64_t>(),
 				   w.newSetPos.as<uint32_t>(), w.newMask, &dc->hashFail);
 		M3G_LAUNCH(kDedupeKeep, blocksFor(total, 256), 256, s, pk, total, w.newSet.as<uint64_t>(),

@@ -746,11 +746,8 @@ __global__ void kReduceKeys(const uint64_t* keys, int64_t n, uint64_t* r)
 	}
 }
 
-__global__ void kFillWords(uint32_t* p, uint32_t v, int64_t words)
+__device__ __forceinline__ void fillRange(uint32_t* p, uint32_t v, int64_t words, int64_t i, int64_t stride)
 {
-	M3G_KERNEL_BEGIN();
-	const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (((uintptr_t)p & 15u) == 0 && (words & 3) == 0)
 	{
 		uint4* q = (uint4*)p;
@@ -767,6 +764,25 @@ __global__ void kFillWords(uint32_t* p, uint32_t v, int64_t words)
 	}
 }
 
+// one or two ranges (p1 null: one)
+__global__ void kFillWords(uint32_t* p0, uint32_t v0, int64_t words0, uint32_t* p1, uint32_t v1, int64_t words1)
+{
+	M3G_KERNEL_BEGIN();
+	const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+	const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	fillRange(p0, v0, words0, i, stride);
+	if (p1 != nullptr)
+	{
+		fillRange(p1, v1, words1, i, stride);
+	}
+}
+
+static int fillBlocks(int64_t words)
+{
+	int blocks = blocksFor(words, 256 * 4);
+	return blocks > 4 * 148 ? 4 * 148 : blocks;
+}
+
 void fillWords(void* p, uint32_t v, size_t bytes, cudaStream_t stream)
 {
 	const int64_t words = (int64_t)(bytes / sizeof(uint32_t));
@@ -774,9 +790,20 @@ void fillWords(void* p, uint32_t v, size_t bytes, cudaStream_t stream)
 	{
 		return;
 	}
-	int blocks = blocksFor(words, 256 * 4);
-	blocks = blocks > 4 * 148 ? 4 * 148 : blocks;
-	M3G_LAUNCH(kFillWords, blocks, 256, stream, (uint32_t*)p, v, words);
+	M3G_LAUNCH(kFillWords, fillBlocks(words), 256, stream, (uint32_t*)p, v, words, (uint32_t*)nullptr, 0u,
+			   (int64_t)0);
+}
+
+void fillWords2(void* p0, uint32_t v0, size_t bytes0, void* p1, uint32_t v1, size_t bytes1, cudaStream_t stream)
+{
+	const int64_t w0 = (int64_t)(bytes0 / sizeof(uint32_t)), w1 = (int64_t)(bytes1 / sizeof(uint32_t));
+	if (w0 <= 0 || w1 <= 0)
+	{
+		fillWords(p0, v0, bytes0, stream);
+		fillWords(p1, v1, bytes1, stream);
+		return;
+	}
+	M3G_LAUNCH(kFillWords, fillBlocks(w0 > w1 ? w0 : w1), 256, stream, (uint32_t*)p0, v0, w0, (uint32_t*)p1, v1, w1);
 }
 
 void reduceKeyRange(const uint64_t* keys, int64_t n, PrimScratch& s, cudaStream_t stream)

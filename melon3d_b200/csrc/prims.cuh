@@ -73,6 +73,8 @@ void radixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, uint64_t varyMask
 // p[0 .. bytes/4) = v, as a kernel of the library (a memset node would break
 // the stream's programmatic launch chain); bytes must be a multiple of 4.
 void fillWords(void* p, uint32_t v, size_t bytes, cudaStream_t stream);
+// two such fills in one launch
+void fillWords2(void* p0, uint32_t v0, size_t bytes0, void* p1, uint32_t v1, size_t bytes1, cudaStream_t stream);
 
 // Device-side OR / AND of n keys into s.reduce (two u64 words), then copied
 // to the pinned host words s.hostReduce[0..1] (stream-ordered, no sync).

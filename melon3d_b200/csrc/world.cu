@@ -2206,21 +2206,19 @@ void m3d_gpu_read_poses(m3d_world* world, float* positions, float* rotations, in
 		cudaMemcpyAsync(world->pinRot, d.B.rot, sizeof(float4) * n, cudaMemcpyDeviceToHost, d.stream);
 	}
 	cudaStreamSynchronize(d.stream);
-	for (int32_t i = 0; i < n; ++i)
+	if (positions != nullptr)
 	{
-		if (positions != nullptr)
+		const float4* src = world->pinPos;
+		for (int32_t i = 0; i < n; ++i)
 		{
-			positions[3 * i + 0] = world->pinPos[i].x;
-			positions[3 * i + 1] = world->pinPos[i].y;
-			positions[3 * i + 2] = world->pinPos[i].z;
+			positions[3 * i + 0] = src[i].x;
+			positions[3 * i + 1] = src[i].y;
+			positions[3 * i + 2] = src[i].z;
 		}
-		if (rotations != nullptr)
-		{
-			rotations[4 * i + 0] = world->pinRot[i].x;
-			rotations[4 * i + 1] = world->pinRot[i].y;
-			rotations[4 * i + 2] = world->pinRot[i].z;
-			rotations[4 * i + 3] = world->pinRot[i].w;
-		}
+	}
+	if (rotations != nullptr)
+	{
+		memcpy(rotations, world->pinRot, sizeof(float4) * (size_t)n);
 	}
 }
 
