@@ -20,7 +20,7 @@ import os
 import numpy as np
 import pytest
 
-from melon3d_b200 import harness
+from melon3d_b200 import api, harness
 
 from . import _util as U
 
@@ -114,6 +114,45 @@ def test_rain_20k_churn_200_settled_phase_bit_exact():
 
 def test_rain_with_churn_bit_exact():
     lockstep(U.oracle_cr(), harness.RAIN, 60, seed=2, a=1500, b=30)
+
+
+def test_rain_churn_with_edits_between_steps_bit_exact():
+    """After a step that followed destroys, the GPU world downloads what the
+    next destroy needs on a second stream.  Edits that reach the device
+    before that destroy (velocities, a material, flushed by the pose
+    read-back of the churn) must drop it; the destroys then download afresh.
+    Compared with the reference after every step: bodies, contacts, events."""
+    ref, g = U.oracle_cr(), U.gpu()
+    sr = harness.Scene(ref, harness.RAIN, 7, 3000, 60)
+    sg = harness.Scene(g, harness.RAIN, 7, 3000, 60)
+    try:
+        for step in range(60):
+            sr.run(1)
+            sg.run(1)
+            if step >= 20 and step % 5 == 0:
+                ir, ig = sr.dynamic_ids(), sg.dynamic_ids()
+                assert [(i.index, i.generation) for i in ir] == [(i.index, i.generation) for i in ig]
+                for k in range(0, len(ir), 97):
+                    v = api.Vec3(0.5, 3.0 + 0.01 * k, -0.25)
+                    ref.m3d_body_set_linear_velocity(sr.world, ir[k], v)
+                    g.m3d_body_set_linear_velocity(sg.world, ig[k], v)
+                ref.m3d_body_set_friction(sr.world, ir[1], 0.9)
+                g.m3d_body_set_friction(sg.world, ig[1], 0.9)
+                sr.churn()  # destroys after the edits, without a step
+                sg.churn()
+                d = U.diff_events(U.events(ref, sr.world), U.events(g, sg.world))
+                assert d is None, "step %d, churn: %s" % (step, d)
+                sr.step_only()
+                sg.step_only()
+            d = U.diff_contacts(U.contacts(ref, sr.world), U.contacts(g, sg.world))
+            assert d is None, "step %d: %s" % (step, d)
+            d = U.diff_bodies(U.bodies(ref, sr.world), U.bodies(g, sg.world))
+            assert d is None, "step %d: %s" % (step, d)
+            d = U.diff_events(U.events(ref, sr.world), U.events(g, sg.world))
+            assert d is None, "step %d: %s" % (step, d)
+    finally:
+        sr.close()
+        sg.close()
 
 
 def test_dense_rain_bit_exact():
