@@ -1276,8 +1276,9 @@ void launchContactMoves(DevWorld& w, const int2* hostMoves, int32_t count)
 	}
 	w.moveSrc.ensure(sizeof(int2) * (size_t)count);
 	cudaMemcpyAsync(w.moveSrc.ptr, hostMoves, sizeof(int2) * (size_t)count, cudaMemcpyHostToDevice, w.stream);
+	// a copy from pageable memory returns once the source is staged, so the
+	// caller may free hostMoves on return without waiting for the kernel
 	M3G_LAUNCH(kContactMoves, blocksFor(count, 128), 128, w.stream, w.C, (const int2*)w.moveSrc.ptr, count);
-	cudaStreamSynchronize(w.stream); // the host vector backing hostMoves is freed on return
 }
 
 __global__ void kContactAdjCount(const int2* bodies, int32_t count, uint32_t* perBody)
